@@ -1,0 +1,148 @@
+/* rivrs_b200.h — C ABI of the B200 numeric phase for sparse symmetric
+ * indefinite LDL^T with a-posteriori threshold pivoting (APTP).
+ *
+ * The entry points replace the numeric half of rivrs-sparse behind its
+ * analyze -> factor -> solve API.  Each declaration cites the reference
+ * interface it stands in for (paths inside the rivrs-linalg project).
+ *
+ * Conventions
+ *   - Indices are int64_t (the reference's usize), matrices are FULL symmetric
+ *     CSC (both triangles stored, sparse/src/lib.rs:121-125).
+ *   - Permutations are "forward": perm_fwd[new] = old.
+ *   - Every call returns an rvg_status; rvg_last_error() gives the message of
+ *     the last failing call on the calling thread.
+ *   - A handle is single-threaded and owns one CUDA stream on the current
+ *     device.  There is no CPU fallback: without a usable GPU the calls that
+ *     need one return RVG_ERR_DEVICE.
+ */
+#ifndef RIVRS_B200_H
+#define RIVRS_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes, one per SparseError variant that the numeric path can raise
+ * (sparse/src/error.rs:20-100) plus the device-side failures. */
+typedef enum {
+  RVG_OK = 0,
+  RVG_ERR_DIMENSION_MISMATCH = 1, /* SparseError::DimensionMismatch */
+  RVG_ERR_INVALID_INPUT = 2,      /* SparseError::InvalidInput / NotSquare */
+  RVG_ERR_SOLVE_BEFORE_FACTOR = 3,/* SparseError::SolveBeforeFactor */
+  RVG_ERR_ANALYSIS = 4,           /* SparseError::AnalysisFailure */
+  RVG_ERR_DEVICE = 5,             /* CUDA error or no device */
+  RVG_ERR_DEVICE_TIMEOUT = 6,     /* a bounded device-side wait gave up */
+  RVG_ERR_OUT_OF_MEMORY = 7
+} rvg_status;
+
+/* FactorOptions / AptpOptions (sparse/src/symmetric/solver.rs:72-116,
+ * sparse/src/symmetric/factor.rs:86-130).  rvg_default_options() fills the
+ * reference defaults: threshold 0.01, small 1e-20, nb 256, ib 32, nemin 32,
+ * small_leaf_threshold 256, failed_pivot_method Tpp. */
+typedef struct {
+  double threshold;
+  double small;
+  int64_t outer_block_size;
+  int64_t inner_block_size;
+  int64_t nemin;
+  int64_t small_leaf_threshold;
+  int32_t failed_pivot_tpp; /* 1 = FailedPivotMethod::Tpp, 0 = Pass */
+  int32_t fallback_bk;      /* 1 = AptpFallback::BunchKaufman, 0 = Delay */
+} rvg_options;
+
+/* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */
+typedef struct {
+  int64_t total_1x1_pivots;
+  int64_t total_2x2_pivots;
+  int64_t total_delayed;
+  int64_t zero_pivots;
+  int64_t max_front_size;
+  int64_t supernodes_before_amalgamation;
+  int64_t supernodes_after_amalgamation;
+  int64_t merges_performed;
+  int64_t small_leaf_subtrees;
+  int64_t small_leaf_nodes;
+} rvg_stats;
+
+typedef struct rvg_symbolic rvg_symbolic;
+typedef struct rvg_handle rvg_handle;
+
+void rvg_default_options(rvg_options* opt);
+const char* rvg_last_error(void);
+
+/* ---- host symbolic analysis -------------------------------------------
+ * Stand-in for AptpSymbolic::analyze(matrix, SymmetricOrdering::Custom(perm))
+ * (sparse/src/symmetric/symbolic.rs:248-310): elimination tree, postorder,
+ * column counts and the supernode partition of P A P^T.  `order` is the
+ * fill-reducing order (order[new] = old, UserSupplied semantics of
+ * solver.rs:51-52) or NULL for the identity; the returned permutation
+ * composes it with the elimination-tree postorder. */
+rvg_status rvg_analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, const int64_t* order,
+                       rvg_symbolic** out);
+/* Sizes: [n, n_supernodes, total pattern length, predicted nnz(L)]. */
+rvg_status rvg_symbolic_sizes(const rvg_symbolic* s, int64_t out4[4]);
+/* Copies out perm_fwd (n), supernode_begin/end/parent (nsup), pattern_ptr
+ * (nsup+1) and pattern_idx (total pattern length); mirrors symbolic.perm_vecs()
+ * (symbolic.rs:420-440) and the SymbolicSupernodalCholesky accessors. */
+rvg_status rvg_symbolic_export(const rvg_symbolic* s, int64_t* perm_fwd, int64_t* sup_begin,
+                               int64_t* sup_end, int64_t* sup_parent, int64_t* pat_ptr, int64_t* pat_idx);
+void rvg_symbolic_free(rvg_symbolic* s);
+
+/* ---- numeric phase -----------------------------------------------------
+ * rvg_create replaces the pattern-only work at the start of
+ * AptpNumeric::factor (numeric.rs:844-905: build_supernode_info, amalgamate,
+ * classify_small_leaf_subtrees, build_assembly_maps) and uploads the
+ * structure to the device once.  The supernode arrays are the
+ * PRE-amalgamation partition (as AptpSymbolic exposes it).  `opt` may be
+ * NULL for the defaults. */
+rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end,
+                      const int64_t* pat_ptr, const int64_t* pat_idx, const int64_t* sup_parent,
+                      const int64_t* perm_fwd, const int64_t* colptr, const int64_t* rowidx,
+                      const rvg_options* opt, rvg_handle** out);
+
+/* AptpNumeric::factor (numeric.rs:844-1023) / SparseLDLT::factor and
+ * ::refactor (solver.rs:296-341).  `values` are the CSC values (host memory),
+ * `scaling` the MC64 scaling in elimination order (solver.rs:276-280) or
+ * NULL.  Replaces any previous factorization held by the handle. */
+rvg_status rvg_factor(rvg_handle* h, const double* values, const double* scaling);
+/* Same with values and scaling already in device memory (nnz and n doubles). */
+rvg_status rvg_factor_device(rvg_handle* h, const double* d_values, const double* d_scaling);
+
+/* SparseLDLT::solve_in_place (solver.rs:370-428): permute, scale,
+ * aptp_solve (solve.rs:57-144), scale, unpermute, in place, for nrhs
+ * right-hand sides stored column-major with leading dimension ldb (host). */
+rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb);
+/* Same on device memory. */
+rvg_status rvg_solve_device(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb);
+
+/* SparseLDLT::inertia (solver.rs:504-519): [positive, negative, zero]. */
+rvg_status rvg_inertia(rvg_handle* h, int64_t out3[3]);
+/* SparseLDLT::stats (solver.rs:530-532). */
+rvg_status rvg_get_stats(rvg_handle* h, rvg_stats* out);
+
+/* Pivot record, fronts in supernode (postorder) order, the eliminated columns
+ * of each front in elimination order (FrontFactors::col_indices, numeric.rs:
+ * 543-596): global permuted column, code (1 = 1x1, 2 = first of a 2x2,
+ * 3 = second of a 2x2) and the D entries (diag, and the off-diagonal on the
+ * first column of a 2x2).  Returns the count through *count. */
+rvg_status rvg_pivot_record(rvg_handle* h, int64_t* col, int8_t* code, double* d_diag, double* d_off,
+                            int64_t* count);
+/* Per supernode (post-amalgamation): m, k, ne, n1x1, n2x2, parent, n_owned,
+ * in_small_leaf, wave (PerSupernodeStats, numeric.rs:604-655). */
+rvg_status rvg_front_info(rvg_handle* h, int64_t* out9, int64_t* nsup);
+/* Algorithmic work of the delay-free structure: [factor flops, Schur GEMM
+ * flops, assembly bytes, solve bytes per RHS, nnz(L), max front]. */
+rvg_status rvg_work(rvg_handle* h, double out6[6]);
+/* Device time of the last factor / solve phases in milliseconds:
+ * [assembly, dense kernel, contribution GEMM, total factor, last solve,
+ *  dominant-kernel time, dominant-kernel launches]. */
+rvg_status rvg_timings(rvg_handle* h, double out7[7]);
+/* The CUDA stream the handle launches on (cudaStream_t as void*). */
+rvg_status rvg_stream(rvg_handle* h, void** stream);
+void rvg_destroy(rvg_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1318 @@
+// ORACLE — test infrastructure only, never the product path.
+//
+// A single-threaded (optionally OpenMP level-parallel) C++ restatement of the
+// rivrs-sparse numeric phase: multifrontal assembly, the dense APTP kernel
+// (complete-pivoting 32x32 blocks, TRSM + a-posteriori threshold check,
+// two-level 256-column outer loop, TPP fallback), the deferred contribution
+// GEMM, and the supernodal forward/diagonal/backward solve.
+//
+// Every routine cites the reference function (file:line within the
+// rivrs-linalg project) whose control flow and comparisons it follows.  The
+// dense BLAS calls of the reference (faer 0.24, a semver range with no lock
+// file, source absent) are replaced by loops with a fixed arithmetic
+// contract:
+//   * where the reference calls faer (TRSM, GEMM, triangular GEMM), each
+//     output entry is an fma chain over the reduction index in ascending
+//     order: c = fma(-a_k, b_k, c);
+//   * where the reference has its own scalar Rust loops, the arithmetic is
+//     unfused, expression for expression (build with -ffp-contract=off).
+// The GPU kernels follow the same contract, which makes the two bit-identical
+// on the same inputs; results agree with the reference to rounding, while
+// every pivot decision follows the same comparisons in the same order.
+//
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load
+// this library, and only as the checker / the timed CPU baseline.
+//
+// Parity pinning: checked by tests/test_oracle.py against the reference's own
+// hand-constructed fixtures (exact inertia, sparse/test-data/hand-constructed),
+// its dense-kernel known-answer tests (sparse/src/symmetric/factor.rs tests)
+// and the backward-error gates of sparse/tests/solve.rs.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+typedef int64_t i64;
+
+// ---------------------------------------------------------------------------
+// Options (sparse/src/symmetric/factor.rs:86-130 AptpOptions, solver.rs:72-116)
+// ---------------------------------------------------------------------------
+struct Opts {
+  double threshold = 0.01;
+  double small = 1e-20;
+  int fallback_bk = 1;        // AptpFallback::BunchKaufman (unused by the blocked path)
+  int failed_pivot_tpp = 1;   // FailedPivotMethod::Tpp
+  i64 nb = 256;               // outer_block_size
+  i64 ib = 32;                // inner_block_size
+  i64 nemin = 32;
+  i64 small_leaf_threshold = 256;
+};
+
+const double BUNCH_KAUFMAN_ALPHA = 0.5;  // factor.rs:50
+
+// near-tie reporting: a comparison a >= b (or a > b) is a near tie when
+// |a - b| <= TIE_REL * max(|a|, |b|).
+const double TIE_REL = 1e-12;
+thread_local i64 g_ties = 0;
+inline void note_tie(double a, double b) {
+  double s = std::max(std::fabs(a), std::fabs(b));
+  if (std::fabs(a - b) <= TIE_REL * s && s > 0) g_ties++;
+}
+
+// ---------------------------------------------------------------------------
+// MixedDiagonal (sparse/src/symmetric/diagonal.rs:49-465)
+// ---------------------------------------------------------------------------
+enum : int8_t { PT_DELAYED = 0, PT_1X1 = 1, PT_2X2 = 2 };
+
+struct MixedD {
+  std::vector<int8_t> type;
+  std::vector<i64> partner;
+  std::vector<double> diag, off;
+  i64 n = 0;
+  void init(i64 n_) {
+    n = n_;
+    type.assign(n, PT_DELAYED);
+    partner.assign(n, -1);
+    diag.assign(n, 0.0);
+    off.assign(n, 0.0);
+  }
+  void set1(i64 c, double v) { type[c] = PT_1X1; diag[c] = v; }
+  void set2(i64 c, double a, double b, double cc) {
+    type[c] = PT_2X2; partner[c] = c + 1;
+    type[c + 1] = PT_2X2; partner[c + 1] = c;
+    diag[c] = a; diag[c + 1] = cc; off[c] = b;
+  }
+  bool is2first(i64 c) const { return type[c] == PT_2X2 && partner[c] > c; }
+  // diagonal.rs:185-198
+  void grow(i64 nn) {
+    if (nn > n) {
+      type.resize(nn, PT_DELAYED); partner.resize(nn, -1);
+      diag.resize(nn, 0.0); off.resize(nn, 0.0); n = nn;
+    }
+  }
+  void truncate(i64 nn) {
+    type.resize(nn); partner.resize(nn); diag.resize(nn); off.resize(nn); n = nn;
+  }
+  // diagonal.rs:216-259 copy_from_offset
+  void copy_from_offset(const MixedD& s, i64 off0, i64 count) {
+    i64 c = 0;
+    while (c < count) {
+      if (s.type[c] == PT_1X1) {
+        type[off0 + c] = PT_1X1; partner[off0 + c] = -1; diag[off0 + c] = s.diag[c]; c += 1;
+      } else if (s.type[c] == PT_2X2 && c + 1 < count) {
+        i64 d = off0 + c;
+        type[d] = PT_2X2; partner[d] = d + 1; type[d + 1] = PT_2X2; partner[d + 1] = d;
+        diag[d] = s.diag[c]; diag[d + 1] = s.diag[c + 1]; off[d] = s.off[c];
+        c += 2;
+      } else {
+        c += 1;
+      }
+    }
+  }
+  // diagonal.rs:312-365 solve_in_place (zero pivot -> 0)
+  void solve(double* x) const {
+    i64 c = 0;
+    while (c < n) {
+      if (type[c] == PT_1X1) {
+        double d = diag[c];
+        if (d == 0.0) x[c] = 0.0; else x[c] /= d;
+        c += 1;
+      } else {
+        i64 p = partner[c];
+        if (p > c) {
+          double a = diag[c], b = off[c], cc = diag[p];
+          double det = a * cc - b * b;
+          if (det == 0.0) { x[c] = 0.0; x[p] = 0.0; }
+          else { double r1 = x[c], r2 = x[p]; x[c] = (cc * r1 - b * r2) / det; x[p] = (a * r2 - b * r1) / det; }
+        }
+        c += 1;
+      }
+    }
+  }
+  // diagonal.rs:391-461 compute_inertia
+  void inertia(i64* pos, i64* neg, i64* zer) const {
+    i64 c = 0;
+    while (c < n) {
+      if (type[c] == PT_1X1) {
+        double d = diag[c];
+        if (d > 0) (*pos)++; else if (d < 0) (*neg)++; else (*zer)++;
+        c += 1;
+      } else {
+        i64 p = partner[c];
+        if (p > c) {
+          double a = diag[c], b = off[c], cc = diag[p];
+          double det = a * cc - b * b, tr = a + cc;
+          if (det > 0) { if (tr > 0) *pos += 2; else *neg += 2; }
+          else if (det < 0) { (*pos)++; (*neg)++; }
+          else { if (tr > 0) { (*pos)++; (*zer)++; } else if (tr < 0) { (*neg)++; (*zer)++; } else *zer += 2; }
+        }
+        c += 1;
+      }
+    }
+  }
+};
+
+struct Stats { i64 n1 = 0, n2 = 0, ndel = 0; double maxl = 0; };
+
+struct FactorResult {
+  MixedD d;
+  std::vector<i64> perm;
+  i64 ne = 0;
+  Stats st;
+};
+
+// column-major dense view
+struct MV {
+  double* a; i64 ld;
+  double& operator()(i64 i, i64 j) const { return a[i + j * ld]; }
+  MV sub(i64 r0, i64 c0) const { return MV{a + r0 + c0 * ld, ld}; }
+};
+
+// ---------------------------------------------------------------------------
+// Symmetric swaps (factor.rs:466-517 swap_symmetric_block, 458-461 swap_symmetric)
+// ---------------------------------------------------------------------------
+void swap_sym_block(MV a, i64 i, i64 j, i64 col_start, i64 row_limit) {
+  if (i == j) return;
+  if (i > j) std::swap(i, j);
+  std::swap(a(i, i), a(j, j));
+  for (i64 k = col_start; k < i; ++k) std::swap(a(i, k), a(j, k));
+  for (i64 k = i + 1; k < j; ++k) std::swap(a(k, i), a(j, k));
+  for (i64 k = j + 1; k < row_limit; ++k) std::swap(a(k, i), a(k, j));
+}
+inline void swap_sym(MV a, i64 m, i64 i, i64 j) { swap_sym_block(a, i, j, 0, m); }
+
+// ---------------------------------------------------------------------------
+// factor_block_diagonal (factor.rs:891-1153): complete pivoting on an ib x ib block
+// ---------------------------------------------------------------------------
+void factor_block_diagonal(MV a, i64 col_start, i64 bs, double small, i64 row_limit,
+                           MixedD& d, std::vector<i64>& lperm, i64& nelim_out, Stats& st) {
+  i64 block_end = col_start + bs;
+  lperm.resize(bs);
+  for (i64 i = 0; i < bs; ++i) lperm[i] = i;
+  d.init(bs);
+  i64 k = 0;
+  while (k < bs) {
+    i64 cur = col_start + k;
+    i64 remaining = bs - k;
+    double maxv = 0.0; i64 mr = cur, mc = cur;
+    for (i64 j = cur; j < block_end; ++j)
+      for (i64 i = j; i < block_end; ++i) {
+        double v = std::fabs(a(i, j));
+        note_tie(v, maxv);
+        if (v > maxv) { maxv = v; mr = i; mc = j; }
+      }
+    if (maxv < small) { st.ndel += remaining; break; }
+    if (mr == mc) {
+      if (mr != cur) { swap_sym_block(a, cur, mr, col_start, row_limit); std::swap(lperm[k], lperm[mr - col_start]); }
+      double dkk = a(cur, cur), inv = 1.0 / dkk, maxl = 0.0;
+      for (i64 i = cur + 1; i < block_end; ++i) { double l = a(i, cur) * inv; a(i, cur) = l; maxl = std::max(maxl, std::fabs(l)); }
+      for (i64 j = cur + 1; j < block_end; ++j) {
+        double ldl = a(j, cur) * dkk;
+        for (i64 i = j; i < block_end; ++i) a(i, j) -= a(i, cur) * ldl;
+      }
+      d.set1(k, dkk); st.n1++; st.maxl = std::max(st.maxl, maxl);
+      k += 1;
+    } else {
+      i64 t = mr, mi = mc;
+      double amm = a(mi, mi), att = a(t, t), atm = a(t, mi);
+      double delta = amm * att - atm * atm;
+      if (remaining < 2) {
+        i64 pp = std::fabs(amm) >= std::fabs(att) ? mi : t;
+        if (pp != cur) { swap_sym_block(a, cur, pp, col_start, row_limit); std::swap(lperm[k], lperm[pp - col_start]); }
+        double dkk = a(cur, cur);
+        if (std::fabs(dkk) < small) { st.ndel += 1; break; }
+        double inv = 1.0 / dkk;
+        for (i64 i = cur + 1; i < block_end; ++i) a(i, cur) *= inv;
+        d.set1(k, dkk); st.n1++;
+        k += 1;
+        continue;
+      }
+      note_tie(std::fabs(delta), BUNCH_KAUFMAN_ALPHA * atm * atm);
+      if (std::fabs(delta) >= BUNCH_KAUFMAN_ALPHA * atm * atm) {
+        if (mi != cur) { swap_sym_block(a, cur, mi, col_start, row_limit); std::swap(lperm[k], lperm[mi - col_start]); }
+        i64 nt = (t == cur) ? mi : t;
+        if (nt != cur + 1) { swap_sym_block(a, cur + 1, nt, col_start, row_limit); std::swap(lperm[k + 1], lperm[nt - col_start]); }
+        double a11 = a(cur, cur), a22 = a(cur + 1, cur + 1), a21 = a(cur + 1, cur);
+        double det = a11 * a22 - a21 * a21, inv_det = 1.0 / det, maxl = 0.0;
+        for (i64 i = cur + 2; i < block_end; ++i) {
+          double ai1 = a(i, cur), ai2 = a(i, cur + 1);
+          double l1 = (ai1 * a22 - ai2 * a21) * inv_det, l2 = (ai2 * a11 - ai1 * a21) * inv_det;
+          a(i, cur) = l1; a(i, cur + 1) = l2;
+          maxl = std::max(maxl, std::max(std::fabs(l1), std::fabs(l2)));
+        }
+        for (i64 j = cur + 2; j < block_end; ++j) {
+          double l1j = a(j, cur), l2j = a(j, cur + 1);
+          double w1 = l1j * a11 + l2j * a21, w2 = l1j * a21 + l2j * a22;
+          for (i64 i = j; i < block_end; ++i) a(i, j) -= a(i, cur) * w1 + a(i, cur + 1) * w2;
+        }
+        d.set2(k, a11, a21, a22); st.n2++; st.maxl = std::max(st.maxl, maxl);
+        k += 2;
+      } else {
+        note_tie(std::fabs(amm), std::fabs(att));
+        i64 pp = std::fabs(amm) >= std::fabs(att) ? mi : t;
+        if (pp != cur) { swap_sym_block(a, cur, pp, col_start, row_limit); std::swap(lperm[k], lperm[pp - col_start]); }
+        double dkk = a(cur, cur), inv = 1.0 / dkk, maxl = 0.0;
+        for (i64 i = cur + 1; i < block_end; ++i) { double l = a(i, cur) * inv; a(i, cur) = l; maxl = std::max(maxl, std::fabs(l)); }
+        for (i64 j = cur + 1; j < block_end; ++j) {
+          double ldl = a(j, cur) * dkk;
+          for (i64 i = j; i < block_end; ++i) a(i, j) -= a(i, cur) * ldl;
+        }
+        d.set1(k, dkk); st.n1++; st.maxl = std::max(st.maxl, maxl);
+        k += 1;
+      }
+    }
+  }
+  nelim_out = k;
+}
+
+// adjust_for_2x2_boundary (factor.rs:1161-1174)
+i64 adjust_2x2(i64 e, const MixedD& d) {
+  if (e == 0) return 0;
+  i64 last = e - 1;
+  if (d.type[last] == PT_2X2 && d.partner[last] > last) return e - 1;
+  return e;
+}
+
+// apply_and_check (factor.rs:1295-1408): TRSM, D^-1 scaling, first failing column
+i64 apply_and_check(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, const MixedD& d, double thr) {
+  if (nelim == 0) return 0;
+  i64 prows = m - col_start - bcols;
+  if (prows == 0) return nelim;
+  i64 ps = col_start + bcols;
+  // panel * L11^T = A21  (L11 unit lower, from a[col_start.., col_start..])
+  // faer TRSM (factor.rs:1338); per entry an fma chain over l ascending
+  for (i64 j = 0; j < nelim; ++j)
+    for (i64 l = 0; l < j; ++l) {
+      double lij = a(col_start + j, col_start + l);
+      for (i64 r = 0; r < prows; ++r)
+        a(ps + r, col_start + j) = std::fma(-a(ps + r, col_start + l), lij, a(ps + r, col_start + j));
+    }
+  i64 c = 0;
+  while (c < nelim) {
+    if (d.type[c] == PT_1X1) {
+      double inv = 1.0 / d.diag[c];
+      for (i64 r = 0; r < prows; ++r) a(ps + r, col_start + c) *= inv;
+      c += 1;
+    } else if (d.is2first(c)) {
+      double A = d.diag[c], B = d.off[c], C = d.diag[c + 1];
+      double inv_det = 1.0 / (A * C - B * B);
+      for (i64 r = 0; r < prows; ++r) {
+        double x1 = a(ps + r, col_start + c), x2 = a(ps + r, col_start + c + 1);
+        a(ps + r, col_start + c) = (x1 * C - x2 * B) * inv_det;
+        a(ps + r, col_start + c + 1) = (x2 * A - x1 * B) * inv_det;
+      }
+      c += 2;
+    } else c += 1;
+  }
+  double bound = 1.0 / thr;
+  i64 eff = nelim, sc = 0;
+  while (sc < nelim) {
+    i64 w = d.is2first(sc) ? 2 : 1;
+    bool ok = true;
+    for (i64 cc = sc; cc < sc + w && ok; ++cc) {
+      if (cc >= nelim) break;
+      for (i64 r = 0; r < prows; ++r) {
+        double v = std::fabs(a(ps + r, col_start + cc));
+        note_tie(v, bound);
+        if (v >= bound) { ok = false; break; }
+      }
+    }
+    if (!ok) { eff = sc; break; }
+    sc += w;
+  }
+  return eff;
+}
+
+// compute_ld_into (factor.rs:1536-1563): W = L * D
+void compute_ld(const double* l, i64 ldl, i64 nrows, const MixedD& d, i64 nelim, double* w, i64 ldw) {
+  i64 c = 0;
+  while (c < nelim) {
+    if (d.type[c] == PT_1X1) {
+      double dv = d.diag[c];
+      for (i64 i = 0; i < nrows; ++i) w[i + c * ldw] = l[i + c * ldl] * dv;
+      c += 1;
+    } else if (d.is2first(c)) {
+      double A = d.diag[c], B = d.off[c], C = d.diag[c + 1];
+      for (i64 i = 0; i < nrows; ++i) {
+        double l1 = l[i + c * ldl], l2 = l[i + (c + 1) * ldl];
+        w[i + c * ldw] = l1 * A + l2 * B;
+        w[i + (c + 1) * ldw] = l1 * B + l2 * C;
+      }
+      c += 2;
+    } else c += 1;
+  }
+}
+
+// update_trailing (factor.rs:1418-1526): FS x FS lower and NFS x FS rectangle
+void update_trailing(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, i64 p, const MixedD& d) {
+  if (nelim == 0) return;
+  i64 ts = col_start + bcols, tsz = m - ts;
+  if (tsz <= 0) return;
+  std::vector<double> W((size_t)tsz * nelim, 0.0), L((size_t)tsz * nelim);
+  for (i64 c = 0; c < nelim; ++c)
+    for (i64 i = 0; i < tsz; ++i) L[i + c * tsz] = a(ts + i, col_start + c);
+  compute_ld(L.data(), tsz, tsz, d, nelim, W.data(), tsz);
+  i64 fs = std::max<i64>(p - ts, 0);
+  // faer triangular / rectangular GEMM (factor.rs:1491, 1513); per entry an
+  // fma chain over c ascending
+  // region 1: lower triangle of A[ts..p, ts..p]
+  for (i64 j = 0; j < fs; ++j)
+    for (i64 c = 0; c < nelim; ++c) {
+      double lj = L[j + c * tsz];
+      for (i64 i = j; i < fs; ++i) a(ts + i, ts + j) = std::fma(-W[i + c * tsz], lj, a(ts + i, ts + j));
+    }
+  // region 2: A[p..m, ts..p]
+  i64 nfs = m - p;
+  if (nfs > 0 && fs > 0)
+    for (i64 j = 0; j < fs; ++j)
+      for (i64 c = 0; c < nelim; ++c) {
+        double lj = L[j + c * tsz];
+        for (i64 i = 0; i < nfs; ++i) a(p + i, ts + j) = std::fma(-W[fs + i + c * tsz], lj, a(p + i, ts + j));
+      }
+}
+
+// update_cross_terms (factor.rs:1669-1766)
+void update_cross_terms(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, const MixedD& d) {
+  if (nelim == 0 || nelim >= bcols) return;
+  i64 nf = bcols - nelim, ts = col_start + bcols, tsz = m - ts;
+  std::vector<double> Lb((size_t)nf * nelim), Wb((size_t)nf * nelim, 0.0);
+  for (i64 c = 0; c < nelim; ++c)
+    for (i64 i = 0; i < nf; ++i) Lb[i + c * nf] = a(col_start + nelim + i, col_start + c);
+  compute_ld(Lb.data(), nf, nf, d, nelim, Wb.data(), nf);
+  for (i64 j = 0; j < nf; ++j)
+    for (i64 i = j; i < nf; ++i) {
+      double s = 0.0;
+      for (i64 c = 0; c < nelim; ++c) s += Wb[i + c * nf] * Lb[j + c * nf];
+      a(col_start + nelim + i, col_start + nelim + j) -= s;
+    }
+  if (tsz > 0) {
+    std::vector<double> Lp((size_t)tsz * nelim), Wp((size_t)tsz * nelim, 0.0);
+    for (i64 c = 0; c < nelim; ++c)
+      for (i64 i = 0; i < tsz; ++i) Lp[i + c * tsz] = a(ts + i, col_start + c);
+    compute_ld(Lp.data(), tsz, tsz, d, nelim, Wp.data(), tsz);
+    for (i64 j = 0; j < nf; ++j)
+      for (i64 i = 0; i < tsz; ++i) {
+        double s = 0.0;
+        for (i64 c = 0; c < nelim; ++c) s += Wp[i + c * tsz] * Lb[j + c * nf];
+        a(ts + i, col_start + nelim + j) -= s;
+      }
+  }
+}
+
+// factor_inner (factor.rs:1811-2095): 32-column Factor / Apply / Update loop
+FactorResult factor_inner(MV a, i64 m, i64 p, i64 nfs_boundary, const Opts& o) {
+  i64 ib = o.ib;
+  FactorResult R;
+  R.perm.resize(m);
+  std::iota(R.perm.begin(), R.perm.end(), 0);
+  R.d.init(p);
+  i64 k = 0, end_pos = p;
+  std::vector<double> backup, buf(ib);
+  std::vector<i64> obuf(ib);
+  while (k < end_pos) {
+    i64 bs = std::min(end_pos - k, ib), be = k + bs;
+    // 1. backup a[k..m, k..k+bs]   (BlockBackup::create, factor.rs:1191-1206)
+    i64 rows = m - k;
+    backup.assign((size_t)rows * bs, 0.0);
+    for (i64 j = 0; j < bs; ++j)
+      for (i64 i = 0; i < rows; ++i) backup[i + j * rows] = a(k + i, k + j);
+    // 2. factor diagonal block
+    MixedD bd; std::vector<i64> bperm; i64 bnelim; Stats bst;
+    factor_block_diagonal(a, k, bs, o.small, be, bd, bperm, bnelim, bst);
+    if (bnelim == 0) {
+      for (i64 j = 0; j < bs; ++j)
+        for (i64 i = 0; i < rows; ++i) a(k + i, k + j) = backup[i + j * rows];
+      for (i64 off = 0; off < bs; ++off) {
+        end_pos -= 1;
+        if (k + off < end_pos) { swap_sym(a, m, k + off, end_pos); std::swap(R.perm[k + off], R.perm[end_pos]); }
+        R.st.ndel += 1;
+      }
+      continue;
+    }
+    // 3. permute panel columns
+    for (i64 r = be; r < m; ++r) {
+      for (i64 i = 0; i < bs; ++i) buf[i] = a(r, k + bperm[i]);
+      for (i64 i = 0; i < bs; ++i) a(r, k + i) = buf[i];
+    }
+    // 4. zero D off-diagonals of 2x2 pivots
+    {
+      i64 bc = 0;
+      while (bc < bnelim) {
+        if (bd.is2first(bc)) { a(k + bc + 1, k + bc) = 0.0; bc += 2; } else bc += 1;
+      }
+    }
+    // 5. row permutation of columns 0..k
+    for (i64 c = 0; c < k; ++c) {
+      for (i64 i = 0; i < bs; ++i) buf[i] = a(k + bperm[i], c);
+      for (i64 i = 0; i < bs; ++i) a(k + i, c) = buf[i];
+    }
+    // 6. col_order
+    for (i64 i = 0; i < bs; ++i) obuf[i] = R.perm[k + i];
+    for (i64 i = 0; i < bs; ++i) R.perm[k + i] = obuf[bperm[i]];
+    // 7. apply + check
+    i64 eff = apply_and_check(a, k, bnelim, bs, m, bd, o.threshold);
+    // 8. adjust
+    eff = adjust_2x2(eff, bd);
+    // 9. partial restore with permutation (restore_diagonal_with_perm, factor.rs:1244-1275)
+    if (eff < bnelim) {
+      for (i64 j = eff; j < bs; ++j) {
+        i64 c = bperm[j];
+        for (i64 i = eff; i < bs; ++i) {
+          i64 r = bperm[i];
+          a(k + i, k + j) = (r >= c) ? backup[r + c * rows] : backup[c + r * rows];
+        }
+      }
+      for (i64 j = eff; j < bs; ++j) {
+        i64 c = bperm[j];
+        for (i64 i = bs; i < rows; ++i) a(k + i, k + j) = backup[i + c * rows];
+      }
+    }
+    i64 nelim = eff;
+    // 10. Schur updates
+    if (nelim > 0) {
+      update_trailing(a, k, nelim, bs, m, nfs_boundary, bd);
+      update_cross_terms(a, k, nelim, bs, m, bd);
+    }
+    // 11. accumulate D and stats
+    R.d.copy_from_offset(bd, k, nelim);
+    {
+      i64 sc = 0;
+      while (sc < nelim) {
+        if (bd.type[sc] == PT_1X1) { R.st.n1++; sc += 1; }
+        else if (bd.is2first(sc)) { R.st.n2++; sc += 2; }
+        else sc += 1;
+      }
+    }
+    R.st.maxl = std::max(R.st.maxl, bst.maxl);
+    for (i64 c = 0; c < nelim; ++c)
+      for (i64 i = be; i < m; ++i) R.st.maxl = std::max(R.st.maxl, std::fabs(a(i, k + c)));
+    // 12. delay failed columns to end_pos
+    if (nelim < bs) {
+      i64 nd = bs - nelim;
+      for (i64 i = nd - 1; i >= 0; --i) {
+        i64 dp = k + nelim + i;
+        end_pos -= 1;
+        if (dp < end_pos) { swap_sym(a, m, dp, end_pos); std::swap(R.perm[dp], R.perm[end_pos]); }
+        R.st.ndel += 1;
+      }
+    }
+    k += nelim;
+  }
+  R.ne = k;
+  R.d.truncate(k);
+  return R;
+}
+
+// two_level_factor (factor.rs:2108-2252)
+FactorResult two_level_factor(MV a, i64 m, i64 p, const Opts& o) {
+  FactorResult R;
+  R.perm.resize(m);
+  std::iota(R.perm.begin(), R.perm.end(), 0);
+  R.d.init(p);
+  i64 gne = 0, rem = p;
+  while (rem > 0) {
+    i64 cs = gne, bcols = std::min(rem, o.nb);
+    i64 bm = m - cs;
+    FactorResult B = factor_inner(a.sub(cs, cs), bm, bcols, p - cs, o);
+    i64 bne = B.ne;
+    if (cs > 0) {
+      std::vector<double> tmp(bcols);
+      for (i64 c = 0; c < cs; ++c) {
+        for (i64 i = 0; i < bcols; ++i) tmp[i] = a(cs + B.perm[i], c);
+        for (i64 i = 0; i < bcols; ++i) a(cs + i, c) = tmp[i];
+      }
+    }
+    {
+      std::vector<i64> orig(R.perm.begin() + cs, R.perm.begin() + cs + bcols);
+      for (i64 i = 0; i < bcols; ++i)
+        if (B.perm[i] < bcols) R.perm[cs + i] = orig[B.perm[i]];
+    }
+    if (bne < bcols) {
+      i64 nf = bcols - bne;
+      for (i64 i = 0; i < nf; ++i) {
+        i64 fp = cs + bne + i, e = cs + rem - 1 - i;
+        if (fp < e) { swap_sym(a, m, fp, e); std::swap(R.perm[fp], R.perm[e]); }
+      }
+      R.st.ndel += nf;
+    }
+    R.d.copy_from_offset(B.d, gne, bne);
+    R.st.n1 += B.st.n1; R.st.n2 += B.st.n2; R.st.maxl = std::max(R.st.maxl, B.st.maxl);
+    gne += bne;
+    rem -= bcols;
+  }
+  R.ne = gne;
+  R.d.truncate(gne);
+  return R;
+}
+
+// ---------------------------------------------------------------------------
+// TPP (factor.rs:2268-2947)
+// ---------------------------------------------------------------------------
+// `nc` = number of stored columns (a.ncols()): m for square fronts, k for the
+// rectangular small-leaf storage.
+struct TppCtx { MV a; i64 m; i64 nc; };
+
+inline double sym_entry(const TppCtx& t, i64 row, i64 col) {  // factor.rs:2597-2606
+  if (col < t.nc && row >= col) return t.a(row, col);
+  return t.a(col, row);
+}
+bool is_col_small(const TppCtx& t, i64 idx, i64 from, i64 to, double small) {  // factor.rs:2674-2690
+  for (i64 c = from; c < std::min(idx, t.nc); ++c) if (std::fabs(t.a(idx, c)) >= small) return false;
+  if (idx < t.nc) for (i64 r = idx; r < to; ++r) if (std::fabs(t.a(r, idx)) >= small) return false;
+  return true;
+}
+i64 find_row_abs_max(const TppCtx& t, i64 p, i64 from, i64 to) {  // factor.rs:2695-2710
+  if (from >= to) return from;
+  i64 bi = from; double bv = std::fabs(sym_entry(t, p, from));
+  for (i64 c = from + 1; c < to; ++c) {
+    double v = std::fabs(sym_entry(t, p, c));
+    note_tie(v, bv);
+    if (v > bv) { bi = c; bv = v; }
+  }
+  return bi;
+}
+double find_rc_abs_max_exclude(const TppCtx& t, i64 col, i64 nelim, i64 m, i64 exclude) {  // 2715-2737
+  double best = 0.0;
+  for (i64 c = nelim; c < std::min(col, t.nc); ++c) { if (c == exclude) continue; best = std::max(best, std::fabs(t.a(col, c))); }
+  if (col < t.nc) for (i64 r = col + 1; r < m; ++r) { if (r == exclude) continue; best = std::max(best, std::fabs(t.a(r, col))); }
+  return best;
+}
+bool test_2x2(const TppCtx& t, i64 ti, i64 p, double maxt, double maxp, double u, double small) {  // 2268-2315
+  double a11 = t.a(ti, ti), a21 = t.a(p, ti), a22 = t.a(p, p);
+  double maxpiv = std::max(std::max(std::fabs(a11), std::fabs(a21)), std::fabs(a22));
+  if (maxpiv < small) return false;
+  double ds = 1.0 / maxpiv;
+  double dp0 = (a11 * ds) * a22, dp1 = (a21 * ds) * a21, dp = dp0 - dp1;
+  double lim = std::max(std::max(small, std::fabs(dp0 / 2.0)), std::fabs(dp1 / 2.0));
+  note_tie(std::fabs(dp), lim);
+  if (std::fabs(dp) < lim) return false;
+  double di11 = (a22 * ds) / dp, di12 = (-a21 * ds) / dp, di22 = (a11 * ds) / dp;
+  if (std::max(maxt, maxp) < small) return true;
+  double x1 = std::fabs(di11) * maxt + std::fabs(di12) * maxp;
+  double x2 = std::fabs(di12) * maxt + std::fabs(di22) * maxp;
+  note_tie(u * std::max(x1, x2), 1.0);
+  return u * std::max(x1, x2) < 1.0;
+}
+// swap_rect (factor.rs:2528-2580); with nc == m it equals swap_symmetric
+void swap_rect(const TppCtx& t, i64 i, i64 j) {
+  if (i == j) return;
+  if (i > j) std::swap(i, j);
+  MV a = t.a; i64 n = t.nc;
+  if (i < n && j < n) std::swap(a(i, i), a(j, j));
+  for (i64 k = 0; k < std::min(i, n); ++k) std::swap(a(i, k), a(j, k));
+  for (i64 k = i + 1; k < j; ++k) {
+    if (k < n) std::swap(a(k, i), a(j, k));
+    else if (i < n) break;
+  }
+  if (i < n && j < n) for (i64 k = j + 1; k < t.m; ++k) std::swap(a(k, i), a(k, j));
+}
+double tpp_apply_1x1(const TppCtx& t, i64 ne, i64 p) {  // 2616-2641
+  MV a = t.a; i64 m = t.m;
+  double d = a(ne, ne), inv = 1.0 / d, maxl = 0.0;
+  for (i64 i = ne + 1; i < m; ++i) { double l = a(i, ne) * inv; a(i, ne) = l; maxl = std::max(maxl, std::fabs(l)); }
+  i64 ce = std::min(p, t.nc);
+  for (i64 j = ne + 1; j < ce; ++j) {
+    double ldlj = a(j, ne) * d;
+    for (i64 i = j; i < m; ++i) a(i, j) -= a(i, ne) * ldlj;
+  }
+  return maxl;
+}
+double tpp_apply_2x2(const TppCtx& t, i64 ne, i64 p) {  // 2649-2683
+  MV a = t.a; i64 m = t.m;
+  double a11 = a(ne, ne), a21 = a(ne + 1, ne), a22 = a(ne + 1, ne + 1);
+  double det = a11 * a22 - a21 * a21, inv_det = 1.0 / det, maxl = 0.0;
+  for (i64 i = ne + 2; i < m; ++i) {
+    double ai1 = a(i, ne), ai2 = a(i, ne + 1);
+    double l1 = (ai1 * a22 - ai2 * a21) * inv_det, l2 = (ai2 * a11 - ai1 * a21) * inv_det;
+    a(i, ne) = l1; a(i, ne + 1) = l2;
+    maxl = std::max(maxl, std::max(std::fabs(l1), std::fabs(l2)));
+  }
+  i64 ce = std::min(p, t.nc);
+  for (i64 j = ne + 2; j < ce; ++j) {
+    double w1 = a(j, ne) * a11 + a(j, ne + 1) * a21, w2 = a(j, ne) * a21 + a(j, ne + 1) * a22;
+    for (i64 i = j; i < m; ++i) a(i, j) -= a(i, ne) * w1 + a(i, ne + 1) * w2;
+  }
+  a(ne + 1, ne) = 0.0;
+  return maxl;
+}
+
+// Shared body of tpp_factor (factor.rs:2335-2506) and tpp_factor_rect
+// (factor.rs:2761-2947): the two loops are identical apart from the storage
+// width, which TppCtx carries.
+i64 tpp_loop(const TppCtx& t, i64 start, i64 n, std::vector<i64>& perm, MixedD& d, Stats& st, const Opts& o) {
+  double u = o.threshold, small = o.small;
+  MV a = t.a; i64 m = t.m;
+  i64 ne = start;
+  while (ne < n) {
+    if (is_col_small(t, ne, ne, m, small)) {
+      d.set1(ne, 0.0); st.n1++;
+      if (ne < t.nc) for (i64 r = ne + 1; r < m; ++r) a(r, ne) = 0.0;
+      ne += 1;
+      continue;
+    }
+    bool found = false;
+    for (i64 p = ne + 1; p < n; ++p) {
+      if (is_col_small(t, p, ne, m, small)) {
+        if (p != ne) { swap_rect(t, p, ne); std::swap(perm[p], perm[ne]); }
+        d.set1(ne, 0.0); st.n1++;
+        for (i64 r = ne + 1; r < m; ++r) a(r, ne) = 0.0;
+        ne += 1; found = true; break;
+      }
+      i64 ti = find_row_abs_max(t, p, ne, p);
+      double maxt = find_rc_abs_max_exclude(t, ti, ne, m, p);
+      double maxp = find_rc_abs_max_exclude(t, p, ne, m, ti);
+      if (test_2x2(t, ti, p, maxt, maxp, u, small)) {
+        if (ti != ne) { swap_rect(t, ti, ne); std::swap(perm[ti], perm[ne]); }
+        i64 np = (p == ne) ? ti : p;
+        if (np != ne + 1) { swap_rect(t, np, ne + 1); std::swap(perm[np], perm[ne + 1]); }
+        double d11 = a(ne, ne), d21 = a(ne + 1, ne), d22 = a(ne + 1, ne + 1);
+        double ml = tpp_apply_2x2(t, ne, n);
+        d.set2(ne, d11, d21, d22); st.n2++; st.maxl = std::max(st.maxl, ml);
+        ne += 2; found = true; break;
+      }
+      double maxp_t = std::max(maxp, std::fabs(sym_entry(t, p, ti)));
+      note_tie(std::fabs(a(p, p)), u * maxp_t);
+      if (std::fabs(a(p, p)) >= u * maxp_t) {
+        if (p != ne) { swap_rect(t, p, ne); std::swap(perm[p], perm[ne]); }
+        double ml = tpp_apply_1x1(t, ne, n);
+        d.set1(ne, a(ne, ne)); st.n1++; st.maxl = std::max(st.maxl, ml);
+        ne += 1; found = true; break;
+      }
+    }
+    if (!found) {
+      double maxp = find_rc_abs_max_exclude(t, ne, ne, m, INT64_MAX);
+      note_tie(std::fabs(a(ne, ne)), u * maxp);
+      if (std::fabs(a(ne, ne)) >= u * maxp) {
+        double ml = tpp_apply_1x1(t, ne, n);
+        d.set1(ne, a(ne, ne)); st.n1++; st.maxl = std::max(st.maxl, ml);
+        ne += 1;
+      } else break;
+    }
+  }
+  return ne - start;
+}
+
+FactorResult tpp_factor_rect(MV a, i64 m, i64 nc, i64 n, const Opts& o) {  // factor.rs:2761-2947
+  FactorResult R;
+  R.perm.resize(m);
+  std::iota(R.perm.begin(), R.perm.end(), 0);
+  R.d.init(n);
+  TppCtx t{a, m, nc};
+  i64 ne = tpp_loop(t, 0, n, R.perm, R.d, R.st, o);
+  R.ne = ne;
+  R.d.truncate(ne);
+  R.st.ndel = n - ne;
+  return R;
+}
+
+// aptp_factor_in_place (factor.rs:301-404)
+FactorResult aptp_factor_in_place(MV a, i64 m, i64 p, const Opts& o) {
+  FactorResult R;
+  if (p < o.ib) R = tpp_factor_rect(a, m, m, p, o);
+  else if (p > o.nb) R = two_level_factor(a, m, p, o);
+  else R = factor_inner(a, m, p, p, o);
+  if (R.ne < p && o.failed_pivot_tpp) {
+    i64 q = R.ne;
+    R.d.grow(p);
+    TppCtx t{a, m, m};
+    i64 add = tpp_loop(t, q, p, R.perm, R.d, R.st, o);
+    R.ne = q + add;
+    R.d.truncate(R.ne);
+    R.st.ndel = p - R.ne;
+  }
+  return R;
+}
+
+// compute_contribution_gemm (factor.rs:1590-1652) with the NFS x NFS block
+// already assembled in `cb` (nfs x nfs, lower); L21_NFS = l[p..m, 0..ne].
+void contribution_gemm(const double* l, i64 ldl, i64 p, i64 ne, i64 m, const MixedD& d, double* cb, i64 ldc) {
+  i64 nfs = m - p;
+  if (nfs == 0 || ne == 0) return;
+  std::vector<double> W((size_t)nfs * ne, 0.0);
+  compute_ld(l + p, ldl, nfs, d, ne, W.data(), nfs);
+  // faer triangular GEMM (factor.rs:1639); per entry an fma chain over c ascending
+  for (i64 j = 0; j < nfs; ++j)
+    for (i64 c = 0; c < ne; ++c) {
+      double lj = l[p + j + c * ldl];
+      const double* w = W.data() + c * nfs;
+      double* col = cb + j * ldc;
+      for (i64 i = j; i < nfs; ++i) col[i] = std::fma(-w[i], lj, col[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Supernodes, amalgamation, small-leaf classification
+// ---------------------------------------------------------------------------
+struct SN {
+  i64 col_begin, col_end;
+  std::vector<i64> pattern;
+  i64 parent;  // -1 = root
+  std::vector<std::pair<i64, i64>> owned;  // [begin, end) ranges
+  bool in_small_leaf = false;
+  i64 n_owned() const { i64 s = 0; for (auto& r : owned) s += r.second - r.first; return s; }
+};
+
+// do_merge (amalgamation.rs:38-54)
+bool do_merge(i64 pn, i64 pcc, i64 cn, i64 ccc, i64 nemin) {
+  if (pn == 1 && pcc == std::max<i64>(ccc - 1, 0)) return true;
+  if (pn < nemin && cn < nemin) return true;
+  return false;
+}
+// sorted_union_excluding (amalgamation.rs:57-95)
+std::vector<i64> union_excl(const std::vector<i64>& a, const std::vector<i64>& b, i64 eb, i64 ee) {
+  std::vector<i64> r; r.reserve(a.size() + b.size());
+  size_t ia = 0, ib = 0;
+  auto push = [&](i64 v) { if (!(v >= eb && v < ee)) r.push_back(v); };
+  while (ia < a.size() && ib < b.size()) {
+    i64 va = a[ia], vb = b[ib], nx;
+    if (va < vb) { ia++; nx = va; } else if (vb < va) { ib++; nx = vb; } else { ia++; ib++; nx = va; }
+    push(nx);
+  }
+  for (; ia < a.size(); ++ia) push(a[ia]);
+  for (; ib < b.size(); ++ib) push(b[ib]);
+  return r;
+}
+// amalgamate (amalgamation.rs:115-231)
+std::vector<SN> amalgamate(std::vector<SN> sn, i64 nemin, i64* merges) {
+  i64 n = (i64)sn.size();
+  *merges = 0;
+  if (n <= 1) return sn;
+  std::vector<bool> del(n, false);
+  std::vector<i64> nel(n);
+  for (i64 s = 0; s < n; ++s) nel[s] = sn[s].col_end - sn[s].col_begin;
+  std::vector<std::vector<i64>> ch(n);
+  for (i64 s = 0; s < n; ++s) if (sn[s].parent >= 0) ch[sn[s].parent].push_back(s);
+  for (i64 p = 0; p < n; ++p) {
+    if (del[p]) continue;
+    std::vector<i64> pch; pch.swap(ch[p]);
+    for (i64 c : pch) {
+      if (del[c]) continue;
+      i64 pn = nel[p], pcc = nel[p] + (i64)sn[p].pattern.size();
+      i64 cn = nel[c], ccc = nel[c] + (i64)sn[c].pattern.size();
+      if (do_merge(pn, pcc, cn, ccc, nemin)) {
+        i64 nb = std::min(sn[p].col_begin, sn[c].col_begin), ne_ = std::max(sn[p].col_end, sn[c].col_end);
+        std::vector<i64> cp; cp.swap(sn[c].pattern);
+        std::vector<i64> pp; pp.swap(sn[p].pattern);
+        sn[p].pattern = union_excl(pp, cp, nb, ne_);
+        for (auto& r : sn[c].owned) sn[p].owned.push_back(r);
+        sn[c].owned.clear();
+        sn[p].col_begin = nb; sn[p].col_end = ne_;
+        nel[p] += nel[c];
+        std::vector<i64> cc; cc.swap(ch[c]);
+        for (i64 g : cc) if (!del[g]) sn[g].parent = p;
+        for (i64 g : cc) ch[p].push_back(g);
+        del[c] = true;
+      }
+    }
+    for (i64 c : pch) if (!del[c]) ch[p].push_back(c);
+  }
+  std::vector<i64> o2n(n, 0);
+  i64 ni = 0;
+  for (i64 s = 0; s < n; ++s) if (!del[s]) o2n[s] = ni++;
+  std::vector<SN> out; out.reserve(ni);
+  for (i64 s = 0; s < n; ++s)
+    if (!del[s]) {
+      SN x = std::move(sn[s]);
+      if (x.parent >= 0) x.parent = o2n[x.parent];
+      out.push_back(std::move(x));
+    }
+  *merges = n - ni;
+  return out;
+}
+
+struct Subtree { i64 root; std::vector<i64> nodes; i64 max_front; i64 parent_of_root; };
+
+// classify_small_leaf_subtrees (numeric.rs:2278-2369)
+std::vector<Subtree> classify_small_leaf(std::vector<SN>& sn, const std::vector<std::vector<i64>>& ch, i64 thr) {
+  std::vector<Subtree> out;
+  if (thr == 0) return out;
+  i64 n = (i64)sn.size();
+  for (i64 s = 0; s < n; ++s) {
+    i64 fs = sn[s].n_owned() + (i64)sn[s].pattern.size();
+    if (fs >= thr) { sn[s].in_small_leaf = false; continue; }
+    if (ch[s].empty()) sn[s].in_small_leaf = true;
+    else {
+      bool all = true;
+      for (i64 c : ch[s]) if (!sn[c].in_small_leaf) { all = false; break; }
+      sn[s].in_small_leaf = all;
+    }
+  }
+  for (i64 s = 0; s < n; ++s) {
+    if (!sn[s].in_small_leaf) continue;
+    bool is_root = sn[s].parent < 0 || !sn[sn[s].parent].in_small_leaf;
+    if (!is_root) continue;
+    std::vector<i64> nodes, stack{s}, visit;
+    while (!stack.empty()) {
+      i64 x = stack.back(); stack.pop_back();
+      visit.push_back(x);
+      for (i64 c : ch[x]) if (sn[c].in_small_leaf) stack.push_back(c);
+    }
+    while (!visit.empty()) { nodes.push_back(visit.back()); visit.pop_back(); }
+    if (nodes.size() < 2) { sn[s].in_small_leaf = false; continue; }
+    i64 mf = 0;
+    for (i64 x : nodes) mf = std::max(mf, sn[x].n_owned() + (i64)sn[x].pattern.size());
+    out.push_back(Subtree{s, nodes, mf, sn[s].parent});
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// Multifrontal driver (numeric.rs:844-1023, 1226-1533, 1562-1938, 1957-2163)
+// ---------------------------------------------------------------------------
+struct Front {      // FrontFactors (numeric.rs:543-596) plus per-supernode stats
+  i64 m = 0, k = 0, ne = 0;
+  std::vector<double> l11, l21;   // ne x ne, r x ne (column-major)
+  MixedD d11;
+  std::vector<i64> col_idx, row_idx, local_perm;
+  i64 n1 = 0, n2 = 0;
+  double maxl = 0;
+  i64 ties = 0;
+};
+
+struct CB { std::vector<double> data; i64 size = 0; std::vector<i64> rows; i64 ndel = 0; };
+
+struct Problem {
+  i64 n;
+  const i64 *colptr, *rowidx;
+  const double* val;
+  const double* scaling;  // elimination order or null
+  std::vector<i64> pfwd, pinv;
+};
+
+struct Oracle {
+  i64 n = 0;
+  Opts o;
+  std::vector<SN> sn;
+  std::vector<std::vector<i64>> ch;
+  std::vector<Front> fr;
+  std::vector<i64> pfwd;
+  std::vector<double> scaling;
+  bool has_scaling = false;
+  i64 sn_before = 0, merges = 0, n_sl_sub = 0, n_sl_nodes = 0;
+  i64 tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
+  i64 ties = 0;
+  std::string err;
+};
+
+// extract_front_factors (numeric.rs:2579-2713) from a front stored as m x nc
+void extract_factors(Front& F, const double* a, i64 lda, i64 m, i64 k, const std::vector<i64>& rows, const FactorResult& R) {
+  i64 ne = R.ne;
+  F.m = m; F.k = k; F.ne = ne;
+  F.l11.assign((size_t)ne * ne, 0.0);
+  i64 c = 0;
+  while (c < ne) {
+    F.l11[c + c * ne] = 1.0;
+    if (R.d.type[c] == PT_1X1) {
+      for (i64 i = c + 1; i < ne; ++i) F.l11[i + c * ne] = a[i + c * lda];
+      c += 1;
+    } else if (R.d.is2first(c)) {
+      F.l11[(c + 1) + (c + 1) * ne] = 1.0;
+      for (i64 i = c + 2; i < ne; ++i) { F.l11[i + c * ne] = a[i + c * lda]; F.l11[i + (c + 1) * ne] = a[i + (c + 1) * lda]; }
+      c += 2;
+    } else c += 1;
+  }
+  F.d11.init(ne);
+  c = 0;
+  while (c < ne) {
+    if (R.d.type[c] == PT_1X1) { F.d11.set1(c, R.d.diag[c]); c += 1; }
+    else { F.d11.set2(c, R.d.diag[c], R.d.off[c], R.d.diag[c + 1]); c += 2; }
+  }
+  i64 r = m - ne;
+  F.l21.assign((size_t)r * ne, 0.0);
+  for (i64 j = 0; j < ne; ++j)
+    for (i64 i = 0; i < r; ++i) F.l21[i + j * r] = a[ne + i + j * lda];
+  F.local_perm.assign(R.perm.begin(), R.perm.begin() + k);
+  F.col_idx.resize(ne);
+  for (i64 i = 0; i < ne; ++i) F.col_idx[i] = rows[R.perm[i]];
+  F.row_idx.clear();
+  for (i64 i = ne; i < k; ++i) F.row_idx.push_back(rows[R.perm[i]]);
+  for (i64 i = k; i < m; ++i) F.row_idx.push_back(rows[i]);
+  F.n1 = R.st.n1; F.n2 = R.st.n2; F.maxl = R.st.maxl;
+}
+
+// extract_contribution (numeric.rs:2739-2809): delayed block from the front,
+// NFS x NFS from `nfsblk` (nfs x nfs).
+CB extract_contrib(const double* a, i64 lda, i64 m, i64 k, const std::vector<i64>& rows, const FactorResult& R, std::vector<double>&& nfsblk) {
+  CB cb;
+  i64 ne = R.ne, size = m - ne, nd = k - ne, nfs = m - k;
+  cb.size = size; cb.ndel = nd;
+  if (nd > 0) {
+    cb.data.assign((size_t)size * size, 0.0);
+    for (i64 j = 0; j < nd; ++j)
+      for (i64 i = j; i < nd; ++i) cb.data[i + j * size] = a[ne + i + (ne + j) * lda];
+    for (i64 j = 0; j < nd; ++j)
+      for (i64 i = 0; i < nfs; ++i) cb.data[nd + i + j * size] = a[k + i + (ne + j) * lda];
+    for (i64 j = 0; j < nfs; ++j)
+      for (i64 i = j; i < nfs; ++i) cb.data[nd + i + (nd + j) * size] = nfsblk[i + j * nfs];
+  } else {
+    cb.data = std::move(nfsblk);
+  }
+  for (i64 i = ne; i < k; ++i) cb.rows.push_back(rows[R.perm[i]]);
+  for (i64 i = k; i < m; ++i) cb.rows.push_back(rows[i]);
+  return cb;
+}
+
+// Assembly shared by both node kinds: scatter original entries of owned columns
+// (scatter_original_entries_multi numeric.rs:2376-2435 and the amap fast path
+// numeric.rs:1306-1332, which produce the same sums) and extend-add of children
+// (extend_add numeric.rs:2445-2485). FS columns go to `fs` (m x k), NFS x NFS
+// entries to `nfsb` (nfs x nfs).
+void assemble(const Oracle& O, const Problem& P, const SN& s, i64 m, i64 k, std::vector<i64>& g2l,
+              double* fs, double* nfsb, bool has_nfs, std::vector<CB*>& cbs) {
+  i64 tot_owned = s.n_owned();
+  i64 nfs = m - k;
+  auto put = [&](i64 r, i64 c, double v) {
+    if (c < k) fs[r + c * m] += v;
+    else if (has_nfs && r >= k) nfsb[(r - k) + (c - k) * nfs] += v;
+  };
+  for (auto& rg : s.owned)
+    for (i64 pj = rg.first; pj < rg.second; ++pj) {
+      i64 oc = P.pfwd[pj];
+      i64 lc = g2l[pj];
+      for (i64 idx = P.colptr[oc]; idx < P.colptr[oc + 1]; ++idx) {
+        i64 orow = P.rowidx[idx];
+        if (orow < oc) {
+          i64 lp = g2l[P.pinv[orow]];
+          if (lp >= 0 && lp < tot_owned) continue;
+        }
+        i64 gr = P.pinv[orow];
+        i64 lr = g2l[gr];
+        if (lr < 0) continue;
+        if (lr >= tot_owned && lr < k) continue;
+        double v = P.val[idx];
+        // amap fast path (no delays): val * s[row] * s[col] (numeric.rs:1317);
+        // per-entry path: val *= s[row] * s[col] (numeric.rs:2421)
+        if (P.scaling) {
+          if (k == tot_owned) v = v * P.scaling[gr] * P.scaling[pj];
+          else v *= P.scaling[gr] * P.scaling[pj];
+        }
+        if (lr >= lc) put(lr, lc, v); else put(lc, lr, v);
+      }
+    }
+  for (CB* cb : cbs) {
+    for (i64 j = 0; j < cb->size; ++j) {
+      i64 lj = g2l[cb->rows[j]];
+      for (i64 i = j; i < cb->size; ++i) {
+        double v = cb->data[i + j * cb->size];
+        if (v != 0.0) {
+          i64 li = g2l[cb->rows[i]];
+          if (li >= lj) put(li, lj, v); else put(lj, li, v);
+        }
+      }
+    }
+  }
+  (void)O;
+}
+
+// One supernode: factor_single_supernode (numeric.rs:1226-1533) when
+// small_leaf is false, the per-node body of factor_small_leaf_subtree
+// (numeric.rs:1597-1935) when true.  Both keep the FS columns as m x k and the
+// NFS x NFS block separately; the square path's NFS x NFS region is only ever
+// copied into the contribution buffer (factor.rs:1615-1619) so the split is
+// value-identical.
+void factor_node(Oracle& O, const Problem& P, i64 s, std::vector<CB>& contrib, std::vector<i64>& g2l) {
+  SN& S = O.sn[s];
+  std::vector<i64> delayed;
+  std::vector<CB*> cbs;
+  for (i64 c : O.ch[s]) {
+    CB& cb = contrib[c];
+    if (cb.size > 0 || !cb.rows.empty()) {
+      for (i64 i = 0; i < cb.ndel; ++i) delayed.push_back(cb.rows[i]);
+      cbs.push_back(&cb);
+    }
+  }
+  i64 nown = S.n_owned();
+  i64 k = nown + (i64)delayed.size();
+  std::vector<i64> rows;
+  rows.reserve(k + S.pattern.size());
+  for (auto& rg : S.owned) for (i64 c = rg.first; c < rg.second; ++c) rows.push_back(c);
+  for (i64 c : delayed) rows.push_back(c);
+  for (i64 c : S.pattern) rows.push_back(c);
+  i64 m = (i64)rows.size();
+  for (i64 i = 0; i < m; ++i) g2l[rows[i]] = i;
+  i64 nfs = m - k;
+  bool has_nfs = nfs > 0 && S.parent >= 0;
+  std::vector<double> fs((size_t)m * k, 0.0);
+  std::vector<double> nfsb(has_nfs ? (size_t)nfs * nfs : 0, 0.0);
+  assemble(O, P, S, m, k, g2l, fs.data(), nfsb.data(), has_nfs, cbs);
+  for (CB* cb : cbs) { cb->data.clear(); cb->data.shrink_to_fit(); cb->rows.clear(); cb->size = 0; }
+  i64 t0 = g_ties;
+  FactorResult R;
+  MV a{fs.data(), m};
+  if (S.in_small_leaf) {
+    R = tpp_factor_rect(a, m, k, k, O.o);
+  } else {
+    // aptp_factor_in_place on the m x m front: it never reads or writes
+    // columns >= k (swaps stay within FS, updates stop at the NFS boundary),
+    // so the m x k storage is sufficient.
+    FactorResult RR;
+    if (k < O.o.ib) {
+      RR = tpp_factor_rect(a, m, k, k, O.o);
+    } else if (k > O.o.nb) RR = two_level_factor(a, m, k, O.o);
+    else RR = factor_inner(a, m, k, k, O.o);
+    if (RR.ne < k && O.o.failed_pivot_tpp) {
+      i64 q = RR.ne;
+      RR.d.grow(k);
+      TppCtx t{a, m, k};
+      i64 add = tpp_loop(t, q, k, RR.perm, RR.d, RR.st, O.o);
+      RR.ne = q + add;
+      RR.d.truncate(RR.ne);
+      RR.st.ndel = k - RR.ne;
+    }
+    R = std::move(RR);
+  }
+  i64 ne = R.ne;
+  Front& F = O.fr[s];
+  F.ties = g_ties - t0;
+  if (S.parent >= 0 && ne < m) {
+    if (has_nfs && ne > 0) contribution_gemm(fs.data(), m, k, ne, m, R.d, nfsb.data(), nfs);
+    contrib[s] = extract_contrib(fs.data(), m, m, k, rows, R, std::move(nfsb));
+  }
+  extract_factors(F, fs.data(), m, m, k, rows, R);
+  for (i64 i = 0; i < m; ++i) g2l[rows[i]] = -1;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C API (test / baseline use only)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+struct orc_options {
+  double threshold;
+  double small;
+  int64_t outer_block_size;
+  int64_t inner_block_size;
+  int64_t nemin;
+  int64_t small_leaf_threshold;
+  int32_t failed_pivot_tpp;
+  int32_t fallback_bk;
+};
+
+// Factor: the symbolic input is the pre-amalgamation supernode partition
+// (what AptpSymbolic exposes), the permutation perm_fwd[new] = old, the full
+// symmetric CSC and the MC64 scaling in elimination order (or NULL).
+void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end,
+                 const int64_t* pat_ptr, const int64_t* pat_idx, const int64_t* sup_parent,
+                 const int64_t* perm_fwd, const int64_t* colptr, const int64_t* rowidx,
+                 const double* values, const double* scaling, const orc_options* opt, int32_t nthreads) {
+  Oracle* O = new Oracle();
+  O->n = n;
+  if (opt) {
+    O->o.threshold = opt->threshold; O->o.small = opt->small; O->o.nb = opt->outer_block_size;
+    O->o.ib = opt->inner_block_size; O->o.nemin = opt->nemin; O->o.small_leaf_threshold = opt->small_leaf_threshold;
+    O->o.failed_pivot_tpp = opt->failed_pivot_tpp; O->o.fallback_bk = opt->fallback_bk;
+  }
+  std::vector<SN> sn(nsup);
+  for (i64 s = 0; s < nsup; ++s) {
+    sn[s].col_begin = sup_begin[s]; sn[s].col_end = sup_end[s];
+    sn[s].pattern.assign(pat_idx + pat_ptr[s], pat_idx + pat_ptr[s + 1]);
+    sn[s].parent = sup_parent[s];
+    sn[s].owned = {{sup_begin[s], sup_end[s]}};
+  }
+  O->sn_before = nsup;
+  O->sn = amalgamate(std::move(sn), O->o.nemin, &O->merges);
+  i64 ns = (i64)O->sn.size();
+  O->ch.assign(ns, {});
+  for (i64 s = 0; s < ns; ++s) if (O->sn[s].parent >= 0) O->ch[O->sn[s].parent].push_back(s);
+  auto subs = classify_small_leaf(O->sn, O->ch, O->o.small_leaf_threshold);
+  O->n_sl_sub = (i64)subs.size();
+  for (auto& st : subs) O->n_sl_nodes += (i64)st.nodes.size();
+  Problem P;
+  P.n = n; P.colptr = colptr; P.rowidx = rowidx; P.val = values; P.scaling = scaling;
+  P.pfwd.assign(perm_fwd, perm_fwd + n);
+  P.pinv.assign(n, 0);
+  for (i64 i = 0; i < n; ++i) P.pinv[P.pfwd[i]] = i;
+  O->pfwd = P.pfwd;
+  if (scaling) { O->has_scaling = true; O->scaling.assign(scaling, scaling + n); }
+  O->fr.assign(ns, Front());
+  std::vector<CB> contrib(ns);
+  g_ties = 0;
+  // small-leaf pre-pass (numeric.rs:1984-2010) then level-set waves (2038-2160)
+  std::vector<i64> remaining(ns);
+  for (i64 s = 0; s < ns; ++s) remaining[s] = (i64)O->ch[s].size();
+  {
+    std::vector<i64> g2l(n, -1);
+    for (auto& st : subs) {
+      for (i64 x : st.nodes) factor_node(*O, P, x, contrib, g2l);
+      if (st.parent_of_root >= 0) remaining[st.parent_of_root] -= 1;
+    }
+  }
+  std::vector<i64> ready;
+  for (i64 s = 0; s < ns; ++s) if (remaining[s] == 0 && !O->sn[s].in_small_leaf) ready.push_back(s);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+  while (!ready.empty()) {
+    i64 nr = (i64)ready.size();
+#ifdef _OPENMP
+#pragma omp parallel
+    {
+      std::vector<i64> g2l(n, -1);
+      i64 ties0 = g_ties; g_ties = 0;
+#pragma omp for schedule(dynamic, 1)
+      for (i64 i = 0; i < nr; ++i) factor_node(*O, P, ready[i], contrib, g2l);
+      g_ties = ties0;
+    }
+#else
+    {
+      std::vector<i64> g2l(n, -1);
+      for (i64 i = 0; i < nr; ++i) factor_node(*O, P, ready[i], contrib, g2l);
+    }
+#endif
+    std::vector<i64> next;
+    for (i64 s : ready) {
+      i64 p = O->sn[s].parent;
+      if (p >= 0) { remaining[p] -= 1; if (remaining[p] == 0) next.push_back(p); }
+    }
+    ready.swap(next);
+  }
+  // aggregate stats (numeric.rs:929-1009)
+  for (i64 s = 0; s < ns; ++s) {
+    Front& F = O->fr[s];
+    O->tot1 += F.n1; O->tot2 += F.n2; O->totdel += F.k - F.ne;
+    O->max_front = std::max(O->max_front, F.m);
+    O->ties += F.ties;
+    for (i64 c = 0; c < F.ne; ++c) if (F.d11.type[c] == PT_1X1 && F.d11.diag[c] == 0.0) O->zero_piv++;
+    if (O->sn[s].parent < 0 && F.ne < F.m) O->zero_piv += F.k - F.ne;
+  }
+  return O;
+}
+
+void orc_free(void* h) { delete (Oracle*)h; }
+
+// counts: [n1x1, n2x2, delayed, zero_pivots, max_front, sn_before, sn_after, merges, sl_subtrees, sl_nodes, ties]
+void orc_stats(void* h, int64_t* out) {
+  Oracle* O = (Oracle*)h;
+  out[0] = O->tot1; out[1] = O->tot2; out[2] = O->totdel; out[3] = O->zero_piv; out[4] = O->max_front;
+  out[5] = O->sn_before; out[6] = (i64)O->sn.size(); out[7] = O->merges; out[8] = O->n_sl_sub; out[9] = O->n_sl_nodes;
+  out[10] = O->ties;
+}
+
+// SparseLDLT::inertia (solver.rs:504-519)
+void orc_inertia(void* h, int64_t* out) {
+  Oracle* O = (Oracle*)h;
+  i64 p = 0, n = 0, z = 0;
+  for (auto& F : O->fr) F.d11.inertia(&p, &n, &z);
+  out[0] = p; out[1] = n; out[2] = z;
+}
+
+int64_t orc_nsup(void* h) { return (i64)((Oracle*)h)->sn.size(); }
+
+// per supernode (post-amalgamation): m, k, ne, n1, n2, parent, n_owned, in_small_leaf, ties
+void orc_front_info(void* h, int64_t* out9) {
+  Oracle* O = (Oracle*)h;
+  for (size_t s = 0; s < O->fr.size(); ++s) {
+    Front& F = O->fr[s];
+    i64* o = out9 + 9 * s;
+    o[0] = F.m; o[1] = F.k; o[2] = F.ne; o[3] = F.n1; o[4] = F.n2; o[5] = O->sn[s].parent;
+    o[6] = O->sn[s].n_owned(); o[7] = O->sn[s].in_small_leaf ? 1 : 0; o[8] = F.ties;
+  }
+}
+
+// Elimination record, fronts in supernode order: eliminated global (permuted)
+// column, pivot code (1 = 1x1, 2 = first of 2x2, 3 = second of 2x2), D diag and
+// D off-diagonal (for the first of a 2x2).  Returns the number of entries.
+int64_t orc_elim(void* h, int64_t* col, int8_t* code, double* dd, double* doff) {
+  Oracle* O = (Oracle*)h;
+  i64 t = 0;
+  for (auto& F : O->fr)
+    for (i64 c = 0; c < F.ne; ++c) {
+      col[t] = F.col_idx[c];
+      code[t] = F.d11.type[c] == PT_1X1 ? 1 : (F.d11.partner[c] > c ? 2 : 3);
+      dd[t] = F.d11.diag[c];
+      doff[t] = (code[t] == 2) ? F.d11.off[c] : 0.0;
+      ++t;
+    }
+  return t;
+}
+
+// SparseLDLT::solve_in_place (solver.rs:370-428) + aptp_solve (solve.rs:57-144)
+void orc_solve(void* h, double* rhs) {
+  Oracle* O = (Oracle*)h;
+  i64 n = O->n;
+  if (n == 0) return;
+  std::vector<double> x(n);
+  for (i64 i = 0; i < n; ++i) x[i] = rhs[O->pfwd[i]];
+  if (O->has_scaling) for (i64 i = 0; i < n; ++i) x[i] *= O->scaling[i];
+  std::vector<double> w, w2;
+  // forward (solve.rs:161-225)
+  for (auto& F : O->fr) {
+    i64 ne = F.ne; if (ne == 0) continue;
+    i64 r = (i64)F.row_idx.size();
+    w.assign(ne, 0.0);
+    for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
+    for (i64 j = 0; j < ne; ++j) { double xj = w[j]; for (i64 i = j + 1; i < ne; ++i) w[i] -= F.l11[i + j * ne] * xj; }
+    for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
+    if (r > 0) {
+      w2.assign(r, 0.0);
+      for (i64 j = 0; j < ne; ++j) { double xj = w[j]; const double* l = F.l21.data() + j * r; for (i64 i = 0; i < r; ++i) w2[i] += l[i] * xj; }
+      for (i64 i = 0; i < r; ++i) x[F.row_idx[i]] -= w2[i];
+    }
+  }
+  // diagonal (solve.rs:232-252)
+  for (auto& F : O->fr) {
+    i64 ne = F.ne; if (ne == 0) continue;
+    w.assign(ne, 0.0);
+    for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
+    F.d11.solve(w.data());
+    for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
+  }
+  // backward (solve.rs:261-326)
+  for (i64 s = (i64)O->fr.size() - 1; s >= 0; --s) {
+    Front& F = O->fr[s];
+    i64 ne = F.ne; if (ne == 0) continue;
+    i64 r = (i64)F.row_idx.size();
+    w.assign(ne, 0.0);
+    for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
+    if (r > 0) {
+      w2.assign(r, 0.0);
+      for (i64 i = 0; i < r; ++i) w2[i] = x[F.row_idx[i]];
+      for (i64 j = 0; j < ne; ++j) { const double* l = F.l21.data() + j * r; double s2 = 0.0; for (i64 i = 0; i < r; ++i) s2 += l[i] * w2[i]; w[j] -= s2; }
+    }
+    for (i64 j = ne - 1; j >= 0; --j) { double s2 = w[j]; for (i64 i = j + 1; i < ne; ++i) s2 -= F.l11[i + j * ne] * w[i]; w[j] = s2; }
+    for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
+  }
+  if (O->has_scaling) for (i64 i = 0; i < n; ++i) x[i] *= O->scaling[i];
+  for (i64 i = 0; i < n; ++i) rhs[O->pfwd[i]] = x[i];
+}
+
+// Dense entry: aptp_factor_in_place (factor.rs:301-404) on an m x m
+// column-major matrix with p fully summed columns.  Outputs the column
+// permutation (m), the D entries (type/diag/off, length p) and
+// [ne, n1x1, n2x2, ndelayed]; `maxl` receives stats.max_l_entry.
+void orc_dense_aptp(int64_t m, int64_t p, double* a, const orc_options* opt, int64_t* perm,
+                    int8_t* dtype, double* ddiag, double* doff, int64_t* st4, double* maxl) {
+  Opts o;
+  if (opt) {
+    o.threshold = opt->threshold; o.small = opt->small; o.nb = opt->outer_block_size; o.ib = opt->inner_block_size;
+    o.failed_pivot_tpp = opt->failed_pivot_tpp;
+  }
+  MV A{a, m};
+  FactorResult R = aptp_factor_in_place(A, m, p, o);
+  for (i64 i = 0; i < m; ++i) perm[i] = R.perm[i];
+  for (i64 c = 0; c < p; ++c) {
+    if (c < R.ne) {
+      dtype[c] = R.d.type[c] == PT_1X1 ? 1 : (R.d.partner[c] > c ? 2 : 3);
+      ddiag[c] = R.d.diag[c];
+      doff[c] = R.d.is2first(c) ? R.d.off[c] : 0.0;
+    } else { dtype[c] = 0; ddiag[c] = 0; doff[c] = 0; }
+  }
+  st4[0] = R.ne; st4[1] = R.st.n1; st4[2] = R.st.n2; st4[3] = R.st.ndel;
+  *maxl = R.st.maxl;
+}
+
+}  // extern "C"

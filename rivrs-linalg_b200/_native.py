@@ -1,0 +1,113 @@
+"""ctypes binding of the in-tree library librivrs_b200.so (include/rivrs_b200.h).
+
+The library is the product: there is no Python or CPU fallback for the
+numeric phase.  Loading fails loudly when the shared object is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librivrs_b200.so")
+
+i64 = C.c_int64
+i64p = C.POINTER(C.c_int64)
+dp = C.POINTER(C.c_double)
+i8p = C.POINTER(C.c_int8)
+vp = C.c_void_p
+
+STATUS = {
+    0: "OK", 1: "DimensionMismatch", 2: "InvalidInput", 3: "SolveBeforeFactor", 4: "AnalysisFailure",
+    5: "DeviceError", 6: "DeviceTimeout", 7: "OutOfMemory",
+}
+
+
+class Options(C.Structure):
+    _fields_ = [("threshold", C.c_double), ("small", C.c_double), ("outer_block_size", i64),
+                ("inner_block_size", i64), ("nemin", i64), ("small_leaf_threshold", i64),
+                ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("total_1x1_pivots", i64), ("total_2x2_pivots", i64), ("total_delayed", i64),
+                ("zero_pivots", i64), ("max_front_size", i64), ("supernodes_before_amalgamation", i64),
+                ("supernodes_after_amalgamation", i64), ("merges_performed", i64),
+                ("small_leaf_subtrees", i64), ("small_leaf_nodes", i64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class RvgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+SIGNATURES = {
+    "rvg_default_options": (None, [C.POINTER(Options)]),
+    "rvg_last_error": (C.c_char_p, []),
+    "rvg_analyze": (C.c_int, [i64, i64p, i64p, i64p, C.POINTER(vp)]),
+    "rvg_symbolic_sizes": (C.c_int, [vp, i64p]),
+    "rvg_symbolic_export": (C.c_int, [vp, i64p, i64p, i64p, i64p, i64p, i64p]),
+    "rvg_symbolic_free": (None, [vp]),
+    "rvg_create": (C.c_int, [i64, i64, i64p, i64p, i64p, i64p, i64p, i64p, i64p, i64p, C.POINTER(Options),
+                             C.POINTER(vp)]),
+    "rvg_factor": (C.c_int, [vp, dp, dp]),
+    "rvg_factor_device": (C.c_int, [vp, vp, vp]),
+    "rvg_solve": (C.c_int, [vp, dp, i64, i64]),
+    "rvg_solve_device": (C.c_int, [vp, vp, i64, i64]),
+    "rvg_inertia": (C.c_int, [vp, i64p]),
+    "rvg_get_stats": (C.c_int, [vp, C.POINTER(Stats)]),
+    "rvg_pivot_record": (C.c_int, [vp, i64p, i8p, dp, dp, i64p]),
+    "rvg_front_info": (C.c_int, [vp, i64p, i64p]),
+    "rvg_work": (C.c_int, [vp, dp]),
+    "rvg_timings": (C.c_int, [vp, dp]),
+    "rvg_stream": (C.c_int, [vp, C.POINTER(vp)]),
+    "rvg_destroy": (None, [vp]),
+}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python rivrs-linalg_b200/build.py` "
+                              "(the numeric phase has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        raise RvgError(status, lib().rvg_last_error().decode())
+
+
+def ptr(a, ctype):
+    return a.ctypes.data_as(ctype) if a is not None else None
+
+
+def as_i64(a):
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def as_f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().rvg_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o

@@ -1,0 +1,1538 @@
+// B200 numeric phase: level-set multifrontal APTP factorization and the
+// supernodal solve, behind the C ABI of include/rivrs_b200.h.
+//
+// Reference path (rivrs-linalg, sparse/src/symmetric/):
+//   AptpNumeric::factor            numeric.rs:844-1023
+//   factor_tree_levelset           numeric.rs:1957-2163
+//   factor_single_supernode        numeric.rs:1226-1533
+//   factor_small_leaf_subtree      numeric.rs:1562-1938
+//   aptp_factor_in_place & kernels factor.rs:301-404, 891-3181
+//   aptp_solve                     solve.rs:57-326
+//   SparseLDLT::solve_in_place     solver.rs:370-428
+//
+// Layout in HBM (one handle):
+//   panel arena   m x k column-major panel per front (the FS columns of the
+//                 frontal matrix); after factorization it IS the factor:
+//                 L11 in rows [0,ne), L21 in rows [ne,m), columns [0,ne).
+//   index arena   per front: row list (m global indices: owned ++ delayed
+//                 ++ pattern) followed by the local pivot order (k).
+//   D arrays      per front k entries (type, diag, off).
+//   contribution  the NFS x NFS Schur block of each non-root front, one
+//                 stream-ordered allocation per wave, released once every
+//                 parent that reads it has been assembled.
+// Each wave (all fronts whose children are done) runs: row lists -> scatter
+// of original entries -> extend-add, one pass per child ordinal so every
+// destination receives its terms in the reference's order without atomics
+// -> dense factorization (warp TPP or CTA APTP) -> contribution GEMM.  One
+// small device->host copy per wave returns the eliminated counts that size
+// the next wave (delays change front sizes at run time).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dense.cuh"
+#include "rvg_internal.h"
+
+namespace rvg {
+
+// ---------------------------------------------------------------------------
+// error plumbing
+// ---------------------------------------------------------------------------
+thread_local std::string g_err;
+void set_error(const std::string& s) { g_err = s; }
+
+#define CK(call)                                                                                \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) {                                                                    \
+      set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call);           \
+      return e_ == cudaErrorMemoryAllocation ? RVG_ERR_OUT_OF_MEMORY : RVG_ERR_DEVICE;          \
+    }                                                                                           \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device descriptors
+// ---------------------------------------------------------------------------
+enum : int32_t { FF_SMALL_LEAF = 1, FF_HAS_CB = 2, FF_HAS_PARENT = 4 };
+
+struct DFront {
+  int64_t panel;    // offset (doubles) in the panel arena, ld = m
+  int64_t idx;      // offset (int32) in the index arena: rows[m], perm[k]
+  int64_t dpos;     // offset in the D arrays (k entries)
+  int64_t scratch;  // offset (doubles) in the wave scratch
+  double* cb;       // NFS x NFS contribution block (ld nfs) or null
+  int32_t m, k, nown, ndin, nfs;
+  int32_t ne, n1, n2;
+  int32_t parent;
+  int32_t dly_off;  // position of this front's delayed columns among the parent's delayed block
+  int32_t flags;
+  int32_t pad;
+};
+
+struct Statics {
+  const int64_t* own_ptr;
+  const int32_t* own_idx;
+  const int64_t* pat_ptr;
+  const int32_t* pat_idx;
+  const int64_t* amap_ptr;
+  const int32_t* amap;
+  const int64_t* ea_ptr;
+  const int32_t* ea_map;
+  const int64_t* ch_ptr;
+  const int32_t* ch_idx;
+};
+
+struct Arenas {
+  double* panel;
+  int32_t* idx;
+  int8_t* dtype;
+  double* ddiag;
+  double* doff;
+  double* scratch;
+};
+
+// ---------------------------------------------------------------------------
+// assembly kernels
+// ---------------------------------------------------------------------------
+
+// Row list of each front: owned ++ delayed-from-children ++ pattern
+// (numeric.rs:1239-1262), and the identity pivot order.
+__global__ void k_front_rows(const int32_t* ids, int n, DFront* F, Statics S, Arenas A) {
+  int f = blockIdx.x;
+  if (f >= n) return;
+  int s = ids[f];
+  const DFront fr = F[s];
+  int32_t* rows = A.idx + fr.idx;
+  int32_t* perm = rows + fr.m;
+  int64_t o0 = S.own_ptr[s];
+  for (int i = threadIdx.x; i < fr.nown; i += blockDim.x) rows[i] = S.own_idx[o0 + i];
+  int64_t p0 = S.pat_ptr[s];
+  for (int i = threadIdx.x; i < fr.nfs; i += blockDim.x) rows[fr.k + i] = S.pat_idx[p0 + i];
+  for (int i = threadIdx.x; i < fr.k; i += blockDim.x) perm[i] = i;
+  for (int64_t q = S.ch_ptr[s]; q < S.ch_ptr[s + 1]; ++q) {
+    const DFront c = F[S.ch_idx[q]];
+    int nd = c.k - c.ne;
+    const int32_t* crow = A.idx + c.idx;
+    const int32_t* cperm = crow + c.m;
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) rows[fr.nown + c.dly_off + i] = crow[cperm[c.ne + i]];
+  }
+}
+
+struct ScatterItem { int32_t front; int32_t pad; int64_t e0; };
+
+// Original entries (numeric.rs:1306-1344 amap path, 2376-2435 per-entry
+// path); each destination receives at most one original entry.
+__global__ void k_scatter(const ScatterItem* items, const DFront* F, Statics S, Arenas A, const double* vals,
+                          const double* scal) {
+  ScatterItem it = items[blockIdx.x];
+  const DFront fr = F[it.front];
+  int64_t e = it.e0 + threadIdx.x;
+  if (e >= S.amap_ptr[it.front + 1]) return;
+  const int32_t* q = S.amap + 5 * e;
+  int32_t r = q[1], c = q[2];
+  if (r >= fr.nown) r += fr.ndin;
+  if (c >= fr.nown) c += fr.ndin;
+  double v = vals[q[0]];
+  if (scal) {
+    if (fr.ndin == 0) v = __dmul_rn(__dmul_rn(v, scal[q[3]]), scal[q[4]]);
+    else v = __dmul_rn(v, __dmul_rn(scal[q[3]], scal[q[4]]));
+  }
+  if (c < fr.k) {
+    double* a = A.panel + fr.panel;
+    a[r + (int64_t)c * fr.m] += v;
+  } else if ((fr.flags & FF_HAS_CB) && r >= fr.k) {
+    fr.cb[(r - fr.k) + (int64_t)(c - fr.k) * fr.nfs] += v;
+  }
+}
+
+struct EaItem { int32_t parent; int32_t child; int32_t j0; int32_t pad; };
+
+// Extend-add of one child's contribution into its parent
+// (numeric.rs:2445-2559): columns [j0, j0+32) of the child block.  The child
+// block is [delayed; NFS] x [delayed; NFS]: its delayed columns live in the
+// child's panel (rows ne..k and k..m of columns ne..k), its NFS x NFS part in
+// the child's contribution buffer.
+__global__ void k_extend_add(const EaItem* items, const DFront* F, Statics S, Arenas A) {
+  EaItem it = items[blockIdx.x];
+  const DFront P = F[it.parent];
+  const DFront C = F[it.child];
+  const int nd = C.k - C.ne;
+  const int sz = C.m - C.ne;
+  const int32_t* ea = S.ea_map + S.ea_ptr[it.child];
+  const double* cp = A.panel + C.panel;
+  double* pp = A.panel + P.panel;
+  auto map = [&](int i) -> int {
+    if (i < nd) return P.nown + C.dly_off + i;
+    int l = ea[i - nd];
+    return l < P.nown ? l : l + P.ndin;
+  };
+  int jend = min(it.j0 + 32, sz);
+  for (int j = it.j0; j < jend; ++j) {
+    int lj = map(j);
+    for (int i = j + threadIdx.x; i < sz; i += blockDim.x) {
+      double v;
+      if (j < nd) {
+        int64_t row = i < nd ? (C.ne + i) : (C.k + (i - nd));
+        v = cp[row + (int64_t)(C.ne + j) * C.m];
+      } else {
+        v = C.cb[(i - nd) + (int64_t)(j - nd) * C.nfs];
+      }
+      if (v == 0.0) continue;
+      int li = map(i);
+      int r = li >= lj ? li : lj, c = li >= lj ? lj : li;
+      if (c < P.k) pp[r + (int64_t)c * P.m] += v;
+      else if ((P.flags & FF_HAS_CB) && r >= P.k) P.cb[(r - P.k) + (int64_t)(c - P.k) * P.nfs] += v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dense factorization kernels
+// ---------------------------------------------------------------------------
+
+// One warp per front: TPP on all k columns (small-leaf fronts, numeric.rs:
+// 1805; fronts with k < ib, factor.rs:360-362).
+__global__ void k_tpp(const int32_t* ids, int n, DFront* F, Arenas A, DevOpts o) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  int lane = threadIdx.x & 31;
+  if (w >= n) return;
+  __shared__ int cnt[8][2];
+  int wl = threadIdx.x >> 5;
+  int s = ids[w];
+  DFront fr = F[s];
+  if (lane == 0) { cnt[wl][0] = 0; cnt[wl][1] = 0; }
+  __syncwarp();
+  WarpTpp T{PanelView{A.panel + fr.panel, fr.m}, fr.m, fr.k, lane};
+  int32_t* perm = A.idx + fr.idx + fr.m;
+  DRec d{A.dtype + fr.dpos, A.ddiag + fr.dpos, A.doff + fr.dpos};
+  int64_t ne = T.run(0, fr.k, perm, d, &cnt[wl][0], &cnt[wl][1], o);
+  __syncwarp();
+  if (lane == 0) { F[s].ne = (int32_t)ne; F[s].n1 = cnt[wl][0]; F[s].n2 = cnt[wl][1]; }
+}
+
+constexpr int NT = 256;   // threads of the CTA APTP kernel
+constexpr int IBMAX = 32; // inner block size supported by the kernels
+
+struct CtaShared {
+  double T[IBMAX][IBMAX + 1];
+  double Lj[IBMAX];
+  int bperm[IBMAX];
+  int8_t bdt[IBMAX];
+  double bdd[IBMAX];
+  double bdo[IBMAX];
+  int bnelim, eff, n1, n2, end_pos, k;
+  int tmpi[NT];
+  double tmpd[NT];
+};
+
+// Complete pivoting on the bs x bs diagonal block held in shared memory,
+// executed by one warp (factor_block_diagonal, factor.rs:891-1153).
+__device__ void warp_block_factor(CtaShared& sh, int bs, double small, int lane) {
+  double(*T)[IBMAX + 1] = sh.T;
+  if (lane < IBMAX) { sh.bperm[lane] = lane; sh.bdt[lane] = PT_DELAYED; sh.bdd[lane] = 0; sh.bdo[lane] = 0; }
+  __syncwarp();
+  auto swp = [&](int i, int j) {  // swap_symmetric_block limited to the block
+    if (i == j) return;
+    if (i > j) { int t = i; i = j; j = t; }
+    if (lane == 0) { double t = T[i][i]; T[i][i] = T[j][j]; T[j][j] = t; }
+    if (lane < i) { double t = T[i][lane]; T[i][lane] = T[j][lane]; T[j][lane] = t; }
+    if (lane > i && lane < j) { double t = T[lane][i]; T[lane][i] = T[j][lane]; T[j][lane] = t; }
+    if (lane > j && lane < bs) { double t = T[lane][i]; T[lane][i] = T[lane][j]; T[lane][j] = t; }
+    if (lane == 0) { int t = sh.bperm[i]; sh.bperm[i] = sh.bperm[j]; sh.bperm[j] = t; }
+    __syncwarp();
+  };
+  int k = 0;
+  while (k < bs) {
+    int cur = k;
+    int remaining = bs - k;
+    // arg-max over the lower triangle of [cur, bs)^2, scan order j then i
+    double bv = 0.0;
+    int64_t key = INT64_MAX;
+    if (lane >= cur && lane < bs) {
+      for (int i = lane; i < bs; ++i) {
+        double v = fabs(T[i][lane]);
+        if (v > bv) { bv = v; key = (int64_t)lane * 64 + i; }
+      }
+    }
+    warp_argmax(bv, key);
+    int mr = cur, mc = cur;
+    if (key != INT64_MAX) { mc = (int)(key / 64); mr = (int)(key % 64); }
+    double maxv = bv;
+    if (maxv < small) break;
+    if (mr == mc) {
+      swp(cur, mr);
+      double dkk = T[cur][cur], inv = 1.0 / dkk;
+      if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
+      __syncwarp();
+      if (lane > cur && lane < bs) {
+        for (int j = cur + 1; j <= lane; ++j) {
+          double ldl = __dmul_rn(T[j][cur], dkk);
+          T[lane][j] = __dsub_rn(T[lane][j], __dmul_rn(T[lane][cur], ldl));
+        }
+      }
+      __syncwarp();
+      if (lane == 0) { sh.bdt[k] = PT_1X1; sh.bdd[k] = dkk; }
+      k += 1;
+    } else {
+      int t = mr, mi = mc;
+      double amm = T[mi][mi], att = T[t][t], atm = T[t][mi];
+      double delta = __dsub_rn(__dmul_rn(amm, att), __dmul_rn(atm, atm));
+      if (remaining < 2) {
+        int pp = fabs(amm) >= fabs(att) ? mi : t;
+        swp(cur, pp);
+        double dkk = T[cur][cur];
+        if (fabs(dkk) < small) break;
+        double inv = 1.0 / dkk;
+        if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
+        __syncwarp();
+        if (lane == 0) { sh.bdt[k] = PT_1X1; sh.bdd[k] = dkk; }
+        k += 1;
+        continue;
+      }
+      if (fabs(delta) >= __dmul_rn(__dmul_rn(0.5, atm), atm)) {
+        swp(cur, mi);
+        int nt = (t == cur) ? mi : t;
+        swp(cur + 1, nt);
+        double a11 = T[cur][cur], a22 = T[cur + 1][cur + 1], a21 = T[cur + 1][cur];
+        double det = __dsub_rn(__dmul_rn(a11, a22), __dmul_rn(a21, a21));
+        double inv_det = 1.0 / det;
+        if (lane >= cur + 2 && lane < bs) {
+          double ai1 = T[lane][cur], ai2 = T[lane][cur + 1];
+          T[lane][cur] = __dmul_rn(__dsub_rn(__dmul_rn(ai1, a22), __dmul_rn(ai2, a21)), inv_det);
+          T[lane][cur + 1] = __dmul_rn(__dsub_rn(__dmul_rn(ai2, a11), __dmul_rn(ai1, a21)), inv_det);
+        }
+        __syncwarp();
+        if (lane >= cur + 2 && lane < bs) {
+          for (int j = cur + 2; j <= lane; ++j) {
+            double l1j = T[j][cur], l2j = T[j][cur + 1];
+            double w1 = __dadd_rn(__dmul_rn(l1j, a11), __dmul_rn(l2j, a21));
+            double w2 = __dadd_rn(__dmul_rn(l1j, a21), __dmul_rn(l2j, a22));
+            T[lane][j] = __dsub_rn(T[lane][j], __dadd_rn(__dmul_rn(T[lane][cur], w1), __dmul_rn(T[lane][cur + 1], w2)));
+          }
+        }
+        __syncwarp();
+        if (lane == 0) {
+          sh.bdt[k] = PT_2X2; sh.bdt[k + 1] = PT_2X2B;
+          sh.bdd[k] = a11; sh.bdd[k + 1] = a22; sh.bdo[k] = a21;
+        }
+        k += 2;
+      } else {
+        int pp = fabs(amm) >= fabs(att) ? mi : t;
+        swp(cur, pp);
+        double dkk = T[cur][cur], inv = 1.0 / dkk;
+        if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
+        __syncwarp();
+        if (lane > cur && lane < bs) {
+          for (int j = cur + 1; j <= lane; ++j) {
+            double ldl = __dmul_rn(T[j][cur], dkk);
+            T[lane][j] = __dsub_rn(T[lane][j], __dmul_rn(T[lane][cur], ldl));
+          }
+        }
+        __syncwarp();
+        if (lane == 0) { sh.bdt[k] = PT_1X1; sh.bdd[k] = dkk; }
+        k += 1;
+      }
+    }
+    __syncwarp();
+  }
+  if (lane == 0) sh.bnelim = k;
+  __syncwarp();
+}
+
+// Full symmetric swap of positions i, j inside a view of `rows` rows
+// (swap_symmetric, factor.rs:458-461), all threads of the CTA.
+__device__ void cta_swap(PanelView V, int64_t rows, int64_t i, int64_t j) {
+  if (i == j) return;
+  if (i > j) { int64_t t = i; i = j; j = t; }
+  __syncthreads();
+  int tid = threadIdx.x;
+  if (tid == 0) { double t = V(i, i); V(i, i) = V(j, j); V(j, j) = t; }
+  for (int64_t k = tid; k < i; k += NT) { double t = V(i, k); V(i, k) = V(j, k); V(j, k) = t; }
+  for (int64_t k = i + 1 + tid; k < j; k += NT) { double t = V(k, i); V(k, i) = V(j, k); V(j, k) = t; }
+  for (int64_t k = j + 1 + tid; k < rows; k += NT) { double t = V(k, i); V(k, i) = V(k, j); V(k, j) = t; }
+  __syncthreads();
+}
+
+// W = L * D for one row of the panel (compute_ld_into, factor.rs:1536-1563)
+__device__ __forceinline__ void row_ld(const double* l, int64_t lstride, const CtaShared& sh, int nelim, double* w) {
+  int c = 0;
+  while (c < nelim) {
+    if (sh.bdt[c] == PT_1X1) { w[c] = __dmul_rn(l[c * lstride], sh.bdd[c]); c += 1; }
+    else {
+      double A_ = sh.bdd[c], B_ = sh.bdo[c], C_ = sh.bdd[c + 1];
+      double l1 = l[c * lstride], l2 = l[(c + 1) * lstride];
+      w[c] = __dadd_rn(__dmul_rn(l1, A_), __dmul_rn(l2, B_));
+      w[c + 1] = __dadd_rn(__dmul_rn(l1, B_), __dmul_rn(l2, C_));
+      c += 2;
+    }
+  }
+}
+
+// factor_inner (factor.rs:1811-2095) on the view V (rows `bm`, `pl` FS
+// columns, NFS boundary `nfsb`), executed by the whole CTA.  D entries go to
+// VD (view-relative), the view-local column order to lp.  Returns the number
+// of eliminated columns.
+__device__ int cta_factor_inner(CtaShared& sh, PanelView V, int64_t bm, int pl, int64_t nfsb, DRec VD, int32_t* lp,
+                                double* bk, int64_t ldb, double* W, const DevOpts& o) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ib = o.ib;
+  for (int i = tid; i < pl; i += NT) lp[i] = i;
+  if (tid == 0) { sh.k = 0; sh.end_pos = pl; sh.n1 = 0; sh.n2 = 0; }
+  __syncthreads();
+  while (true) {
+    int k = sh.k, end_pos = sh.end_pos;
+    if (k >= end_pos) break;
+    int bs = min(end_pos - k, ib), be = k + bs;
+    int64_t rows = bm - k;
+    // 1. backup a[k..bm, k..k+bs]
+    for (int j = 0; j < bs; ++j)
+      for (int64_t i = tid; i < rows; i += NT) bk[i + j * ldb] = V(k + i, k + j);
+    // 2. load the diagonal block, factor it with one warp
+    for (int t = tid; t < bs * bs; t += NT) {
+      int i = t % bs, j = t / bs;
+      if (i >= j) sh.T[i][j] = V(k + i, k + j);
+    }
+    __syncthreads();
+    if (warp == 0) warp_block_factor(sh, bs, o.small, lane);
+    __syncthreads();
+    int bnelim = sh.bnelim;
+    if (bnelim == 0) {
+      for (int j = 0; j < bs; ++j)
+        for (int64_t i = tid; i < rows; i += NT) V(k + i, k + j) = bk[i + j * ldb];
+      __syncthreads();
+      for (int off = 0; off < bs; ++off) {
+        end_pos -= 1;
+        if (k + off < end_pos) {
+          cta_swap(V, bm, k + off, end_pos);
+          if (tid == 0) { int32_t t = lp[k + off]; lp[k + off] = lp[end_pos]; lp[end_pos] = t; }
+        }
+      }
+      __syncthreads();
+      if (tid == 0) sh.end_pos = end_pos;
+      __syncthreads();
+      continue;
+    }
+    // write the factored block back (lower triangle) and zero the D
+    // off-diagonals of 2x2 pivots (step 4) both there and in the L11 copy
+    for (int t = tid; t < bs * bs; t += NT) {
+      int i = t % bs, j = t / bs;
+      if (i >= j) V(k + i, k + j) = sh.T[i][j];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int bc = 0;
+      while (bc < bnelim) {
+        if (sh.bdt[bc] == PT_2X2) { V(k + bc + 1, k + bc) = 0.0; sh.T[bc + 1][bc] = 0.0; bc += 2; }
+        else bc += 1;
+      }
+      sh.eff = bnelim;
+    }
+    // 5. row permutation of view columns 0..k
+    for (int64_t c = tid; c < k; c += NT) {
+      double buf[IBMAX];
+      for (int i = 0; i < bs; ++i) buf[i] = V(k + sh.bperm[i], c);
+      for (int i = 0; i < bs; ++i) V(k + i, c) = buf[i];
+    }
+    // 6. column order
+    if (tid == 0) {
+      int32_t ob[IBMAX];
+      for (int i = 0; i < bs; ++i) ob[i] = lp[k + i];
+      for (int i = 0; i < bs; ++i) lp[k + i] = ob[sh.bperm[i]];
+    }
+    __syncthreads();
+    // 3 + 7. permute each panel row, TRSM with L11, D^-1 scaling and the
+    // threshold scan (apply_and_check, factor.rs:1295-1408)
+    const double bound = 1.0 / o.threshold;
+    for (int64_t r = be + tid; r < bm; r += NT) {
+      double x[IBMAX];
+      for (int i = 0; i < bs; ++i) x[i] = V(r, k + sh.bperm[i]);
+      for (int j = 0; j < bnelim; ++j)
+        for (int l = 0; l < j; ++l) x[j] = __fma_rn(-x[l], sh.T[j][l], x[j]);
+      int c = 0;
+      while (c < bnelim) {
+        if (sh.bdt[c] == PT_1X1) { x[c] = __dmul_rn(x[c], 1.0 / sh.bdd[c]); c += 1; }
+        else {
+          double A_ = sh.bdd[c], B_ = sh.bdo[c], C_ = sh.bdd[c + 1];
+          double inv_det = 1.0 / __dsub_rn(__dmul_rn(A_, C_), __dmul_rn(B_, B_));
+          double x1 = x[c], x2 = x[c + 1];
+          x[c] = __dmul_rn(__dsub_rn(__dmul_rn(x1, C_), __dmul_rn(x2, B_)), inv_det);
+          x[c + 1] = __dmul_rn(__dsub_rn(__dmul_rn(x2, A_), __dmul_rn(x1, B_)), inv_det);
+          c += 2;
+        }
+      }
+      for (int i = 0; i < bs; ++i) V(r, k + i) = x[i];
+      int fail = bnelim;
+      c = 0;
+      while (c < bnelim) {
+        int w = sh.bdt[c] == PT_2X2 ? 2 : 1;
+        bool bad = fabs(x[c]) >= bound || (w == 2 && fabs(x[c + 1]) >= bound);
+        if (bad) { fail = c; break; }
+        c += w;
+      }
+      if (fail < bnelim) atomicMin(&sh.eff, fail);
+    }
+    __syncthreads();
+    int eff = sh.eff;
+    // 8. adjust_for_2x2_boundary (factor.rs:1161-1174)
+    if (eff > 0 && sh.bdt[eff - 1] == PT_2X2) eff -= 1;
+    // 9. partial restore of the failed columns
+    if (eff < bnelim) {
+      for (int t = tid; t < bs * bs; t += NT) {
+        int i = t % bs, j = t / bs;
+        if (i < eff || j < eff) continue;
+        int c = sh.bperm[j], r = sh.bperm[i];
+        V(k + i, k + j) = (r >= c) ? bk[r + (int64_t)c * ldb] : bk[c + (int64_t)r * ldb];
+      }
+      for (int j = eff; j < bs; ++j) {
+        int c = sh.bperm[j];
+        for (int64_t i = bs + tid; i < rows; i += NT) V(k + i, k + j) = bk[i + (int64_t)c * ldb];
+      }
+    }
+    __syncthreads();
+    const int nelim = eff;
+    const int64_t ts = be, tsz = bm - be;
+    // 10. Schur updates (update_trailing factor.rs:1418-1526, update_cross_terms 1669-1766)
+    if (nelim > 0) {
+      for (int64_t i = tid; i < tsz; i += NT) row_ld(&V(ts + i, k), V.ld, sh, nelim, W + i * IBMAX);
+      __syncthreads();
+      for (int64_t j = ts; j < nfsb; ++j) {
+        if (tid < nelim) sh.Lj[tid] = V(j, k + tid);
+        __syncthreads();
+        for (int64_t i = j + tid; i < bm; i += NT) {
+          const double* w = W + (i - ts) * IBMAX;
+          double acc = V(i, j);
+          for (int c = 0; c < nelim; ++c) acc = __fma_rn(-w[c], sh.Lj[c], acc);
+          V(i, j) = acc;
+        }
+        __syncthreads();
+      }
+      if (nelim < bs) {
+        const int nf = bs - nelim;
+        // failed x failed, and trailing x failed; W_blk from the failed rows
+        for (int t = tid; t < nf * nf; t += NT) {
+          int i = t % nf, j = t / nf;
+          if (i < j) continue;
+          double wb[IBMAX];
+          row_ld(&V(k + nelim + i, k), V.ld, sh, nelim, wb);
+          double s = 0.0;
+          for (int c = 0; c < nelim; ++c) s = __dadd_rn(s, __dmul_rn(wb[c], V(k + nelim + j, k + c)));
+          V(k + nelim + i, k + nelim + j) = __dsub_rn(V(k + nelim + i, k + nelim + j), s);
+        }
+        for (int j = 0; j < nf; ++j) {
+          if (tid < nelim) sh.Lj[tid] = V(k + nelim + j, k + tid);
+          __syncthreads();
+          for (int64_t i = tid; i < tsz; i += NT) {
+            const double* w = W + i * IBMAX;
+            double s = 0.0;
+            for (int c = 0; c < nelim; ++c) s = __dadd_rn(s, __dmul_rn(w[c], sh.Lj[c]));
+            V(ts + i, k + nelim + j) = __dsub_rn(V(ts + i, k + nelim + j), s);
+          }
+          __syncthreads();
+        }
+      }
+    }
+    // 11. D entries and counts for the passed columns
+    if (tid == 0) {
+      int c = 0;
+      while (c < nelim) {
+        if (sh.bdt[c] == PT_1X1) {
+          VD.type[k + c] = PT_1X1; VD.diag[k + c] = sh.bdd[c]; VD.off[k + c] = 0.0; sh.n1++; c += 1;
+        } else if (c + 1 < nelim) {
+          VD.type[k + c] = PT_2X2; VD.type[k + c + 1] = PT_2X2B;
+          VD.diag[k + c] = sh.bdd[c]; VD.diag[k + c + 1] = sh.bdd[c + 1];
+          VD.off[k + c] = sh.bdo[c]; VD.off[k + c + 1] = 0.0; sh.n2++; c += 2;
+        } else c += 1;
+      }
+    }
+    __syncthreads();
+    // 12. delay the failed columns to end_pos
+    if (nelim < bs) {
+      int nd = bs - nelim;
+      for (int i = nd - 1; i >= 0; --i) {
+        int dp = k + nelim + i;
+        end_pos -= 1;
+        if (dp < end_pos) {
+          cta_swap(V, bm, dp, end_pos);
+          if (tid == 0) { int32_t t = lp[dp]; lp[dp] = lp[end_pos]; lp[end_pos] = t; }
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0) { sh.k = k + nelim; sh.end_pos = end_pos; }
+    __syncthreads();
+  }
+  return sh.k;
+}
+
+// One CTA per front: aptp_factor_in_place (factor.rs:301-404) for fronts with
+// k >= ib outside small-leaf subtrees: factor_inner (k <= nb) or
+// two_level_factor (k > nb), then the TPP fallback on the leftover columns.
+__global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* F, Arenas A, DevOpts o) {
+  if ((int)blockIdx.x >= n) return;
+  __shared__ CtaShared sh;
+  __shared__ int tpp_cnt[2];
+  const int tid = threadIdx.x;
+  const int s = ids[blockIdx.x];
+  const DFront fr = F[s];
+  const int64_t m = fr.m;
+  const int p = fr.k;
+  PanelView Av{A.panel + fr.panel, m};
+  int32_t* perm = A.idx + fr.idx + m;
+  DRec D{A.dtype + fr.dpos, A.ddiag + fr.dpos, A.doff + fr.dpos};
+  double* bk = A.scratch + fr.scratch;            // m x ib
+  double* W = bk + m * IBMAX;                     // m x IBMAX (row-major)
+  int32_t* lp = (int32_t*)(W + m * IBMAX);        // nb ints
+  int n1 = 0, n2 = 0;
+  int gne = 0;
+  if (p <= o.nb) {
+    gne = cta_factor_inner(sh, Av, m, p, p, D, lp, bk, m, W, o);
+    n1 = sh.n1; n2 = sh.n2;
+    for (int i = tid; i < p; i += NT) perm[i] = lp[i];
+    __syncthreads();
+  } else {
+    // two_level_factor (factor.rs:2108-2252)
+    int rem = p;
+    while (rem > 0) {
+      int cs = gne, bcols = min(rem, o.nb);
+      PanelView V{&Av(cs, cs), m};
+      DRec VD{D.type + cs, D.diag + cs, D.off + cs};
+      int bne = cta_factor_inner(sh, V, m - cs, bcols, (int64_t)p - cs, VD, lp, bk, m, W, o);
+      n1 += sh.n1; n2 += sh.n2;
+      // propagate the row permutation to columns 0..cs
+      if (cs > 0) {
+        // two-pass propagation through the backup buffer: gather, then write
+        for (int64_t c0 = 0; c0 < cs; c0 += IBMAX) {
+          int nc = (int)(cs - c0 < IBMAX ? cs - c0 : IBMAX);
+          for (int t = tid; t < nc * bcols; t += NT) {
+            int i = t % bcols, cc = t / bcols;
+            bk[i + (int64_t)cc * m] = Av(cs + lp[i], c0 + cc);
+          }
+          __syncthreads();
+          for (int t = tid; t < nc * bcols; t += NT) {
+            int i = t % bcols, cc = t / bcols;
+            Av(cs + i, c0 + cc) = bk[i + (int64_t)cc * m];
+          }
+          __syncthreads();
+        }
+      }
+      // column order of the outer block
+      if (tid == 0) {
+        for (int i = 0; i < bcols; ++i) ((int32_t*)W)[i] = perm[cs + i];
+        for (int i = 0; i < bcols; ++i) perm[cs + i] = ((int32_t*)W)[lp[i]];
+      }
+      __syncthreads();
+      // delayed columns to the end of the unprocessed region
+      if (bne < bcols) {
+        int nf = bcols - bne;
+        for (int i = 0; i < nf; ++i) {
+          int fp = cs + bne + i, e = cs + rem - 1 - i;
+          if (fp < e) {
+            cta_swap(Av, m, fp, e);
+            if (tid == 0) { int32_t t = perm[fp]; perm[fp] = perm[e]; perm[e] = t; }
+          }
+        }
+      }
+      __syncthreads();
+      gne += bne;
+      rem -= bcols;
+    }
+  }
+  // TPP fallback on columns gne..p (factor.rs:376-401)
+  if (gne < p && o.failed_pivot_tpp) {
+    if (tid < 32) {
+      if (tid == 0) { tpp_cnt[0] = 0; tpp_cnt[1] = 0; }
+      __syncwarp();
+      WarpTpp T{Av, m, p, tid};
+      int64_t add = T.run(gne, p, perm, D, &tpp_cnt[0], &tpp_cnt[1], o);
+      if (tid == 0) sh.tmpi[0] = (int)add;
+    }
+    __syncthreads();
+    gne += sh.tmpi[0];
+    n1 += tpp_cnt[0];
+    n2 += tpp_cnt[1];
+  }
+  if (tid == 0) { F[s].ne = gne; F[s].n1 = n1; F[s].n2 = n2; }
+}
+
+// ---------------------------------------------------------------------------
+// contribution GEMM: CB -= (L21_NFS D) L21_NFS^T, lower triangle
+// (compute_contribution_gemm, factor.rs:1590-1652)
+// ---------------------------------------------------------------------------
+struct TileItem { int32_t front; int32_t ti; int32_t tj; int32_t pad; };
+
+// W = L21_NFS * D into scratch (nfs x ne, column-major)
+__global__ void k_cb_w(const TileItem* items, const DFront* F, Arenas A) {
+  TileItem it = items[blockIdx.x];
+  const DFront fr = F[it.front];
+  const double* L = A.panel + fr.panel;
+  double* W = A.scratch + fr.scratch;
+  const int8_t* dt = A.dtype + fr.dpos;
+  const double* dd = A.ddiag + fr.dpos;
+  const double* dof = A.doff + fr.dpos;
+  int64_t i = (int64_t)it.ti * 256 + threadIdx.x;
+  if (i >= fr.nfs) return;
+  const double* l = L + fr.k + i;
+  int c = 0;
+  while (c < fr.ne) {
+    if (dt[c] == PT_1X1) { W[i + (int64_t)c * fr.nfs] = __dmul_rn(l[(int64_t)c * fr.m], dd[c]); c += 1; }
+    else {
+      double l1 = l[(int64_t)c * fr.m], l2 = l[(int64_t)(c + 1) * fr.m];
+      W[i + (int64_t)c * fr.nfs] = __dadd_rn(__dmul_rn(l1, dd[c]), __dmul_rn(l2, dof[c]));
+      W[i + (int64_t)(c + 1) * fr.nfs] = __dadd_rn(__dmul_rn(l1, dof[c]), __dmul_rn(l2, dd[c + 1]));
+      c += 2;
+    }
+  }
+}
+
+constexpr int GT = 64;  // output tile
+constexpr int GK = 16;  // reduction chunk
+
+// C[i,j] = fma(-W[i,c], L[j,c], C[i,j]) for c ascending (each output entry an
+// fma chain in the oracle's order); 256 threads, 4x4 outputs per thread.
+__global__ void __launch_bounds__(256) k_cb_gemm(const TileItem* items, const DFront* F, Arenas A) {
+  TileItem it = items[blockIdx.x];
+  const DFront fr = F[it.front];
+  const int64_t nfs = fr.nfs, ne = fr.ne, ldl = fr.m;
+  const double* L = A.panel + fr.panel + fr.k;  // L21_NFS(j, c) = L[j + c*ldl]
+  const double* W = A.scratch + fr.scratch;     // W(i, c) = W[i + c*nfs]
+  double* C = fr.cb;
+  __shared__ double sW[GK][GT + 1];
+  __shared__ double sL[GK][GT + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int64_t i0 = (int64_t)it.ti * GT, j0 = (int64_t)it.tj * GT;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      acc[a][b] = (i < nfs && j < nfs && i >= j) ? C[i + j * nfs] : 0.0;
+    }
+  for (int64_t c0 = 0; c0 < ne; c0 += GK) {
+    for (int t = threadIdx.x; t < GK * GT; t += 256) {
+      int r = t % GT, c = t / GT;
+      int64_t cc = c0 + c;
+      sW[c][r] = (i0 + r < nfs && cc < ne) ? W[i0 + r + cc * nfs] : 0.0;
+      sL[c][r] = (j0 + r < nfs && cc < ne) ? L[j0 + r + cc * ldl] : 0.0;
+    }
+    __syncthreads();
+    int kc = (int)(ne - c0 < GK ? ne - c0 : GK);
+    for (int c = 0; c < kc; ++c) {
+      double wv[4], lv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) wv[a] = sW[c][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) lv[b] = sL[c][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = __fma_rn(-wv[a], lv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      if (i < nfs && j < nfs && i >= j) C[i + j * nfs] = acc[a][b];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// solve kernels (aptp_solve, solve.rs:57-326; SparseLDLT::solve_in_place,
+// solver.rs:396-425)
+// ---------------------------------------------------------------------------
+__global__ void k_perm_scale_in(const double* rhs, int64_t ldb, int64_t nrhs, double* x, int64_t n,
+                                const int64_t* pfwd, const double* scal) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nrhs) return;
+  int64_t i = t % n, r = t / n;
+  double v = rhs[pfwd[i] + r * ldb];
+  if (scal) v = __dmul_rn(v, scal[i]);
+  x[i + r * n] = v;
+}
+__global__ void k_perm_scale_out(double* rhs, int64_t ldb, int64_t nrhs, const double* x, int64_t n,
+                                 const int64_t* pfwd, const double* scal) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n * nrhs) return;
+  int64_t i = t % n, r = t / n;
+  double v = x[i + r * n];
+  if (scal) v = __dmul_rn(v, scal[i]);
+  rhs[pfwd[i] + r * ldb] = v;
+}
+
+__device__ __forceinline__ int32_t front_col(const int32_t* rows, const int32_t* perm, int i) { return rows[perm[i]]; }
+__device__ __forceinline__ int32_t front_row(const int32_t* rows, const int32_t* perm, int ne, int k, int t) {
+  int q = ne + t;
+  return q < k ? rows[perm[q]] : rows[q];
+}
+
+// Forward substitution and the diagonal solve of one front per CTA:
+// y = L11^{-1} x[col]; x[row] -= L21 y (atomically: sibling fronts of a wave
+// may share rows); x[col] = D^{-1} y.
+__global__ void k_solve_fwd(const int32_t* ids, int n, const DFront* F, Arenas A, double* x, int64_t nvec,
+                            int64_t nrhs, double* work) {
+  int f = blockIdx.x;
+  if (f >= n) return;
+  int s = ids[f];
+  const DFront fr = F[s];
+  const int ne = fr.ne;
+  if (ne == 0) return;
+  const int64_t m = fr.m, r = m - ne;
+  const double* L = A.panel + fr.panel;
+  const int32_t* rows = A.idx + fr.idx;
+  const int32_t* perm = rows + m;
+  const int8_t* dt = A.dtype + fr.dpos;
+  const double* dd = A.ddiag + fr.dpos;
+  const double* dof = A.doff + fr.dpos;
+  double* w = work + fr.scratch;  // ne
+  for (int64_t rh = 0; rh < nrhs; ++rh) {
+    double* xv = x + rh * nvec;
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) w[i] = xv[front_col(rows, perm, i)];
+    __syncthreads();
+    for (int j = 0; j < ne; ++j) {
+      double xj = w[j];
+      for (int i = j + 1 + threadIdx.x; i < ne; i += blockDim.x) w[i] = __fma_rn(-L[i + (int64_t)j * m], xj, w[i]);
+      __syncthreads();
+    }
+    for (int64_t t = threadIdx.x; t < r; t += blockDim.x) {
+      double acc = 0.0;
+      for (int j = 0; j < ne; ++j) acc = __fma_rn(L[ne + t + (int64_t)j * m], w[j], acc);
+      atomicAdd(&xv[front_row(rows, perm, ne, fr.k, (int)t)], -acc);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < ne; c += blockDim.x) {
+      int32_t g = front_col(rows, perm, c);
+      if (dt[c] == PT_1X1) {
+        double d = dd[c];
+        xv[g] = d == 0.0 ? 0.0 : w[c] / d;
+      } else {
+        int c0 = dt[c] == PT_2X2 ? c : c - 1;  // first column of the pair
+        double a = dd[c0], b = dof[c0], cc = dd[c0 + 1];
+        double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(b, b));
+        double r1 = w[c0], r2 = w[c0 + 1];
+        if (det == 0.0) xv[g] = 0.0;
+        else xv[g] = (c == c0) ? __ddiv_rn(__dsub_rn(__dmul_rn(cc, r1), __dmul_rn(b, r2)), det)
+                               : __ddiv_rn(__dsub_rn(__dmul_rn(a, r2), __dmul_rn(b, r1)), det);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Backward substitution of one front per CTA: z = x[col] - L21^T x[row];
+// x[col] = L11^{-T} z.
+__global__ void k_solve_bwd(const int32_t* ids, int n, const DFront* F, Arenas A, double* x, int64_t nvec,
+                            int64_t nrhs, double* work) {
+  int f = blockIdx.x;
+  if (f >= n) return;
+  int s = ids[f];
+  const DFront fr = F[s];
+  const int ne = fr.ne;
+  if (ne == 0) return;
+  const int64_t m = fr.m, r = m - ne;
+  const double* L = A.panel + fr.panel;
+  const int32_t* rows = A.idx + fr.idx;
+  const int32_t* perm = rows + m;
+  double* w = work + fr.scratch;       // ne
+  double* xr = w + ne;                 // r
+  __shared__ double red[8];
+  for (int64_t rh = 0; rh < nrhs; ++rh) {
+    double* xv = x + rh * nvec;
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) w[i] = xv[front_col(rows, perm, i)];
+    for (int64_t t = threadIdx.x; t < r; t += blockDim.x) xr[t] = xv[front_row(rows, perm, ne, fr.k, (int)t)];
+    __syncthreads();
+    for (int j = 0; j < ne; ++j) {
+      double part = 0.0;
+      for (int64_t t = threadIdx.x; t < r; t += blockDim.x) part = __fma_rn(L[ne + t + (int64_t)j * m], xr[t], part);
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s2 = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s2 += red[q];
+        w[j] -= s2;
+      }
+      __syncthreads();
+    }
+    for (int j = ne - 1; j >= 0; --j) {
+      double part = 0.0;
+      for (int i = j + 1 + threadIdx.x; i < ne; i += blockDim.x) part = __fma_rn(L[i + (int64_t)j * m], w[i], part);
+      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double s2 = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s2 += red[q];
+        w[j] -= s2;
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < ne; i += blockDim.x) xv[front_col(rows, perm, i)] = w[i];
+    __syncthreads();
+  }
+}
+
+}  // namespace rvg
+
+// ===========================================================================
+// host driver
+// ===========================================================================
+namespace rvg {
+
+// publish a wave's descriptors / pick up the children's delay offsets
+__global__ void k_put_fronts(const DFront* staged, const int32_t* ids, int n, DFront* F) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) F[ids[i]] = staged[i];
+}
+__global__ void k_put_dly(const int32_t* ids, const int32_t* vals, int n, DFront* F) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) F[ids[i]].dly_off = vals[i];
+}
+__global__ void k_get_counts(const int32_t* ids, int n, const DFront* F, int32_t* out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) { const DFront& f = F[ids[i]]; out[3 * i] = f.ne; out[3 * i + 1] = f.n1; out[3 * i + 2] = f.n2; }
+}
+
+}  // namespace rvg
+
+using namespace rvg;
+
+struct rvg_handle {
+  Plan P;
+  rvg_options opt;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[8] = {};
+  int64_t nnz = 0;
+  // static device data
+  int64_t *d_own_ptr = nullptr, *d_pat_ptr = nullptr, *d_amap_ptr = nullptr, *d_ea_ptr = nullptr, *d_ch_ptr = nullptr;
+  int32_t *d_own_idx = nullptr, *d_pat_idx = nullptr, *d_amap = nullptr, *d_ea_map = nullptr, *d_ch_idx = nullptr;
+  int64_t* d_pfwd = nullptr;
+  // per-factor device data
+  DFront* d_fronts = nullptr;
+  std::vector<DFront> h_fronts;
+  double* panel = nullptr; size_t panel_cap = 0;
+  int32_t* idx = nullptr; size_t idx_cap = 0;
+  int8_t* dtype = nullptr; double* ddiag = nullptr; double* doff = nullptr; size_t d_cap = 0;
+  double* d_vals = nullptr; double* d_scal = nullptr; bool has_scaling = false;
+  double* d_x = nullptr; size_t x_cap = 0;
+  double* solve_work = nullptr; size_t solve_work_cap = 0;
+  char* d_stage = nullptr; size_t stage_cap = 0;   // per-wave packed launch data
+  char* h_stage = nullptr; size_t h_stage_cap = 0; // pinned host mirror
+  int32_t* h_counts = nullptr; size_t h_counts_cap = 0;
+  bool factored = false;
+  // results
+  int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
+  double t_assembly = 0, t_kernel = 0, t_gemm = 0, t_factor = 0, t_solve = 0, t_dom = 0, n_dom = 0;
+};
+
+namespace {
+
+template <class T>
+int ensure(T*& p, size_t& cap, size_t need, cudaStream_t st) {
+  if (need <= cap && p) return RVG_OK;
+  size_t nc = std::max(need, cap + cap / 2);
+  if (nc == 0) nc = 1;
+  T* np = nullptr;
+  CK(cudaMallocAsync((void**)&np, nc * sizeof(T), st));
+  if (p) {
+    if (cap) CK(cudaMemcpyAsync(np, p, cap * sizeof(T), cudaMemcpyDeviceToDevice, st));
+    CK(cudaFreeAsync(p, st));
+  }
+  p = np;
+  cap = nc;
+  return RVG_OK;
+}
+
+int ensure_host(char*& p, size_t& cap, size_t need) {
+  if (need <= cap && p) return RVG_OK;
+  size_t nc = std::max(need, cap + cap / 2);
+  if (p) CK(cudaFreeHost(p));
+  p = nullptr;
+  CK(cudaMallocHost((void**)&p, nc));
+  cap = nc;
+  return RVG_OK;
+}
+
+int ensure_d_arrays(rvg_handle* h, size_t need) {  // type / diag / off share one capacity
+  if (need <= h->d_cap && h->dtype) return RVG_OK;
+  size_t nc = std::max(need, h->d_cap + h->d_cap / 2);
+  int8_t* t; double *a, *b;
+  CK(cudaMallocAsync((void**)&t, nc, h->st));
+  CK(cudaMallocAsync((void**)&a, nc * 8, h->st));
+  CK(cudaMallocAsync((void**)&b, nc * 8, h->st));
+  if (h->dtype) {
+    CK(cudaMemcpyAsync(t, h->dtype, h->d_cap, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(a, h->ddiag, h->d_cap * 8, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaMemcpyAsync(b, h->doff, h->d_cap * 8, cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaFreeAsync(h->dtype, h->st)); CK(cudaFreeAsync(h->ddiag, h->st)); CK(cudaFreeAsync(h->doff, h->st));
+  }
+  h->dtype = t; h->ddiag = a; h->doff = b; h->d_cap = nc;
+  return RVG_OK;
+}
+
+template <class T>
+int upload(T*& d, const std::vector<T>& h, cudaStream_t st) {
+  size_t n = std::max<size_t>(h.size(), 1);
+  CK(cudaMallocAsync((void**)&d, n * sizeof(T), st));
+  if (!h.empty()) CK(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  return RVG_OK;
+}
+
+// Packs the typed arrays of one wave into one buffer (16-byte aligned
+// sections) so the whole wave is a single host->device copy.
+struct Packer {
+  std::vector<char> buf;
+  template <class T>
+  size_t add(const std::vector<T>& v) {
+    size_t off = (buf.size() + 15) & ~size_t(15);
+    buf.resize(off + v.size() * sizeof(T));
+    if (!v.empty()) std::memcpy(buf.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+  }
+};
+
+Statics statics(rvg_handle* h) {
+  return Statics{h->d_own_ptr, h->d_own_idx, h->d_pat_ptr, h->d_pat_idx, h->d_amap_ptr,
+                 h->d_amap, h->d_ea_ptr, h->d_ea_map, h->d_ch_ptr, h->d_ch_idx};
+}
+
+DevOpts devopts(const rvg_options& o) {
+  return DevOpts{o.threshold, o.small, (int)o.outer_block_size, (int)o.inner_block_size, o.failed_pivot_tpp};
+}
+
+unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// The numeric factorization proper: the level-set schedule of
+// factor_tree_levelset (numeric.rs:1957-2163) with every front of a wave
+// processed by the same launches.
+int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
+  Plan& P = h->P;
+  cudaStream_t st = h->st;
+  const int64_t ns = (int64_t)P.sn.size();
+  h->factored = false;
+  h->h_fronts.assign(ns, DFront());
+  int64_t panel_used = 0, idx_used = 0, d_used = 0;
+  std::vector<double*> cb_block(P.waves.size(), nullptr);
+  std::vector<int64_t> cb_release(P.waves.size(), -1);
+  const DevOpts dop = devopts(h->opt);
+  const int ib = (int)h->opt.inner_block_size;
+  double t_asm = 0, t_ker = 0, t_gem = 0;
+  int rc;
+  CK(cudaEventRecord(h->ev[0], st));
+  for (size_t w = 0; w < P.waves.size(); ++w) {
+    const std::vector<int64_t>& wave = P.waves[w];
+    const int nw = (int)wave.size();
+    // ---- sizes from the children's eliminated counts (numeric.rs:1239-1262)
+    int64_t panel_need = 0, idx_need = 0, d_need = 0, cb_need = 0, scratch_need = 0;
+    std::vector<int32_t> dly_ids, dly_vals;
+    for (int64_t s : wave) {
+      DFront& f = h->h_fronts[s];
+      int64_t nown = P.sn[s].n_owned(), ndin = 0;
+      for (int64_t c : P.children[s]) {
+        DFront& cf = h->h_fronts[c];
+        cf.dly_off = (int32_t)ndin;
+        dly_ids.push_back((int32_t)c);
+        dly_vals.push_back((int32_t)ndin);
+        ndin += cf.k - cf.ne;
+      }
+      int64_t k = nown + ndin, nfs = (int64_t)P.sn[s].pattern.size(), m = k + nfs;
+      f.m = (int32_t)m; f.k = (int32_t)k; f.nown = (int32_t)nown; f.ndin = (int32_t)ndin; f.nfs = (int32_t)nfs;
+      f.ne = 0; f.n1 = 0; f.n2 = 0;
+      f.parent = (int32_t)P.sn[s].parent;
+      f.flags = (P.sn[s].in_small_leaf ? FF_SMALL_LEAF : 0) | (f.parent >= 0 ? FF_HAS_PARENT : 0) |
+                ((f.parent >= 0 && nfs > 0) ? FF_HAS_CB : 0);
+      f.panel = panel_used + panel_need; panel_need += m * k;
+      f.idx = idx_used + idx_need; idx_need += m + k;
+      f.dpos = d_used + d_need; d_need += k;
+      if (f.flags & FF_HAS_CB) cb_need += nfs * nfs;
+      const bool tpp = (f.flags & FF_SMALL_LEAF) || k < ib;
+      int64_t sc = tpp ? 0 : (2 * IBMAX * m + h->opt.outer_block_size);
+      if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
+      f.scratch = scratch_need; scratch_need += sc;
+    }
+    if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st))) return rc;
+    if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx_used + idx_need), st))) return rc;
+    if ((rc = ensure_d_arrays(h, (size_t)(d_used + d_need)))) return rc;
+    double* scratch = nullptr;
+    CK(cudaMallocAsync((void**)&scratch, (size_t)std::max<int64_t>(scratch_need, 1) * 8, st));
+    if (cb_need) {
+      CK(cudaMallocAsync((void**)&cb_block[w], (size_t)cb_need * 8, st));
+      CK(cudaMemsetAsync(cb_block[w], 0, (size_t)cb_need * 8, st));
+    }
+    {
+      int64_t off = 0;
+      for (int64_t s : wave) {
+        DFront& f = h->h_fronts[s];
+        if (f.flags & FF_HAS_CB) { f.cb = cb_block[w] + off; off += (int64_t)f.nfs * f.nfs; }
+        else f.cb = nullptr;
+      }
+    }
+    if (panel_need) CK(cudaMemsetAsync(h->panel + panel_used, 0, (size_t)panel_need * 8, st));
+    const Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, scratch};
+    // ---- launch data of the whole wave, packed into one upload
+    std::vector<int32_t> ids(wave.begin(), wave.end()), tpp_ids, aptp_ids;
+    std::vector<DFront> staged;
+    staged.reserve(nw);
+    for (int64_t s : wave) {
+      staged.push_back(h->h_fronts[s]);
+      const DFront& f = h->h_fronts[s];
+      if ((f.flags & FF_SMALL_LEAF) || f.k < ib) tpp_ids.push_back((int32_t)s); else aptp_ids.push_back((int32_t)s);
+    }
+    std::vector<ScatterItem> sitems;
+    for (int64_t s : wave)
+      for (int64_t e = P.amap_ptr[s]; e < P.amap_ptr[s + 1]; e += 256) sitems.push_back(ScatterItem{(int32_t)s, 0, e});
+    size_t maxch = 0;
+    for (int64_t s : wave) maxch = std::max(maxch, P.children[s].size());
+    std::vector<std::vector<EaItem>> eitems(maxch);
+    for (size_t q = 0; q < maxch; ++q)
+      for (int64_t s : wave) {
+        if (q >= P.children[s].size()) continue;
+        int64_t c = P.children[s][q];
+        const DFront& cf = h->h_fronts[c];
+        if (!(cf.flags & FF_HAS_PARENT) || cf.ne >= cf.m) continue;
+        int sz = cf.m - cf.ne;
+        for (int j0 = 0; j0 < sz; j0 += 32) eitems[q].push_back(EaItem{(int32_t)s, (int32_t)c, j0, 0});
+      }
+    std::vector<TileItem> witems, gitems;
+    for (int64_t s : wave) {
+      const DFront& f = h->h_fronts[s];
+      if (!(f.flags & FF_HAS_CB) || f.k == 0) continue;
+      for (int ti = 0; ti * 256 < f.nfs; ++ti) witems.push_back(TileItem{(int32_t)s, ti, 0, 0});
+      int nt = (f.nfs + GT - 1) / GT;
+      for (int tj = 0; tj < nt; ++tj)
+        for (int ti = tj; ti < nt; ++ti) gitems.push_back(TileItem{(int32_t)s, ti, tj, 0});
+    }
+    Packer pk;
+    size_t o_staged = pk.add(staged), o_ids = pk.add(ids), o_dly_ids = pk.add(dly_ids), o_dly_vals = pk.add(dly_vals);
+    size_t o_tpp = pk.add(tpp_ids), o_aptp = pk.add(aptp_ids), o_s = pk.add(sitems);
+    std::vector<size_t> o_e(maxch);
+    for (size_t q = 0; q < maxch; ++q) o_e[q] = pk.add(eitems[q]);
+    size_t o_w = pk.add(witems), o_g = pk.add(gitems);
+    size_t o_cnt = pk.add(std::vector<int32_t>(3 * (size_t)nw + 4, 0));
+    if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size(), st))) return rc;
+    if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size()))) return rc;
+    std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
+    CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
+    char* D = h->d_stage;
+    const int32_t* d_ids = (const int32_t*)(D + o_ids);
+    // ---- descriptors
+    k_put_fronts<<<blocks_for(nw, 128), 128, 0, st>>>((const DFront*)(D + o_staged), d_ids, nw, h->d_fronts);
+    if (!dly_ids.empty())
+      k_put_dly<<<blocks_for(dly_ids.size(), 128), 128, 0, st>>>((const int32_t*)(D + o_dly_ids),
+                                                                 (const int32_t*)(D + o_dly_vals), (int)dly_ids.size(),
+                                                                 h->d_fronts);
+    CK(cudaEventRecord(h->ev[1], st));
+    // ---- assembly
+    k_front_rows<<<nw, 128, 0, st>>>(d_ids, nw, h->d_fronts, statics(h), A);
+    if (!sitems.empty())
+      k_scatter<<<(unsigned)sitems.size(), 256, 0, st>>>((const ScatterItem*)(D + o_s), h->d_fronts, statics(h), A,
+                                                         d_vals, d_scal);
+    for (size_t q = 0; q < maxch; ++q)
+      if (!eitems[q].empty())
+        k_extend_add<<<(unsigned)eitems[q].size(), 256, 0, st>>>((const EaItem*)(D + o_e[q]), h->d_fronts,
+                                                                  statics(h), A);
+    CK(cudaEventRecord(h->ev[2], st));
+    // contribution blocks whose parents are now all assembled
+    for (size_t w2 = 0; w2 < w; ++w2)
+      if (cb_block[w2] && cb_release[w2] == (int64_t)w) { CK(cudaFreeAsync(cb_block[w2], st)); cb_block[w2] = nullptr; }
+    // ---- dense factorization
+    if (!tpp_ids.empty())
+      k_tpp<<<blocks_for(tpp_ids.size(), 8), 256, 0, st>>>((const int32_t*)(D + o_tpp), (int)tpp_ids.size(),
+                                                            h->d_fronts, A, dop);
+    if (!aptp_ids.empty())
+      k_aptp<<<(unsigned)aptp_ids.size(), NT, 0, st>>>((const int32_t*)(D + o_aptp), (int)aptp_ids.size(),
+                                                        h->d_fronts, A, dop);
+    CK(cudaEventRecord(h->ev[3], st));
+    // ---- contribution GEMM (fronts with nothing eliminated skip inside)
+    if (!gitems.empty()) {
+      k_cb_w<<<(unsigned)witems.size(), 256, 0, st>>>((const TileItem*)(D + o_w), h->d_fronts, A);
+      k_cb_gemm<<<(unsigned)gitems.size(), 256, 0, st>>>((const TileItem*)(D + o_g), h->d_fronts, A);
+    }
+    CK(cudaEventRecord(h->ev[4], st));
+    CK(cudaGetLastError());
+    // ---- eliminated counts back to the host
+    k_get_counts<<<blocks_for(nw, 128), 128, 0, st>>>(d_ids, nw, h->d_fronts, (int32_t*)(D + o_cnt));
+    if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4) * 4))) return rc;
+    CK(cudaMemcpyAsync(h->h_counts, D + o_cnt, (size_t)3 * nw * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaFreeAsync(scratch, st));
+    CK(cudaStreamSynchronize(st));
+    for (int i = 0; i < nw; ++i) {
+      DFront& f = h->h_fronts[wave[i]];
+      f.ne = h->h_counts[3 * i]; f.n1 = h->h_counts[3 * i + 1]; f.n2 = h->h_counts[3 * i + 2];
+    }
+    int64_t last = -1;
+    for (int64_t s : wave) if (P.sn[s].parent >= 0) last = std::max(last, P.height[P.sn[s].parent]);
+    cb_release[w] = last;
+    float a1 = 0, a2 = 0, a3 = 0;
+    cudaEventElapsedTime(&a1, h->ev[1], h->ev[2]);
+    cudaEventElapsedTime(&a2, h->ev[2], h->ev[3]);
+    cudaEventElapsedTime(&a3, h->ev[3], h->ev[4]);
+    t_asm += a1; t_ker += a2; t_gem += a3;
+    panel_used += panel_need; idx_used += idx_need; d_used += d_need;
+  }
+  for (size_t w = 0; w < cb_block.size(); ++w)
+    if (cb_block[w]) { CK(cudaFreeAsync(cb_block[w], st)); cb_block[w] = nullptr; }
+  CK(cudaEventRecord(h->ev[5], st));
+  CK(cudaStreamSynchronize(st));
+  float tot = 0;
+  cudaEventElapsedTime(&tot, h->ev[0], h->ev[5]);
+  h->t_assembly = t_asm; h->t_kernel = t_ker; h->t_gemm = t_gem; h->t_factor = tot;
+  // aggregate stats (numeric.rs:929-1009)
+  h->tot1 = h->tot2 = h->totdel = h->zero_piv = h->max_front = 0;
+  std::vector<int8_t> dt(d_used);
+  std::vector<double> dd(d_used);
+  if (d_used) {
+    CK(cudaMemcpy(dt.data(), h->dtype, d_used, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dd.data(), h->ddiag, d_used * 8, cudaMemcpyDeviceToHost));
+  }
+  for (int64_t s = 0; s < ns; ++s) {
+    const DFront& f = h->h_fronts[s];
+    h->tot1 += f.n1; h->tot2 += f.n2; h->totdel += f.k - f.ne;
+    h->max_front = std::max<int64_t>(h->max_front, f.m);
+    for (int c = 0; c < f.ne; ++c)
+      if (dt[f.dpos + c] == PT_1X1 && dd[f.dpos + c] == 0.0) h->zero_piv++;
+    if (f.parent < 0 && f.ne < f.m) h->zero_piv += f.k - f.ne;
+  }
+  h->factored = true;
+  return RVG_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI (numeric part)
+// ===========================================================================
+extern "C" {
+
+const char* rvg_last_error(void) { return g_err.c_str(); }
+
+void rvg_default_options(rvg_options* o) {
+  o->threshold = 0.01;
+  o->small = 1e-20;
+  o->outer_block_size = 256;
+  o->inner_block_size = 32;
+  o->nemin = 32;
+  o->small_leaf_threshold = 256;
+  o->failed_pivot_tpp = 1;
+  o->fallback_bk = 1;
+}
+
+static int check_opts(const rvg_options& o) {  // factor.rs:307-347
+  if (!(o.threshold > 0.0 && o.threshold <= 1.0)) { set_error("threshold must be in (0, 1]"); return RVG_ERR_INVALID_INPUT; }
+  if (!(o.small >= 0.0)) { set_error("small must be >= 0.0"); return RVG_ERR_INVALID_INPUT; }
+  if (o.outer_block_size <= 0) { set_error("outer_block_size must be > 0"); return RVG_ERR_INVALID_INPUT; }
+  if (o.inner_block_size <= 0) { set_error("inner_block_size must be > 0"); return RVG_ERR_INVALID_INPUT; }
+  if (o.inner_block_size > o.outer_block_size) {
+    set_error("inner_block_size must be <= outer_block_size");
+    return RVG_ERR_INVALID_INPUT;
+  }
+  if (o.inner_block_size > IBMAX) { set_error("inner_block_size above 32 is not supported by the B200 kernels"); return RVG_ERR_INVALID_INPUT; }
+  if (o.nemin < 1) { set_error("nemin must be >= 1"); return RVG_ERR_INVALID_INPUT; }
+  return RVG_OK;
+}
+
+rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end, const int64_t* pat_ptr,
+                      const int64_t* pat_idx, const int64_t* sup_parent, const int64_t* perm_fwd, const int64_t* colptr,
+                      const int64_t* rowidx, const rvg_options* opt, rvg_handle** out) {
+  if (!out) { set_error("null output handle"); return RVG_ERR_INVALID_INPUT; }
+  *out = nullptr;
+  rvg_options o;
+  rvg_default_options(&o);
+  if (opt) o = *opt;
+  int rc = check_opts(o);
+  if (rc) return (rvg_status)rc;
+  if (n < 0 || nsup < 0) { set_error("negative size"); return RVG_ERR_INVALID_INPUT; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device available (the numeric phase has no CPU fallback)");
+    return RVG_ERR_DEVICE;
+  }
+  std::unique_ptr<rvg_handle> h(new rvg_handle());
+  h->opt = o;
+  h->nnz = n ? colptr[n] : 0;
+  std::string err;
+  rc = build_plan(nullptr, n, nsup, sup_begin, sup_end, pat_ptr, pat_idx, sup_parent, perm_fwd, colptr, rowidx, o, h->P, &err);
+  if (rc) { set_error(err); return (rvg_status)rc; }
+  CK(cudaGetDevice(&h->device));
+  CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  for (auto& e : h->ev) CK(cudaEventCreate(&e));
+  {
+    cudaMemPool_t pool;
+    CK(cudaDeviceGetDefaultMemPool(&pool, h->device));
+    uint64_t thr = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  }
+  Plan& P = h->P;
+  const int64_t ns = (int64_t)P.sn.size();
+  std::vector<int64_t> chp(ns + 1, 0);
+  std::vector<int32_t> chi;
+  for (int64_t s = 0; s < ns; ++s) {
+    chp[s + 1] = chp[s] + (int64_t)P.children[s].size();
+    for (int64_t c : P.children[s]) chi.push_back((int32_t)c);
+  }
+  cudaStream_t st = h->st;
+  if ((rc = upload(h->d_own_ptr, P.own_ptr, st)) || (rc = upload(h->d_own_idx, P.own_idx, st)) ||
+      (rc = upload(h->d_pat_ptr, P.pat_ptr, st)) || (rc = upload(h->d_pat_idx, P.pat_idx, st)) ||
+      (rc = upload(h->d_amap_ptr, P.amap_ptr, st)) || (rc = upload(h->d_amap, P.amap, st)) ||
+      (rc = upload(h->d_ea_ptr, P.ea_ptr, st)) || (rc = upload(h->d_ea_map, P.ea_map, st)) ||
+      (rc = upload(h->d_ch_ptr, chp, st)) || (rc = upload(h->d_ch_idx, chi, st)) ||
+      (rc = upload(h->d_pfwd, P.perm_fwd, st)))
+    return (rvg_status)rc;
+  CK(cudaMallocAsync((void**)&h->d_fronts, std::max<int64_t>(ns, 1) * sizeof(DFront), st));
+  CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
+  CK(cudaMallocAsync((void**)&h->d_scal, std::max<int64_t>(n, 1) * 8, st));
+  CK(cudaStreamSynchronize(st));
+  *out = h.release();
+  return RVG_OK;
+}
+
+static int factor_common(rvg_handle* h, const double* dv, const double* ds) { return run_factor(h, dv, ds); }
+
+rvg_status rvg_factor(rvg_handle* h, const double* values, const double* scaling) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (h->P.n > 0 && !values) { set_error("null values"); return RVG_ERR_INVALID_INPUT; }
+  CK(cudaSetDevice(h->device));
+  if (h->nnz) CK(cudaMemcpyAsync(h->d_vals, values, h->nnz * 8, cudaMemcpyHostToDevice, h->st));
+  h->has_scaling = scaling != nullptr;
+  if (scaling && h->P.n) CK(cudaMemcpyAsync(h->d_scal, scaling, h->P.n * 8, cudaMemcpyHostToDevice, h->st));
+  return (rvg_status)factor_common(h, h->d_vals, h->has_scaling ? h->d_scal : nullptr);
+}
+
+rvg_status rvg_factor_device(rvg_handle* h, const double* d_values, const double* d_scaling) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  CK(cudaSetDevice(h->device));
+  h->has_scaling = d_scaling != nullptr;
+  if (d_scaling && h->P.n) CK(cudaMemcpyAsync(h->d_scal, d_scaling, h->P.n * 8, cudaMemcpyDeviceToDevice, h->st));
+  return (rvg_status)factor_common(h, d_values, h->has_scaling ? h->d_scal : nullptr);
+}
+
+static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb) {
+  Plan& P = h->P;
+  const int64_t n = P.n;
+  cudaStream_t st = h->st;
+  if (n == 0 || nrhs == 0) return RVG_OK;
+  int rc = ensure(h->d_x, h->x_cap, (size_t)(n * nrhs), st);
+  if (rc) return rc;
+  // per-front solve workspace: m doubles each
+  int64_t wneed = 0;
+  std::vector<DFront> fr = h->h_fronts;
+  for (auto& f : fr) { f.scratch = wneed; wneed += f.m; }
+  if ((rc = ensure(h->solve_work, h->solve_work_cap, (size_t)std::max<int64_t>(wneed, 1), st))) return rc;
+  CK(cudaMemcpyAsync(h->d_fronts, fr.data(), fr.size() * sizeof(DFront), cudaMemcpyHostToDevice, st));
+  Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, nullptr};
+  CK(cudaEventRecord(h->ev[6], st));
+  int64_t tot = n * nrhs;
+  k_perm_scale_in<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
+                                                                 h->has_scaling ? h->d_scal : nullptr);
+  // wave lists, packed once per solve
+  Packer pk;
+  std::vector<size_t> off(P.waves.size());
+  for (size_t w = 0; w < P.waves.size(); ++w) {
+    std::vector<int32_t> ids(P.waves[w].begin(), P.waves[w].end());
+    off[w] = pk.add(ids);
+  }
+  if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size() + 16, st))) return rc;
+  if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size() + 16))) return rc;
+  std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
+  CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
+  for (size_t w = 0; w < P.waves.size(); ++w)
+    k_solve_fwd<<<(unsigned)P.waves[w].size(), 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]),
+                                                             (int)P.waves[w].size(), h->d_fronts, A, h->d_x, n, nrhs,
+                                                             h->solve_work);
+  for (size_t w = P.waves.size(); w-- > 0;)
+    k_solve_bwd<<<(unsigned)P.waves[w].size(), 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]),
+                                                             (int)P.waves[w].size(), h->d_fronts, A, h->d_x, n, nrhs,
+                                                             h->solve_work);
+  k_perm_scale_out<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
+                                                                  h->has_scaling ? h->d_scal : nullptr);
+  CK(cudaEventRecord(h->ev[7], st));
+  CK(cudaGetLastError());
+  return RVG_OK;
+}
+
+rvg_status rvg_solve_device(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  if (nrhs < 0 || (nrhs > 0 && ldb < h->P.n)) { set_error("RHS length must match matrix dimension"); return RVG_ERR_DIMENSION_MISMATCH; }
+  CK(cudaSetDevice(h->device));
+  int rc = solve_common(h, d_rhs, nrhs, ldb);
+  if (rc) return (rvg_status)rc;
+  CK(cudaStreamSynchronize(h->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]);
+  h->t_solve = ms;
+  return RVG_OK;
+}
+
+rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  if (nrhs < 0 || (nrhs > 0 && ldb < h->P.n)) { set_error("RHS length must match matrix dimension"); return RVG_ERR_DIMENSION_MISMATCH; }
+  if (h->P.n == 0 || nrhs == 0) return RVG_OK;
+  CK(cudaSetDevice(h->device));
+  double* d = nullptr;
+  size_t bytes = (size_t)ldb * (size_t)(nrhs - 1) * 8 + (size_t)h->P.n * 8;
+  CK(cudaMallocAsync((void**)&d, bytes, h->st));
+  CK(cudaMemcpyAsync(d, rhs, bytes, cudaMemcpyHostToDevice, h->st));
+  int rc = solve_common(h, d, nrhs, ldb);
+  if (rc) return (rvg_status)rc;
+  CK(cudaMemcpyAsync(rhs, d, bytes, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaFreeAsync(d, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]);
+  h->t_solve = ms;
+  return RVG_OK;
+}
+
+rvg_status rvg_inertia(rvg_handle* h, int64_t out3[3]) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called first"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  int64_t pos = 0, neg = 0, zer = 0;
+  int64_t tot = 0;
+  for (auto& f : h->h_fronts) tot = std::max<int64_t>(tot, f.dpos + f.k);
+  std::vector<int8_t> dt(tot);
+  std::vector<double> dd(tot), dof(tot);
+  if (tot) {
+    CK(cudaMemcpy(dt.data(), h->dtype, tot, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dd.data(), h->ddiag, tot * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dof.data(), h->doff, tot * 8, cudaMemcpyDeviceToHost));
+  }
+  // MixedDiagonal::compute_inertia (diagonal.rs:391-461) per front
+  for (auto& f : h->h_fronts) {
+    int c = 0;
+    while (c < f.ne) {
+      int64_t q = f.dpos + c;
+      if (dt[q] == PT_1X1) {
+        double d = dd[q];
+        if (d > 0) pos++; else if (d < 0) neg++; else zer++;
+        c += 1;
+      } else {
+        double a = dd[q], b = dof[q], cc = dd[q + 1];
+        double det = a * cc - b * b, tr = a + cc;
+        if (det > 0) { if (tr > 0) pos += 2; else neg += 2; }
+        else if (det < 0) { pos++; neg++; }
+        else { if (tr > 0) { pos++; zer++; } else if (tr < 0) { neg++; zer++; } else zer += 2; }
+        c += 2;
+      }
+    }
+  }
+  out3[0] = pos; out3[1] = neg; out3[2] = zer;
+  return RVG_OK;
+}
+
+rvg_status rvg_get_stats(rvg_handle* h, rvg_stats* o) {
+  if (!h || !o) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called first"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  o->total_1x1_pivots = h->tot1;
+  o->total_2x2_pivots = h->tot2;
+  o->total_delayed = h->totdel;
+  o->zero_pivots = h->zero_piv;
+  o->max_front_size = h->max_front;
+  o->supernodes_before_amalgamation = h->P.nsup_before;
+  o->supernodes_after_amalgamation = (int64_t)h->P.sn.size();
+  o->merges_performed = h->P.merges;
+  o->small_leaf_subtrees = h->P.sl_subtrees;
+  o->small_leaf_nodes = h->P.sl_nodes;
+  return RVG_OK;
+}
+
+rvg_status rvg_pivot_record(rvg_handle* h, int64_t* col, int8_t* code, double* d_diag, double* d_off, int64_t* count) {
+  if (!h || !count) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called first"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  int64_t tot = 0, isz = 0;
+  for (auto& f : h->h_fronts) { tot = std::max<int64_t>(tot, f.dpos + f.k); isz = std::max<int64_t>(isz, f.idx + f.m + f.k); }
+  std::vector<int8_t> dt(tot);
+  std::vector<double> dd(tot), dof(tot);
+  std::vector<int32_t> ix(isz);
+  if (tot) {
+    CK(cudaMemcpy(dt.data(), h->dtype, tot, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dd.data(), h->ddiag, tot * 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dof.data(), h->doff, tot * 8, cudaMemcpyDeviceToHost));
+  }
+  if (isz) CK(cudaMemcpy(ix.data(), h->idx, isz * 4, cudaMemcpyDeviceToHost));
+  int64_t t = 0;
+  for (auto& f : h->h_fronts) {
+    const int32_t* rows = ix.data() + f.idx;
+    const int32_t* perm = rows + f.m;
+    for (int c = 0; c < f.ne; ++c) {
+      int64_t q = f.dpos + c;
+      if (col) col[t] = rows[perm[c]];
+      int8_t cd = dt[q];
+      if (code) code[t] = cd;
+      if (d_diag) d_diag[t] = dd[q];
+      if (d_off) d_off[t] = cd == 2 ? dof[q] : 0.0;
+      ++t;
+    }
+  }
+  *count = t;
+  return RVG_OK;
+}
+
+rvg_status rvg_front_info(rvg_handle* h, int64_t* out9, int64_t* nsup) {
+  if (!h || !nsup) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  *nsup = (int64_t)h->P.sn.size();
+  if (!out9) return RVG_OK;
+  for (size_t s = 0; s < h->P.sn.size(); ++s) {
+    const DFront& f = h->factored ? h->h_fronts[s] : DFront();
+    int64_t* o = out9 + 9 * s;
+    o[0] = f.m; o[1] = f.k; o[2] = f.ne; o[3] = f.n1; o[4] = f.n2; o[5] = h->P.sn[s].parent;
+    o[6] = h->P.sn[s].n_owned(); o[7] = h->P.sn[s].in_small_leaf ? 1 : 0; o[8] = h->P.height[s];
+  }
+  return RVG_OK;
+}
+
+rvg_status rvg_work(rvg_handle* h, double out6[6]) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  Plan& P = h->P;
+  double solve_bytes = 0;
+  for (auto& s : P.sn) {
+    double k = (double)s.n_owned(), r = (double)s.pattern.size();
+    double stored = k * (k + 1) / 2 + r * k;
+    solve_bytes += 2 * 8 * stored + 8 * k + 2 * 4 * (k + r) + 2 * 2 * 8 * (k + r);
+  }
+  out6[0] = P.flops_factor; out6[1] = P.flops_schur; out6[2] = P.bytes_assembly; out6[3] = solve_bytes;
+  out6[4] = (double)P.nnz_l; out6[5] = (double)P.max_front;
+  return RVG_OK;
+}
+
+rvg_status rvg_timings(rvg_handle* h, double out7[7]) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  out7[0] = h->t_assembly; out7[1] = h->t_kernel; out7[2] = h->t_gemm; out7[3] = h->t_factor; out7[4] = h->t_solve;
+  out7[5] = h->t_dom; out7[6] = h->n_dom;
+  return RVG_OK;
+}
+
+rvg_status rvg_stream(rvg_handle* h, void** s) {
+  if (!h || !s) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  *s = (void*)h->st;
+  return RVG_OK;
+}
+
+void rvg_destroy(rvg_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  cudaStream_t st = h->st;
+  auto fr = [&](void* p) { if (p) cudaFreeAsync(p, st); };
+  fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
+  fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
+  fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage);
+  if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
+  if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->h_counts) cudaFreeHost(h->h_counts);
+  for (auto& e : h->ev) if (e) cudaEventDestroy(e);
+  delete h;
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+"""Fill-reducing orderings supplied to the analysis (UserSupplied semantics,
+sparse/src/symmetric/solver.rs:51-52).
+
+METIS (the reference's default, reached through the metis-sys crate at
+sparse/src/ordering/metis.rs:559-600) is not available to this build, so:
+
+* grid problems use exact geometric nested dissection: a box is split along
+  its longest side by a one-node-thick plane, which separates both the
+  7-point and the 27-point stencil; halves first, separator last;
+* the KKT systems order H by the same dissection of its grid and put the
+  constraint rows last (their Schur complement -J H^-1 J^T is dense and
+  negative definite, so the last front takes 1x1 pivots);
+* other matrices fall back to reverse Cuthill-McKee or the natural order.
+
+All functions return ``order`` with ``order[new] = old`` (int64).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def nested_dissection_grid(dims, leaf: int = 8) -> np.ndarray:
+    """Geometric nested dissection of an nx*ny*nz grid (x fastest varying
+    within the linear index i*ny*nz + j*nz + k, i.e. C order of (i, j, k))."""
+    nx, ny, nz = dims
+    out = []
+
+    def emit(x0, x1, y0, y1, z0, z1):
+        i, j, k = np.meshgrid(np.arange(x0, x1), np.arange(y0, y1), np.arange(z0, z1), indexing="ij")
+        out.append((i * ny * nz + j * nz + k).ravel())
+
+    # explicit stack of (box, state): state 0 = visit, 1 = emit separator
+    stack = [((0, nx, 0, ny, 0, nz), None)]
+    while stack:
+        box, sep = stack.pop()
+        if sep is not None:
+            emit(*sep)
+            continue
+        x0, x1, y0, y1, z0, z1 = box
+        sx, sy, sz = x1 - x0, y1 - y0, z1 - z0
+        if sx <= 0 or sy <= 0 or sz <= 0:
+            continue
+        if sx * sy * sz <= leaf or max(sx, sy, sz) < 3:
+            emit(*box)
+            continue
+        if sx >= sy and sx >= sz:
+            mid = x0 + sx // 2
+            a, b, s = (x0, mid, y0, y1, z0, z1), (mid + 1, x1, y0, y1, z0, z1), (mid, mid + 1, y0, y1, z0, z1)
+        elif sy >= sz:
+            mid = y0 + sy // 2
+            a, b, s = (x0, x1, y0, mid, z0, z1), (x0, x1, mid + 1, y1, z0, z1), (x0, x1, mid, mid + 1, z0, z1)
+        else:
+            mid = z0 + sz // 2
+            a, b, s = (x0, x1, y0, y1, z0, mid), (x0, x1, y0, y1, mid + 1, z1), (x0, x1, y0, y1, mid, mid + 1)
+        # LIFO: push in reverse of the desired order (a, b, separator)
+        stack.append((None, s))
+        stack.append((b, None))
+        stack.append((a, None))
+    order = np.concatenate(out).astype(np.int64)
+    assert order.size == nx * ny * nz
+    return order
+
+
+def kkt_order(sysm, leaf: int = 8) -> np.ndarray:
+    """H by nested dissection of its grid, then the constraint rows."""
+    h = nested_dissection_grid(sysm.grid, leaf)
+    return np.concatenate([h, np.arange(sysm.n_h, sysm.n, dtype=np.int64)])
+
+
+def rcm_order(sysm) -> np.ndarray:
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    a = sysm.to_scipy()
+    return np.asarray(reverse_cuthill_mckee(a.tocsr(), symmetric_mode=True), dtype=np.int64)
+
+
+def natural_order(n: int) -> np.ndarray:
+    return np.arange(n, dtype=np.int64)
+
+
+def default_order(sysm) -> np.ndarray:
+    if sysm.grid is not None and sysm.n_h == 0:
+        return nested_dissection_grid(sysm.grid)
+    if sysm.grid is not None and sysm.n_h > 0:
+        return kkt_order(sysm)
+    if sysm.n <= 2:
+        return natural_order(sysm.n)
+    return rcm_order(sysm)
