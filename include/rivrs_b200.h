@@ -39,7 +39,8 @@ typedef enum {
 /* FactorOptions / AptpOptions (sparse/src/symmetric/solver.rs:72-116,
  * sparse/src/symmetric/factor.rs:86-130).  rvg_default_options() fills the
  * reference defaults: threshold 0.01, small 1e-20, nb 256, ib 32, nemin 32,
- * small_leaf_threshold 256, failed_pivot_method Tpp. */
+ * small_leaf_threshold 256, failed_pivot_method Tpp (and
+ * large_front_threshold 2048). */
 typedef struct {
   double threshold;
   double small;
@@ -49,6 +50,10 @@ typedef struct {
   int64_t small_leaf_threshold;
   int32_t failed_pivot_tpp; /* 1 = FailedPivotMethod::Tpp, 0 = Pass */
   int32_t fallback_bk;      /* 1 = AptpFallback::BunchKaufman, 0 = Delay */
+  /* B200 scheduling, no reference counterpart: fronts of order >= this use
+   * the multi-kernel path (whole GPU per front); smaller ones are batched one
+   * CTA or warp per front.  Results do not depend on it.  Default 2048. */
+  int64_t large_front_threshold;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */
@@ -138,6 +143,20 @@ rvg_status rvg_work(rvg_handle* h, double out6[6]);
  * [assembly, dense kernel, contribution GEMM, total factor, last solve,
  *  dominant-kernel time, dominant-kernel launches]. */
 rvg_status rvg_timings(rvg_handle* h, double out7[7]);
+/* Measurement counters of the last factor and solve.  With profiling on,
+ * every launch of the FP64 Schur-complement GEMM is bracketed by CUDA events
+ * on the handle's stream, so syrk_ms is its device time; flops count the
+ * executed work of those launches (2 per multiply-add, lower triangle only). */
+typedef struct {
+  double factor_ms, solve_ms;
+  double assembly_ms, dense_ms, cbgemm_ms;
+  double syrk_ms, syrk_flops;
+  int64_t syrk_launches;
+  int64_t factor_launches, solve_launches;
+  int64_t peak_bytes;
+} rvg_profile;
+rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable);
+rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* out);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 rvg_status rvg_stream(rvg_handle* h, void** stream);
 void rvg_destroy(rvg_handle* h);

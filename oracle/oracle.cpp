@@ -291,12 +291,25 @@ i64 apply_and_check(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, const Mixe
   i64 ps = col_start + bcols;
   // panel * L11^T = A21  (L11 unit lower, from a[col_start.., col_start..])
   // faer TRSM (factor.rs:1338); per entry an fma chain over l ascending
-  for (i64 j = 0; j < nelim; ++j)
-    for (i64 l = 0; l < j; ++l) {
-      double lij = a(col_start + j, col_start + l);
-      for (i64 r = 0; r < prows; ++r)
-        a(ps + r, col_start + j) = std::fma(-a(ps + r, col_start + l), lij, a(ps + r, col_start + j));
+  {
+    const i64 RB = 256;
+    i64 nrb = (prows + RB - 1) / RB;
+    bool par = prows * nelim > 200000;
+#ifdef _OPENMP
+    par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) if (par)
+#endif
+    for (i64 rb = 0; rb < nrb; ++rb) {
+      i64 r0 = rb * RB, r1 = std::min(prows, r0 + RB);
+      for (i64 j = 0; j < nelim; ++j)
+        for (i64 l = 0; l < j; ++l) {
+          double lij = a(col_start + j, col_start + l);
+          for (i64 r = r0; r < r1; ++r)
+            a(ps + r, col_start + j) = std::fma(-a(ps + r, col_start + l), lij, a(ps + r, col_start + j));
+        }
     }
+    (void)par;
+  }
   i64 c = 0;
   while (c < nelim) {
     if (d.type[c] == PT_1X1) {
@@ -353,6 +366,40 @@ void compute_ld(const double* l, i64 ldl, i64 nrows, const MixedD& d, i64 nelim,
   }
 }
 
+// Cache-blocked rank-K update used by every faer GEMM call site:
+//   C[i, j] = fma(-W[i, c], L[j, c], C[i, j]) for c = 0..K-1 in order,
+// over i in [0, nr), j in [0, nc), where i + row_shift >= j (lower part of
+// the output relative to the diagonal).  Blocking reorders only independent
+// entries; each entry's fma chain keeps its order.  OpenMP over column blocks
+// when not already inside a parallel region.
+void syrk_fma(double* C, i64 ldc, const double* W, i64 ldw, const double* L, i64 ldl, i64 nr, i64 nc, i64 K,
+              i64 row_shift) {
+  const i64 JB = 32, IB = 512;
+  i64 njb = (nc + JB - 1) / JB;
+  bool par = (double)nr * (double)nc * (double)K > 4e6;
+#ifdef _OPENMP
+  par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(dynamic, 1) if (par)
+#endif
+  for (i64 jb = 0; jb < njb; ++jb) {
+    i64 j0 = jb * JB, j1 = std::min(nc, j0 + JB);
+    i64 ilo = std::max<i64>(0, j0 - row_shift);
+    for (i64 i0 = ilo; i0 < nr; i0 += IB) {
+      i64 i1 = std::min(nr, i0 + IB);
+      for (i64 c = 0; c < K; ++c) {
+        const double* w = W + c * ldw;
+        for (i64 j = j0; j < j1; ++j) {
+          double lj = L[j + c * ldl];
+          double* col = C + j * ldc;
+          i64 is = std::max(i0, j - row_shift);
+          for (i64 i = is; i < i1; ++i) col[i] = std::fma(-w[i], lj, col[i]);
+        }
+      }
+    }
+  }
+  (void)par;
+}
+
 // update_trailing (factor.rs:1418-1526): FS x FS lower and NFS x FS rectangle
 void update_trailing(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, i64 p, const MixedD& d) {
   if (nelim == 0) return;
@@ -364,21 +411,10 @@ void update_trailing(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, i64 p, co
   compute_ld(L.data(), tsz, tsz, d, nelim, W.data(), tsz);
   i64 fs = std::max<i64>(p - ts, 0);
   // faer triangular / rectangular GEMM (factor.rs:1491, 1513); per entry an
-  // fma chain over c ascending
-  // region 1: lower triangle of A[ts..p, ts..p]
-  for (i64 j = 0; j < fs; ++j)
-    for (i64 c = 0; c < nelim; ++c) {
-      double lj = L[j + c * tsz];
-      for (i64 i = j; i < fs; ++i) a(ts + i, ts + j) = std::fma(-W[i + c * tsz], lj, a(ts + i, ts + j));
-    }
-  // region 2: A[p..m, ts..p]
-  i64 nfs = m - p;
-  if (nfs > 0 && fs > 0)
-    for (i64 j = 0; j < fs; ++j)
-      for (i64 c = 0; c < nelim; ++c) {
-        double lj = L[j + c * tsz];
-        for (i64 i = 0; i < nfs; ++i) a(p + i, ts + j) = std::fma(-W[fs + i + c * tsz], lj, a(p + i, ts + j));
-      }
+  // fma chain over c ascending.  Region 1 is the lower triangle of
+  // A[ts..p, ts..p], region 2 the rectangle A[p..m, ts..p]: together the
+  // rows i >= j of the trailing columns ts..p.
+  if (fs > 0) syrk_fma(&a(ts, ts), a.ld, W.data(), tsz, L.data(), tsz, tsz, fs, nelim, 0);
 }
 
 // update_cross_terms (factor.rs:1669-1766)
@@ -741,13 +777,7 @@ void contribution_gemm(const double* l, i64 ldl, i64 p, i64 ne, i64 m, const Mix
   std::vector<double> W((size_t)nfs * ne, 0.0);
   compute_ld(l + p, ldl, nfs, d, ne, W.data(), nfs);
   // faer triangular GEMM (factor.rs:1639); per entry an fma chain over c ascending
-  for (i64 j = 0; j < nfs; ++j)
-    for (i64 c = 0; c < ne; ++c) {
-      double lj = l[p + j + c * ldl];
-      const double* w = W.data() + c * nfs;
-      double* col = cb + j * ldc;
-      for (i64 i = j; i < nfs; ++i) col[i] = std::fma(-w[i], lj, col[i]);
-    }
+  syrk_fma(cb, ldc, W.data(), nfs, l + p, ldl, nfs, nfs, ne, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1159,7 +1189,10 @@ void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_
   while (!ready.empty()) {
     i64 nr = (i64)ready.size();
 #ifdef _OPENMP
-#pragma omp parallel
+    // many fronts: one thread per front; few fronts: one at a time with the
+    // dense loops inside running in parallel
+    const bool wave_par = nr >= (i64)omp_get_max_threads() && nr > 1;
+#pragma omp parallel if (wave_par)
     {
       std::vector<i64> g2l(n, -1);
       i64 ties0 = g_ties; g_ties = 0;

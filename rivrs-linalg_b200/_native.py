@@ -28,7 +28,7 @@ STATUS = {
 class Options(C.Structure):
     _fields_ = [("threshold", C.c_double), ("small", C.c_double), ("outer_block_size", i64),
                 ("inner_block_size", i64), ("nemin", i64), ("small_leaf_threshold", i64),
-                ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32)]
+                ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64)]
 
 
 class Stats(C.Structure):
@@ -39,6 +39,16 @@ class Stats(C.Structure):
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class Profile(C.Structure):
+    _fields_ = [("factor_ms", C.c_double), ("solve_ms", C.c_double), ("assembly_ms", C.c_double),
+                ("dense_ms", C.c_double), ("cbgemm_ms", C.c_double), ("syrk_ms", C.c_double),
+                ("syrk_flops", C.c_double), ("syrk_launches", i64), ("factor_launches", i64),
+                ("solve_launches", i64), ("peak_bytes", i64)]
+
+    def as_dict(self):
+        return {k: (float(getattr(self, k)) if t is C.c_double else int(getattr(self, k))) for k, t in self._fields_}
 
 
 class RvgError(RuntimeError):
@@ -69,6 +79,8 @@ SIGNATURES = {
     "rvg_work": (C.c_int, [vp, dp]),
     "rvg_timings": (C.c_int, [vp, dp]),
     "rvg_stream": (C.c_int, [vp, C.POINTER(vp)]),
+    "rvg_set_profiling": (C.c_int, [vp, C.c_int32]),
+    "rvg_get_profile": (C.c_int, [vp, C.POINTER(Profile)]),
     "rvg_destroy": (None, [vp]),
 }
 

@@ -1,0 +1,464 @@
+// Multi-kernel APTP for one large front (front order >= the large-front
+// threshold): the same algorithm as the CTA kernel (factor_inner,
+// factor.rs:1811-2095; two_level_factor, factor.rs:2108-2252) with every
+// row-parallel step spread over the whole GPU and the pivot state kept on the
+// device, so the host issues a fixed launch sequence:
+//
+//   per 32-column inner block (view-local position k):
+//     lf_block   1 CTA    complete pivoting on the diagonal block, row
+//                         permutation of the outer block's earlier columns
+//     lf_panel   grid     backup, column permutation, TRSM, D^-1 scaling and
+//                         the a-posteriori threshold scan of every panel row
+//     lf_post    1 CTA    2x2 boundary adjustment, restore of the failed part
+//                         of the diagonal block, failed x failed cross term,
+//                         D entries
+//     lf_update  grid     restore of the failed panel columns, rank-nelim
+//                         update of the outer block's trailing columns, the
+//                         trailing x failed cross term
+//     lf_delay   1 CTA    delayed columns to the end of the outer block
+//   per 256-column outer block:
+//     lf_prop    grid     row permutation of the front's earlier columns
+//     lf_w       grid     W = L D for the rows below the outer block
+//     k_syrk_lower        the deferred rank-nelim update of every later
+//                         column (mathematically the reference's per-block
+//                         updates; each output keeps its fma chain in the
+//                         same order, so the result is bit-identical)
+//     lf_outer   1 CTA    column order, delays to the end of the remaining
+//                         fully-summed columns
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dense.cuh"
+
+namespace rvg {
+
+struct LFState {
+  int32_t k, end_pos, bs, bnelim, eff, nelim;
+  int32_t gne, n1, n2, bne;
+  int32_t bperm[32];
+  int8_t bdt[32];
+  double bdd[32], bdo[32];
+  double T[32][33];   // factored block, 2x2 off-diagonals zeroed (the L11 of the TRSM)
+  double Tb[32][33];  // the block before factorization
+};
+
+struct LFArgs {
+  double* a;        // front panel (m x p), ld m
+  int64_t m, p;
+  int32_t* perm;    // front pivot order (p)
+  DRec D;           // front D (p)
+  LFState* st;
+  int32_t* lp;      // outer-block local column order (nb)
+  double* pb;       // panel backup, rows x 32 (ld = bm)
+  double* w;        // inner W, rows x 32 (row-major, stride 32)
+  double* wo;       // outer W, (m - oe) x nb (column-major)
+  int64_t cs, bcols, nfsb;  // outer block start, width, NFS boundary (global p)
+  DevOpts o;
+};
+
+__global__ void k_lf_init(LFState* st, int32_t* perm, int64_t p) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) { st->gne = 0; st->n1 = 0; st->n2 = 0; }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < p; i += (int64_t)gridDim.x * blockDim.x)
+    perm[i] = (int32_t)i;
+}
+
+__global__ void k_lf_begin_outer(LFArgs A) {
+  LFState* st = A.st;
+  if (threadIdx.x == 0) { st->k = 0; st->end_pos = (int32_t)A.bcols; st->bne = 0; }
+  for (int i = threadIdx.x; i < A.bcols; i += blockDim.x) A.lp[i] = i;
+}
+
+// complete pivoting on the diagonal block (1 CTA)
+__global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
+  __shared__ CtaShared sh;
+  LFState* st = A.st;
+  const int tid = threadIdx.x;
+  const int64_t cs = A.cs;
+  PanelView V{A.a + cs + cs * A.m, A.m};
+  const int k = st->k, end_pos = st->end_pos;
+  const int bs = min(end_pos - k, A.o.ib);
+  if (k >= end_pos) {  // no columns left in this outer block
+    if (tid == 0) { st->bs = 0; st->bnelim = 0; st->eff = 0; st->nelim = 0; }
+    return;
+  }
+  for (int t = tid; t < bs * bs; t += NT) {
+    int i = t % bs, j = t / bs;
+    if (i >= j) { double v = V(k + i, k + j); sh.T[i][j] = v; st->Tb[i][j] = v; }
+  }
+  __syncthreads();
+  if (tid < 32) warp_block_factor(sh, bs, A.o.small, tid);
+  __syncthreads();
+  const int bnelim = sh.bnelim;
+  if (bnelim > 0) {
+    for (int t = tid; t < bs * bs; t += NT) {
+      int i = t % bs, j = t / bs;
+      if (i >= j) V(k + i, k + j) = sh.T[i][j];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      int bc = 0;
+      while (bc < bnelim) {
+        if (sh.bdt[bc] == PT_2X2) { V(k + bc + 1, k + bc) = 0.0; sh.T[bc + 1][bc] = 0.0; bc += 2; }
+        else bc += 1;
+      }
+    }
+    // row permutation of the view columns 0..k (step 5)
+    for (int64_t c = tid; c < k; c += NT) {
+      double buf[IBMAX];
+      for (int i = 0; i < bs; ++i) buf[i] = V(k + sh.bperm[i], c);
+      for (int i = 0; i < bs; ++i) V(k + i, c) = buf[i];
+    }
+    if (tid == 0) {  // column order (step 6)
+      int32_t ob[IBMAX];
+      for (int i = 0; i < bs; ++i) ob[i] = A.lp[k + i];
+      for (int i = 0; i < bs; ++i) A.lp[k + i] = ob[sh.bperm[i]];
+    }
+    __syncthreads();
+  }
+  for (int t = tid; t < bs * bs; t += NT) {
+    int i = t % bs, j = t / bs;
+    if (i >= j) st->T[i][j] = sh.T[i][j];
+  }
+  if (tid < 32) {
+    st->bperm[tid] = sh.bperm[tid];
+    st->bdt[tid] = sh.bdt[tid];
+    st->bdd[tid] = sh.bdd[tid];
+    st->bdo[tid] = sh.bdo[tid];
+  }
+  if (tid == 0) { st->bs = bs; st->bnelim = bnelim; st->eff = bnelim; }
+}
+
+// panel rows: backup, permute, TRSM, D^-1, threshold scan (grid over rows)
+__global__ void __launch_bounds__(256) k_lf_panel(LFArgs A) {
+  LFState* st = A.st;
+  const int bnelim = st->bnelim;
+  if (bnelim == 0) return;
+  __shared__ double T[IBMAX][IBMAX + 1];
+  __shared__ int bperm[IBMAX];
+  __shared__ int8_t bdt[IBMAX];
+  __shared__ double bdd[IBMAX], bdo[IBMAX];
+  __shared__ int s_fail;
+  const int bs = st->bs, k = st->k;
+  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
+    int i = t % bs, j = t / bs;
+    if (i >= j) T[i][j] = st->T[i][j];
+  }
+  if (threadIdx.x < IBMAX) {
+    bperm[threadIdx.x] = st->bperm[threadIdx.x];
+    bdt[threadIdx.x] = st->bdt[threadIdx.x];
+    bdd[threadIdx.x] = st->bdd[threadIdx.x];
+    bdo[threadIdx.x] = st->bdo[threadIdx.x];
+  }
+  if (threadIdx.x == 0) s_fail = bnelim;
+  __syncthreads();
+  const int64_t bm = A.m - A.cs;
+  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t be = k + bs;
+  const double bound = 1.0 / A.o.threshold;
+  if (r >= be && r < bm) {
+    double x[IBMAX], raw[IBMAX];
+    for (int i = 0; i < bs; ++i) raw[i] = V(r, k + i);
+    for (int i = 0; i < bs; ++i) A.pb[r + (int64_t)i * bm] = raw[i];
+    for (int i = 0; i < bs; ++i) x[i] = raw[bperm[i]];
+    for (int j = 0; j < bnelim; ++j)
+      for (int l = 0; l < j; ++l) x[j] = __fma_rn(-x[l], T[j][l], x[j]);
+    int c = 0;
+    while (c < bnelim) {
+      if (bdt[c] == PT_1X1) { x[c] = __dmul_rn(x[c], 1.0 / bdd[c]); c += 1; }
+      else {
+        double A_ = bdd[c], B_ = bdo[c], C_ = bdd[c + 1];
+        double inv_det = 1.0 / __dsub_rn(__dmul_rn(A_, C_), __dmul_rn(B_, B_));
+        double x1 = x[c], x2 = x[c + 1];
+        x[c] = __dmul_rn(__dsub_rn(__dmul_rn(x1, C_), __dmul_rn(x2, B_)), inv_det);
+        x[c + 1] = __dmul_rn(__dsub_rn(__dmul_rn(x2, A_), __dmul_rn(x1, B_)), inv_det);
+        c += 2;
+      }
+    }
+    for (int i = 0; i < bs; ++i) V(r, k + i) = x[i];
+    int fail = bnelim;
+    c = 0;
+    while (c < bnelim) {
+      int w = bdt[c] == PT_2X2 ? 2 : 1;
+      if (fabs(x[c]) >= bound || (w == 2 && fabs(x[c + 1]) >= bound)) { fail = c; break; }
+      c += w;
+    }
+    if (fail < bnelim) atomicMin(&s_fail, fail);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && s_fail < bnelim) atomicMin(&st->eff, s_fail);
+}
+
+// 2x2 boundary, restore of the failed diagonal part, failed x failed term,
+// D entries (1 CTA)
+__global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
+  LFState* st = A.st;
+  const int bnelim = st->bnelim, bs = st->bs, k = st->k;
+  const int tid = threadIdx.x;
+  if (bnelim == 0) {
+    if (tid == 0) st->nelim = 0;
+    return;
+  }
+  int eff = st->eff;
+  if (eff > 0 && st->bdt[eff - 1] == PT_2X2) eff -= 1;
+  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
+  if (eff < bnelim) {
+    for (int t = tid; t < bs * bs; t += blockDim.x) {
+      int i = t % bs, j = t / bs;
+      if (i < eff || j < eff) continue;
+      int c = st->bperm[j], r = st->bperm[i];
+      V(k + i, k + j) = r >= c ? st->Tb[r][c] : st->Tb[c][r];
+    }
+  }
+  __syncthreads();
+  const int nelim = eff;
+  if (nelim > 0 && nelim < bs) {
+    const int nf = bs - nelim;
+    for (int t = tid; t < nf * nf; t += blockDim.x) {
+      int i = t % nf, j = t / nf;
+      if (i < j) continue;
+      double wb[IBMAX];
+      const double* l = &V(k + nelim + i, k);
+      int c = 0;
+      while (c < nelim) {
+        if (st->bdt[c] == PT_1X1) { wb[c] = __dmul_rn(l[c * A.m], st->bdd[c]); c += 1; }
+        else {
+          double A_ = st->bdd[c], B_ = st->bdo[c], C_ = st->bdd[c + 1];
+          double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
+          wb[c] = __dadd_rn(__dmul_rn(l1, A_), __dmul_rn(l2, B_));
+          wb[c + 1] = __dadd_rn(__dmul_rn(l1, B_), __dmul_rn(l2, C_));
+          c += 2;
+        }
+      }
+      double s = 0.0;
+      for (int c2 = 0; c2 < nelim; ++c2) s = __dadd_rn(s, __dmul_rn(wb[c2], V(k + nelim + j, k + c2)));
+      V(k + nelim + i, k + nelim + j) = __dsub_rn(V(k + nelim + i, k + nelim + j), s);
+    }
+  }
+  if (tid == 0) {
+    DRec VD{A.D.type + A.cs, A.D.diag + A.cs, A.D.off + A.cs};
+    int c = 0, n1 = 0, n2 = 0;
+    while (c < nelim) {
+      if (st->bdt[c] == PT_1X1) {
+        VD.type[k + c] = PT_1X1; VD.diag[k + c] = st->bdd[c]; VD.off[k + c] = 0.0; n1++; c += 1;
+      } else if (c + 1 < nelim) {
+        VD.type[k + c] = PT_2X2; VD.type[k + c + 1] = PT_2X2B;
+        VD.diag[k + c] = st->bdd[c]; VD.diag[k + c + 1] = st->bdd[c + 1];
+        VD.off[k + c] = st->bdo[c]; VD.off[k + c + 1] = 0.0; n2++; c += 2;
+      } else c += 1;
+    }
+    st->n1 += n1; st->n2 += n2;
+    st->nelim = nelim;
+    st->eff = eff;
+  }
+}
+
+// restore of the failed panel columns, trailing update inside the outer
+// block, trailing x failed cross term (grid over rows >= ts, one row per thread)
+__global__ void __launch_bounds__(256) k_lf_update(LFArgs A) {
+  LFState* st = A.st;
+  const int bnelim = st->bnelim;
+  if (bnelim == 0) return;
+  const int bs = st->bs, k = st->k, nelim = st->nelim, eff = st->eff;
+  const int64_t bm = A.m - A.cs;
+  const int64_t ts = k + bs;
+  const int64_t pl = A.bcols;  // trailing columns updated here: [ts, pl)
+  __shared__ double Ls[32][IBMAX + 1];
+  __shared__ int bperm[IBMAX];
+  __shared__ int8_t bdt[IBMAX];
+  __shared__ double bdd[IBMAX], bdo[IBMAX];
+  if (threadIdx.x < IBMAX) {
+    bperm[threadIdx.x] = st->bperm[threadIdx.x];
+    bdt[threadIdx.x] = st->bdt[threadIdx.x];
+    bdd[threadIdx.x] = st->bdd[threadIdx.x];
+    bdo[threadIdx.x] = st->bdo[threadIdx.x];
+  }
+  __syncthreads();
+  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
+  const int64_t i = ts + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool row = i < bm;
+  if (row && eff < bnelim) {
+    for (int j = eff; j < bs; ++j) V(i, k + j) = A.pb[i + (int64_t)bperm[j] * bm];
+  }
+  if (nelim == 0) return;
+  double w[IBMAX];
+  if (row) {
+    const double* l = &V(i, k);
+    int c = 0;
+    while (c < nelim) {
+      if (bdt[c] == PT_1X1) { w[c] = __dmul_rn(l[c * A.m], bdd[c]); c += 1; }
+      else {
+        double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
+        w[c] = __dadd_rn(__dmul_rn(l1, bdd[c]), __dmul_rn(l2, bdo[c]));
+        w[c + 1] = __dadd_rn(__dmul_rn(l1, bdo[c]), __dmul_rn(l2, bdd[c + 1]));
+        c += 2;
+      }
+    }
+  }
+  // trailing columns of the outer block, 32 at a time through shared memory
+  const int64_t i_lo = ts + (int64_t)blockIdx.x * blockDim.x;
+  for (int64_t j0 = ts; j0 < pl; j0 += 32) {
+    const int nj = (int)((pl - j0) < 32 ? (pl - j0) : 32);
+    if (j0 > i_lo + (int64_t)blockDim.x - 1) break;  // all rows of this CTA are above these columns
+    __syncthreads();
+    for (int t = threadIdx.x; t < nj * nelim; t += blockDim.x) {
+      int jj = t % nj, c = t / nj;
+      Ls[jj][c] = V(j0 + jj, k + c);
+    }
+    __syncthreads();
+    if (row) {
+      for (int jj = 0; jj < nj; ++jj) {
+        int64_t j = j0 + jj;
+        if (j > i) break;
+        double acc = V(i, j);
+        for (int c = 0; c < nelim; ++c) acc = __fma_rn(-w[c], Ls[jj][c], acc);
+        V(i, j) = acc;
+      }
+    }
+  }
+  // trailing x failed cross term
+  if (nelim < bs) {
+    const int nf = bs - nelim;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nf * nelim; t += blockDim.x) {
+      int jj = t % nf, c = t / nf;
+      Ls[jj][c] = V(k + nelim + jj, k + c);
+    }
+    __syncthreads();
+    if (row) {
+      for (int jj = 0; jj < nf; ++jj) {
+        double s = 0.0;
+        for (int c = 0; c < nelim; ++c) s = __dadd_rn(s, __dmul_rn(w[c], Ls[jj][c]));
+        V(i, k + nelim + jj) = __dsub_rn(V(i, k + nelim + jj), s);
+      }
+    }
+  }
+}
+
+// delayed columns of the inner block to the end of the outer block (1 CTA)
+__global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
+  LFState* st = A.st;
+  const int tid = threadIdx.x;
+  const int k = st->k, bs = st->bs, bnelim = st->bnelim, nelim = st->nelim;
+  int end_pos = st->end_pos;
+  if (bs == 0) return;
+  const int64_t bm = A.m - A.cs;
+  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
+  __syncthreads();
+  if (bnelim == 0) {
+    for (int off = 0; off < bs; ++off) {
+      end_pos -= 1;
+      if (k + off < end_pos) {
+        cta_swap(V, bm, k + off, end_pos);
+        if (tid == 0) { int32_t t = A.lp[k + off]; A.lp[k + off] = A.lp[end_pos]; A.lp[end_pos] = t; }
+      }
+    }
+  } else if (nelim < bs) {
+    int nd = bs - nelim;
+    for (int i = nd - 1; i >= 0; --i) {
+      int dp = k + nelim + i;
+      end_pos -= 1;
+      if (dp < end_pos) {
+        cta_swap(V, bm, dp, end_pos);
+        if (tid == 0) { int32_t t = A.lp[dp]; A.lp[dp] = A.lp[end_pos]; A.lp[end_pos] = t; }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) { st->k = k + nelim; st->end_pos = end_pos; st->bne = k + nelim; }
+}
+
+// row permutation of the outer block applied to the front's earlier columns
+// 0..cs (two_level_factor, factor.rs:2165-2181): 16 columns per CTA
+constexpr int LF_PROP_COLS = 16;
+__global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
+  extern __shared__ double buf[];  // bcols x LF_PROP_COLS
+  const int64_t c0 = (int64_t)blockIdx.x * LF_PROP_COLS;
+  const int nc = (int)((A.cs - c0) < LF_PROP_COLS ? (A.cs - c0) : LF_PROP_COLS);
+  if (nc <= 0) return;
+  const int bc = (int)A.bcols;
+  for (int t = threadIdx.x; t < nc * bc; t += blockDim.x) {
+    int i = t % bc, c = t / bc;
+    buf[t] = A.a[(A.cs + A.lp[i]) + (c0 + c) * A.m];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nc * bc; t += blockDim.x) {
+    int i = t % bc, c = t / bc;
+    A.a[(A.cs + i) + (c0 + c) * A.m] = buf[t];
+  }
+}
+
+// W = L D for the rows below the outer block, over its bne eliminated columns
+__global__ void k_lf_w(LFArgs A) {
+  const int bne = A.st->bne;
+  const int64_t oe = A.cs + A.bcols;
+  const int64_t i = oe + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.m) return;
+  const int64_t ldw = A.m - oe;
+  const int8_t* dt = A.D.type + A.cs;
+  const double* dd = A.D.diag + A.cs;
+  const double* dof = A.D.off + A.cs;
+  const double* l = A.a + i + A.cs * A.m;
+  int c = 0;
+  while (c < bne) {
+    if (dt[c] == PT_1X1) { A.wo[(i - oe) + c * ldw] = __dmul_rn(l[c * A.m], dd[c]); c += 1; }
+    else {
+      double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
+      A.wo[(i - oe) + c * ldw] = __dadd_rn(__dmul_rn(l1, dd[c]), __dmul_rn(l2, dof[c]));
+      A.wo[(i - oe) + (c + 1) * ldw] = __dadd_rn(__dmul_rn(l1, dof[c]), __dmul_rn(l2, dd[c + 1]));
+      c += 2;
+    }
+  }
+}
+
+// end of an outer block: column order, delays to the end of the remaining
+// fully-summed columns (two_level), eliminated total (1 CTA)
+__global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_level) {
+  LFState* st = A.st;
+  const int tid = threadIdx.x;
+  const int bne = st->bne;
+  const int64_t cs = A.cs, bcols = A.bcols;
+  if (tid == 0) {
+    // perm[cs + i] = orig[lp[i]], via the inner W scratch as the copy buffer
+    int32_t* orig = (int32_t*)A.w;
+    for (int i = 0; i < bcols; ++i) orig[i] = A.perm[cs + i];
+    for (int i = 0; i < bcols; ++i) A.perm[cs + i] = orig[A.lp[i]];
+  }
+  __syncthreads();
+  if (two_level && bne < bcols) {
+    PanelView F{A.a, A.m};
+    const int nf = (int)(bcols - bne);
+    for (int i = 0; i < nf; ++i) {
+      int64_t fp = cs + bne + i, e = cs + rem - 1 - i;
+      if (fp < e) {
+        cta_swap(F, A.m, fp, e);
+        if (tid == 0) { int32_t t = A.perm[fp]; A.perm[fp] = A.perm[e]; A.perm[e] = t; }
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) st->gne += bne;
+}
+
+// TPP fallback on the leftover columns, then the front's results
+__global__ void k_lf_finish(LFArgs A, DFront* F, int s) {
+  LFState* st = A.st;
+  __shared__ int cnt[2];
+  const int lane = threadIdx.x;
+  int gne = st->gne;
+  if (lane == 0) { cnt[0] = 0; cnt[1] = 0; }
+  __syncwarp();
+  if (gne < A.p && A.o.failed_pivot_tpp) {
+    WarpTpp T{PanelView{A.a, A.m}, A.m, A.p, lane};
+    gne += (int)T.run(gne, A.p, A.perm, A.D, &cnt[0], &cnt[1], A.o);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    F[s].ne = gne;
+    F[s].n1 = st->n1 + cnt[0];
+    F[s].n2 = st->n2 + cnt[1];
+  }
+}
+
+}  // namespace rvg

@@ -661,6 +661,13 @@ __global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* 
   if (tid == 0) { F[s].ne = gne; F[s].n1 = n1; F[s].n2 = n2; }
 }
 
+}  // namespace rvg
+
+#include "gemm64.cuh"
+#include "large.cuh"
+
+namespace rvg {
+
 // ---------------------------------------------------------------------------
 // contribution GEMM: CB -= (L21_NFS D) L21_NFS^T, lower triangle
 // (compute_contribution_gemm, factor.rs:1590-1652)
@@ -929,7 +936,15 @@ struct rvg_handle {
   char* d_stage = nullptr; size_t stage_cap = 0;   // per-wave packed launch data
   char* h_stage = nullptr; size_t h_stage_cap = 0; // pinned host mirror
   int32_t* h_counts = nullptr; size_t h_counts_cap = 0;
+  LFState* d_lf = nullptr;                          // state of the large-front path
   bool factored = false;
+  // measurement
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  double syrk_flops = 0, syrk_ms = 0;
+  int64_t syrk_launches = 0, launches = 0, factor_launches = 0, solve_launches = 0;
+  int64_t arena_bytes = 0, peak_bytes = 0;
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
   double t_assembly = 0, t_kernel = 0, t_gemm = 0, t_factor = 0, t_solve = 0, t_dom = 0, n_dom = 0;
@@ -1012,6 +1027,105 @@ DevOpts devopts(const rvg_options& o) {
 
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+double lower_entries(int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
+  double e = 0;
+  for (int64_t j = c0; j < c1; ++j) {
+    int64_t lo = j > r0 ? j : r0;
+    if (r1 > lo) e += (double)(r1 - lo);
+  }
+  return e;
+}
+
+int launch_syrk(rvg_handle* h, const SyrkArgs& ga) {
+  cudaStream_t st = h->st;
+  if (h->profiling) {
+    if (h->ev_used + 2 > h->ev_pool.size()) {
+      for (int i = 0; i < 64; ++i) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        h->ev_pool.push_back(e);
+      }
+    }
+    CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
+  }
+  k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
+  h->launches++;
+  h->syrk_launches++;
+  if (h->profiling) CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
+  return RVG_OK;
+}
+
+// One large front on the whole GPU: the launch sequence of large.cuh, with
+// one host synchronisation per 256-column outer block (its start column
+// depends on the delays of the previous block).
+int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts& dop) {
+  cudaStream_t st = h->st;
+  const DFront& f = h->h_fronts[s];
+  const int64_t m = f.m, p = f.k, nb = h->opt.outer_block_size, ib = h->opt.inner_block_size;
+  LFArgs a{};
+  a.a = Ar.panel + f.panel;
+  a.m = m;
+  a.p = p;
+  a.perm = Ar.idx + f.idx + m;
+  a.D = DRec{Ar.dtype + f.dpos, Ar.ddiag + f.dpos, Ar.doff + f.dpos};
+  a.st = h->d_lf;
+  double* sc = Ar.scratch + f.scratch;
+  a.pb = sc;
+  a.w = sc + m * IBMAX;
+  a.wo = sc + 2 * m * IBMAX;
+  a.lp = (int32_t*)(sc + m * (2 * IBMAX + nb));
+  a.nfsb = p;
+  a.o = dop;
+  const int two_level = p > nb;
+  k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
+  h->launches++;
+  int64_t rem = p, gne = 0;
+  while (rem > 0) {
+    const int64_t bcols = std::min(rem, nb), cs = gne, bm = m - cs, oe = cs + bcols;
+    a.cs = cs;
+    a.bcols = bcols;
+    k_lf_begin_outer<<<1, 256, 0, st>>>(a);
+    const unsigned rows_grid = blocks_for(bm, 256);
+    const int64_t ninner = (bcols + ib - 1) / ib;
+    for (int64_t it = 0; it < ninner; ++it) {
+      k_lf_block<<<1, NT, 0, st>>>(a);
+      k_lf_panel<<<rows_grid, 256, 0, st>>>(a);
+      k_lf_post<<<1, 256, 0, st>>>(a);
+      k_lf_update<<<rows_grid, 256, 0, st>>>(a);
+      k_lf_delay<<<1, NT, 0, st>>>(a);
+    }
+    h->launches += 1 + 5 * ninner;
+    bool syrk = false;
+    if (two_level) {
+      if (cs > 0) {
+        k_lf_prop<<<(unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256, (size_t)bcols * LF_PROP_COLS * 8, st>>>(a);
+        h->launches++;
+      }
+      if (oe < p) {
+        k_lf_w<<<blocks_for(m - oe, 256), 256, 0, st>>>(a);
+        h->launches++;
+        SyrkArgs ga{a.a, m, a.wo, m - oe, a.a + cs * m, m, oe, m, oe, p, 0, &a.st->bne};
+        int rc = launch_syrk(h, ga);
+        if (rc) return rc;
+        syrk = true;
+      }
+    }
+    k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level);
+    h->launches++;
+    CK(cudaGetLastError());
+    int32_t g = 0;
+    CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (syrk) h->syrk_flops += 2.0 * (double)(g - gne) * lower_entries(oe, m, oe, p);
+    gne = g;
+    rem -= bcols;
+  }
+  k_lf_finish<<<1, 32, 0, st>>>(a, h->d_fronts, s);
+  h->launches++;
+  CK(cudaGetLastError());
+  return RVG_OK;
+}
+
 // The numeric factorization proper: the level-set schedule of
 // factor_tree_levelset (numeric.rs:1957-2163) with every front of a wave
 // processed by the same launches.
@@ -1028,6 +1142,12 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   const int ib = (int)h->opt.inner_block_size;
   double t_asm = 0, t_ker = 0, t_gem = 0;
   int rc;
+  h->ev_used = 0;
+  h->syrk_flops = 0;
+  h->syrk_ms = 0;
+  h->syrk_launches = 0;
+  h->launches = 0;
+  h->peak_bytes = 0;
   CK(cudaEventRecord(h->ev[0], st));
   for (size_t w = 0; w < P.waves.size(); ++w) {
     const std::vector<int64_t>& wave = P.waves[w];
@@ -1056,7 +1176,9 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       f.dpos = d_used + d_need; d_need += k;
       if (f.flags & FF_HAS_CB) cb_need += nfs * nfs;
       const bool tpp = (f.flags & FF_SMALL_LEAF) || k < ib;
+      const bool large = !tpp && m >= h->opt.large_front_threshold;
       int64_t sc = tpp ? 0 : (2 * IBMAX * m + h->opt.outer_block_size);
+      if (large) sc = m * (2 * IBMAX + h->opt.outer_block_size) + h->opt.outer_block_size;
       if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
       f.scratch = scratch_need; scratch_need += sc;
     }
@@ -1080,13 +1202,15 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     if (panel_need) CK(cudaMemsetAsync(h->panel + panel_used, 0, (size_t)panel_need * 8, st));
     const Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, scratch};
     // ---- launch data of the whole wave, packed into one upload
-    std::vector<int32_t> ids(wave.begin(), wave.end()), tpp_ids, aptp_ids;
+    std::vector<int32_t> ids(wave.begin(), wave.end()), tpp_ids, aptp_ids, large_ids;
     std::vector<DFront> staged;
     staged.reserve(nw);
     for (int64_t s : wave) {
       staged.push_back(h->h_fronts[s]);
       const DFront& f = h->h_fronts[s];
-      if ((f.flags & FF_SMALL_LEAF) || f.k < ib) tpp_ids.push_back((int32_t)s); else aptp_ids.push_back((int32_t)s);
+      if ((f.flags & FF_SMALL_LEAF) || f.k < ib) tpp_ids.push_back((int32_t)s);
+      else if (f.m >= h->opt.large_front_threshold) large_ids.push_back((int32_t)s);
+      else aptp_ids.push_back((int32_t)s);
     }
     std::vector<ScatterItem> sitems;
     for (int64_t s : wave)
@@ -1104,10 +1228,12 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
         for (int j0 = 0; j0 < sz; j0 += 32) eitems[q].push_back(EaItem{(int32_t)s, (int32_t)c, j0, 0});
       }
     std::vector<TileItem> witems, gitems;
+    std::vector<int64_t> cb_syrk_fronts;
     for (int64_t s : wave) {
       const DFront& f = h->h_fronts[s];
       if (!(f.flags & FF_HAS_CB) || f.k == 0) continue;
       for (int ti = 0; ti * 256 < f.nfs; ++ti) witems.push_back(TileItem{(int32_t)s, ti, 0, 0});
+      if (f.m >= h->opt.large_front_threshold && f.nfs >= 256) continue;  // GEMM by k_syrk_lower
       int nt = (f.nfs + GT - 1) / GT;
       for (int tj = 0; tj < nt; ++tj)
         for (int ti = tj; ti < nt; ++ti) gitems.push_back(TileItem{(int32_t)s, ti, tj, 0});
@@ -1152,11 +1278,21 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     if (!aptp_ids.empty())
       k_aptp<<<(unsigned)aptp_ids.size(), NT, 0, st>>>((const int32_t*)(D + o_aptp), (int)aptp_ids.size(),
                                                         h->d_fronts, A, dop);
+    for (int32_t s : large_ids)
+      if ((rc = factor_large_front(h, s, A, dop))) return rc;
     CK(cudaEventRecord(h->ev[3], st));
     // ---- contribution GEMM (fronts with nothing eliminated skip inside)
-    if (!gitems.empty()) {
+    if (!witems.empty())
       k_cb_w<<<(unsigned)witems.size(), 256, 0, st>>>((const TileItem*)(D + o_w), h->d_fronts, A);
+    if (!gitems.empty())
       k_cb_gemm<<<(unsigned)gitems.size(), 256, 0, st>>>((const TileItem*)(D + o_g), h->d_fronts, A);
+    for (int64_t s : wave) {
+      const DFront& f = h->h_fronts[s];
+      if (!(f.flags & FF_HAS_CB) || f.k == 0 || !(f.m >= h->opt.large_front_threshold && f.nfs >= 256)) continue;
+      SyrkArgs ga{f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
+                  0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
+      if ((rc = launch_syrk(h, ga))) return rc;
+      cb_syrk_fronts.push_back(s);
     }
     CK(cudaEventRecord(h->ev[4], st));
     CK(cudaGetLastError());
@@ -1169,6 +1305,19 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     for (int i = 0; i < nw; ++i) {
       DFront& f = h->h_fronts[wave[i]];
       f.ne = h->h_counts[3 * i]; f.n1 = h->h_counts[3 * i + 1]; f.n2 = h->h_counts[3 * i + 2];
+    }
+    for (int64_t s : cb_syrk_fronts) {
+      const DFront& f = h->h_fronts[s];
+      h->syrk_flops += 2.0 * (double)f.ne * (double)f.nfs * (double)(f.nfs + 1) / 2.0;
+    }
+    h->launches += 1 + (int64_t)eitems.size() * 0 + (sitems.empty() ? 0 : 1) + (tpp_ids.empty() ? 0 : 1) +
+                   (aptp_ids.empty() ? 0 : 1) + (witems.empty() ? 0 : 1) + (gitems.empty() ? 0 : 1) + 2 +
+                   (dly_ids.empty() ? 0 : 1);
+    for (size_t q = 0; q < maxch; ++q) h->launches += eitems[q].empty() ? 0 : 1;
+    {
+      size_t fb = 0, tb = 0;
+      cudaMemGetInfo(&fb, &tb);
+      h->peak_bytes = std::max<int64_t>(h->peak_bytes, (int64_t)(tb - fb));
     }
     int64_t last = -1;
     for (int64_t s : wave) if (P.sn[s].parent >= 0) last = std::max(last, P.height[P.sn[s].parent]);
@@ -1187,6 +1336,13 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   float tot = 0;
   cudaEventElapsedTime(&tot, h->ev[0], h->ev[5]);
   h->t_assembly = t_asm; h->t_kernel = t_ker; h->t_gemm = t_gem; h->t_factor = tot;
+  h->factor_launches = h->launches;
+  if (h->profiling)
+    for (size_t e = 0; e + 1 < h->ev_used; e += 2) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, h->ev_pool[e], h->ev_pool[e + 1]);
+      h->syrk_ms += ms;
+    }
   // aggregate stats (numeric.rs:929-1009)
   h->tot1 = h->tot2 = h->totdel = h->zero_piv = h->max_front = 0;
   std::vector<int8_t> dt(d_used);
@@ -1225,6 +1381,7 @@ void rvg_default_options(rvg_options* o) {
   o->small_leaf_threshold = 256;
   o->failed_pivot_tpp = 1;
   o->fallback_bk = 1;
+  o->large_front_threshold = 2048;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347
@@ -1238,6 +1395,7 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347
   }
   if (o.inner_block_size > IBMAX) { set_error("inner_block_size above 32 is not supported by the B200 kernels"); return RVG_ERR_INVALID_INPUT; }
   if (o.nemin < 1) { set_error("nemin must be >= 1"); return RVG_ERR_INVALID_INPUT; }
+  if (o.large_front_threshold < 1) { set_error("large_front_threshold must be >= 1"); return RVG_ERR_INVALID_INPUT; }
   return RVG_OK;
 }
 
@@ -1289,6 +1447,8 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
       (rc = upload(h->d_pfwd, P.perm_fwd, st)))
     return (rvg_status)rc;
   CK(cudaMallocAsync((void**)&h->d_fronts, std::max<int64_t>(ns, 1) * sizeof(DFront), st));
+  CK(cudaMallocAsync((void**)&h->d_lf, sizeof(LFState), st));
+  CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
   CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
   CK(cudaMallocAsync((void**)&h->d_scal, std::max<int64_t>(n, 1) * 8, st));
   CK(cudaStreamSynchronize(st));
@@ -1355,6 +1515,7 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
                                                              h->solve_work);
   k_perm_scale_out<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
                                                                   h->has_scaling ? h->d_scal : nullptr);
+  h->solve_launches = 2 + 2 * (int64_t)P.waves.size();
   CK(cudaEventRecord(h->ev[7], st));
   CK(cudaGetLastError());
   return RVG_OK;
@@ -1513,6 +1674,28 @@ rvg_status rvg_timings(rvg_handle* h, double out7[7]) {
   return RVG_OK;
 }
 
+rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  h->profiling = enable != 0;
+  return RVG_OK;
+}
+
+rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
+  if (!h || !o) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  o->factor_ms = h->t_factor;
+  o->solve_ms = h->t_solve;
+  o->assembly_ms = h->t_assembly;
+  o->dense_ms = h->t_kernel;
+  o->cbgemm_ms = h->t_gemm;
+  o->syrk_ms = h->syrk_ms;
+  o->syrk_flops = h->syrk_flops;
+  o->syrk_launches = h->syrk_launches;
+  o->factor_launches = h->factor_launches;
+  o->solve_launches = h->solve_launches;
+  o->peak_bytes = h->peak_bytes;
+  return RVG_OK;
+}
+
 rvg_status rvg_stream(rvg_handle* h, void** s) {
   if (!h || !s) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
   *s = (void*)h->st;
@@ -1527,10 +1710,11 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
   if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->h_counts) cudaFreeHost(h->h_counts);
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
   for (auto& e : h->ev) if (e) cudaEventDestroy(e);
   delete h;
 }

@@ -49,13 +49,15 @@ class FactorOptions:
     small_leaf_threshold: int = 256
     failed_pivot_tpp: bool = True
     fallback_bunch_kaufman: bool = True
+    large_front_threshold: int = 2048  # B200 scheduling only; results do not depend on it
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
                                  outer_block_size=self.outer_block_size, inner_block_size=self.inner_block_size,
                                  nemin=self.nemin, small_leaf_threshold=self.small_leaf_threshold,
                                  failed_pivot_tpp=int(self.failed_pivot_tpp),
-                                 fallback_bk=int(self.fallback_bunch_kaufman))
+                                 fallback_bk=int(self.fallback_bunch_kaufman),
+                                 large_front_threshold=self.large_front_threshold)
 
 
 class SparseError(RuntimeError):
@@ -262,6 +264,16 @@ class SparseLDLT:
         out = np.zeros(7)
         _check(N.lib().rvg_timings(self._handle, N.ptr(out, N.dp)))
         return dict(assembly_ms=out[0], kernel_ms=out[1], gemm_ms=out[2], factor_ms=out[3], solve_ms=out[4])
+
+    def set_profiling(self, enable: bool = True):
+        if self._handle is None:
+            self._ensure_handle(self._opts or FactorOptions())
+        _check(N.lib().rvg_set_profiling(self._handle, int(enable)))
+
+    def profile(self):
+        p = N.Profile()
+        _check(N.lib().rvg_get_profile(self._handle, C.byref(p)))
+        return p.as_dict()
 
     def stream(self) -> int:
         s = C.c_void_p()

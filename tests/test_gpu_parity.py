@@ -146,3 +146,34 @@ def test_errors(rv):
         solver.solve(np.ones(s.n + 1))
     with pytest.raises(rv.DimensionMismatch):
         solver.factor(np.ones(3))
+
+
+# ---- the multi-kernel large-front path, forced onto small fronts ----------
+LARGE = dict(large_front_threshold=33)
+
+
+@pytest.mark.parametrize("n", [48, 100, 257, 300, 520, 700])
+@pytest.mark.parametrize("kind", ["plain", "delay", "singular"])
+def test_large_front_path_dense(rv, orc, n, kind):
+    s = dense_system(rv, n, n + 1, kind)
+    solver, ref, b = run_both(rv, orc, s, **LARGE)
+    assert_parity(rv, s, solver, ref, b, bwd=1e-8 if kind == "singular" else 1e-13)
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(outer_block_size=64), dict(outer_block_size=32),
+                                  dict(small_leaf_threshold=0, nemin=8)])
+def test_large_front_path_sparse(rv, orc, opts):
+    o = dict(LARGE)
+    o.update(opts)
+    for s in (rv.problems.shifted_laplacian(14, 0.1), rv.problems.kkt(7, seed=3)):
+        solver, ref, b = run_both(rv, orc, s, **o)
+        assert solver.inertia() == s.inertia
+        assert_parity(rv, s, solver, ref, b)
+
+
+def test_large_front_path_nfs_gemm(rv, orc):
+    # fronts with >= 256 NFS rows take the syrk contribution GEMM
+    s = rv.problems.kkt(10, seed=1)
+    solver, ref, b = run_both(rv, orc, s, large_front_threshold=300)
+    assert solver.inertia() == s.inertia
+    assert_parity(rv, s, solver, ref, b)

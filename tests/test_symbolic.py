@@ -36,12 +36,15 @@ def test_supernodes_match_brute_force(rv, n, density, seed):
     sym = rv.symbolic_analyze(n, s.colptr, s.rowidx, order)
     assert sorted(sym.perm_fwd.tolist()) == list(range(n))
     cols, parent = brute_force_structure(s.to_scipy(), sym.perm_fwd)
-    # every column's structure equals its supernode's columns below it plus the pattern
+    # relaxed supernodes: every column's structure lies inside its supernode's
+    # columns below it plus the pattern, and the pattern is exactly the
+    # structure of the last column
     for sidx in range(sym.sup_begin.size):
         b, e = sym.sup_begin[sidx], sym.sup_end[sidx]
         pat = set(sym.pat_idx[sym.pat_ptr[sidx]:sym.pat_ptr[sidx + 1]].tolist())
         for j in range(b, e):
-            assert cols[j] == set(range(j + 1, e)) | pat, (sidx, j)
+            assert cols[j] <= set(range(j + 1, e)) | pat, (sidx, j)
+        assert cols[e - 1] == pat
         # parent supernode holds etree parent of the last column
         p = parent[e - 1]
         if p == -1:
