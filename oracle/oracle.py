@@ -25,7 +25,9 @@ class OrcOptions(C.Structure):
 
 
 def options(threshold=0.01, small=1e-20, outer_block_size=256, inner_block_size=32, nemin=32,
-            small_leaf_threshold=256, failed_pivot_tpp=True, fallback_bunch_kaufman=True):
+            small_leaf_threshold=256, failed_pivot_tpp=True, fallback_bunch_kaufman=True, **device_only):
+    # device_only: scheduling options of the GPU path (e.g. large_front_threshold)
+    # that do not change results and have no meaning for the oracle
     return OrcOptions(threshold, small, outer_block_size, inner_block_size, nemin, small_leaf_threshold,
                       int(failed_pivot_tpp), int(fallback_bunch_kaufman))
 

@@ -11,10 +11,12 @@
 // (compute_contribution_gemm, factor.rs:1590-1652).
 //
 // sm_100a has no FP64 tcgen05 kind, so this is a register-blocked SIMT DFMA
-// kernel: 128 x 128 CTA tile, 256 threads, 8 x 8 outputs per thread (rows
-// tx + 16a, columns ty + 16b so C loads and stores coalesce along columns),
-// K staged through shared memory in chunks of 16 with a register-prefetched
-// double buffer.  Each output keeps one fma chain in K order, so the result is
+// kernel: 128 x 128 CTA tile, 256 threads (one CTA per SM: the 64 FP64
+// accumulators of a thread take 128 registers), 8 x 8 outputs per thread
+// (rows tx + 16a, columns ty + 16b so C loads and stores coalesce along
+// columns), K staged through shared memory in chunks of 16 by cp.async in a
+// three-stage pipeline (8-byte copies: panel leading dimensions are odd in
+// general; out-of-range elements are zero-filled by the copy itself).  Each output keeps one fma chain in K order, so the result is
 // bit-identical to the oracle's per-entry loop.
 #pragma once
 #include <cstdint>
@@ -22,7 +24,7 @@
 
 namespace rvg {
 
-constexpr int G_BM = 128, G_BN = 128, G_BK = 16, G_T = 256;
+constexpr int G_BM = 128, G_BN = 128, G_BK = 16, G_T = 256, G_STAGES = 3;
 
 struct SyrkArgs {
   double* C;
@@ -36,79 +38,99 @@ struct SyrkArgs {
   const int32_t* Kdev;  // when set, K is read from device memory
 };
 
-constexpr size_t G_SMEM = 2 * 2 * G_BK * G_BM * sizeof(double);  // 64 KB, dynamic
+// dynamic shared memory: G_STAGES x (W chunk + L chunk)
+constexpr size_t G_SMEM = (size_t)G_STAGES * 2 * G_BK * G_BM * sizeof(double);
 
-__global__ void __launch_bounds__(G_T, 2) k_syrk_lower(SyrkArgs a) {
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  int n = valid ? 8 : 0;  // 0 source bytes: the 8 destination bytes are zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__global__ void __launch_bounds__(G_T, 1) k_syrk_lower(SyrkArgs a) {
   const int64_t i0 = a.r0 + (int64_t)blockIdx.y * G_BM;
   const int64_t j0 = a.c0 + (int64_t)blockIdx.x * G_BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
   if (i0 + G_BM - 1 < j0) return;  // tile entirely above the diagonal
-  if (a.Kdev) a.K = *a.Kdev;
+  const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
   extern __shared__ double gsm[];
-  double(*sW)[G_BK][G_BM] = reinterpret_cast<double(*)[G_BK][G_BM]>(gsm);
-  double(*sL)[G_BK][G_BN] = reinterpret_cast<double(*)[G_BK][G_BN]>(gsm + 2 * G_BK * G_BM);
+  // stage s: W chunk at gsm + s*2*BK*BM, L chunk right after; layout [k][row]
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
+  const int64_t nchunk = (K + G_BK - 1) / G_BK;
+  auto issue = [&](int64_t ch) {
+    double* sw = gsm + (ch % G_STAGES) * 2 * G_BK * G_BM;
+    double* sl = sw + G_BK * G_BM;
+    const int64_t k0 = ch * G_BK;
+#pragma unroll
+    for (int e = 0; e < (G_BK * G_BM) / G_T; ++e) {
+      const int idx = tid + G_T * e;
+      const int r = idx & (G_BM - 1), k = idx >> 7;
+      const int64_t kk = k0 + k, i = i0 + r, j = j0 + r;
+      const bool kv = kk < K;
+      const bool wv = kv && i < a.r1, lv = kv && j < a.c1;
+      cp_async8(sw + k * G_BM + r, wv ? a.W + (i - a.r0) + kk * a.ldw : a.W, wv);
+      cp_async8(sl + k * G_BN + r, lv ? a.L + j + kk * a.ldl : a.L, lv);
+    }
+  };
+  // prologue: up to G_STAGES - 1 chunks in flight
+#pragma unroll
+  for (int s = 0; s < G_STAGES - 1; ++s) {
+    if (s < nchunk) issue(s);
+    cp_async_commit();
+  }
   double acc[8][8];
 #pragma unroll
   for (int x = 0; x < 8; ++x)
 #pragma unroll
     for (int y = 0; y < 8; ++y) {
-      int64_t i = i0 + tx + 16 * x, j = j0 + ty + 16 * y;
+      const int64_t i = i0 + tx + 16 * x, j = j0 + ty + 16 * y;
       acc[x][y] = (i < a.r1 && j < a.c1 && i >= j) ? a.C[i + j * a.ldc] : 0.0;
     }
-  // loader: element e (0..2047) of a 128 x 16 chunk -> row e % 128, k e / 128
-  double pw[8], pl[8];
-  auto load = [&](int64_t k0) {
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      int idx = tid + G_T * e;
-      int r = idx & (G_BM - 1), k = idx >> 7;
-      int64_t kk = k0 + k;
-      int64_t i = i0 + r, j = j0 + r;
-      pw[e] = (i < a.r1 && kk < a.K) ? a.W[(i - a.r0) + kk * a.ldw] : 0.0;
-      pl[e] = (j < a.c1 && kk < a.K) ? a.L[j + kk * a.ldl] : 0.0;
-    }
-  };
-  auto store = [&](int buf) {
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      int idx = tid + G_T * e;
-      int r = idx & (G_BM - 1), k = idx >> 7;
-      sW[buf][k][r] = pw[e];
-      sL[buf][k][r] = pl[e];
-    }
-  };
-  const int64_t nchunk = (a.K + G_BK - 1) / G_BK;
-  if (nchunk > 0) {
-    load(0);
-    store(0);
-  }
-  __syncthreads();
   for (int64_t ch = 0; ch < nchunk; ++ch) {
-    const int buf = (int)(ch & 1);
-    if (ch + 1 < nchunk) load((ch + 1) * G_BK);
-    const int kc = (int)((a.K - ch * G_BK) < G_BK ? (a.K - ch * G_BK) : G_BK);
-#pragma unroll 4
-    for (int k = 0; k < kc; ++k) {
-      double wv[8], lv[8];
+    cp_async_wait<G_STAGES - 2>();  // chunk ch has landed
+    __syncthreads();                // ... for every thread, and chunk ch-1's buffer is free
+    if (ch + G_STAGES - 1 < nchunk) issue(ch + G_STAGES - 1);
+    cp_async_commit();
+    const double* sw = gsm + (ch % G_STAGES) * 2 * G_BK * G_BM;
+    const double* sl = sw + G_BK * G_BM;
+    const int kc = (int)((K - ch * G_BK) < G_BK ? (K - ch * G_BK) : G_BK);
+    if (kc == G_BK) {
 #pragma unroll
-      for (int x = 0; x < 8; ++x) wv[x] = -sW[buf][k][tx + 16 * x];
+      for (int k = 0; k < G_BK; ++k) {
+        double wv[8], lv[8];
 #pragma unroll
-      for (int y = 0; y < 8; ++y) lv[y] = sL[buf][k][ty + 16 * y];
+        for (int x = 0; x < 8; ++x) wv[x] = -sw[k * G_BM + tx + 16 * x];
 #pragma unroll
-      for (int x = 0; x < 8; ++x)
+        for (int y = 0; y < 8; ++y) lv[y] = sl[k * G_BN + ty + 16 * y];
 #pragma unroll
-        for (int y = 0; y < 8; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
+        for (int x = 0; x < 8; ++x)
+#pragma unroll
+          for (int y = 0; y < 8; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
+      }
+    } else {
+      for (int k = 0; k < kc; ++k) {
+        double wv[8], lv[8];
+#pragma unroll
+        for (int x = 0; x < 8; ++x) wv[x] = -sw[k * G_BM + tx + 16 * x];
+#pragma unroll
+        for (int y = 0; y < 8; ++y) lv[y] = sl[k * G_BN + ty + 16 * y];
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+#pragma unroll
+          for (int y = 0; y < 8; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
+      }
     }
-    if (ch + 1 < nchunk) store(buf ^ 1);
-    __syncthreads();
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int x = 0; x < 8; ++x)
 #pragma unroll
     for (int y = 0; y < 8; ++y) {
-      int64_t i = i0 + tx + 16 * x, j = j0 + ty + 16 * y;
+      const int64_t i = i0 + tx + 16 * x, j = j0 + ty + 16 * y;
       if (i < a.r1 && j < a.c1 && i >= j) a.C[i + j * a.ldc] = acc[x][y];
     }
 }

@@ -502,17 +502,18 @@ __device__ int cta_factor_inner(CtaShared& sh, PanelView V, int64_t bm, int pl, 
     if (nelim > 0) {
       for (int64_t i = tid; i < tsz; i += NT) row_ld(&V(ts + i, k), V.ld, sh, nelim, W + i * IBMAX);
       __syncthreads();
+      // columns are independent: no barrier between them; L[j, :] is a
+      // warp-uniform (broadcast) read
       for (int64_t j = ts; j < nfsb; ++j) {
-        if (tid < nelim) sh.Lj[tid] = V(j, k + tid);
-        __syncthreads();
+        const double* lj = &V(j, k);
         for (int64_t i = j + tid; i < bm; i += NT) {
           const double* w = W + (i - ts) * IBMAX;
           double acc = V(i, j);
-          for (int c = 0; c < nelim; ++c) acc = __fma_rn(-w[c], sh.Lj[c], acc);
+          for (int c = 0; c < nelim; ++c) acc = __fma_rn(-w[c], lj[c * V.ld], acc);
           V(i, j) = acc;
         }
-        __syncthreads();
       }
+      __syncthreads();
       if (nelim < bs) {
         const int nf = bs - nelim;
         // failed x failed, and trailing x failed; W_blk from the failed rows
@@ -526,16 +527,15 @@ __device__ int cta_factor_inner(CtaShared& sh, PanelView V, int64_t bm, int pl, 
           V(k + nelim + i, k + nelim + j) = __dsub_rn(V(k + nelim + i, k + nelim + j), s);
         }
         for (int j = 0; j < nf; ++j) {
-          if (tid < nelim) sh.Lj[tid] = V(k + nelim + j, k + tid);
-          __syncthreads();
+          const double* lj = &V(k + nelim + j, k);
           for (int64_t i = tid; i < tsz; i += NT) {
             const double* w = W + i * IBMAX;
             double s = 0.0;
-            for (int c = 0; c < nelim; ++c) s = __dadd_rn(s, __dmul_rn(w[c], sh.Lj[c]));
+            for (int c = 0; c < nelim; ++c) s = __dadd_rn(s, __dmul_rn(w[c], lj[c * V.ld]));
             V(ts + i, k + nelim + j) = __dsub_rn(V(ts + i, k + nelim + j), s);
           }
-          __syncthreads();
         }
+        __syncthreads();
       }
     }
     // 11. D entries and counts for the passed columns
@@ -665,6 +665,7 @@ __global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* 
 
 #include "gemm64.cuh"
 #include "large.cuh"
+#include "solve_large.cuh"
 
 namespace rvg {
 
@@ -1476,6 +1477,8 @@ rvg_status rvg_factor_device(rvg_handle* h, const double* d_values, const double
   return (rvg_status)factor_common(h, d_values, h->has_scaling ? h->d_scal : nullptr);
 }
 
+static bool solve_is_large(const DFront& f) { return (int64_t)f.ne * (int64_t)f.m >= (1 << 18); }
+
 static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb) {
   Plan& P = h->P;
   const int64_t n = P.n;
@@ -1483,39 +1486,95 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   if (n == 0 || nrhs == 0) return RVG_OK;
   int rc = ensure(h->d_x, h->x_cap, (size_t)(n * nrhs), st);
   if (rc) return rc;
-  // per-front solve workspace: m doubles each
+  // per-front solve workspace: m doubles (+ the partial sums of large fronts)
   int64_t wneed = 0;
   std::vector<DFront> fr = h->h_fronts;
-  for (auto& f : fr) { f.scratch = wneed; wneed += f.m; }
+  for (auto& f : fr) { f.scratch = wneed; wneed += f.m + (solve_is_large(f) ? LS_RS * LS_B : 0); }
   if ((rc = ensure(h->solve_work, h->solve_work_cap, (size_t)std::max<int64_t>(wneed, 1), st))) return rc;
   CK(cudaMemcpyAsync(h->d_fronts, fr.data(), fr.size() * sizeof(DFront), cudaMemcpyHostToDevice, st));
   Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, nullptr};
   CK(cudaEventRecord(h->ev[6], st));
+  int64_t launches = 0;
   int64_t tot = n * nrhs;
   k_perm_scale_in<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
                                                                  h->has_scaling ? h->d_scal : nullptr);
-  // wave lists, packed once per solve
+  launches++;
+  // wave lists of the batched (small) fronts, packed once per solve
   Packer pk;
   std::vector<size_t> off(P.waves.size());
+  std::vector<int> cnt(P.waves.size());
+  std::vector<std::vector<int64_t>> large(P.waves.size());
   for (size_t w = 0; w < P.waves.size(); ++w) {
-    std::vector<int32_t> ids(P.waves[w].begin(), P.waves[w].end());
+    std::vector<int32_t> ids;
+    for (int64_t s : P.waves[w]) {
+      if (fr[s].ne == 0) continue;
+      if (solve_is_large(fr[s])) large[w].push_back(s); else ids.push_back((int32_t)s);
+    }
+    cnt[w] = (int)ids.size();
     off[w] = pk.add(ids);
   }
   if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size() + 16, st))) return rc;
   if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size() + 16))) return rc;
   std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
   CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
-  for (size_t w = 0; w < P.waves.size(); ++w)
-    k_solve_fwd<<<(unsigned)P.waves[w].size(), 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]),
-                                                             (int)P.waves[w].size(), h->d_fronts, A, h->d_x, n, nrhs,
-                                                             h->solve_work);
-  for (size_t w = P.waves.size(); w-- > 0;)
-    k_solve_bwd<<<(unsigned)P.waves[w].size(), 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]),
-                                                             (int)P.waves[w].size(), h->d_fronts, A, h->d_x, n, nrhs,
-                                                             h->solve_work);
+  auto ls_args = [&](int64_t s, int64_t rh) {
+    const DFront& f = fr[s];
+    LSArgs a;
+    a.L = h->panel + f.panel;
+    a.m = f.m; a.k = f.k; a.ne = f.ne;
+    a.rows = h->idx + f.idx;
+    a.perm = a.rows + f.m;
+    a.dt = h->dtype + f.dpos; a.dd = h->ddiag + f.dpos; a.dof = h->doff + f.dpos;
+    a.v = h->solve_work + f.scratch;
+    a.part = a.v + f.m;
+    a.x = h->d_x + rh * n;
+    return a;
+  };
+  for (size_t w = 0; w < P.waves.size(); ++w) {
+    if (cnt[w]) {
+      k_solve_fwd<<<(unsigned)cnt[w], 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]), cnt[w], h->d_fronts, A,
+                                                    h->d_x, n, nrhs, h->solve_work);
+      launches++;
+    }
+    for (int64_t s : large[w])
+      for (int64_t rh = 0; rh < nrhs; ++rh) {
+        LSArgs a = ls_args(s, rh);
+        k_lsf_gather<<<blocks_for(a.m, 256), 256, 0, st>>>(a);
+        for (int64_t b0 = 0; b0 < a.ne; b0 += LS_B) {
+          const int64_t b1 = std::min<int64_t>(a.ne, b0 + LS_B);
+          k_lsf_diag<<<1, 32, 0, st>>>(a, b0);
+          if (a.m > b1) k_lsf_update<<<blocks_for(a.m - b1, 256), 256, 0, st>>>(a, b0);
+          launches += 2;
+        }
+        k_lsf_finish<<<blocks_for(a.m, 256), 256, 0, st>>>(a);
+        launches += 2;
+      }
+  }
+  for (size_t w = P.waves.size(); w-- > 0;) {
+    for (int64_t s : large[w])
+      for (int64_t rh = 0; rh < nrhs; ++rh) {
+        LSArgs a = ls_args(s, rh);
+        k_lsb_gather<<<blocks_for(a.m, 256), 256, 0, st>>>(a);
+        const int64_t nblk = (a.ne + LS_B - 1) / LS_B;
+        for (int64_t bi = nblk - 1; bi >= 0; --bi) {
+          const int64_t b0 = bi * LS_B;
+          k_lsb_dot<<<dim3(LS_B, LS_RS), 256, 0, st>>>(a, b0);
+          k_lsb_diag<<<1, 32, 0, st>>>(a, b0);
+          launches += 2;
+        }
+        k_lsb_scatter<<<blocks_for(a.ne, 256), 256, 0, st>>>(a);
+        launches += 2;
+      }
+    if (cnt[w]) {
+      k_solve_bwd<<<(unsigned)cnt[w], 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]), cnt[w], h->d_fronts, A,
+                                                    h->d_x, n, nrhs, h->solve_work);
+      launches++;
+    }
+  }
   k_perm_scale_out<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
                                                                   h->has_scaling ? h->d_scal : nullptr);
-  h->solve_launches = 2 + 2 * (int64_t)P.waves.size();
+  launches++;
+  h->solve_launches = launches;
   CK(cudaEventRecord(h->ev[7], st));
   CK(cudaGetLastError());
   return RVG_OK;
