@@ -254,11 +254,14 @@ def main():
     barrier()
     clocks = ClockSampler()
     times, syrk_ms, syrk_flops, syrk_launch, launches = [], 0.0, 0.0, 0, 0
+    walls = []
     for _ in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
             e0.record(stream)
+        w0 = time.perf_counter()
         step()
+        walls.append(time.perf_counter() - w0)
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()
@@ -319,7 +322,9 @@ def main():
                                         "measured-peaks file)",
                          "launches_per_step": syrk_launch // max(args.steps, 1),
                          "share_of_step": (syrk_ms / args.steps * 1e-3) / t_step if t_step else None},
-            "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms")},
+            "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
+                                               "host_total_ms", "host_alloc_ms", "host_sync_ms")},
+            "step_wall_s": walls, "step_event_s": times,
             "peak_device_bytes": prof["peak_bytes"],
             "clocks": clk,
             "cpu_baseline": cb,

@@ -154,6 +154,9 @@ typedef struct {
   int64_t syrk_launches;
   int64_t factor_launches, solve_launches;
   int64_t peak_bytes;
+  /* host wall time of the last factor: total, in allocation calls, waiting
+   * in stream synchronisations */
+  double host_total_ms, host_alloc_ms, host_sync_ms;
 } rvg_profile;
 rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable);
 rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* out);

@@ -45,7 +45,8 @@ class Profile(C.Structure):
     _fields_ = [("factor_ms", C.c_double), ("solve_ms", C.c_double), ("assembly_ms", C.c_double),
                 ("dense_ms", C.c_double), ("cbgemm_ms", C.c_double), ("syrk_ms", C.c_double),
                 ("syrk_flops", C.c_double), ("syrk_launches", i64), ("factor_launches", i64),
-                ("solve_launches", i64), ("peak_bytes", i64)]
+                ("solve_launches", i64), ("peak_bytes", i64), ("host_total_ms", C.c_double),
+                ("host_alloc_ms", C.c_double), ("host_sync_ms", C.c_double)]
 
     def as_dict(self):
         return {k: (float(getattr(self, k)) if t is C.c_double else int(getattr(self, k))) for k, t in self._fields_}

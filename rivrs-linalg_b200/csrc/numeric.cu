@@ -946,12 +946,17 @@ struct rvg_handle {
   double syrk_flops = 0, syrk_ms = 0;
   int64_t syrk_launches = 0, launches = 0, factor_launches = 0, solve_launches = 0;
   int64_t arena_bytes = 0, peak_bytes = 0;
+  double host_alloc_ms = 0, host_sync_ms = 0, host_total_ms = 0;
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
   double t_assembly = 0, t_kernel = 0, t_gemm = 0, t_factor = 0, t_solve = 0, t_dom = 0, n_dom = 0;
 };
 
 namespace {
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 template <class T>
 int ensure(T*& p, size_t& cap, size_t need, cudaStream_t st) {
@@ -1116,7 +1121,11 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
     CK(cudaGetLastError());
     int32_t g = 0;
     CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    {
+      double ts0 = now_ms();
+      CK(cudaStreamSynchronize(st));
+      h->host_sync_ms += now_ms() - ts0;
+    }
     if (syrk) h->syrk_flops += 2.0 * (double)(g - gne) * lower_entries(oe, m, oe, p);
     gne = g;
     rem -= bcols;
@@ -1143,6 +1152,9 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   const int ib = (int)h->opt.inner_block_size;
   double t_asm = 0, t_ker = 0, t_gem = 0;
   int rc;
+  const double t_start = now_ms();
+  h->host_alloc_ms = 0;
+  h->host_sync_ms = 0;
   h->ev_used = 0;
   h->syrk_flops = 0;
   h->syrk_ms = 0;
@@ -1183,6 +1195,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
       f.scratch = scratch_need; scratch_need += sc;
     }
+    double ta = now_ms();
     if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st))) return rc;
     if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx_used + idx_need), st))) return rc;
     if ((rc = ensure_d_arrays(h, (size_t)(d_used + d_need)))) return rc;
@@ -1192,6 +1205,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       CK(cudaMallocAsync((void**)&cb_block[w], (size_t)cb_need * 8, st));
       CK(cudaMemsetAsync(cb_block[w], 0, (size_t)cb_need * 8, st));
     }
+    h->host_alloc_ms += now_ms() - ta;
     {
       int64_t off = 0;
       for (int64_t s : wave) {
@@ -1302,7 +1316,11 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4) * 4))) return rc;
     CK(cudaMemcpyAsync(h->h_counts, D + o_cnt, (size_t)3 * nw * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaFreeAsync(scratch, st));
-    CK(cudaStreamSynchronize(st));
+    {
+      double ts0 = now_ms();
+      CK(cudaStreamSynchronize(st));
+      h->host_sync_ms += now_ms() - ts0;
+    }
     for (int i = 0; i < nw; ++i) {
       DFront& f = h->h_fronts[wave[i]];
       f.ne = h->h_counts[3 * i]; f.n1 = h->h_counts[3 * i + 1]; f.n2 = h->h_counts[3 * i + 2];
@@ -1338,6 +1356,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   cudaEventElapsedTime(&tot, h->ev[0], h->ev[5]);
   h->t_assembly = t_asm; h->t_kernel = t_ker; h->t_gemm = t_gem; h->t_factor = tot;
   h->factor_launches = h->launches;
+  h->host_total_ms = now_ms() - t_start;
   if (h->profiling)
     for (size_t e = 0; e + 1 < h->ev_used; e += 2) {
       float ms = 0;
@@ -1752,6 +1771,9 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
   o->factor_launches = h->factor_launches;
   o->solve_launches = h->solve_launches;
   o->peak_bytes = h->peak_bytes;
+  o->host_total_ms = h->host_total_ms;
+  o->host_alloc_ms = h->host_alloc_ms;
+  o->host_sync_ms = h->host_sync_ms;
   return RVG_OK;
 }
 
