@@ -24,7 +24,7 @@
 
 namespace rvg {
 
-constexpr int G_BM = 128, G_BN = 128, G_BK = 16, G_T = 256, G_STAGES = 3;
+constexpr int G_BK = 16, G_STAGES = 3;
 
 struct SyrkArgs {
   double* C;
@@ -38,9 +38,6 @@ struct SyrkArgs {
   const int32_t* Kdev;  // when set, K is read from device memory
 };
 
-// dynamic shared memory: G_STAGES x (W chunk + L chunk)
-constexpr size_t G_SMEM = (size_t)G_STAGES * 2 * G_BK * G_BM * sizeof(double);
-
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
   unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   int n = valid ? 8 : 0;  // 0 source bytes: the 8 destination bytes are zero-filled
@@ -50,44 +47,61 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-__global__ void __launch_bounds__(G_T, 1) k_syrk_lower(SyrkArgs a) {
-  const int64_t i0 = a.r0 + (int64_t)blockIdx.y * G_BM;
-  const int64_t j0 = a.c0 + (int64_t)blockIdx.x * G_BN;
+// NT threads; thread (tx = tid % 16, ty = tid / 16) owns rows tx + 16x
+// (x < TM) and columns ty + (NT/16) y (y < TN) of a (16 TM) x ((NT/16) TN)
+// tile.
+template <int NT, int TM, int TN>
+struct SyrkCfg {
+  static constexpr int BM = 16 * TM, BN = (NT / 16) * TN, CSTR = NT / 16;
+  static constexpr size_t SMEM = (size_t)G_STAGES * G_BK * (BM + BN) * sizeof(double);
+};
+
+template <int NT, int TM, int TN, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_syrk_lower_t(SyrkArgs a) {
+  using Cfg = SyrkCfg<NT, TM, TN>;
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, CS = Cfg::CSTR;
+  const int64_t i0 = a.r0 + (int64_t)blockIdx.y * BM;
+  const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
-  if (i0 + G_BM - 1 < j0) return;  // tile entirely above the diagonal
+  if (i0 + BM - 1 < j0) return;  // tile entirely above the diagonal
   const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
   extern __shared__ double gsm[];
-  // stage s: W chunk at gsm + s*2*BK*BM, L chunk right after; layout [k][row]
+  // stage s: W chunk [k][BM] then L chunk [k][BN]
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
   const int64_t nchunk = (K + G_BK - 1) / G_BK;
   auto issue = [&](int64_t ch) {
-    double* sw = gsm + (ch % G_STAGES) * 2 * G_BK * G_BM;
-    double* sl = sw + G_BK * G_BM;
+    double* sw = gsm + (ch % G_STAGES) * G_BK * (BM + BN);
+    double* sl = sw + G_BK * BM;
     const int64_t k0 = ch * G_BK;
 #pragma unroll
-    for (int e = 0; e < (G_BK * G_BM) / G_T; ++e) {
-      const int idx = tid + G_T * e;
-      const int r = idx & (G_BM - 1), k = idx >> 7;
-      const int64_t kk = k0 + k, i = i0 + r, j = j0 + r;
-      const bool kv = kk < K;
-      const bool wv = kv && i < a.r1, lv = kv && j < a.c1;
-      cp_async8(sw + k * G_BM + r, wv ? a.W + (i - a.r0) + kk * a.ldw : a.W, wv);
-      cp_async8(sl + k * G_BN + r, lv ? a.L + j + kk * a.ldl : a.L, lv);
+    for (int e = 0; e < (G_BK * BM) / NT; ++e) {
+      const int idx = tid + NT * e;
+      const int r = idx % BM, k = idx / BM;
+      const int64_t kk = k0 + k, i = i0 + r;
+      const bool v = kk < K && i < a.r1;
+      cp_async8(sw + k * BM + r, v ? a.W + (i - a.r0) + kk * a.ldw : a.W, v);
+    }
+#pragma unroll
+    for (int e = 0; e < (G_BK * BN) / NT; ++e) {
+      const int idx = tid + NT * e;
+      const int r = idx % BN, k = idx / BN;
+      const int64_t kk = k0 + k, j = j0 + r;
+      const bool v = kk < K && j < a.c1;
+      cp_async8(sl + k * BN + r, v ? a.L + j + kk * a.ldl : a.L, v);
     }
   };
-  // prologue: up to G_STAGES - 1 chunks in flight
 #pragma unroll
   for (int s = 0; s < G_STAGES - 1; ++s) {
     if (s < nchunk) issue(s);
     cp_async_commit();
   }
-  double acc[8][8];
+  double acc[TM][TN];
 #pragma unroll
-  for (int x = 0; x < 8; ++x)
+  for (int x = 0; x < TM; ++x)
 #pragma unroll
-    for (int y = 0; y < 8; ++y) {
-      const int64_t i = i0 + tx + 16 * x, j = j0 + ty + 16 * y;
+    for (int y = 0; y < TN; ++y) {
+      const int64_t i = i0 + tx + 16 * x, j = j0 + ty + CS * y;
       acc[x][y] = (i < a.r1 && j < a.c1 && i >= j) ? a.C[i + j * a.ldc] : 0.0;
     }
   for (int64_t ch = 0; ch < nchunk; ++ch) {
@@ -95,49 +109,63 @@ __global__ void __launch_bounds__(G_T, 1) k_syrk_lower(SyrkArgs a) {
     __syncthreads();                // ... for every thread, and chunk ch-1's buffer is free
     if (ch + G_STAGES - 1 < nchunk) issue(ch + G_STAGES - 1);
     cp_async_commit();
-    const double* sw = gsm + (ch % G_STAGES) * 2 * G_BK * G_BM;
-    const double* sl = sw + G_BK * G_BM;
+    const double* sw = gsm + (ch % G_STAGES) * G_BK * (BM + BN);
+    const double* sl = sw + G_BK * BM;
     const int kc = (int)((K - ch * G_BK) < G_BK ? (K - ch * G_BK) : G_BK);
     if (kc == G_BK) {
 #pragma unroll
       for (int k = 0; k < G_BK; ++k) {
-        double wv[8], lv[8];
+        double wv[TM], lv[TN];
 #pragma unroll
-        for (int x = 0; x < 8; ++x) wv[x] = -sw[k * G_BM + tx + 16 * x];
+        for (int x = 0; x < TM; ++x) wv[x] = -sw[k * BM + tx + 16 * x];
 #pragma unroll
-        for (int y = 0; y < 8; ++y) lv[y] = sl[k * G_BN + ty + 16 * y];
+        for (int y = 0; y < TN; ++y) lv[y] = sl[k * BN + ty + CS * y];
 #pragma unroll
-        for (int x = 0; x < 8; ++x)
+        for (int x = 0; x < TM; ++x)
 #pragma unroll
-          for (int y = 0; y < 8; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
+          for (int y = 0; y < TN; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
       }
     } else {
       for (int k = 0; k < kc; ++k) {
-        double wv[8], lv[8];
+        double wv[TM], lv[TN];
 #pragma unroll
-        for (int x = 0; x < 8; ++x) wv[x] = -sw[k * G_BM + tx + 16 * x];
+        for (int x = 0; x < TM; ++x) wv[x] = -sw[k * BM + tx + 16 * x];
 #pragma unroll
-        for (int y = 0; y < 8; ++y) lv[y] = sl[k * G_BN + ty + 16 * y];
+        for (int y = 0; y < TN; ++y) lv[y] = sl[k * BN + ty + CS * y];
 #pragma unroll
-        for (int x = 0; x < 8; ++x)
+        for (int x = 0; x < TM; ++x)
 #pragma unroll
-          for (int y = 0; y < 8; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
+          for (int y = 0; y < TN; ++y) acc[x][y] = __fma_rn(wv[x], lv[y], acc[x][y]);
       }
     }
   }
   cp_async_wait<0>();
 #pragma unroll
-  for (int x = 0; x < 8; ++x)
+  for (int x = 0; x < TM; ++x)
 #pragma unroll
-    for (int y = 0; y < 8; ++y) {
-      const int64_t i = i0 + tx + 16 * x, j = j0 + ty + 16 * y;
+    for (int y = 0; y < TN; ++y) {
+      const int64_t i = i0 + tx + 16 * x, j = j0 + ty + CS * y;
       if (i < a.r1 && j < a.c1 && i >= j) a.C[i + j * a.ldc] = acc[x][y];
     }
 }
 
-inline dim3 syrk_grid(const SyrkArgs& a) {
-  int64_t nr = (a.r1 - a.r0 + G_BM - 1) / G_BM, nc = (a.c1 - a.c0 + G_BN - 1) / G_BN;
+// the configuration used by the library
+#ifndef RVG_SYRK_NT
+#define RVG_SYRK_NT 256
+#define RVG_SYRK_TM 8
+#define RVG_SYRK_TN 8
+#define RVG_SYRK_MINB 1
+#endif
+using SyrkMain = SyrkCfg<RVG_SYRK_NT, RVG_SYRK_TM, RVG_SYRK_TN>;
+constexpr int G_T = RVG_SYRK_NT;
+constexpr size_t G_SMEM = SyrkMain::SMEM;
+#define k_syrk_lower k_syrk_lower_t<RVG_SYRK_NT, RVG_SYRK_TM, RVG_SYRK_TN, RVG_SYRK_MINB>
+
+template <class Cfg>
+inline dim3 syrk_grid_cfg(const SyrkArgs& a) {
+  int64_t nr = (a.r1 - a.r0 + Cfg::BM - 1) / Cfg::BM, nc = (a.c1 - a.c0 + Cfg::BN - 1) / Cfg::BN;
   return dim3((unsigned)(nc > 0 ? nc : 0), (unsigned)(nr > 0 ? nr : 0));
 }
+inline dim3 syrk_grid(const SyrkArgs& a) { return syrk_grid_cfg<SyrkMain>(a); }
 
 }  // namespace rvg

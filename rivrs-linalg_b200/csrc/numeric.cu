@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -67,7 +68,7 @@ struct DFront {
   int64_t idx;      // offset (int32) in the index arena: rows[m], perm[k]
   int64_t dpos;     // offset in the D arrays (k entries)
   int64_t scratch;  // offset (doubles) in the wave scratch
-  double* cb;       // NFS x NFS contribution block (ld nfs) or null
+  int64_t cb;       // offset (doubles) of the NFS x NFS contribution block (ld nfs) in the CB arena, -1 if none
   int32_t m, k, nown, ndin, nfs;
   int32_t ne, n1, n2;
   int32_t parent;
@@ -96,6 +97,7 @@ struct Arenas {
   double* ddiag;
   double* doff;
   double* scratch;
+  double* cbase;  // contribution-block arena
 };
 
 // ---------------------------------------------------------------------------
@@ -148,7 +150,7 @@ __global__ void k_scatter(const ScatterItem* items, const DFront* F, Statics S, 
     double* a = A.panel + fr.panel;
     a[r + (int64_t)c * fr.m] += v;
   } else if ((fr.flags & FF_HAS_CB) && r >= fr.k) {
-    fr.cb[(r - fr.k) + (int64_t)(c - fr.k) * fr.nfs] += v;
+    A.cbase[fr.cb + (r - fr.k) + (int64_t)(c - fr.k) * fr.nfs] += v;
   }
 }
 
@@ -182,13 +184,13 @@ __global__ void k_extend_add(const EaItem* items, const DFront* F, Statics S, Ar
         int64_t row = i < nd ? (C.ne + i) : (C.k + (i - nd));
         v = cp[row + (int64_t)(C.ne + j) * C.m];
       } else {
-        v = C.cb[(i - nd) + (int64_t)(j - nd) * C.nfs];
+        v = A.cbase[C.cb + (i - nd) + (int64_t)(j - nd) * C.nfs];
       }
       if (v == 0.0) continue;
       int li = map(i);
       int r = li >= lj ? li : lj, c = li >= lj ? lj : li;
       if (c < P.k) pp[r + (int64_t)c * P.m] += v;
-      else if ((P.flags & FF_HAS_CB) && r >= P.k) P.cb[(r - P.k) + (int64_t)(c - P.k) * P.nfs] += v;
+      else if ((P.flags & FF_HAS_CB) && r >= P.k) A.cbase[P.cb + (r - P.k) + (int64_t)(c - P.k) * P.nfs] += v;
     }
   }
 }
@@ -710,7 +712,7 @@ __global__ void __launch_bounds__(256) k_cb_gemm(const TileItem* items, const DF
   const int64_t nfs = fr.nfs, ne = fr.ne, ldl = fr.m;
   const double* L = A.panel + fr.panel + fr.k;  // L21_NFS(j, c) = L[j + c*ldl]
   const double* W = A.scratch + fr.scratch;     // W(i, c) = W[i + c*nfs]
-  double* C = fr.cb;
+  double* C = A.cbase + fr.cb;
   __shared__ double sW[GK][GT + 1];
   __shared__ double sL[GK][GT + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -938,6 +940,9 @@ struct rvg_handle {
   char* h_stage = nullptr; size_t h_stage_cap = 0; // pinned host mirror
   int32_t* h_counts = nullptr; size_t h_counts_cap = 0;
   LFState* d_lf = nullptr;                          // state of the large-front path
+  double* scratch = nullptr; size_t scratch_cap = 0; // per-wave scratch, persistent across factors
+  double* cb_arena = nullptr; size_t cb_cap = 0;     // contribution blocks, first-fit by wave
+  std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
   bool factored = false;
   // measurement
   bool profiling = false;
@@ -1002,6 +1007,63 @@ int ensure_d_arrays(rvg_handle* h, size_t need) {  // type / diag / off share on
 }
 
 template <class T>
+int ensure_nocopy(T*& p, size_t& cap, size_t need, cudaStream_t st) {
+  if (need <= cap && p) return RVG_OK;
+  size_t nc = std::max(need, cap + cap / 4);
+  if (nc == 0) nc = 1;
+  if (p) CK(cudaFreeAsync(p, st));
+  p = nullptr;
+  CK(cudaMallocAsync((void**)&p, nc * sizeof(T), st));
+  cap = nc;
+  return RVG_OK;
+}
+
+// first-fit allocation of `len` doubles in the CB arena; grows (with a copy of
+// the live contents) when no free range fits
+int cb_alloc(rvg_handle* h, int64_t len, int64_t* off) {
+  for (auto it = h->cb_free.begin(); it != h->cb_free.end(); ++it) {
+    if (it->second >= len) {
+      *off = it->first;
+      int64_t rest = it->second - len, start = it->first + len;
+      h->cb_free.erase(it);
+      if (rest > 0) h->cb_free[start] = rest;
+      return RVG_OK;
+    }
+  }
+  // grow: new capacity covers the old one plus the request
+  size_t old = h->cb_cap;
+  size_t nc = std::max(old + (size_t)len, old + old / 4);
+  double* np = nullptr;
+  CK(cudaMallocAsync((void**)&np, nc * sizeof(double), h->st));
+  if (h->cb_arena) {
+    if (old) CK(cudaMemcpyAsync(np, h->cb_arena, old * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    CK(cudaFreeAsync(h->cb_arena, h->st));
+  }
+  h->cb_arena = np;
+  h->cb_cap = nc;
+  // the tail [old, nc) is free; merge with a free range ending at `old`
+  int64_t start = (int64_t)old, length = (int64_t)(nc - old);
+  auto it = h->cb_free.lower_bound(start);
+  if (it != h->cb_free.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == start) { start = pv->first; length += pv->second; h->cb_free.erase(pv); }
+  }
+  h->cb_free[start] = length;
+  return cb_alloc(h, len, off);
+}
+
+void cb_release(rvg_handle* h, int64_t off, int64_t len) {
+  if (len <= 0) return;
+  auto it = h->cb_free.emplace(off, len).first;
+  auto nx = std::next(it);
+  if (nx != h->cb_free.end() && it->first + it->second == nx->first) { it->second += nx->second; h->cb_free.erase(nx); }
+  if (it != h->cb_free.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) { pv->second += it->second; h->cb_free.erase(it); }
+  }
+}
+
+template <class T>
 int upload(T*& d, const std::vector<T>& h, cudaStream_t st) {
   size_t n = std::max<size_t>(h.size(), 1);
   CK(cudaMallocAsync((void**)&d, n * sizeof(T), st));
@@ -1032,6 +1094,85 @@ DevOpts devopts(const rvg_options& o) {
 }
 
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// Arena sizes of the delay-free schedule, computed from the pattern alone
+// (delays can only add to them; the arenas grow in that case).
+int presize_arenas(rvg_handle* h) {
+  Plan& P = h->P;
+  const int64_t nb = h->opt.outer_block_size, ib = h->opt.inner_block_size;
+  int64_t panel = 0, idx = 0, dsz = 0, scratch = 0;
+  std::vector<int64_t> cbw(P.waves.size(), 0), rel(P.waves.size(), -1);
+  for (size_t w = 0; w < P.waves.size(); ++w) {
+    int64_t sc_w = 0;
+    for (int64_t s : P.waves[w]) {
+      const Snode& x = P.sn[s];
+      int64_t k = x.n_owned(), nfs = (int64_t)x.pattern.size(), m = k + nfs;
+      panel += m * k;
+      idx += m + k;
+      dsz += k;
+      bool has_cb = x.parent >= 0 && nfs > 0;
+      if (has_cb) cbw[w] += nfs * nfs;
+      bool tpp = x.in_small_leaf || k < ib;
+      bool large = !tpp && m >= h->opt.large_front_threshold;
+      int64_t sc = tpp ? 0 : (2 * IBMAX * m + nb);
+      if (large) sc = m * (2 * IBMAX + nb) + nb;
+      if (has_cb) sc = std::max<int64_t>(sc, nfs * k);
+      sc_w += sc;
+      if (x.parent >= 0) rel[w] = std::max<int64_t>(rel[w], P.height[x.parent]);
+    }
+    scratch = std::max(scratch, sc_w);
+  }
+  // first-fit simulation of the contribution arena
+  std::map<int64_t, int64_t> fr;
+  int64_t hw = 0;
+  std::vector<int64_t> off(P.waves.size(), -1);
+  auto sim_free = [&](int64_t o, int64_t l) {
+    auto it = fr.emplace(o, l).first;
+    auto nx = std::next(it);
+    if (nx != fr.end() && it->first + it->second == nx->first) { it->second += nx->second; fr.erase(nx); }
+    if (it != fr.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) { pv->second += it->second; fr.erase(it); }
+    }
+  };
+  for (size_t w = 0; w < P.waves.size(); ++w) {
+    for (size_t w2 = 0; w2 < w; ++w2)
+      if (off[w2] >= 0 && rel[w2] == (int64_t)w) { sim_free(off[w2], cbw[w2]); off[w2] = -1; }
+    if (!cbw[w]) continue;
+    bool placed = false;
+    for (auto it = fr.begin(); it != fr.end(); ++it)
+      if (it->second >= cbw[w]) {
+        off[w] = it->first;
+        int64_t rest = it->second - cbw[w], st = it->first + cbw[w];
+        fr.erase(it);
+        if (rest > 0) fr[st] = rest;
+        placed = true;
+        break;
+      }
+    if (!placed) {
+      // extend at the end (merging a free tail)
+      int64_t start = hw;
+      auto it = fr.end();
+      if (!fr.empty()) {
+        auto last = std::prev(it);
+        if (last->first + last->second == hw) { start = last->first; fr.erase(last); }
+      }
+      off[w] = start;
+      hw = start + cbw[w];
+    }
+  }
+  int rc;
+  cudaStream_t st = h->st;
+  if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel + panel / 16 + 1024), st))) return rc;
+  if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx + idx / 16 + 1024), st))) return rc;
+  if ((rc = ensure_d_arrays(h, (size_t)(dsz + dsz / 8 + 1024)))) return rc;
+  if ((rc = ensure_nocopy(h->scratch, h->scratch_cap, (size_t)(scratch + 1024), st))) return rc;
+  if (hw > 0 && !h->cb_arena) {
+    h->cb_cap = (size_t)(hw + hw / 16 + 1024);
+    CK(cudaMallocAsync((void**)&h->cb_arena, h->cb_cap * sizeof(double), st));
+  }
+  return RVG_OK;
+}
 
 double lower_entries(int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
   double e = 0;
@@ -1146,8 +1287,10 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   h->factored = false;
   h->h_fronts.assign(ns, DFront());
   int64_t panel_used = 0, idx_used = 0, d_used = 0;
-  std::vector<double*> cb_block(P.waves.size(), nullptr);
-  std::vector<int64_t> cb_release(P.waves.size(), -1);
+  std::vector<int64_t> cb_block(P.waves.size(), -1), cb_len(P.waves.size(), 0);
+  std::vector<int64_t> cb_release_at(P.waves.size(), -1);
+  h->cb_free.clear();
+  if (h->cb_cap) h->cb_free[0] = (int64_t)h->cb_cap;
   const DevOpts dop = devopts(h->opt);
   const int ib = (int)h->opt.inner_block_size;
   double t_asm = 0, t_ker = 0, t_gem = 0;
@@ -1199,23 +1342,24 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st))) return rc;
     if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx_used + idx_need), st))) return rc;
     if ((rc = ensure_d_arrays(h, (size_t)(d_used + d_need)))) return rc;
-    double* scratch = nullptr;
-    CK(cudaMallocAsync((void**)&scratch, (size_t)std::max<int64_t>(scratch_need, 1) * 8, st));
+    if ((rc = ensure_nocopy(h->scratch, h->scratch_cap, (size_t)std::max<int64_t>(scratch_need, 1), st))) return rc;
+    double* scratch = h->scratch;
     if (cb_need) {
-      CK(cudaMallocAsync((void**)&cb_block[w], (size_t)cb_need * 8, st));
-      CK(cudaMemsetAsync(cb_block[w], 0, (size_t)cb_need * 8, st));
+      if ((rc = cb_alloc(h, cb_need, &cb_block[w]))) return rc;
+      cb_len[w] = cb_need;
+      CK(cudaMemsetAsync(h->cb_arena + cb_block[w], 0, (size_t)cb_need * 8, st));
     }
     h->host_alloc_ms += now_ms() - ta;
     {
-      int64_t off = 0;
+      int64_t off = cb_block[w];
       for (int64_t s : wave) {
         DFront& f = h->h_fronts[s];
-        if (f.flags & FF_HAS_CB) { f.cb = cb_block[w] + off; off += (int64_t)f.nfs * f.nfs; }
-        else f.cb = nullptr;
+        if (f.flags & FF_HAS_CB) { f.cb = off; off += (int64_t)f.nfs * f.nfs; }
+        else f.cb = -1;
       }
     }
     if (panel_need) CK(cudaMemsetAsync(h->panel + panel_used, 0, (size_t)panel_need * 8, st));
-    const Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, scratch};
+    const Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, scratch, h->cb_arena};
     // ---- launch data of the whole wave, packed into one upload
     std::vector<int32_t> ids(wave.begin(), wave.end()), tpp_ids, aptp_ids, large_ids;
     std::vector<DFront> staged;
@@ -1285,7 +1429,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     CK(cudaEventRecord(h->ev[2], st));
     // contribution blocks whose parents are now all assembled
     for (size_t w2 = 0; w2 < w; ++w2)
-      if (cb_block[w2] && cb_release[w2] == (int64_t)w) { CK(cudaFreeAsync(cb_block[w2], st)); cb_block[w2] = nullptr; }
+      if (cb_block[w2] >= 0 && cb_release_at[w2] == (int64_t)w) { cb_release(h, cb_block[w2], cb_len[w2]); cb_block[w2] = -1; }
     // ---- dense factorization
     if (!tpp_ids.empty())
       k_tpp<<<blocks_for(tpp_ids.size(), 8), 256, 0, st>>>((const int32_t*)(D + o_tpp), (int)tpp_ids.size(),
@@ -1304,7 +1448,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     for (int64_t s : wave) {
       const DFront& f = h->h_fronts[s];
       if (!(f.flags & FF_HAS_CB) || f.k == 0 || !(f.m >= h->opt.large_front_threshold && f.nfs >= 256)) continue;
-      SyrkArgs ga{f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
+      SyrkArgs ga{A.cbase + f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
                   0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
       if ((rc = launch_syrk(h, ga))) return rc;
       cb_syrk_fronts.push_back(s);
@@ -1315,7 +1459,6 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     k_get_counts<<<blocks_for(nw, 128), 128, 0, st>>>(d_ids, nw, h->d_fronts, (int32_t*)(D + o_cnt));
     if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4) * 4))) return rc;
     CK(cudaMemcpyAsync(h->h_counts, D + o_cnt, (size_t)3 * nw * 4, cudaMemcpyDeviceToHost, st));
-    CK(cudaFreeAsync(scratch, st));
     {
       double ts0 = now_ms();
       CK(cudaStreamSynchronize(st));
@@ -1340,7 +1483,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     }
     int64_t last = -1;
     for (int64_t s : wave) if (P.sn[s].parent >= 0) last = std::max(last, P.height[P.sn[s].parent]);
-    cb_release[w] = last;
+    cb_release_at[w] = last;
     float a1 = 0, a2 = 0, a3 = 0;
     cudaEventElapsedTime(&a1, h->ev[1], h->ev[2]);
     cudaEventElapsedTime(&a2, h->ev[2], h->ev[3]);
@@ -1349,7 +1492,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     panel_used += panel_need; idx_used += idx_need; d_used += d_need;
   }
   for (size_t w = 0; w < cb_block.size(); ++w)
-    if (cb_block[w]) { CK(cudaFreeAsync(cb_block[w], st)); cb_block[w] = nullptr; }
+    if (cb_block[w] >= 0) { cb_release(h, cb_block[w], cb_len[w]); cb_block[w] = -1; }
   CK(cudaEventRecord(h->ev[5], st));
   CK(cudaStreamSynchronize(st));
   float tot = 0;
@@ -1468,6 +1611,7 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
     return (rvg_status)rc;
   CK(cudaMallocAsync((void**)&h->d_fronts, std::max<int64_t>(ns, 1) * sizeof(DFront), st));
   CK(cudaMallocAsync((void**)&h->d_lf, sizeof(LFState), st));
+  if ((rc = presize_arenas(h.get()))) return (rvg_status)rc;
   CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
   CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
   CK(cudaMallocAsync((void**)&h->d_scal, std::max<int64_t>(n, 1) * 8, st));
@@ -1511,7 +1655,7 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   for (auto& f : fr) { f.scratch = wneed; wneed += f.m + (solve_is_large(f) ? LS_RS * LS_B : 0); }
   if ((rc = ensure(h->solve_work, h->solve_work_cap, (size_t)std::max<int64_t>(wneed, 1), st))) return rc;
   CK(cudaMemcpyAsync(h->d_fronts, fr.data(), fr.size() * sizeof(DFront), cudaMemcpyHostToDevice, st));
-  Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, nullptr};
+  Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, nullptr, h->cb_arena};
   CK(cudaEventRecord(h->ev[6], st));
   int64_t launches = 0;
   int64_t tot = n * nrhs;
@@ -1791,7 +1935,7 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
   if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->h_counts) cudaFreeHost(h->h_counts);
