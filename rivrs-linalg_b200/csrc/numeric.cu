@@ -1136,8 +1136,11 @@ int presize_arenas(rvg_handle* h) {
     }
   };
   for (size_t w = 0; w < P.waves.size(); ++w) {
-    for (size_t w2 = 0; w2 < w; ++w2)
-      if (off[w2] >= 0 && rel[w2] == (int64_t)w) { sim_free(off[w2], cbw[w2]); off[w2] = -1; }
+    // same order as run_factor: this wave's block is allocated before the
+    // blocks its assembly consumed are released
+    if (w > 0)
+      for (size_t w2 = 0; w2 + 1 < w; ++w2)
+        if (off[w2] >= 0 && rel[w2] == (int64_t)(w - 1)) { sim_free(off[w2], cbw[w2]); off[w2] = -1; }
     if (!cbw[w]) continue;
     bool placed = false;
     for (auto it = fr.begin(); it != fr.end(); ++it)
