@@ -10,7 +10,9 @@
 // 256-column outer block) and the NFS x NFS contribution block
 // (compute_contribution_gemm, factor.rs:1590-1652).
 //
-// sm_100a has no FP64 tcgen05 kind, so this is a register-blocked SIMT DFMA
+// sm_100a has no FP64 tcgen05 kind.  The library uses the FP64 tensor-core
+// mma.sync (DMMA) kernel below; the register-blocked SIMT DFMA kernel
+// k_syrk_lower_t is kept as the reference formulation.  SIMT design:
 // kernel: 128 x 128 CTA tile, 256 threads (one CTA per SM: the 64 FP64
 // accumulators of a thread take 128 registers), 8 x 8 outputs per thread
 // (rows tx + 16a, columns ty + 16b so C loads and stores coalesce along
@@ -149,17 +151,118 @@ __global__ void __launch_bounds__(NT, MINB) k_syrk_lower_t(SyrkArgs a) {
     }
 }
 
-// the configuration used by the library
-#ifndef RVG_SYRK_NT
-#define RVG_SYRK_NT 256
-#define RVG_SYRK_TM 8
-#define RVG_SYRK_TN 8
-#define RVG_SYRK_MINB 1
+// ---------------------------------------------------------------------------
+// FP64 tensor-core variant: mma.sync m8n8k4 (DMMA).  Each 8x8x4 step adds a
+// chain of four products to the accumulator in k order, the same
+// per-output fma sequence as the SIMT kernel and the oracle (checked bit for
+// bit on the device).  WR x WC warps of 32 x 32 outputs (4 x 4 fragments of
+// 8 x 8); W is negated when its fragments are read.
+// ---------------------------------------------------------------------------
+template <int WR, int WC>
+struct DmmaCfg {
+  static constexpr int NT = 32 * WR * WC, BM = 32 * WR, BN = 32 * WC;
+  static constexpr int LDW = BM + 8, LDL = BN + 8;  // k rows shifted 64 B apart: conflict-free fragment reads
+  static constexpr size_t SMEM = (size_t)G_STAGES * G_BK * (LDW + LDL) * sizeof(double);
+};
+
+template <int WR, int WC, int MINB>
+__global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
+  using Cfg = DmmaCfg<WR, WC>;
+  constexpr int NT = Cfg::NT, BM = Cfg::BM, BN = Cfg::BN, LDW = Cfg::LDW, LDL = Cfg::LDL;
+  const int64_t i0 = a.r0 + (int64_t)blockIdx.y * BM;
+  const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
+  if (i0 >= a.r1 || j0 >= a.c1) return;
+  if (i0 + BM - 1 < j0) return;
+  const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
+  extern __shared__ double gsm[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = (warp % WR) * 32, wc = (warp / WR) * 32;
+  const int64_t nchunk = (K + G_BK - 1) / G_BK;
+  auto issue = [&](int64_t ch) {
+    double* sw = gsm + (ch % G_STAGES) * G_BK * (LDW + LDL);
+    double* sl = sw + G_BK * LDW;
+    const int64_t k0 = ch * G_BK;
+#pragma unroll
+    for (int e = 0; e < (G_BK * BM) / NT; ++e) {
+      const int idx = tid + NT * e;
+      const int r = idx % BM, k = idx / BM;
+      const int64_t kk = k0 + k, i = i0 + r;
+      const bool v = kk < K && i < a.r1;
+      cp_async8(sw + k * LDW + r, v ? a.W + (i - a.r0) + kk * a.ldw : a.W, v);
+    }
+#pragma unroll
+    for (int e = 0; e < (G_BK * BN) / NT; ++e) {
+      const int idx = tid + NT * e;
+      const int r = idx % BN, k = idx / BN;
+      const int64_t kk = k0 + k, j = j0 + r;
+      const bool v = kk < K && j < a.c1;
+      cp_async8(sl + k * LDL + r, v ? a.L + j + kk * a.ldl : a.L, v);
+    }
+  };
+#pragma unroll
+  for (int s = 0; s < G_STAGES - 1; ++s) {
+    if (s < nchunk) issue(s);
+    cp_async_commit();
+  }
+  double acc[4][4][2];
+  const int fr = lane >> 2, fc = (lane & 3) * 2;
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int64_t i = i0 + wr + mi * 8 + fr, j = j0 + wc + ni * 8 + fc + q;
+        acc[mi][ni][q] = (i < a.r1 && j < a.c1 && i >= j) ? a.C[i + j * a.ldc] : 0.0;
+      }
+  for (int64_t ch = 0; ch < nchunk; ++ch) {
+    cp_async_wait<G_STAGES - 2>();
+    __syncthreads();
+    if (ch + G_STAGES - 1 < nchunk) issue(ch + G_STAGES - 1);
+    cp_async_commit();
+    const double* sw = gsm + (ch % G_STAGES) * G_BK * (LDW + LDL);
+    const double* sl = sw + G_BK * LDW;
+    // k beyond K is zero-filled in both operands: those steps add exact zeros
+#pragma unroll
+    for (int k4 = 0; k4 < G_BK; k4 += 4) {
+      double af[4], bf[4];
+      const int kk = k4 + (lane & 3);
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) af[mi] = -sw[kk * LDW + wr + mi * 8 + fr];
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = sl[kk * LDL + wc + ni * 8 + fr];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+          asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                       : "+d"(acc[mi][ni][0]), "+d"(acc[mi][ni][1])
+                       : "d"(af[mi]), "d"(bf[ni]));
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int64_t i = i0 + wr + mi * 8 + fr, j = j0 + wc + ni * 8 + fc + q;
+        if (i < a.r1 && j < a.c1 && i >= j) a.C[i + j * a.ldc] = acc[mi][ni][q];
+      }
+}
+
+// the configuration used by the library: DMMA, 4 x 2 warps (128 x 64 tile),
+// two CTAs per SM
+#ifndef RVG_SYRK_WR
+#define RVG_SYRK_WR 4
+#define RVG_SYRK_WC 2
+#define RVG_SYRK_MINB 2
 #endif
-using SyrkMain = SyrkCfg<RVG_SYRK_NT, RVG_SYRK_TM, RVG_SYRK_TN>;
-constexpr int G_T = RVG_SYRK_NT;
+using SyrkMain = DmmaCfg<RVG_SYRK_WR, RVG_SYRK_WC>;
+constexpr int G_T = SyrkMain::NT;
 constexpr size_t G_SMEM = SyrkMain::SMEM;
-#define k_syrk_lower k_syrk_lower_t<RVG_SYRK_NT, RVG_SYRK_TM, RVG_SYRK_TN, RVG_SYRK_MINB>
+#define k_syrk_lower k_syrk_dmma<RVG_SYRK_WR, RVG_SYRK_WC, RVG_SYRK_MINB>
 
 template <class Cfg>
 inline dim3 syrk_grid_cfg(const SyrkArgs& a) {
