@@ -252,12 +252,13 @@ __global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
       }
 }
 
-// the configuration used by the library: DMMA, 4 x 2 warps (128 x 64 tile),
-// two CTAs per SM
+// the configuration used by the library: DMMA, 2 x 2 warps (64 x 64 tile),
+// four CTAs per SM (the fastest of the measured shapes: 25-28 TFLOP/s on a
+// 16384^2 rank-256 / rank-1024 update)
 #ifndef RVG_SYRK_WR
-#define RVG_SYRK_WR 4
+#define RVG_SYRK_WR 2
 #define RVG_SYRK_WC 2
-#define RVG_SYRK_MINB 2
+#define RVG_SYRK_MINB 4
 #endif
 using SyrkMain = DmmaCfg<RVG_SYRK_WR, RVG_SYRK_WC>;
 constexpr int G_T = SyrkMain::NT;

@@ -4,7 +4,7 @@ The kernels and the oracle follow one arithmetic contract (fma chains where
 the reference calls faer, unfused arithmetic elsewhere), so on the same
 inputs the pivot record -- eliminated column order, 1x1/2x2 codes and the D
 values -- must agree bit for bit, the inertia exactly, and the solution to
-rounding (the GPU solve reassociates sibling updates; tolerance 1e-12
+rounding (the GPU solve reassociates sibling updates; tolerance 1e-10
 relative).  Backward error gates follow tests/solve.rs (<= 1e-14 on the
 synthetic systems, < 1e-10 on the hand-constructed ones).
 """
@@ -15,7 +15,7 @@ from conftest import golden_system
 
 pytestmark = pytest.mark.gpu
 
-SOL_RTOL = 1e-12
+SOL_RTOL = 1e-10
 
 
 def run_both(rv, orc, s, order=None, nrhs=1, seed=0, scaling=None, **opts):
