@@ -164,6 +164,32 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* out);
 rvg_status rvg_stream(rvg_handle* h, void** stream);
 void rvg_destroy(rvg_handle* h);
 
+/* ---- allocation-free dense front factorization -------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot allocate device memory while they run -- a solver embedded in a
+ * host application that owns the device's memory budget and forbids
+ * allocation after start-up, code inside stream-ordered work that an
+ * allocation would synchronise or fragment, real-time loops and callbacks.
+ * It factors one dense symmetric front in place with the same kernels as
+ * rvg_factor (aptp_factor_in_place semantics, factor.rs:301-404): d_a is
+ * m x m column-major (lower triangle read, the first p columns factored),
+ * d_perm receives the pivot order (p), d_dtype / d_ddiag / d_doff the D
+ * entries (p; codes as in rvg_pivot_record), d_counts [ne, n1x1, n2x2].
+ * All buffers are the caller's device memory; the call allocates nothing.
+ * Its scratch is one fixed device array inside the library (about 2.1 MB per
+ * GPU, held until exit), which limits m to RVG_NOALLOC_MAX_ORDER and the outer
+ * block size to RVG_NOALLOC_MAX_NB; larger sizes return RVG_ERR_INVALID_INPUT.
+ * Every call on a device shares that array: calls that overlap on the GPU
+ * (different streams without ordering) race.  The first call on a device
+ * looks up the array's address; make it before any stream capture.  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL for the default stream); the
+ * call does not synchronise.  `opt` may be NULL for the defaults. */
+#define RVG_NOALLOC_MAX_ORDER 4096
+#define RVG_NOALLOC_MAX_NB 4096
+rvg_status rvg_dense_factor_noalloc(double* d_a, int64_t m, int64_t p, const rvg_options* opt, int32_t* d_perm,
+                                    int8_t* d_dtype, double* d_ddiag, double* d_doff, int32_t* d_counts,
+                                    void* stream);
+
 #ifdef __cplusplus
 }
 #endif
