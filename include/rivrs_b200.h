@@ -54,6 +54,14 @@ typedef struct {
    * the multi-kernel path (whole GPU per front); smaller ones are batched one
    * CTA or warp per front.  Results do not depend on it.  Default 2048. */
   int64_t large_front_threshold;
+  /* Arithmetic of the large Schur-complement updates, no reference
+   * counterpart: 0 = plain FP64 (tensor-core DMMA, bit-identical to the CPU
+   * restatement), 1 = mixed: the updates on the TF32 tensor path with each
+   * operand split in two (FP32-level products, FP32 partial sums flushed to
+   * FP64 every 16 terms); pivot tests, 2x2 inversions, TRSM and storage stay
+   * FP64.  Pair the mixed form with rvg_solve_refine. */
+  int32_t precision;
+  int32_t reserved;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */
@@ -120,6 +128,18 @@ rvg_status rvg_factor_device(rvg_handle* h, const double* d_values, const double
 rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb);
 /* Same on device memory. */
 rvg_status rvg_solve_device(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb);
+
+/* Solve with iterative refinement in FP64 (no reference counterpart; the
+ * mixed form's way back to full accuracy): x = solve(b), then while the
+ * scaled backward error ||Ax-b|| / (||A||_F ||x|| + ||b||)
+ * (sparse/src/validate.rs:209-258) is above `tol`, r = b - A x in FP64 and
+ * x += solve(r), at most `max_iter` corrections.  One right-hand side; `rhs`
+ * and `x` are host (rvg_solve_refine) or device (_device) vectors of length
+ * n.  Reports the corrections made and the final backward error. */
+rvg_status rvg_solve_refine(rvg_handle* h, const double* rhs, double* x, double tol, int32_t max_iter,
+                            int32_t* iters, double* bwd_err);
+rvg_status rvg_solve_refine_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
+                                   int32_t* iters, double* bwd_err);
 
 /* SparseLDLT::inertia (solver.rs:504-519): [positive, negative, zero]. */
 rvg_status rvg_inertia(rvg_handle* h, int64_t out3[3]);

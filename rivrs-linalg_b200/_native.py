@@ -28,7 +28,8 @@ STATUS = {
 class Options(C.Structure):
     _fields_ = [("threshold", C.c_double), ("small", C.c_double), ("outer_block_size", i64),
                 ("inner_block_size", i64), ("nemin", i64), ("small_leaf_threshold", i64),
-                ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64)]
+                ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -73,6 +74,9 @@ SIGNATURES = {
     "rvg_factor_device": (C.c_int, [vp, vp, vp]),
     "rvg_solve": (C.c_int, [vp, dp, i64, i64]),
     "rvg_solve_device": (C.c_int, [vp, vp, i64, i64]),
+    "rvg_solve_refine": (C.c_int, [vp, dp, dp, C.c_double, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "rvg_solve_refine_device": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
+                                          C.POINTER(C.c_double)]),
     "rvg_inertia": (C.c_int, [vp, i64p]),
     "rvg_get_stats": (C.c_int, [vp, C.POINTER(Stats)]),
     "rvg_pivot_record": (C.c_int, [vp, i64p, i8p, dp, dp, i64p]),

@@ -850,6 +850,42 @@ __global__ void k_solve_bwd(const int32_t* ids, int n, const DFront* F, Arenas A
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 iterative refinement (residual of the unfactored matrix)
+// ---------------------------------------------------------------------------
+// r = b - A x; A full symmetric CSC, so column i is also row i
+__global__ void k_residual(const int64_t* colptr, const int32_t* rowidx, const double* val, const double* x,
+                           const double* b, double* r, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int64_t p = colptr[i]; p < colptr[i + 1]; ++p) s = __fma_rn(val[p], x[rowidx[p]], s);
+  r[i] = b[i] - s;
+}
+// out[0] += ||r||^2, out[1] += ||x||^2, out[2] += ||b||^2
+__global__ void k_norms3(const double* r, const double* x, const double* b, int64_t n, double* out) {
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    s0 += r[i] * r[i]; s1 += x[i] * x[i]; s2 += b[i] * b[i];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) { atomicAdd(out, s0); atomicAdd(out + 1, s1); atomicAdd(out + 2, s2); }
+}
+__global__ void k_sumsq(const double* v, int64_t n, double* out) {
+  double s = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += v[i] * v[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+__global__ void k_axpy1(double* x, const double* d, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += d[i];
+}
+
 }  // namespace rvg
 
 // ===========================================================================
@@ -899,6 +935,11 @@ struct rvg_handle {
   char* h_stage = nullptr; size_t h_stage_cap = 0; // pinned host mirror
   int32_t* h_counts = nullptr; size_t h_counts_cap = 0;
   LFState* d_lf = nullptr;                          // state of the large-front path
+  int64_t* d_colptr = nullptr;                      // matrix pattern (full symmetric CSC = its own CSR)
+  int32_t* d_rowidx = nullptr;
+  double a_fro = 0;                                 // ||A||_F of the last factored values
+  double* d_ref = nullptr; size_t ref_cap = 0;      // refinement vectors r, d, b (3n) and norms
+  double* h_norms = nullptr;
   double* scratch = nullptr; size_t scratch_cap = 0; // per-wave scratch, persistent across factors
   double* cb_arena = nullptr; size_t cb_cap = 0;     // contribution blocks, first-fit by wave
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
@@ -1157,7 +1198,8 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga) {
     }
     CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
   }
-  k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
+  if (h->opt.precision == 1) k_syrk_mixed<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
+  else k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
   h->launches++;
   h->syrk_launches++;
   if (h->profiling) CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
@@ -1507,6 +1549,8 @@ void rvg_default_options(rvg_options* o) {
   o->failed_pivot_tpp = 1;
   o->fallback_bk = 1;
   o->large_front_threshold = 2048;
+  o->precision = 0;
+  o->reserved = 0;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347
@@ -1521,6 +1565,7 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347
   if (o.inner_block_size > IBMAX) { set_error("inner_block_size above 32 is not supported by the B200 kernels"); return RVG_ERR_INVALID_INPUT; }
   if (o.nemin < 1) { set_error("nemin must be >= 1"); return RVG_ERR_INVALID_INPUT; }
   if (o.large_front_threshold < 1) { set_error("large_front_threshold must be >= 1"); return RVG_ERR_INVALID_INPUT; }
+  if (o.precision != 0 && o.precision != 1) { set_error("precision must be 0 (FP64) or 1 (mixed)"); return RVG_ERR_INVALID_INPUT; }
   return RVG_OK;
 }
 
@@ -1573,8 +1618,15 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
     return (rvg_status)rc;
   CK(cudaMallocAsync((void**)&h->d_fronts, std::max<int64_t>(ns, 1) * sizeof(DFront), st));
   CK(cudaMallocAsync((void**)&h->d_lf, sizeof(LFState), st));
+  {
+    std::vector<int64_t> cp(colptr, colptr + n + 1);
+    std::vector<int32_t> ri(rowidx, rowidx + h->nnz);
+    if ((rc = upload(h->d_colptr, cp, st)) || (rc = upload(h->d_rowidx, ri, st))) return (rvg_status)rc;
+  }
+  CK(cudaMallocHost((void**)&h->h_norms, 4 * sizeof(double)));
   if ((rc = presize_arenas(h.get()))) return (rvg_status)rc;
   CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
   CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
   CK(cudaMallocAsync((void**)&h->d_scal, std::max<int64_t>(n, 1) * 8, st));
   CK(cudaStreamSynchronize(st));
@@ -1582,7 +1634,21 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   return RVG_OK;
 }
 
-static int factor_common(rvg_handle* h, const double* dv, const double* ds) { return run_factor(h, dv, ds); }
+static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
+  // the refinement needs the unfactored values and ||A||_F
+  if (dv != h->d_vals && h->nnz) CK(cudaMemcpyAsync(h->d_vals, dv, h->nnz * 8, cudaMemcpyDeviceToDevice, h->st));
+  int rc = run_factor(h, h->d_vals, ds);
+  if (rc) return rc;
+  double* d_acc = nullptr;
+  CK(cudaMallocAsync((void**)&d_acc, 8, h->st));
+  CK(cudaMemsetAsync(d_acc, 0, 8, h->st));
+  if (h->nnz) k_sumsq<<<296, 256, 0, h->st>>>(h->d_vals, h->nnz, d_acc);
+  CK(cudaMemcpyAsync(h->h_norms, d_acc, 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaFreeAsync(d_acc, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->a_fro = std::sqrt(h->h_norms[0]);
+  return RVG_OK;
+}
 
 rvg_status rvg_factor(rvg_handle* h, const double* values, const double* scaling) {
   if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
@@ -1737,6 +1803,70 @@ rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb) {
   float ms = 0;
   cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]);
   h->t_solve = ms;
+  return RVG_OK;
+}
+
+static int refine_common(rvg_handle* h, const double* d_b, double* d_x, double tol, int32_t max_iter, int32_t* iters,
+                         double* bwd) {
+  const int64_t n = h->P.n;
+  cudaStream_t st = h->st;
+  int rc = ensure(h->d_ref, h->ref_cap, (size_t)(2 * n + 8), st);
+  if (rc) return rc;
+  double* r = h->d_ref;
+  double* nrm = h->d_ref + n;  // 3 doubles (the rest of the buffer is unused)
+  CK(cudaMemcpyAsync(d_x, d_b, n * 8, cudaMemcpyDeviceToDevice, st));
+  if ((rc = solve_common(h, d_x, 1, n))) return rc;
+  int it = 0;
+  double e = 0;
+  const unsigned nb = blocks_for(n, 256);
+  for (;;) {
+    k_residual<<<nb, 256, 0, st>>>(h->d_colptr, h->d_rowidx, h->d_vals, d_x, d_b, r, n);
+    CK(cudaMemsetAsync(nrm, 0, 3 * 8, st));
+    k_norms3<<<296, 256, 0, st>>>(r, d_x, d_b, n, nrm);
+    CK(cudaMemcpyAsync(h->h_norms, nrm, 3 * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double denom = h->a_fro * std::sqrt(h->h_norms[1]) + std::sqrt(h->h_norms[2]);
+    e = denom == 0 ? 0.0 : std::sqrt(h->h_norms[0]) / denom;
+    if (e <= tol || it >= max_iter) break;
+    if ((rc = solve_common(h, r, 1, n))) return rc;
+    k_axpy1<<<nb, 256, 0, st>>>(d_x, r, n);
+    ++it;
+  }
+  CK(cudaGetLastError());
+  if (iters) *iters = it;
+  if (bwd) *bwd = e;
+  return RVG_OK;
+}
+
+rvg_status rvg_solve_refine_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
+                                   int32_t* iters, double* bwd_err) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  if (h->P.n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  int rc = refine_common(h, d_rhs, d_x, tol, max_iter, iters, bwd_err);
+  h->t_solve = now_ms() - t0;
+  return (rvg_status)rc;
+}
+
+rvg_status rvg_solve_refine(rvg_handle* h, const double* rhs, double* x, double tol, int32_t max_iter, int32_t* iters,
+                            double* bwd_err) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  const int64_t n = h->P.n;
+  if (n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  double* d = nullptr;
+  CK(cudaMallocAsync((void**)&d, 2 * n * 8, h->st));
+  CK(cudaMemcpyAsync(d, rhs, n * 8, cudaMemcpyHostToDevice, h->st));
+  int rc = refine_common(h, d, d + n, tol, max_iter, iters, bwd_err);
+  if (rc) return (rvg_status)rc;
+  CK(cudaMemcpyAsync(x, d + n, n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaFreeAsync(d, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->t_solve = now_ms() - t0;
   return RVG_OK;
 }
 
@@ -1898,9 +2028,11 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
   fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena);
+  fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
   if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->h_counts) cudaFreeHost(h->h_counts);
+  if (h->h_norms) cudaFreeHost(h->h_norms);
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   for (auto& e : h->ev) if (e) cudaEventDestroy(e);
   delete h;

@@ -50,6 +50,7 @@ class FactorOptions:
     failed_pivot_tpp: bool = True
     fallback_bunch_kaufman: bool = True
     large_front_threshold: int = 2048  # B200 scheduling only; results do not depend on it
+    precision: str = "fp64"  # "fp64" (plain) or "mixed" (split-TF32 Schur updates; pair with solve_refine)
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
@@ -57,7 +58,8 @@ class FactorOptions:
                                  nemin=self.nemin, small_leaf_threshold=self.small_leaf_threshold,
                                  failed_pivot_tpp=int(self.failed_pivot_tpp),
                                  fallback_bk=int(self.fallback_bunch_kaufman),
-                                 large_front_threshold=self.large_front_threshold)
+                                 large_front_threshold=self.large_front_threshold,
+                                 precision={"fp64": 0, "mixed": 1}[self.precision])
 
 
 class SparseError(RuntimeError):
@@ -211,6 +213,30 @@ class SparseLDLT:
             raise DimensionMismatch(f"RHS length must match matrix dimension: expected {n}, got {rhs.shape[0]}")
         nrhs = 1 if rhs.ndim == 1 else rhs.shape[1]
         _check(N.lib().rvg_solve(self._handle, rhs.ctypes.data_as(N.dp), nrhs, n))
+
+    def solve_refine(self, rhs: np.ndarray, tol: float = 1e-14, max_iter: int = 10):
+        """x with FP64 iterative refinement until the scaled backward error is <= tol.
+        Returns (x, corrections, backward error)."""
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        b = N.as_f64(rhs)
+        if b.ndim != 1 or b.size != self.system.n:
+            raise DimensionMismatch("RHS length must match matrix dimension")
+        x = np.empty_like(b)
+        it = C.c_int32()
+        err = C.c_double()
+        _check(N.lib().rvg_solve_refine(self._handle, N.ptr(b, N.dp), N.ptr(x, N.dp), tol, max_iter, C.byref(it),
+                                        C.byref(err)))
+        return x, it.value, err.value
+
+    def solve_refine_device(self, d_rhs_ptr: int, d_x_ptr: int, tol: float = 1e-14, max_iter: int = 10):
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        it = C.c_int32()
+        err = C.c_double()
+        _check(N.lib().rvg_solve_refine_device(self._handle, C.c_void_p(d_rhs_ptr), C.c_void_p(d_x_ptr), tol, max_iter,
+                                               C.byref(it), C.byref(err)))
+        return it.value, err.value
 
     def solve_device(self, d_rhs_ptr: int, nrhs: int = 1, ldb: int | None = None):
         if not self._factored:

@@ -1,0 +1,59 @@
+"""Mixed form: the large Schur-complement updates on the split-TF32 tensor path,
+everything else FP64, then FP64 iterative refinement (rvg_solve_refine).
+
+The mixed factor is not bit-identical to the oracle (its products are rounded
+differently), so the gates are the ones the solution must meet: exact
+inertia where it is known, and a scaled backward error <= 1e-14 after at most
+10 corrections; the plain form must reach it with at most one correction.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# force the multi-kernel large-front path (and with it the Schur GEMM) onto small fronts
+SMALL_LARGE = dict(large_front_threshold=64)
+
+
+def factor_refine(rv, s, b, **opts):
+    solver = rv.SparseLDLT.analyze(s)
+    solver.factor(None, rv.FactorOptions(**opts))
+    x, iters, err = solver.solve_refine(b, tol=1e-14, max_iter=10)
+    inertia = solver.inertia()
+    solver.close()
+    return x, iters, err, inertia
+
+
+@pytest.mark.parametrize("name", ["lap", "kkt", "dense"])
+def test_mixed_reaches_fp64_accuracy(rv, name):
+    if name == "lap":
+        s = rv.problems.shifted_laplacian(16, 0.1)
+    elif name == "kkt":
+        s = rv.problems.kkt(12, seed=2)
+    else:
+        rng = np.random.default_rng(5)
+        a = rng.standard_normal((700, 700))
+        a = a + a.T + np.diag(np.full(700, 60.0))
+        import scipy.sparse as sp
+        s = rv.problems.from_scipy("dense700", sp.csc_matrix(a))
+    b = rv.problems.rhs_normal(s.n, 3)
+    for precision in ("fp64", "mixed"):
+        x, iters, err, inertia = factor_refine(rv, s, b, precision=precision, **SMALL_LARGE)
+        assert err <= 1e-14, (precision, err, iters)
+        assert rv.problems.backward_error(s, x, b) <= 1e-14
+        if s.inertia is not None:
+            assert inertia == s.inertia
+        if precision == "fp64":
+            assert iters <= 1
+
+
+def test_refine_errors(rv):
+    s = rv.problems.shifted_laplacian(4, 0.1)
+    solver = rv.SparseLDLT.analyze(s)
+    with pytest.raises(rv.SolveBeforeFactor):
+        solver.solve_refine(np.ones(s.n))
+    solver.factor()
+    with pytest.raises(rv.DimensionMismatch):
+        solver.solve_refine(np.ones(s.n + 2))
+    with pytest.raises(rv.InvalidInput):
+        solver.factor(None, rv.FactorOptions(precision="fp64", threshold=2.0))
