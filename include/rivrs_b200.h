@@ -56,12 +56,17 @@ typedef struct {
   int64_t large_front_threshold;
   /* Arithmetic of the large Schur-complement updates, no reference
    * counterpart: 0 = plain FP64 (tensor-core DMMA, bit-identical to the CPU
-   * restatement), 1 = mixed: the updates on the TF32 tensor path with each
-   * operand split in two (FP32-level products, FP32 partial sums flushed to
-   * FP64 every 16 terms); pivot tests, 2x2 inversions, TRSM and storage stay
-   * FP64.  Pair the mixed form with rvg_solve_refine. */
+   * restatement), 1 = mixed: the updates on the TF32 tensor cores (tcgen05)
+   * with each FP64 operand split once into two TF32 parts (three products per
+   * term, FP32-level products), FP32 partial sums added into FP64; pivot
+   * tests, 2x2 inversions, TRSM and storage stay FP64.  Pair the mixed form
+   * with rvg_solve_refine. */
   int32_t precision;
-  int32_t reserved;
+  /* Mixed form only: 32-deep K chunks per FP32 partial sum before it is
+   * added in FP64 (1, 2, 4 or 8; 0 = one partial sum over the whole K range).
+   * Smaller is more accurate (the tensor cores accumulate FP32 with
+   * truncation) and slower.  Default 4. */
+  int32_t mixed_flush;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */

@@ -252,137 +252,6 @@ __global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
       }
 }
 
-// ---------------------------------------------------------------------------
-// Mixed form: the same update with the products on the TF32 tensor path,
-// each operand split into two TF32 parts (v = hi + lo) and three products
-// per term (lo*hi + hi*lo + hi*hi; the dropped lo*lo is below FP32 rounding).
-// Partial sums of one 16-deep K chunk are accumulated in FP32 by
-// mma.sync.m16n8k8.tf32 and flushed into FP64 accumulators that start from C.
-// Storage and everything outside the Schur updates stay FP64.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void split_tf32(double v, uint32_t& hi, uint32_t& lo) {
-  float f = (float)v;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(f));
-  float r = f - __uint_as_float(hi);
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
-}
-
-__device__ __forceinline__ void mma_tf32(float* c, const uint32_t* a, const uint32_t* b) {
-  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-               : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-template <int WR, int WC, int MINB>
-__global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_tf32x3(SyrkArgs a) {
-  using Cfg = DmmaCfg<WR, WC>;
-  constexpr int NT = Cfg::NT, BM = Cfg::BM, BN = Cfg::BN, LDW = Cfg::LDW, LDL = Cfg::LDL;
-  const int64_t i0 = a.r0 + (int64_t)blockIdx.y * BM;
-  const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
-  if (i0 >= a.r1 || j0 >= a.c1) return;
-  if (i0 + BM - 1 < j0) return;
-  const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
-  extern __shared__ double gsm[];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wr = (warp % WR) * 32, wc = (warp / WR) * 32;
-  const int g = lane >> 2, t = lane & 3;
-  const int64_t nchunk = (K + G_BK - 1) / G_BK;
-  auto issue = [&](int64_t ch) {
-    double* sw = gsm + (ch % G_STAGES) * G_BK * (LDW + LDL);
-    double* sl = sw + G_BK * LDW;
-    const int64_t k0 = ch * G_BK;
-#pragma unroll
-    for (int e = 0; e < (G_BK * BM) / NT; ++e) {
-      const int idx = tid + NT * e;
-      const int r = idx % BM, k = idx / BM;
-      const int64_t kk = k0 + k, i = i0 + r;
-      const bool v = kk < K && i < a.r1;
-      cp_async8(sw + k * LDW + r, v ? a.W + (i - a.r0) + kk * a.ldw : a.W, v);
-    }
-#pragma unroll
-    for (int e = 0; e < (G_BK * BN) / NT; ++e) {
-      const int idx = tid + NT * e;
-      const int r = idx % BN, k = idx / BN;
-      const int64_t kk = k0 + k, j = j0 + r;
-      const bool v = kk < K && j < a.c1;
-      cp_async8(sl + k * LDL + r, v ? a.L + j + kk * a.ldl : a.L, v);
-    }
-  };
-#pragma unroll
-  for (int s = 0; s < G_STAGES - 1; ++s) {
-    if (s < nchunk) issue(s);
-    cp_async_commit();
-  }
-  // FP64 accumulators (m16 x n8 fragments: rows g, g+8; columns 2t, 2t+1)
-  double acc[2][4][4];
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t i = i0 + wr + mt * 16 + g + (q >> 1) * 8, j = j0 + wc + nt * 8 + 2 * t + (q & 1);
-        acc[mt][nt][q] = (i < a.r1 && j < a.c1 && i >= j) ? a.C[i + j * a.ldc] : 0.0;
-      }
-  for (int64_t ch = 0; ch < nchunk; ++ch) {
-    cp_async_wait<G_STAGES - 2>();
-    __syncthreads();
-    if (ch + G_STAGES - 1 < nchunk) issue(ch + G_STAGES - 1);
-    cp_async_commit();
-    const double* sw = gsm + (ch % G_STAGES) * G_BK * (LDW + LDL);
-    const double* sl = sw + G_BK * LDW;
-    float part[2][4][4];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) part[mt][nt][q] = 0.f;
-#pragma unroll
-    for (int k8 = 0; k8 < G_BK; k8 += 8) {
-      uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt) {
-        const int rb = wr + mt * 16 + g;
-        split_tf32(sw[(k8 + t) * LDW + rb], ah[mt][0], al[mt][0]);
-        split_tf32(sw[(k8 + t) * LDW + rb + 8], ah[mt][1], al[mt][1]);
-        split_tf32(sw[(k8 + t + 4) * LDW + rb], ah[mt][2], al[mt][2]);
-        split_tf32(sw[(k8 + t + 4) * LDW + rb + 8], ah[mt][3], al[mt][3]);
-      }
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int cb = wc + nt * 8 + g;
-        split_tf32(sl[(k8 + t) * LDL + cb], bh[nt][0], bl[nt][0]);
-        split_tf32(sl[(k8 + t + 4) * LDL + cb], bh[nt][1], bl[nt][1]);
-      }
-#pragma unroll
-      for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          mma_tf32(part[mt][nt], al[mt], bh[nt]);
-          mma_tf32(part[mt][nt], ah[mt], bl[nt]);
-          mma_tf32(part[mt][nt], ah[mt], bh[nt]);
-        }
-    }
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[mt][nt][q] -= (double)part[mt][nt][q];
-  }
-  cp_async_wait<0>();
-#pragma unroll
-  for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int64_t i = i0 + wr + mt * 16 + g + (q >> 1) * 8, j = j0 + wc + nt * 8 + 2 * t + (q & 1);
-        if (i < a.r1 && j < a.c1 && i >= j) a.C[i + j * a.ldc] = acc[mt][nt][q];
-      }
-}
-#define k_syrk_mixed k_syrk_tf32x3<2, 2, 3>
 
 // the configuration used by the library: DMMA, 2 x 2 warps (64 x 64 tile),
 // four CTAs per SM (the fastest of the measured shapes: 25-28 TFLOP/s on a

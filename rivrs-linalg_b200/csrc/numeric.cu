@@ -625,6 +625,7 @@ __global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* 
 }  // namespace rvg
 
 #include "gemm64.cuh"
+#include "umma.cuh"
 #include "large.cuh"
 #include "solve_large.cuh"
 
@@ -942,6 +943,9 @@ struct rvg_handle {
   double* h_norms = nullptr;
   double* scratch = nullptr; size_t scratch_cap = 0; // per-wave scratch, persistent across factors
   double* cb_arena = nullptr; size_t cb_cap = 0;     // contribution blocks, first-fit by wave
+  float* pack = nullptr; size_t pack_cap = 0;        // TF32 hi/lo operand tiles of the mixed-form updates
+  int32_t* d_err = nullptr;                          // set by a device wait that timed out
+  int nsm = 0;                                       // SMs of the device (persistent grids)
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
   bool factored = false;
   // measurement
@@ -1186,7 +1190,9 @@ double lower_entries(int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
   return e;
 }
 
-int launch_syrk(rvg_handle* h, const SyrkArgs& ga) {
+// The Schur update C -= W L^T (lower) of one deferred trailing block or one
+// contribution block.  kmax bounds the device-side K (columns eliminated).
+int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
   cudaStream_t st = h->st;
   if (h->profiling) {
     if (h->ev_used + 2 > h->ev_pool.size()) {
@@ -1198,10 +1204,35 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga) {
     }
     CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
   }
-  if (h->opt.precision == 1) k_syrk_mixed<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
-  else k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
-  h->launches++;
-  h->syrk_launches++;
+  if (h->opt.precision == 1) {
+    const int64_t nr = (ga.r1 - ga.r0 + TC_BM - 1) / TC_BM, nc = (ga.c1 - ga.c0 + TC_BN - 1) / TC_BN;
+    const int64_t Q = (kmax + TC_BK - 1) / TC_BK;
+    const int64_t ntiles = (nr > 0 && nc > 0) ? tc_count_tiles(nr, nc, ga.r0, ga.c0) : 0;
+    if (ntiles > 0 && Q > 0) {
+      int rc = ensure_nocopy(h->pack, h->pack_cap, (size_t)(nr + nc) * Q * TC_BLOCK, st);
+      if (rc) return rc;
+      float* pl = h->pack + (size_t)nr * Q * TC_BLOCK;
+      PackArgs aw{ga.W, ga.ldw, ga.r1 - ga.r0, Q, ga.Kdev, ga.K, h->pack};
+      PackArgs al{ga.L + ga.c0, ga.ldl, ga.c1 - ga.c0, Q, ga.Kdev, ga.K, pl};
+      k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nr), 256, 0, st>>>(aw);
+      k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nc), 256, 0, st>>>(al);
+      TcArgs ta{ga.C, ga.ldc, ga.r0, ga.r1, ga.c0, ga.c1, h->pack, pl, Q, ga.Kdev, ga.K, nr, nc, ntiles, h->d_err};
+      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, h->nsm);
+      switch (h->opt.mixed_flush) {
+        case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+        case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+        case 4: k_syrk_tc<4><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+        case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+        default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+      }
+      h->launches += 3;
+      h->syrk_launches++;
+    }
+  } else {
+    k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
+    h->launches++;
+    h->syrk_launches++;
+  }
   if (h->profiling) CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
   return RVG_OK;
 }
@@ -1256,7 +1287,7 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
         k_lf_w<<<blocks_for(m - oe, 256), 256, 0, st>>>(a);
         h->launches++;
         SyrkArgs ga{a.a, m, a.wo, m - oe, a.a + cs * m, m, oe, m, oe, p, 0, &a.st->bne};
-        int rc = launch_syrk(h, ga);
+        int rc = launch_syrk(h, ga, bcols);
         if (rc) return rc;
         syrk = true;
       }
@@ -1454,7 +1485,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       if (!(f.flags & FF_HAS_CB) || f.k == 0 || !(f.m >= h->opt.large_front_threshold && f.nfs >= 256)) continue;
       SyrkArgs ga{A.cbase + f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
                   0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
-      if ((rc = launch_syrk(h, ga))) return rc;
+      if ((rc = launch_syrk(h, ga, f.k))) return rc;
       cb_syrk_fronts.push_back(s);
     }
     CK(cudaEventRecord(h->ev[4], st));
@@ -1463,10 +1494,16 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     k_get_counts<<<blocks_for(nw, 128), 128, 0, st>>>(d_ids, nw, h->d_fronts, (int32_t*)(D + o_cnt));
     if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4) * 4))) return rc;
     CK(cudaMemcpyAsync(h->h_counts, D + o_cnt, (size_t)3 * nw * 4, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h->h_counts + 3 * nw, h->d_err, 4, cudaMemcpyDeviceToHost, st));
     {
       double ts0 = now_ms();
       CK(cudaStreamSynchronize(st));
       h->host_sync_ms += now_ms() - ts0;
+    }
+    if (h->h_counts[3 * nw]) {
+      CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
+      set_error("a tensor-core Schur update gave up waiting on its pipeline (device timeout)");
+      return RVG_ERR_DEVICE_TIMEOUT;
     }
     for (int i = 0; i < nw; ++i) {
       DFront& f = h->h_fronts[wave[i]];
@@ -1550,7 +1587,7 @@ void rvg_default_options(rvg_options* o) {
   o->fallback_bk = 1;
   o->large_front_threshold = 2048;
   o->precision = 0;
-  o->reserved = 0;
+  o->mixed_flush = 4;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347
@@ -1566,6 +1603,10 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347
   if (o.nemin < 1) { set_error("nemin must be >= 1"); return RVG_ERR_INVALID_INPUT; }
   if (o.large_front_threshold < 1) { set_error("large_front_threshold must be >= 1"); return RVG_ERR_INVALID_INPUT; }
   if (o.precision != 0 && o.precision != 1) { set_error("precision must be 0 (FP64) or 1 (mixed)"); return RVG_ERR_INVALID_INPUT; }
+  if (o.mixed_flush != 0 && o.mixed_flush != 1 && o.mixed_flush != 2 && o.mixed_flush != 4 && o.mixed_flush != 8) {
+    set_error("mixed_flush must be 0, 1, 2, 4 or 8");
+    return RVG_ERR_INVALID_INPUT;
+  }
   return RVG_OK;
 }
 
@@ -1626,7 +1667,14 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   CK(cudaMallocHost((void**)&h->h_norms, 4 * sizeof(double)));
   if ((rc = presize_arenas(h.get()))) return (rvg_status)rc;
   CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<TC_NO_FLUSH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+  CK(cudaMallocAsync((void**)&h->d_err, sizeof(int32_t), st));
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
   CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
   CK(cudaMallocAsync((void**)&h->d_scal, std::max<int64_t>(n, 1) * 8, st));
   CK(cudaStreamSynchronize(st));
@@ -2027,7 +2075,8 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack);
+  fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
   if (h->h_stage) cudaFreeHost(h->h_stage);

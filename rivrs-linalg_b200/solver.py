@@ -51,6 +51,7 @@ class FactorOptions:
     fallback_bunch_kaufman: bool = True
     large_front_threshold: int = 2048  # B200 scheduling only; results do not depend on it
     precision: str = "fp64"  # "fp64" (plain) or "mixed" (split-TF32 Schur updates; pair with solve_refine)
+    mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
@@ -59,7 +60,8 @@ class FactorOptions:
                                  failed_pivot_tpp=int(self.failed_pivot_tpp),
                                  fallback_bk=int(self.fallback_bunch_kaufman),
                                  large_front_threshold=self.large_front_threshold,
-                                 precision={"fp64": 0, "mixed": 1}[self.precision])
+                                 precision={"fp64": 0, "mixed": 1}[self.precision],
+                                 mixed_flush=self.mixed_flush)
 
 
 class SparseError(RuntimeError):

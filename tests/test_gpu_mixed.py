@@ -1,5 +1,6 @@
-"""Mixed form: the large Schur-complement updates on the split-TF32 tensor path,
-everything else FP64, then FP64 iterative refinement (rvg_solve_refine).
+"""Mixed form: the large Schur-complement updates on the TF32 tensor cores
+(tcgen05, operands split hi + lo), everything else FP64, then FP64 iterative
+refinement (rvg_solve_refine).
 
 The mixed factor is not bit-identical to the oracle (its products are rounded
 differently), so the gates are the ones the solution must meet: exact
@@ -37,9 +38,9 @@ def test_mixed_reaches_fp64_accuracy(rv, name):
         import scipy.sparse as sp
         s = rv.problems.from_scipy("dense700", sp.csc_matrix(a))
     b = rv.problems.rhs_normal(s.n, 3)
-    for precision in ("fp64", "mixed"):
-        x, iters, err, inertia = factor_refine(rv, s, b, precision=precision, **SMALL_LARGE)
-        assert err <= 1e-14, (precision, err, iters)
+    for precision, flush in (("fp64", 2), ("mixed", 1), ("mixed", 2), ("mixed", 8), ("mixed", 0)):
+        x, iters, err, inertia = factor_refine(rv, s, b, precision=precision, mixed_flush=flush, **SMALL_LARGE)
+        assert err <= 1e-14, (precision, flush, err, iters)
         assert rv.problems.backward_error(s, x, b) <= 1e-14
         if s.inertia is not None:
             assert inertia == s.inertia
@@ -57,3 +58,5 @@ def test_refine_errors(rv):
         solver.solve_refine(np.ones(s.n + 2))
     with pytest.raises(rv.InvalidInput):
         solver.factor(None, rv.FactorOptions(precision="fp64", threshold=2.0))
+    with pytest.raises(rv.InvalidInput):
+        solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=3))
