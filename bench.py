@@ -317,6 +317,7 @@ def main():
     e2e = max_over_ranks(statistics.mean(e2e_times))
     bwd_e2e = rv.problems.backward_error(s, xh, b)
 
+    work = solver.work()
     dpeak = gemm_peak_tflops(torch, torch.float64)
     tpeak = gemm_peak_tflops(torch, torch.float32)
     if chosen_name == "mixed":
@@ -370,6 +371,8 @@ def main():
                          "share_of_step": (syrk_ms / args.steps * 1e-3) / t_step if t_step else None},
             "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
                                                "host_total_ms", "host_alloc_ms", "host_sync_ms")},
+            "parts_ms": prof["part_ms"],
+            "work": work,
             "step_wall_s": walls, "step_event_s": times,
             "peak_device_bytes": prof["peak_bytes"],
             "clocks": clk,

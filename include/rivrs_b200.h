@@ -182,7 +182,32 @@ typedef struct {
   /* host wall time of the last factor: total, in allocation calls, waiting
    * in stream synchronisations */
   double host_total_ms, host_alloc_ms, host_sync_ms;
+  /* device time of the last factor by kind of work (CUDA events between
+   * consecutive launches, profiling mode only), indexed by rvg_part */
+  double part_ms[16];
 } rvg_profile;
+
+/* Indices of rvg_profile.part_ms.  Large fronts (whole GPU per front): */
+enum {
+  RVG_PART_LF_SETUP = 0,   /* per-front and per-outer-block bookkeeping */
+  RVG_PART_LF_BLOCK = 1,   /* 32x32 diagonal block, complete pivoting */
+  RVG_PART_LF_PANEL = 2,   /* TRSM + D^-1 of the rows below, threshold test */
+  RVG_PART_LF_POST = 3,    /* first failing column */
+  RVG_PART_LF_UPDATE = 4,  /* rank-32 update inside the outer block */
+  RVG_PART_LF_DELAY = 5,   /* delayed columns to the end */
+  RVG_PART_LF_PROP = 6,    /* row order propagated to earlier columns */
+  RVG_PART_LF_W = 7,       /* W = L D of the outer block */
+  RVG_PART_LF_SYRK = 8,    /* deferred trailing Schur update */
+  RVG_PART_LF_OUTER = 9,   /* end of outer block */
+  /* batched fronts and contribution blocks: */
+  RVG_PART_TPP = 10,       /* warp-per-front TPP fronts */
+  RVG_PART_APTP = 11,      /* CTA-per-front APTP fronts */
+  RVG_PART_CB_W = 12,      /* W = L21 D of contribution blocks */
+  RVG_PART_CB_GEMM = 13,   /* small contribution GEMMs (batched) */
+  RVG_PART_CB_SYRK = 14,   /* large contribution GEMMs */
+  RVG_PART_OTHER = 15,
+  RVG_PARTS = 16
+};
 rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable);
 rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* out);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */

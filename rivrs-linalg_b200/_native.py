@@ -47,10 +47,19 @@ class Profile(C.Structure):
                 ("dense_ms", C.c_double), ("cbgemm_ms", C.c_double), ("syrk_ms", C.c_double),
                 ("syrk_flops", C.c_double), ("syrk_launches", i64), ("factor_launches", i64),
                 ("solve_launches", i64), ("peak_bytes", i64), ("host_total_ms", C.c_double),
-                ("host_alloc_ms", C.c_double), ("host_sync_ms", C.c_double)]
+                ("host_alloc_ms", C.c_double), ("host_sync_ms", C.c_double), ("part_ms", C.c_double * 16)]
+
+    PARTS = ("lf_setup", "lf_block", "lf_panel", "lf_post", "lf_update", "lf_delay", "lf_prop", "lf_w", "lf_syrk",
+             "lf_outer", "tpp", "aptp", "cb_w", "cb_gemm", "cb_syrk", "other")
 
     def as_dict(self):
-        return {k: (float(getattr(self, k)) if t is C.c_double else int(getattr(self, k))) for k, t in self._fields_}
+        d = {}
+        for k, t in self._fields_:
+            if k == "part_ms":
+                d[k] = {n: float(v) for n, v in zip(self.PARTS, self.part_ms)}
+            else:
+                d[k] = float(getattr(self, k)) if t is C.c_double else int(getattr(self, k))
+        return d
 
 
 class RvgError(RuntimeError):

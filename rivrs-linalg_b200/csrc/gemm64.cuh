@@ -38,6 +38,11 @@ struct SyrkArgs {
   int64_t r0, r1, c0, c1;
   int64_t K;
   const int32_t* Kdev;  // when set, K is read from device memory
+  // k_syrk_inner only: the region starts on the device: rows and
+  // columns at ts = *dk + *dbs (r0 = c0 = 0 on the host), L's columns at
+  // *dk, and W is indexed by absolute row
+  const int32_t* dk;
+  const int32_t* dbs;
 };
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
@@ -165,15 +170,23 @@ struct DmmaCfg {
   static constexpr size_t SMEM = (size_t)G_STAGES * G_BK * (LDW + LDL) * sizeof(double);
 };
 
-template <int WR, int WC, int MINB>
+template <int WR, int WC, int MINB, bool DEV = false>
 __global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
   using Cfg = DmmaCfg<WR, WC>;
   constexpr int NT = Cfg::NT, BM = Cfg::BM, BN = Cfg::BN, LDW = Cfg::LDW, LDL = Cfg::LDL;
+  if (DEV) {
+    const int64_t k = *a.dk, ts = k + *a.dbs;
+    a.L += k * a.ldl;
+    a.W += ts;
+    a.r0 = ts;
+    a.c0 = ts;
+  }
   const int64_t i0 = a.r0 + (int64_t)blockIdx.y * BM;
   const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
   if (i0 + BM - 1 < j0) return;
   const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
+  if (K <= 0) return;  // nothing eliminated: C unchanged
   extern __shared__ double gsm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wr = (warp % WR) * 32, wc = (warp / WR) * 32;
@@ -265,6 +278,8 @@ using SyrkMain = DmmaCfg<RVG_SYRK_WR, RVG_SYRK_WC>;
 constexpr int G_T = SyrkMain::NT;
 constexpr size_t G_SMEM = SyrkMain::SMEM;
 #define k_syrk_lower k_syrk_dmma<RVG_SYRK_WR, RVG_SYRK_WC, RVG_SYRK_MINB>
+// the same kernel with the region start read from the device (SyrkArgs::dk)
+#define k_syrk_inner k_syrk_dmma<RVG_SYRK_WR, RVG_SYRK_WC, 3, true>
 
 template <class Cfg>
 inline dim3 syrk_grid_cfg(const SyrkArgs& a) {

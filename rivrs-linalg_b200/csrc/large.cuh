@@ -12,9 +12,10 @@
 //     lf_post    1 CTA    2x2 boundary adjustment, restore of the failed part
 //                         of the diagonal block, failed x failed cross term,
 //                         D entries
-//     lf_update  grid     restore of the failed panel columns, rank-nelim
-//                         update of the outer block's trailing columns, the
+//     lf_wi      grid     restore of the failed panel columns, W = L D, the
 //                         trailing x failed cross term
+//     k_syrk_dmma         rank-nelim update of the outer block's trailing
+//                         columns (region start read from the device)
 //     lf_delay   1 CTA    delayed columns to the end of the outer block
 //   per 256-column outer block:
 //     lf_prop    grid     row permutation of the front's earlier columns
@@ -51,7 +52,7 @@ struct LFArgs {
   LFState* st;
   int32_t* lp;      // outer-block local column order (nb)
   double* pb;       // panel backup, rows x 32 (ld = bm)
-  double* w;        // inner W, rows x 32 (row-major, stride 32)
+  double* w;        // inner W, rows x 32 (column-major, ld = rows of the view)
   double* wo;       // outer W, (m - oe) x nb (column-major)
   int64_t cs, bcols, nfsb;  // outer block start, width, NFS boundary (global p)
   DevOpts o;
@@ -129,8 +130,11 @@ __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
   if (tid == 0) { st->bs = bs; st->bnelim = bnelim; st->eff = bnelim; }
 }
 
-// panel rows: backup, permute, TRSM, D^-1, threshold scan (grid over rows)
-__global__ void __launch_bounds__(256) k_lf_panel(LFArgs A) {
+// panel rows: backup, permute, TRSM, D^-1, threshold scan (grid over rows,
+// one row per thread, the row's 32 values in registers: every index into
+// them is a compile-time constant)
+constexpr int LF_PANEL_T = 64;
+__global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
   LFState* st = A.st;
   const int bnelim = st->bnelim;
   if (bnelim == 0) return;
@@ -158,31 +162,43 @@ __global__ void __launch_bounds__(256) k_lf_panel(LFArgs A) {
   const int64_t be = k + bs;
   const double bound = 1.0 / A.o.threshold;
   if (r >= be && r < bm) {
-    double x[IBMAX], raw[IBMAX];
-    for (int i = 0; i < bs; ++i) raw[i] = V(r, k + i);
-    for (int i = 0; i < bs; ++i) A.pb[r + (int64_t)i * bm] = raw[i];
-    for (int i = 0; i < bs; ++i) x[i] = raw[bperm[i]];
-    for (int j = 0; j < bnelim; ++j)
-      for (int l = 0; l < j; ++l) x[j] = __fma_rn(-x[l], T[j][l], x[j]);
-    int c = 0;
-    while (c < bnelim) {
-      if (bdt[c] == PT_1X1) { x[c] = __dmul_rn(x[c], 1.0 / bdd[c]); c += 1; }
-      else {
-        double A_ = bdd[c], B_ = bdo[c], C_ = bdd[c + 1];
-        double inv_det = 1.0 / __dsub_rn(__dmul_rn(A_, C_), __dmul_rn(B_, B_));
-        double x1 = x[c], x2 = x[c + 1];
+    double x[IBMAX];
+#pragma unroll
+    for (int i = 0; i < IBMAX; ++i)
+      if (i < bs) A.pb[r + (int64_t)i * bm] = V(r, k + i);
+#pragma unroll
+    for (int i = 0; i < IBMAX; ++i) x[i] = i < bs ? V(r, k + bperm[i]) : 0.0;
+#pragma unroll
+    for (int j = 1; j < IBMAX; ++j)
+      if (j < bnelim) {
+#pragma unroll
+        for (int l = 0; l < j; ++l) x[j] = __fma_rn(-x[l], T[j][l], x[j]);
+      }
+    // D^-1 over the pivots (the second column of a 2x2 is handled with its first)
+#pragma unroll
+    for (int c = 0; c < IBMAX; ++c) {
+      if (c >= bnelim) continue;
+      if (bdt[c] == PT_1X1) {
+        x[c] = __dmul_rn(x[c], 1.0 / bdd[c]);
+      } else if (bdt[c] == PT_2X2 && c + 1 < IBMAX) {
+        const double A_ = bdd[c], B_ = bdo[c], C_ = bdd[c + 1];
+        const double inv_det = 1.0 / __dsub_rn(__dmul_rn(A_, C_), __dmul_rn(B_, B_));
+        const double x1 = x[c], x2 = x[c + 1];
         x[c] = __dmul_rn(__dsub_rn(__dmul_rn(x1, C_), __dmul_rn(x2, B_)), inv_det);
         x[c + 1] = __dmul_rn(__dsub_rn(__dmul_rn(x2, A_), __dmul_rn(x1, B_)), inv_det);
-        c += 2;
       }
     }
-    for (int i = 0; i < bs; ++i) V(r, k + i) = x[i];
+#pragma unroll
+    for (int i = 0; i < IBMAX; ++i)
+      if (i < bs) V(r, k + i) = x[i];
+    // first pivot (1x1 or 2x2 start) with an entry at or above 1/u
     int fail = bnelim;
-    c = 0;
-    while (c < bnelim) {
-      int w = bdt[c] == PT_2X2 ? 2 : 1;
-      if (fabs(x[c]) >= bound || (w == 2 && fabs(x[c + 1]) >= bound)) { fail = c; break; }
-      c += w;
+#pragma unroll
+    for (int c = IBMAX - 1; c >= 0; --c) {
+      if (c >= bnelim || bdt[c] == PT_2X2B) continue;
+      const bool two = bdt[c] == PT_2X2;
+      const double x2 = c + 1 < IBMAX ? x[c + 1 < IBMAX ? c + 1 : c] : 0.0;
+      if (fabs(x[c]) >= bound || (two && fabs(x2) >= bound)) fail = c;
     }
     if (fail < bnelim) atomicMin(&s_fail, fail);
   }
@@ -254,85 +270,60 @@ __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
   }
 }
 
-// restore of the failed panel columns, trailing update inside the outer
-// block, trailing x failed cross term (grid over rows >= ts, one row per thread)
-__global__ void __launch_bounds__(256) k_lf_update(LFArgs A) {
+// Rows below the inner block (one thread per row): restore of the failed
+// panel columns from the backup, W = L D over the eliminated columns
+// (column-major, ld = rows of the view, indexed by absolute row) and the
+// trailing x failed cross term.  The rank-nelim update of the outer block's
+// trailing columns that follows is the DMMA GEMM (k_syrk_dmma with the
+// region start read from the device), the same fma chain per entry.
+__global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
   LFState* st = A.st;
   const int bnelim = st->bnelim;
   if (bnelim == 0) return;
   const int bs = st->bs, k = st->k, nelim = st->nelim, eff = st->eff;
   const int64_t bm = A.m - A.cs;
   const int64_t ts = k + bs;
-  const int64_t pl = A.bcols;  // trailing columns updated here: [ts, pl)
-  __shared__ double Ls[32][IBMAX + 1];
+  const int nf = bs - nelim;
+  __shared__ double Ls[IBMAX][IBMAX + 1];
   __shared__ int bperm[IBMAX];
   __shared__ int8_t bdt[IBMAX];
   __shared__ double bdd[IBMAX], bdo[IBMAX];
+  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
   if (threadIdx.x < IBMAX) {
     bperm[threadIdx.x] = st->bperm[threadIdx.x];
     bdt[threadIdx.x] = st->bdt[threadIdx.x];
     bdd[threadIdx.x] = st->bdd[threadIdx.x];
     bdo[threadIdx.x] = st->bdo[threadIdx.x];
   }
-  __syncthreads();
-  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
-  const int64_t i = ts + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool row = i < bm;
-  if (row && eff < bnelim) {
-    for (int j = eff; j < bs; ++j) V(i, k + j) = A.pb[i + (int64_t)bperm[j] * bm];
-  }
-  if (nelim == 0) return;
-  double w[IBMAX];
-  if (row) {
-    const double* l = &V(i, k);
-    int c = 0;
-    while (c < nelim) {
-      if (bdt[c] == PT_1X1) { w[c] = __dmul_rn(l[c * A.m], bdd[c]); c += 1; }
-      else {
-        double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
-        w[c] = __dadd_rn(__dmul_rn(l1, bdd[c]), __dmul_rn(l2, bdo[c]));
-        w[c + 1] = __dadd_rn(__dmul_rn(l1, bdo[c]), __dmul_rn(l2, bdd[c + 1]));
-        c += 2;
-      }
-    }
-  }
-  // trailing columns of the outer block, 32 at a time through shared memory
-  const int64_t i_lo = ts + (int64_t)blockIdx.x * blockDim.x;
-  for (int64_t j0 = ts; j0 < pl; j0 += 32) {
-    const int nj = (int)((pl - j0) < 32 ? (pl - j0) : 32);
-    if (j0 > i_lo + (int64_t)blockDim.x - 1) break;  // all rows of this CTA are above these columns
-    __syncthreads();
-    for (int t = threadIdx.x; t < nj * nelim; t += blockDim.x) {
-      int jj = t % nj, c = t / nj;
-      Ls[jj][c] = V(j0 + jj, k + c);
-    }
-    __syncthreads();
-    if (row) {
-      for (int jj = 0; jj < nj; ++jj) {
-        int64_t j = j0 + jj;
-        if (j > i) break;
-        double acc = V(i, j);
-        for (int c = 0; c < nelim; ++c) acc = __fma_rn(-w[c], Ls[jj][c], acc);
-        V(i, j) = acc;
-      }
-    }
-  }
-  // trailing x failed cross term
-  if (nelim < bs) {
-    const int nf = bs - nelim;
-    __syncthreads();
+  if (nelim > 0 && nf > 0)
     for (int t = threadIdx.x; t < nf * nelim; t += blockDim.x) {
       int jj = t % nf, c = t / nf;
       Ls[jj][c] = V(k + nelim + jj, k + c);
     }
-    __syncthreads();
-    if (row) {
-      for (int jj = 0; jj < nf; ++jj) {
-        double s = 0.0;
-        for (int c = 0; c < nelim; ++c) s = __dadd_rn(s, __dmul_rn(w[c], Ls[jj][c]));
-        V(i, k + nelim + jj) = __dsub_rn(V(i, k + nelim + jj), s);
-      }
+  __syncthreads();
+  const int64_t i = ts + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= bm) return;
+  if (eff < bnelim)
+    for (int j = eff; j < bs; ++j) V(i, k + j) = A.pb[i + (int64_t)bperm[j] * bm];
+  if (nelim == 0) return;
+  double* W = A.w + i;
+  const double* l = &V(i, k);
+  int c = 0;
+  while (c < nelim) {
+    if (bdt[c] == PT_1X1) {
+      W[(int64_t)c * bm] = __dmul_rn(l[c * A.m], bdd[c]);
+      c += 1;
+    } else {
+      const double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
+      W[(int64_t)c * bm] = __dadd_rn(__dmul_rn(l1, bdd[c]), __dmul_rn(l2, bdo[c]));
+      W[(int64_t)(c + 1) * bm] = __dadd_rn(__dmul_rn(l1, bdo[c]), __dmul_rn(l2, bdd[c + 1]));
+      c += 2;
     }
+  }
+  for (int jj = 0; jj < nf; ++jj) {
+    double s = 0.0;
+    for (int c2 = 0; c2 < nelim; ++c2) s = __dadd_rn(s, __dmul_rn(W[(int64_t)c2 * bm], Ls[jj][c2]));
+    V(i, k + nelim + jj) = __dsub_rn(V(i, k + nelim + jj), s);
   }
 }
 

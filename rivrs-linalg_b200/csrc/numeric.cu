@@ -953,6 +953,10 @@ struct rvg_handle {
   std::vector<cudaEvent_t> ev_pool;
   size_t ev_used = 0;
   double syrk_flops = 0, syrk_ms = 0;
+  std::vector<cudaEvent_t> mk_pool;                  // per-kind marks (profiling): event, kind
+  std::vector<int> mk_kind;
+  size_t mk_used = 0;
+  double part_ms[RVG_PARTS] = {};
   int64_t syrk_launches = 0, launches = 0, factor_launches = 0, solve_launches = 0;
   int64_t arena_bytes = 0, peak_bytes = 0;
   double host_alloc_ms = 0, host_sync_ms = 0, host_total_ms = 0;
@@ -965,6 +969,29 @@ namespace {
 
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Profiling marks: the time between a mark and the one before it is charged
+// to the later mark's kind (a kind < 0 starts a new segment).  Read back
+// after each stream synchronisation.
+void mark(rvg_handle* h, int kind) {
+  if (!h->profiling) return;
+  if (h->mk_used == h->mk_pool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    h->mk_pool.push_back(e);
+    h->mk_kind.push_back(-1);
+  }
+  cudaEventRecord(h->mk_pool[h->mk_used], h->st);
+  h->mk_kind[h->mk_used++] = kind;
+}
+void mark_flush(rvg_handle* h) {
+  for (size_t i = 1; i < h->mk_used; ++i) {
+    float ms = 0;
+    if (h->mk_kind[i] >= 0 && cudaEventElapsedTime(&ms, h->mk_pool[i - 1], h->mk_pool[i]) == cudaSuccess)
+      h->part_ms[h->mk_kind[i]] += ms;
+  }
+  h->mk_used = 0;
 }
 
 template <class T>
@@ -1259,6 +1286,7 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
   a.nfsb = p;
   a.o = dop;
   const int two_level = p > nb;
+  mark(h, -1);
   k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
   h->launches++;
   int64_t rem = p, gne = 0;
@@ -1267,33 +1295,57 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
     a.cs = cs;
     a.bcols = bcols;
     k_lf_begin_outer<<<1, 256, 0, st>>>(a);
-    const unsigned rows_grid = blocks_for(bm, 256);
+    mark(h, RVG_PART_LF_SETUP);
     const int64_t ninner = (bcols + ib - 1) / ib;
+    // the inner block's trailing update: rows and columns from ts = k + bs
+    // (device values) within the outer block's view
+    SyrkArgs gi{};
+    gi.C = a.a + cs + cs * m;
+    gi.ldc = m;
+    gi.W = a.w;
+    gi.ldw = bm;
+    gi.L = a.a + cs + cs * m;
+    gi.ldl = m;
+    gi.r1 = bm;
+    gi.c1 = bcols;
+    gi.Kdev = &a.st->nelim;
+    gi.dk = &a.st->k;
+    gi.dbs = &a.st->bs;
     for (int64_t it = 0; it < ninner; ++it) {
       k_lf_block<<<1, NT, 0, st>>>(a);
-      k_lf_panel<<<rows_grid, 256, 0, st>>>(a);
+      mark(h, RVG_PART_LF_BLOCK);
+      k_lf_panel<<<blocks_for(bm, LF_PANEL_T), LF_PANEL_T, 0, st>>>(a);
+      mark(h, RVG_PART_LF_PANEL);
       k_lf_post<<<1, 256, 0, st>>>(a);
-      k_lf_update<<<rows_grid, 256, 0, st>>>(a);
+      mark(h, RVG_PART_LF_POST);
+      k_lf_wi<<<blocks_for(bm, 256), 256, 0, st>>>(a);
+      k_syrk_inner<<<syrk_grid(gi), G_T, G_SMEM, st>>>(gi);
+      mark(h, RVG_PART_LF_UPDATE);
       k_lf_delay<<<1, NT, 0, st>>>(a);
+      mark(h, RVG_PART_LF_DELAY);
     }
-    h->launches += 1 + 5 * ninner;
+    h->launches += 1 + 6 * ninner;
     bool syrk = false;
     if (two_level) {
       if (cs > 0) {
         k_lf_prop<<<(unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256, (size_t)bcols * LF_PROP_COLS * 8, st>>>(a);
         h->launches++;
+        mark(h, RVG_PART_LF_PROP);
       }
       if (oe < p) {
         k_lf_w<<<blocks_for(m - oe, 256), 256, 0, st>>>(a);
         h->launches++;
+        mark(h, RVG_PART_LF_W);
         SyrkArgs ga{a.a, m, a.wo, m - oe, a.a + cs * m, m, oe, m, oe, p, 0, &a.st->bne};
         int rc = launch_syrk(h, ga, bcols);
         if (rc) return rc;
+        mark(h, RVG_PART_LF_SYRK);
         syrk = true;
       }
     }
     k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level);
     h->launches++;
+    mark(h, RVG_PART_LF_OUTER);
     CK(cudaGetLastError());
     int32_t g = 0;
     CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
@@ -1302,12 +1354,15 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
       CK(cudaStreamSynchronize(st));
       h->host_sync_ms += now_ms() - ts0;
     }
+    mark_flush(h);
+    mark(h, -1);
     if (syrk) h->syrk_flops += 2.0 * (double)(g - gne) * lower_entries(oe, m, oe, p);
     gne = g;
     rem -= bcols;
   }
   k_lf_finish<<<1, 32, 0, st>>>(a, h->d_fronts, s);
   h->launches++;
+  mark(h, RVG_PART_LF_SETUP);
   CK(cudaGetLastError());
   return RVG_OK;
 }
@@ -1334,6 +1389,8 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   h->host_alloc_ms = 0;
   h->host_sync_ms = 0;
   h->ev_used = 0;
+  h->mk_used = 0;
+  for (double& v : h->part_ms) v = 0;
   h->syrk_flops = 0;
   h->syrk_ms = 0;
   h->syrk_launches = 0;
@@ -1466,26 +1523,33 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     for (size_t w2 = 0; w2 < w; ++w2)
       if (cb_block[w2] >= 0 && cb_release_at[w2] == (int64_t)w) { cb_release(h, cb_block[w2], cb_len[w2]); cb_block[w2] = -1; }
     // ---- dense factorization
+    mark(h, -1);
     if (!tpp_ids.empty())
       k_tpp<<<blocks_for(tpp_ids.size(), 8), 256, 0, st>>>((const int32_t*)(D + o_tpp), (int)tpp_ids.size(),
                                                             h->d_fronts, A, dop);
+    mark(h, RVG_PART_TPP);
     if (!aptp_ids.empty())
       k_aptp<<<(unsigned)aptp_ids.size(), NT, 0, st>>>((const int32_t*)(D + o_aptp), (int)aptp_ids.size(),
                                                         h->d_fronts, A, dop);
+    mark(h, RVG_PART_APTP);
     for (int32_t s : large_ids)
       if ((rc = factor_large_front(h, s, A, dop))) return rc;
     CK(cudaEventRecord(h->ev[3], st));
     // ---- contribution GEMM (fronts with nothing eliminated skip inside)
+    mark(h, -1);
     if (!witems.empty())
       k_cb_w<<<(unsigned)witems.size(), 256, 0, st>>>((const TileItem*)(D + o_w), h->d_fronts, A);
+    mark(h, RVG_PART_CB_W);
     if (!gitems.empty())
       k_cb_gemm<<<(unsigned)gitems.size(), 256, 0, st>>>((const TileItem*)(D + o_g), h->d_fronts, A);
+    mark(h, RVG_PART_CB_GEMM);
     for (int64_t s : wave) {
       const DFront& f = h->h_fronts[s];
       if (!(f.flags & FF_HAS_CB) || f.k == 0 || !(f.m >= h->opt.large_front_threshold && f.nfs >= 256)) continue;
       SyrkArgs ga{A.cbase + f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
                   0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
       if ((rc = launch_syrk(h, ga, f.k))) return rc;
+      mark(h, RVG_PART_CB_SYRK);
       cb_syrk_fronts.push_back(s);
     }
     CK(cudaEventRecord(h->ev[4], st));
@@ -1500,6 +1564,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       CK(cudaStreamSynchronize(st));
       h->host_sync_ms += now_ms() - ts0;
     }
+    mark_flush(h);
     if (h->h_counts[3 * nw]) {
       CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
       set_error("a tensor-core Schur update gave up waiting on its pipeline (device timeout)");
@@ -1667,6 +1732,7 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   CK(cudaMallocHost((void**)&h->h_norms, 4 * sizeof(double)));
   if ((rc = presize_arenas(h.get()))) return (rvg_status)rc;
   CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
@@ -2058,6 +2124,7 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
   o->host_total_ms = h->host_total_ms;
   o->host_alloc_ms = h->host_alloc_ms;
   o->host_sync_ms = h->host_sync_ms;
+  for (int i = 0; i < RVG_PARTS; ++i) o->part_ms[i] = h->part_ms[i];
   return RVG_OK;
 }
 
@@ -2083,6 +2150,7 @@ void rvg_destroy(rvg_handle* h) {
   if (h->h_counts) cudaFreeHost(h->h_counts);
   if (h->h_norms) cudaFreeHost(h->h_norms);
   for (auto e : h->ev_pool) cudaEventDestroy(e);
+  for (auto e : h->mk_pool) cudaEventDestroy(e);
   for (auto& e : h->ev) if (e) cudaEventDestroy(e);
   delete h;
 }
