@@ -37,12 +37,15 @@ struct SyrkArgs {
   int64_t ldl;
   int64_t r0, r1, c0, c1;
   int64_t K;
-  const int32_t* Kdev;  // when set, K is read from device memory
+  const int32_t* Kdev;  // when set, *Kdev is added to K (columns counted on the device)
   // k_syrk_inner only: the region starts on the device: rows and
   // columns at ts = *dk + *dbs (r0 = c0 = 0 on the host), L's columns at
   // *dk, and W is indexed by absolute row
   const int32_t* dk;
   const int32_t* dbs;
+  // when set, the update runs only if *cond < cond_lt (decided on the device)
+  const int32_t* cond;
+  int32_t cond_lt;
 };
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
@@ -71,7 +74,8 @@ __global__ void __launch_bounds__(NT, MINB) k_syrk_lower_t(SyrkArgs a) {
   const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
   if (i0 + BM - 1 < j0) return;  // tile entirely above the diagonal
-  const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
+  if (a.cond && *a.cond >= a.cond_lt) return;
+  const int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   extern __shared__ double gsm[];
   // stage s: W chunk [k][BM] then L chunk [k][BN]
   const int tid = threadIdx.x;
@@ -185,7 +189,8 @@ __global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
   const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
   if (i0 + BM - 1 < j0) return;
-  const int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
+  if (a.cond && *a.cond >= a.cond_lt) return;
+  const int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K <= 0) return;  // nothing eliminated: C unchanged
   extern __shared__ double gsm[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

@@ -19,11 +19,18 @@
 //     lf_delay   1 CTA    delayed columns to the end of the outer block
 //   per 256-column outer block:
 //     lf_prop    grid     row permutation of the front's earlier columns
-//     lf_w       grid     W = L D for the rows below the outer block
-//     k_syrk_lower        the deferred rank-nelim update of every later
-//                         column (mathematically the reference's per-block
-//                         updates; each output keeps its fma chain in the
-//                         same order, so the result is bit-identical)
+//     lf_w       grid     W = L D for the rows below the outer block, into
+//                         the window of pending columns
+//     Schur GEMM          the deferred update (update_trailing), split in
+//                         two: the next outer block's columns take every
+//                         pending column at once (near field); the columns
+//                         after it (far field) only when the window is full
+//                         (LF_WINDOW outer blocks) or when this block delayed
+//                         a column (decided on the device), so each far-field
+//                         entry is read and written once per window instead
+//                         of once per block.  Each entry still takes one fma
+//                         chain over the eliminated columns in order, so the
+//                         result is bit-identical to the per-block update.
 //     lf_outer   1 CTA    column order, delays to the end of the remaining
 //                         fully-summed columns
 #pragma once
@@ -53,7 +60,8 @@ struct LFArgs {
   int32_t* lp;      // outer-block local column order (nb)
   double* pb;       // panel backup, rows x 32 (ld = bm)
   double* w;        // inner W, rows x 32 (column-major, ld = rows of the view)
-  double* wo;       // outer W, (m - oe) x nb (column-major)
+  double* wo;       // pending W (column-major, ld wld): row i, pending column c at wo[(i - wrow0) + c * wld]
+  int64_t wld, wrow0, wcol0;  // leading dimension, first row, this block's first pending column
   int64_t cs, bcols, nfsb;  // outer block start, width, NFS boundary (global p)
   DevOpts o;
 };
@@ -380,24 +388,25 @@ __global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
   }
 }
 
-// W = L D for the rows below the outer block, over its bne eliminated columns
+// W = L D for the rows below the outer block, over its bne eliminated
+// columns, appended to the pending window
 __global__ void k_lf_w(LFArgs A) {
   const int bne = A.st->bne;
   const int64_t oe = A.cs + A.bcols;
   const int64_t i = oe + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.m) return;
-  const int64_t ldw = A.m - oe;
   const int8_t* dt = A.D.type + A.cs;
   const double* dd = A.D.diag + A.cs;
   const double* dof = A.D.off + A.cs;
   const double* l = A.a + i + A.cs * A.m;
+  double* w = A.wo + (i - A.wrow0) + A.wcol0 * A.wld;
   int c = 0;
   while (c < bne) {
-    if (dt[c] == PT_1X1) { A.wo[(i - oe) + c * ldw] = __dmul_rn(l[c * A.m], dd[c]); c += 1; }
+    if (dt[c] == PT_1X1) { w[c * A.wld] = __dmul_rn(l[c * A.m], dd[c]); c += 1; }
     else {
       double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
-      A.wo[(i - oe) + c * ldw] = __dadd_rn(__dmul_rn(l1, dd[c]), __dmul_rn(l2, dof[c]));
-      A.wo[(i - oe) + (c + 1) * ldw] = __dadd_rn(__dmul_rn(l1, dof[c]), __dmul_rn(l2, dd[c + 1]));
+      w[c * A.wld] = __dadd_rn(__dmul_rn(l1, dd[c]), __dmul_rn(l2, dof[c]));
+      w[(c + 1) * A.wld] = __dadd_rn(__dmul_rn(l1, dof[c]), __dmul_rn(l2, dd[c + 1]));
       c += 2;
     }
   }

@@ -944,6 +944,7 @@ struct rvg_handle {
   double* scratch = nullptr; size_t scratch_cap = 0; // per-wave scratch, persistent across factors
   double* cb_arena = nullptr; size_t cb_cap = 0;     // contribution blocks, first-fit by wave
   float* pack = nullptr; size_t pack_cap = 0;        // TF32 hi/lo operand tiles of the mixed-form updates
+  float* wpack = nullptr; size_t wpack_cap = 0;      // the same for a large front's window of pending columns
   int32_t* d_err = nullptr;                          // set by a device wait that timed out
   int nsm = 0;                                       // SMs of the device (persistent grids)
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
@@ -1126,6 +1127,13 @@ DevOpts devopts(const rvg_options& o) {
 
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+// Columns of the pending window of a large front's deferred updates: LF_WINDOW
+// outer blocks, except in the mixed form when the outer block is not a whole
+// number of 128-row tiles (its packed TF32 operands are appended tile- and
+// chunk-aligned): then one block (every block's update applied at once).
+constexpr int64_t LF_WINDOW = 4;
+int64_t lf_window_cols(int64_t nb, bool mixed) { return (!mixed || nb % 128 == 0) ? LF_WINDOW * nb : nb; }
+
 // Arena sizes of the delay-free schedule, computed from the pattern alone
 // (delays can only add to them; the arenas grow in that case).
 int presize_arenas(rvg_handle* h) {
@@ -1146,7 +1154,7 @@ int presize_arenas(rvg_handle* h) {
       bool tpp = x.in_small_leaf || k < ib;
       bool large = !tpp && m >= h->opt.large_front_threshold;
       int64_t sc = tpp ? 0 : (2 * IBMAX * m + nb);
-      if (large) sc = m * (2 * IBMAX + nb) + nb;
+      if (large) sc = m * (2 * IBMAX + LF_WINDOW * nb) + nb;
       if (has_cb) sc = std::max<int64_t>(sc, nfs * k);
       sc_w += sc;
       if (x.parent >= 0) rel[w] = std::max<int64_t>(rel[w], P.height[x.parent]);
@@ -1217,20 +1225,25 @@ double lower_entries(int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
   return e;
 }
 
-// The Schur update C -= W L^T (lower) of one deferred trailing block or one
-// contribution block.  kmax bounds the device-side K (columns eliminated).
+// CUDA events around each Schur GEMM launch (profiling): their sum is the
+// GEMM time the measured rate is based on.
+int syrk_ev(rvg_handle* h) {
+  if (!h->profiling) return RVG_OK;
+  if (h->ev_used + 1 > h->ev_pool.size()) {
+    for (int i = 0; i < 64; ++i) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      h->ev_pool.push_back(e);
+    }
+  }
+  CK(cudaEventRecord(h->ev_pool[h->ev_used++], h->st));
+  return RVG_OK;
+}
+
+// The Schur update C -= W L^T (lower) of one contribution block.  kmax bounds
+// the device-side K (columns eliminated).
 int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
   cudaStream_t st = h->st;
-  if (h->profiling) {
-    if (h->ev_used + 2 > h->ev_pool.size()) {
-      for (int i = 0; i < 64; ++i) {
-        cudaEvent_t e;
-        CK(cudaEventCreate(&e));
-        h->ev_pool.push_back(e);
-      }
-    }
-    CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
-  }
   if (h->opt.precision == 1) {
     const int64_t nr = (ga.r1 - ga.r0 + TC_BM - 1) / TC_BM, nc = (ga.c1 - ga.c0 + TC_BN - 1) / TC_BN;
     const int64_t Q = (kmax + TC_BK - 1) / TC_BK;
@@ -1245,6 +1258,7 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
       k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nc), 256, 0, st>>>(al);
       TcArgs ta{ga.C, ga.ldc, ga.r0, ga.r1, ga.c0, ga.c1, h->pack, pl, Q, ga.Kdev, ga.K, nr, nc, ntiles, h->d_err};
       const unsigned grid = (unsigned)std::min<int64_t>(ntiles, h->nsm);
+      if ((rc = syrk_ev(h))) return rc;
       switch (h->opt.mixed_flush) {
         case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
         case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
@@ -1252,15 +1266,69 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
         case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
         default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
       }
+      if ((rc = syrk_ev(h))) return rc;
       h->launches += 3;
       h->syrk_launches++;
     }
   } else {
+    int rc = syrk_ev(h);
+    if (rc) return rc;
     k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
+    if ((rc = syrk_ev(h))) return rc;
     h->launches++;
     h->syrk_launches++;
   }
-  if (h->profiling) CK(cudaEventRecord(h->ev_pool[h->ev_used++], st));
+  return RVG_OK;
+}
+
+// Deferred update of a large front's columns [c0, c1) (rows [c0, m)) by the
+// window of pending columns [wd, wd + kadd + *kdev): W rows start at wrow
+// (ld m - wrow), L is the panel itself; the mixed form reads the packed
+// window (tile 0 = rows [wrow, wrow + 128), F / 32 chunks per tile).  With
+// cond set the launch only acts if *cond < cond_lt.
+int launch_window_gemm(rvg_handle* h, const LFArgs& a, int64_t m, int64_t c0, int64_t c1, int64_t wd, int64_t wrow,
+                       int64_t F, const float* pk_w, const float* pk_l, int64_t kadd, const int32_t* kdev,
+                       const int32_t* cond, int32_t cond_lt) {
+  cudaStream_t st = h->st;
+  if (c1 <= c0) return RVG_OK;
+  int rc = syrk_ev(h);
+  if (rc) return rc;
+  if (h->opt.precision == 1) {
+    const int64_t Fq = F / TC_BK;
+    const int64_t nr = (m - c0 + TC_BM - 1) / TC_BM, nc = (c1 - c0 + TC_BN - 1) / TC_BN;
+    const int64_t ntiles = tc_count_tiles(nr, nc, c0, c0);
+    const int64_t t0 = (c0 - wrow) / TC_BM;
+    TcArgs ta{a.a, m, c0, m, c0, c1, pk_w + (size_t)t0 * Fq * TC_BLOCK, pk_l + (size_t)t0 * Fq * TC_BLOCK, Fq, kdev,
+              kadd, nr, nc, ntiles, h->d_err, cond, cond_lt};
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, h->nsm);
+    switch (h->opt.mixed_flush) {
+      case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+      case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+      case 4: k_syrk_tc<4><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+      case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+      default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    }
+  } else {
+    SyrkArgs ga{};
+    ga.C = a.a;
+    ga.ldc = m;
+    ga.W = a.wo + (c0 - wrow);
+    ga.ldw = m - wrow;
+    ga.L = a.a + wd * m;
+    ga.ldl = m;
+    ga.r0 = c0;
+    ga.r1 = m;
+    ga.c0 = c0;
+    ga.c1 = c1;
+    ga.K = kadd;
+    ga.Kdev = kdev;
+    ga.cond = cond;
+    ga.cond_lt = cond_lt;
+    k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
+  }
+  if ((rc = syrk_ev(h))) return rc;
+  h->launches++;
+  h->syrk_launches++;
   return RVG_OK;
 }
 
@@ -1282,10 +1350,23 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
   a.pb = sc;
   a.w = sc + m * IBMAX;
   a.wo = sc + 2 * m * IBMAX;
-  a.lp = (int32_t*)(sc + m * (2 * IBMAX + nb));
+  const int64_t F = lf_window_cols(nb, h->opt.precision == 1);
+  a.lp = (int32_t*)(sc + m * (2 * IBMAX + LF_WINDOW * nb));
   a.nfsb = p;
   a.o = dop;
   const int two_level = p > nb;
+  // window of pending columns [wd, gne) of the deferred updates; its W rows start at wrow
+  int64_t wd = 0, wrow = std::min(p, nb);
+  const bool mixed = h->opt.precision == 1;
+  const int64_t Fq = F / TC_BK;
+  float *pk_w = nullptr, *pk_l = nullptr;
+  if (mixed && two_level) {
+    const int64_t tiles = (m + TC_BM - 1) / TC_BM;
+    int rc = ensure_nocopy(h->wpack, h->wpack_cap, (size_t)2 * tiles * Fq * TC_BLOCK, st);
+    if (rc) return rc;
+    pk_w = h->wpack;
+    pk_l = h->wpack + (size_t)tiles * Fq * TC_BLOCK;
+  }
   mark(h, -1);
   k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
   h->launches++;
@@ -1325,7 +1406,8 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
       mark(h, RVG_PART_LF_DELAY);
     }
     h->launches += 1 + 6 * ninner;
-    bool syrk = false;
+    bool flush = false;
+    int64_t kadd = 0, ncol = 0;
     if (two_level) {
       if (cs > 0) {
         k_lf_prop<<<(unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256, (size_t)bcols * LF_PROP_COLS * 8, st>>>(a);
@@ -1333,14 +1415,47 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
         mark(h, RVG_PART_LF_PROP);
       }
       if (oe < p) {
+        // this block's W joins the window [wd, gne + bne)
+        kadd = cs - wd;
+        a.wld = m - wrow;
+        a.wrow0 = wrow;
+        a.wcol0 = kadd;
         k_lf_w<<<blocks_for(m - oe, 256), 256, 0, st>>>(a);
         h->launches++;
         mark(h, RVG_PART_LF_W);
-        SyrkArgs ga{a.a, m, a.wo, m - oe, a.a + cs * m, m, oe, m, oe, p, 0, &a.st->bne};
-        int rc = launch_syrk(h, ga, bcols);
-        if (rc) return rc;
+        // The next outer block is [g, g + min(rem - bcols, nb)); columns past
+        // rem (delayed ones parked at the end) belong to no later block.  The
+        // window is applied everywhere when it is full, or when the next block
+        // is the last one (so no column is left pending for the end of the front).
+        flush = kadd + bcols >= F || rem - bcols < nb;
+        ncol = nb;
+        const int32_t* bne_dev = &a.st->bne;
+        if (mixed) {
+          // append this block's chunks of W (rows [oe, m)) and L (rows [oe, p))
+          const int64_t q0 = kadd / TC_BK, nqb = (bcols + TC_BK - 1) / TC_BK, t0 = (oe - wrow) / TC_BM;
+          PackArgs pw{a.wo + (oe - wrow), a.wld, m - oe, Fq, bne_dev, kadd, pk_w, q0, t0, nullptr, 0};
+          PackArgs pl{a.a + wd * m + oe, m, p - oe, Fq, bne_dev, kadd, pk_l, q0, t0, nullptr, 0};
+          k_pack_tf32x3<<<dim3((unsigned)nqb, blocks_for(m - oe, TC_BM)), 256, 0, st>>>(pw);
+          k_pack_tf32x3<<<dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), 256, 0, st>>>(pl);
+          h->launches += 2;
+        }
+        int rc;
+        if (flush) {
+          // the window is full: every trailing column takes it (one GEMM)
+          rc = launch_window_gemm(h, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
+          if (rc) return rc;
+        } else {
+          // near field: the next outer block's columns (oe + nb <= p here) take the whole window
+          rc = launch_window_gemm(h, a, m, oe, oe + ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
+          if (rc) return rc;
+          // far field: only if this block delayed columns (decided on the device)
+          if (oe + nb < p) {
+            rc = launch_window_gemm(h, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, bne_dev,
+                                    (int32_t)bcols);
+            if (rc) return rc;
+          }
+        }
         mark(h, RVG_PART_LF_SYRK);
-        syrk = true;
       }
     }
     k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level);
@@ -1356,7 +1471,21 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
     }
     mark_flush(h);
     mark(h, -1);
-    if (syrk) h->syrk_flops += 2.0 * (double)(g - gne) * lower_entries(oe, m, oe, p);
+    const int64_t bne = g - gne;
+    if (two_level && oe < p) {
+      const bool delayed = bne < bcols;
+      const double K = (double)(kadd + bne);
+      if (flush) {
+        h->syrk_flops += 2.0 * K * lower_entries(oe, m, oe, p);
+      } else {
+        h->syrk_flops += 2.0 * K * lower_entries(oe, m, oe, oe + ncol);
+        if (oe + nb < p && delayed) h->syrk_flops += 2.0 * K * lower_entries(oe + nb, m, oe + nb, p);
+      }
+      if (flush || delayed) {  // every column is up to date: a new, empty window
+        wd = g;
+        wrow = g + std::min(rem - bcols, nb);
+      }
+    }
     gne = g;
     rem -= bcols;
   }
@@ -1426,7 +1555,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       const bool tpp = (f.flags & FF_SMALL_LEAF) || k < ib;
       const bool large = !tpp && m >= h->opt.large_front_threshold;
       int64_t sc = tpp ? 0 : (2 * IBMAX * m + h->opt.outer_block_size);
-      if (large) sc = m * (2 * IBMAX + h->opt.outer_block_size) + h->opt.outer_block_size;
+      if (large) sc = m * (2 * IBMAX + LF_WINDOW * h->opt.outer_block_size) + h->opt.outer_block_size;
       if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
       f.scratch = scratch_need; scratch_need += sc;
     }
@@ -2142,7 +2271,7 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack);
   fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }

@@ -80,18 +80,23 @@ struct TcArgs {
   const float* Ap;  // packed W: tile t (C rows r0 + 128 t ...), chunk q at Ap + (t * Q + q) * TC_BLOCK
   const float* Bp;  // packed L: tile u (C columns c0 + 128 u ...)
   int64_t Q;        // chunks per packed tile
-  const int32_t* Kdev;
+  const int32_t* Kdev;  // K = *Kdev (when set) + K
   int64_t K;
   int64_t nr, nc, ntiles;
   int32_t* err;
+  const int32_t* cond;  // when set, the update runs only if *cond < cond_lt
+  int32_t cond_lt;
 };
 
 struct PackArgs {
   const double* X;  // row r, column c at X[r + c * ldx]
   int64_t ldx, R, Q;
-  const int32_t* Kdev;
+  const int32_t* Kdev;  // K = *Kdev (when set) + K: columns >= K are zeros
   int64_t K;
-  float* P;
+  float* P;         // block (t0 + t, q) at P + ((t0 + t) * Q + q) * TC_BLOCK
+  int64_t q0, t0;   // first chunk packed (blockIdx.x = q - q0), first tile
+  const int32_t* cond;  // when set, packs only if *cond < cond_lt
+  int32_t cond_lt;
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -199,11 +204,12 @@ __device__ __forceinline__ void split_tf32_exact(double x, float& hi, float& lo)
 
 // grid (Q chunks, tiles), 256 threads; thread item = one row x 4 consecutive k
 __global__ void __launch_bounds__(256) k_pack_tf32x3(PackArgs a) {
-  int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
+  if (a.cond && *a.cond >= a.cond_lt) return;
+  int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the chunks the buffer holds
-  const int64_t q = blockIdx.x, t = blockIdx.y;
+  const int64_t q = a.q0 + blockIdx.x, t = blockIdx.y;
   if (q * TC_BK >= K) return;  // the GEMM reads chunks < ceil(K / 32) only
-  float* hi = a.P + (t * a.Q + q) * TC_BLOCK;
+  float* hi = a.P + ((a.t0 + t) * a.Q + q) * TC_BLOCK;
   float* lo = hi + TC_PART;
 #pragma unroll
   for (int e = 0; e < (TC_BM * TC_BK / 4) / 256; ++e) {
@@ -263,7 +269,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
   __shared__ uint32_t tslot;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int64_t K = a.Kdev ? (int64_t)*a.Kdev : a.K;
+  if (a.cond && *a.cond >= a.cond_lt) return;  // uniform over the CTA
+  int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the packed chunks
   if (K <= 0) return;  // nothing eliminated: C unchanged (uniform over the CTA)
   const int64_t nq = (K + TC_BK - 1) / TC_BK;

@@ -48,6 +48,28 @@ def test_mixed_reaches_fp64_accuracy(rv, name):
             assert iters <= 1
 
 
+@pytest.mark.parametrize("n,nb,kind", [(1400, 256, "plain"), (1400, 256, "delay"), (900, 128, "plain"),
+                                       (700, 64, "delay")])
+def test_mixed_window(rv, n, nb, kind):
+    # the mixed form's packed window of pending columns (flushed every four outer
+    # blocks, or at once after a delay; one block when nb is not a multiple of 128)
+    import scipy.sparse as sp
+    rng = np.random.default_rng(n + nb)
+    a = rng.standard_normal((n, n))
+    a = a + a.T
+    if kind == "delay":
+        a[np.arange(n), np.arange(n)] *= 1e-6
+    s = rv.problems.from_scipy(f"dense{n}", sp.csc_matrix(a))
+    b = rv.problems.rhs_normal(s.n, 4)
+    for flush in (4, 0):
+        x, iters, err, inertia = factor_refine(rv, s, b, precision="mixed", mixed_flush=flush,
+                                               large_front_threshold=33, outer_block_size=nb)
+        assert err <= 1e-14, (flush, err, iters)
+        assert rv.problems.backward_error(s, x, b) <= 1e-14
+    xp, _, _, inertia_p = factor_refine(rv, s, b, precision="fp64", large_front_threshold=33, outer_block_size=nb)
+    assert inertia == inertia_p
+
+
 def test_refine_errors(rv):
     s = rv.problems.shifted_laplacian(4, 0.1)
     solver = rv.SparseLDLT.analyze(s)

@@ -171,6 +171,16 @@ def test_large_front_path_sparse(rv, orc, opts):
         assert_parity(rv, s, solver, ref, b)
 
 
+@pytest.mark.parametrize("n,nb", [(1400, 256), (700, 64), (600, 96), (520, 128)])
+@pytest.mark.parametrize("kind", ["plain", "delay"])
+def test_large_front_window(rv, orc, n, nb, kind):
+    # deferred far-field updates: windows of four outer blocks, applied when
+    # full or as soon as a block delays columns; bit-identical to per-block updates
+    s = dense_system(rv, n, n + 2, kind)
+    solver, ref, b = run_both(rv, orc, s, large_front_threshold=33, outer_block_size=nb)
+    assert_parity(rv, s, solver, ref, b)
+
+
 def test_large_front_path_nfs_gemm(rv, orc):
     # fronts with >= 256 NFS rows take the syrk contribution GEMM
     s = rv.problems.kkt(10, seed=1)
