@@ -50,7 +50,7 @@ class FactorOptions:
     failed_pivot_tpp: bool = True
     fallback_bunch_kaufman: bool = True
     large_front_threshold: int = 2048  # B200 scheduling only; results do not depend on it
-    precision: str = "fp64"  # "fp64" (plain) or "mixed" (split-TF32 Schur updates; pair with solve_refine)
+    precision: str = "fp64"  # "fp64" (plain) or "mixed" (TF32 tensor-core Schur updates; pair with solve_refine)
     mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
 
     def native(self) -> N.Options:
