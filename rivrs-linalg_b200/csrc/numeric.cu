@@ -627,7 +627,7 @@ __global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* 
 #include "gemm64.cuh"
 #include "umma.cuh"
 #include "large.cuh"
-#include "solve_large.cuh"
+#include "solve_sf.cuh"
 
 namespace rvg {
 
@@ -739,118 +739,6 @@ __global__ void k_perm_scale_out(double* rhs, int64_t ldb, int64_t nrhs, const d
   rhs[pfwd[i] + r * ldb] = v;
 }
 
-__device__ __forceinline__ int32_t front_col(const int32_t* rows, const int32_t* perm, int i) { return rows[perm[i]]; }
-__device__ __forceinline__ int32_t front_row(const int32_t* rows, const int32_t* perm, int ne, int k, int t) {
-  int q = ne + t;
-  return q < k ? rows[perm[q]] : rows[q];
-}
-
-// Forward substitution and the diagonal solve of one front per CTA:
-// y = L11^{-1} x[col]; x[row] -= L21 y (atomically: sibling fronts of a wave
-// may share rows); x[col] = D^{-1} y.
-__global__ void k_solve_fwd(const int32_t* ids, int n, const DFront* F, Arenas A, double* x, int64_t nvec,
-                            int64_t nrhs, double* work) {
-  int f = blockIdx.x;
-  if (f >= n) return;
-  int s = ids[f];
-  const DFront fr = F[s];
-  const int ne = fr.ne;
-  if (ne == 0) return;
-  const int64_t m = fr.m, r = m - ne;
-  const double* L = A.panel + fr.panel;
-  const int32_t* rows = A.idx + fr.idx;
-  const int32_t* perm = rows + m;
-  const int8_t* dt = A.dtype + fr.dpos;
-  const double* dd = A.ddiag + fr.dpos;
-  const double* dof = A.doff + fr.dpos;
-  double* w = work + fr.scratch;  // ne
-  for (int64_t rh = 0; rh < nrhs; ++rh) {
-    double* xv = x + rh * nvec;
-    for (int i = threadIdx.x; i < ne; i += blockDim.x) w[i] = xv[front_col(rows, perm, i)];
-    __syncthreads();
-    for (int j = 0; j < ne; ++j) {
-      double xj = w[j];
-      for (int i = j + 1 + threadIdx.x; i < ne; i += blockDim.x) w[i] = __fma_rn(-L[i + (int64_t)j * m], xj, w[i]);
-      __syncthreads();
-    }
-    for (int64_t t = threadIdx.x; t < r; t += blockDim.x) {
-      double acc = 0.0;
-      for (int j = 0; j < ne; ++j) acc = __fma_rn(L[ne + t + (int64_t)j * m], w[j], acc);
-      atomicAdd(&xv[front_row(rows, perm, ne, fr.k, (int)t)], -acc);
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < ne; c += blockDim.x) {
-      int32_t g = front_col(rows, perm, c);
-      if (dt[c] == PT_1X1) {
-        double d = dd[c];
-        xv[g] = d == 0.0 ? 0.0 : w[c] / d;
-      } else {
-        int c0 = dt[c] == PT_2X2 ? c : c - 1;  // first column of the pair
-        double a = dd[c0], b = dof[c0], cc = dd[c0 + 1];
-        double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(b, b));
-        double r1 = w[c0], r2 = w[c0 + 1];
-        if (det == 0.0) xv[g] = 0.0;
-        else xv[g] = (c == c0) ? __ddiv_rn(__dsub_rn(__dmul_rn(cc, r1), __dmul_rn(b, r2)), det)
-                               : __ddiv_rn(__dsub_rn(__dmul_rn(a, r2), __dmul_rn(b, r1)), det);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Backward substitution of one front per CTA: z = x[col] - L21^T x[row];
-// x[col] = L11^{-T} z.
-__global__ void k_solve_bwd(const int32_t* ids, int n, const DFront* F, Arenas A, double* x, int64_t nvec,
-                            int64_t nrhs, double* work) {
-  int f = blockIdx.x;
-  if (f >= n) return;
-  int s = ids[f];
-  const DFront fr = F[s];
-  const int ne = fr.ne;
-  if (ne == 0) return;
-  const int64_t m = fr.m, r = m - ne;
-  const double* L = A.panel + fr.panel;
-  const int32_t* rows = A.idx + fr.idx;
-  const int32_t* perm = rows + m;
-  double* w = work + fr.scratch;       // ne
-  double* xr = w + ne;                 // r
-  __shared__ double red[8];
-  for (int64_t rh = 0; rh < nrhs; ++rh) {
-    double* xv = x + rh * nvec;
-    for (int i = threadIdx.x; i < ne; i += blockDim.x) w[i] = xv[front_col(rows, perm, i)];
-    for (int64_t t = threadIdx.x; t < r; t += blockDim.x) xr[t] = xv[front_row(rows, perm, ne, fr.k, (int)t)];
-    __syncthreads();
-    for (int j = 0; j < ne; ++j) {
-      double part = 0.0;
-      for (int64_t t = threadIdx.x; t < r; t += blockDim.x) part = __fma_rn(L[ne + t + (int64_t)j * m], xr[t], part);
-      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double s2 = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s2 += red[q];
-        w[j] -= s2;
-      }
-      __syncthreads();
-    }
-    for (int j = ne - 1; j >= 0; --j) {
-      double part = 0.0;
-      for (int i = j + 1 + threadIdx.x; i < ne; i += blockDim.x) part = __fma_rn(L[i + (int64_t)j * m], w[i], part);
-      for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-      if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        double s2 = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) s2 += red[q];
-        w[j] -= s2;
-      }
-      __syncthreads();
-    }
-    for (int i = threadIdx.x; i < ne; i += blockDim.x) xv[front_col(rows, perm, i)] = w[i];
-    __syncthreads();
-  }
-}
-
 // ---------------------------------------------------------------------------
 // FP64 iterative refinement (residual of the unfactored matrix)
 // ---------------------------------------------------------------------------
@@ -946,6 +834,7 @@ struct rvg_handle {
   float* pack = nullptr; size_t pack_cap = 0;        // TF32 hi/lo operand tiles of the mixed-form updates
   float* wpack = nullptr; size_t wpack_cap = 0;      // the same for a large front's window of pending columns
   int32_t* d_err = nullptr;                          // set by a device wait that timed out
+  int32_t* sf_sync = nullptr; size_t sf_sync_cap = 0; // solve: ticket counter and block flags of one wave
   int nsm = 0;                                       // SMs of the device (persistent grids)
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
   bool factored = false;
@@ -1911,8 +1800,24 @@ rvg_status rvg_factor_device(rvg_handle* h, const double* d_values, const double
   return (rvg_status)factor_common(h, d_values, h->has_scaling ? h->d_scal : nullptr);
 }
 
-static bool solve_is_large(const DFront& f) { return (int64_t)f.ne * (int64_t)f.m >= (1 << 18); }
+// Status of the bounded device waits (mixed-form GEMM pipeline, solve
+// dependencies) since the last check; resets the word.  Synchronises.
+static int device_wait_status(rvg_handle* h) {
+  int32_t e = 0;
+  CK(cudaMemcpyAsync(&e, h->d_err, 4, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (e) {
+    CK(cudaMemsetAsync(h->d_err, 0, 4, h->st));
+    set_error(e == 2 ? "a solve block gave up waiting for the blocks it depends on (device timeout)"
+                     : "a tensor-core Schur update gave up waiting on its pipeline (device timeout)");
+    return RVG_ERR_DEVICE_TIMEOUT;
+  }
+  return RVG_OK;
+}
 
+// aptp_solve (solve.rs:57-326) with the permutation and scaling of
+// SparseLDLT::solve_in_place (solver.rs:396-425): per wave one forward launch
+// (leaves first) and, in reverse, one backward launch of solve_sf.cuh.
 static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb) {
   Plan& P = h->P;
   const int64_t n = P.n;
@@ -1920,10 +1825,10 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   if (n == 0 || nrhs == 0) return RVG_OK;
   int rc = ensure(h->d_x, h->x_cap, (size_t)(n * nrhs), st);
   if (rc) return rc;
-  // per-front solve workspace: m doubles (+ the partial sums of large fronts)
+  // per-front solve workspace: forward results, then final values (m each)
   int64_t wneed = 0;
   std::vector<DFront> fr = h->h_fronts;
-  for (auto& f : fr) { f.scratch = wneed; wneed += f.m + (solve_is_large(f) ? LS_RS * LS_B : 0); }
+  for (auto& f : fr) { f.scratch = wneed; wneed += 2 * (int64_t)f.m; }
   if ((rc = ensure(h->solve_work, h->solve_work_cap, (size_t)std::max<int64_t>(wneed, 1), st))) return rc;
   CK(cudaMemcpyAsync(h->d_fronts, fr.data(), fr.size() * sizeof(DFront), cudaMemcpyHostToDevice, st));
   Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, nullptr, h->cb_arena};
@@ -1933,75 +1838,56 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   k_perm_scale_in<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
                                                                  h->has_scaling ? h->d_scal : nullptr);
   launches++;
-  // wave lists of the batched (small) fronts, packed once per solve
+  // block layout of every wave: forward (diagonal then L21 blocks per front) and backward (diagonal blocks)
+  const size_t nw = P.waves.size();
   Packer pk;
-  std::vector<size_t> off(P.waves.size());
-  std::vector<int> cnt(P.waves.size());
-  std::vector<std::vector<int64_t>> large(P.waves.size());
-  for (size_t w = 0; w < P.waves.size(); ++w) {
-    std::vector<int32_t> ids;
+  std::vector<size_t> offf(nw), offb(nw);
+  std::vector<int32_t> nfr(nw, 0), nbf(nw, 0), nbb(nw, 0);
+  int32_t maxblk = 1;
+  for (size_t w = 0; w < nw; ++w) {
+    std::vector<SfFront> vf, vb;
     for (int64_t s : P.waves[w]) {
-      if (fr[s].ne == 0) continue;
-      if (solve_is_large(fr[s])) large[w].push_back(s); else ids.push_back((int32_t)s);
+      const DFront& f = fr[s];
+      if (f.ne == 0) continue;
+      const int32_t nbd = (f.ne + SF_B - 1) / SF_B, nbr = (f.m - f.ne + SF_B - 1) / SF_B;
+      vf.push_back(SfFront{(int32_t)s, nbf[w], nbd, nbr});
+      vb.push_back(SfFront{(int32_t)s, nbb[w], nbd, 0});
+      nbf[w] += nbd + nbr;
+      nbb[w] += nbd;
     }
-    cnt[w] = (int)ids.size();
-    off[w] = pk.add(ids);
+    nfr[w] = (int32_t)vf.size();
+    offf[w] = pk.add(vf);
+    offb[w] = pk.add(vb);
+    maxblk = std::max(maxblk, std::max(nbf[w], nbb[w]));
   }
   if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size() + 16, st))) return rc;
   if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size() + 16))) return rc;
   std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
   CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
-  auto ls_args = [&](int64_t s, int64_t rh) {
-    const DFront& f = fr[s];
-    LSArgs a;
-    a.L = h->panel + f.panel;
-    a.m = f.m; a.k = f.k; a.ne = f.ne;
-    a.rows = h->idx + f.idx;
-    a.perm = a.rows + f.m;
-    a.dt = h->dtype + f.dpos; a.dd = h->ddiag + f.dpos; a.dof = h->doff + f.dpos;
-    a.v = h->solve_work + f.scratch;
-    a.part = a.v + f.m;
-    a.x = h->d_x + rh * n;
-    return a;
+  if ((rc = ensure(h->sf_sync, h->sf_sync_cap, (size_t)maxblk + 1, st))) return rc;
+  auto wave = [&](size_t w, bool fwd, int64_t rh) {
+    SfWave sw;
+    sw.fr = (const SfFront*)(h->d_stage + (fwd ? offf[w] : offb[w]));
+    sw.nfr = nfr[w];
+    sw.nblk = fwd ? nbf[w] : nbb[w];
+    sw.ticket = h->sf_sync;
+    sw.flags = h->sf_sync + 1;
+    sw.x = h->d_x + rh * n;
+    sw.work = h->solve_work;
+    sw.err = h->d_err;
+    return sw;
   };
-  for (size_t w = 0; w < P.waves.size(); ++w) {
-    if (cnt[w]) {
-      k_solve_fwd<<<(unsigned)cnt[w], 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]), cnt[w], h->d_fronts, A,
-                                                    h->d_x, n, nrhs, h->solve_work);
+  for (int64_t rh = 0; rh < nrhs; ++rh) {
+    for (size_t w = 0; w < nw; ++w) {
+      if (!nbf[w]) continue;
+      CK(cudaMemsetAsync(h->sf_sync, 0, (size_t)(nbf[w] + 1) * 4, st));
+      k_sf_fwd<<<(unsigned)std::min<int64_t>(nbf[w], 16LL * h->nsm), SF_B, 0, st>>>(wave(w, true, rh), h->d_fronts, A);
       launches++;
     }
-    for (int64_t s : large[w])
-      for (int64_t rh = 0; rh < nrhs; ++rh) {
-        LSArgs a = ls_args(s, rh);
-        k_lsf_gather<<<blocks_for(a.m, 256), 256, 0, st>>>(a);
-        for (int64_t b0 = 0; b0 < a.ne; b0 += LS_B) {
-          const int64_t b1 = std::min<int64_t>(a.ne, b0 + LS_B);
-          k_lsf_diag<<<1, 32, 0, st>>>(a, b0);
-          if (a.m > b1) k_lsf_update<<<blocks_for(a.m - b1, 256), 256, 0, st>>>(a, b0);
-          launches += 2;
-        }
-        k_lsf_finish<<<blocks_for(a.m, 256), 256, 0, st>>>(a);
-        launches += 2;
-      }
-  }
-  for (size_t w = P.waves.size(); w-- > 0;) {
-    for (int64_t s : large[w])
-      for (int64_t rh = 0; rh < nrhs; ++rh) {
-        LSArgs a = ls_args(s, rh);
-        k_lsb_gather<<<blocks_for(a.m, 256), 256, 0, st>>>(a);
-        const int64_t nblk = (a.ne + LS_B - 1) / LS_B;
-        for (int64_t bi = nblk - 1; bi >= 0; --bi) {
-          const int64_t b0 = bi * LS_B;
-          k_lsb_dot<<<dim3(LS_B, LS_RS), 256, 0, st>>>(a, b0);
-          k_lsb_diag<<<1, 32, 0, st>>>(a, b0);
-          launches += 2;
-        }
-        k_lsb_scatter<<<blocks_for(a.ne, 256), 256, 0, st>>>(a);
-        launches += 2;
-      }
-    if (cnt[w]) {
-      k_solve_bwd<<<(unsigned)cnt[w], 256, 0, st>>>((const int32_t*)(h->d_stage + off[w]), cnt[w], h->d_fronts, A,
-                                                    h->d_x, n, nrhs, h->solve_work);
+    for (size_t w = nw; w-- > 0;) {
+      if (!nbb[w]) continue;
+      CK(cudaMemsetAsync(h->sf_sync, 0, (size_t)(nbb[w] + 1) * 4, st));
+      k_sf_bwd<<<(unsigned)std::min<int64_t>(nbb[w], 6LL * h->nsm), SF_B, 0, st>>>(wave(w, false, rh), h->d_fronts, A);
       launches++;
     }
   }
@@ -2042,7 +1928,7 @@ rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb) {
   if (rc) return (rvg_status)rc;
   CK(cudaMemcpyAsync(rhs, d, bytes, cudaMemcpyDeviceToHost, h->st));
   CK(cudaFreeAsync(d, h->st));
-  CK(cudaStreamSynchronize(h->st));
+  if ((rc = device_wait_status(h))) return (rvg_status)rc;
   float ms = 0;
   cudaEventElapsedTime(&ms, h->ev[6], h->ev[7]);
   h->t_solve = ms;
@@ -2076,6 +1962,7 @@ static int refine_common(rvg_handle* h, const double* d_b, double* d_x, double t
     ++it;
   }
   CK(cudaGetLastError());
+  if ((rc = device_wait_status(h))) return rc;
   if (iters) *iters = it;
   if (bwd) *bwd = e;
   return RVG_OK;
@@ -2271,7 +2158,7 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync);
   fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }

@@ -1,0 +1,281 @@
+// Supernodal solve (aptp_solve, sparse/src/symmetric/solve.rs:57-326) as one
+// launch per wave and direction: forward_solve_supernode (solve.rs:161-230)
+// with the diagonal solve (solve.rs:232-252) folded into the backward pass,
+// and backward_solve_supernode (solve.rs:254-326).
+//
+// Every front of the wave is cut into 64-row blocks; CTAs take blocks in
+// ticket order from one atomic counter (front by front, and inside a front in
+// dependency order), so a block only ever waits for blocks with a smaller
+// ticket, which are held by CTAs that are already running: no deadlock, and
+// no co-residency assumption beyond that.  Waits are bounded by the global
+// timer; one that runs out sets *err and the solve goes on (the caller gets
+// RVG_ERR_DEVICE_TIMEOUT).
+//
+// forward, per front (y kept in the front's work vector v, rows < ne):
+//   diagonal block r (rows [64r, 64r + 64) of L11): y = x[col] - sum over the
+//     finished column blocks b < r of L[rows, b] y_b (each as soon as its flag
+//     is up), then the unit lower solve of the 64 x 64 diagonal block by one
+//     warp; publish y_r, raise flag r;
+//   L21 block (rows >= ne): -sum over all column blocks of L[rows, b] y_b,
+//     added atomically into x at the parent's rows (siblings share rows).
+// backward, per front (descending column blocks; x_final in v + m):
+//   z = D^-1 y on the block's columns (2x2 pairs may straddle blocks: y is
+//   still intact in v), minus L21^T x[row] (parent's final values), minus
+//   L[rows of later blocks, cols]^T x_final of those blocks (each once its
+//   flag is up), then the unit upper solve (L11^T) of the diagonal block by
+//   one warp; x[col] = x_final; raise the flag.
+// Per row (forward) and per column (backward) the sums run in ascending
+// column / row order inside each 64-block.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "front.cuh"
+
+namespace rvg {
+
+constexpr int SF_B = 64;                            // block rows / columns
+constexpr uint64_t SF_TIMEOUT_NS = 1000000000ull;   // 1 s per wait
+
+// one front of a wave: its first ticket and its block counts
+struct SfFront {
+  int32_t s;     // supernode
+  int32_t blk0;  // first ticket of the front
+  int32_t nbd;   // diagonal blocks (ceil(ne / 64))
+  int32_t nbr;   // L21 blocks (forward only: ceil((m - ne) / 64))
+};
+
+struct SfWave {
+  const SfFront* fr;
+  int32_t nfr, nblk;
+  int32_t* ticket;  // zeroed before the launch
+  int32_t* flags;   // nblk entries, zeroed before the launch
+  double* x;        // solution vector (one RHS), permuted order
+  double* work;     // per-front work: v (m) then x_final (m), at DFront::scratch
+  int32_t* err;
+};
+
+__device__ __forceinline__ int32_t sf_ld_acquire(const int32_t* p) {
+  int32_t v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void sf_st_release(int32_t* p, int32_t v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t sf_timer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// bounded wait for a published block (thread 0 of the CTA)
+__device__ __forceinline__ void sf_wait(const int32_t* flag, int32_t* err) {
+  if (sf_ld_acquire(flag)) return;
+  const uint64_t t0 = sf_timer();
+  while (!sf_ld_acquire(flag)) {
+    if (sf_timer() - t0 > SF_TIMEOUT_NS) {
+      atomicExch(err, 2);
+      return;
+    }
+  }
+}
+
+// the wave's front holding ticket blk (last front with blk0 <= blk)
+__device__ __forceinline__ int sf_front(const SfWave& w, int blk) {
+  int lo = 0, hi = w.nfr - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (w.fr[mid].blk0 <= blk) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int32_t sf_col(const int32_t* rows, const int32_t* perm, int64_t i) { return rows[perm[i]]; }
+__device__ __forceinline__ int32_t sf_row(const int32_t* rows, const int32_t* perm, int64_t ne, int64_t k,
+                                          int64_t t) {
+  const int64_t q = ne + t;
+  return q < k ? rows[perm[q]] : rows[q];
+}
+
+// One row of a 64-column strip (columns at stride m) into dst[0, nc), 16
+// loads in flight per thread (the loads are independent; issuing them before
+// the first use keeps the row's memory latency from serialising).
+__device__ __forceinline__ void sf_load_strip(const double* src, int64_t m, int nc, double* dst) {
+#pragma unroll
+  for (int c0 = 0; c0 < SF_B; c0 += 16) {
+    double r[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) r[u] = c0 + u < nc ? __ldg(src + (int64_t)(c0 + u) * m) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 16; ++u) dst[c0 + u] = r[u];
+  }
+}
+
+__global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Arenas A) {
+  __shared__ int s_blk;
+  __shared__ double yb[SF_B];
+  __shared__ double Ls[SF_B][SF_B + 1];
+  const int t = threadIdx.x;
+  for (;;) {
+    if (t == 0) s_blk = atomicAdd(w.ticket, 1);
+    __syncthreads();
+    const int blk = s_blk;
+    __syncthreads();
+    if (blk >= w.nblk) break;
+    const SfFront sf = w.fr[sf_front(w, blk)];
+    const DFront fr = F[sf.s];
+    const int64_t m = fr.m, ne = fr.ne;
+    const double* L = A.panel + fr.panel;
+    const int32_t* rows = A.idx + fr.idx;
+    const int32_t* perm = rows + m;
+    double* v = w.work + fr.scratch;
+    int32_t* flags = w.flags + sf.blk0;
+    const int b = blk - sf.blk0;
+    const bool diag = b < sf.nbd;
+    const int64_t r0 = diag ? (int64_t)b * SF_B : ne + (int64_t)(b - sf.nbd) * SF_B;
+    const int64_t r1 = diag ? (r0 + SF_B < ne ? r0 + SF_B : ne) : (r0 + SF_B < m ? r0 + SF_B : m);
+    const int64_t i = r0 + t;
+    const bool row = i < r1;
+    double acc = (diag && row) ? w.x[sf_col(rows, perm, i)] : 0.0;
+    const int ncb = diag ? b : sf.nbd;
+    for (int cb = 0; cb < ncb; ++cb) {
+      if (t == 0) sf_wait(&flags[cb], w.err);
+      __syncthreads();
+      const int64_t c0 = (int64_t)cb * SF_B;
+      const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
+      if (t < nc) yb[t] = __ldcg(&v[c0 + t]);
+      __syncthreads();
+      if (row) {
+        double lr[SF_B];
+        sf_load_strip(L + i + c0 * m, m, nc, lr);
+#pragma unroll
+        for (int c = 0; c < SF_B; ++c)
+          if (c < nc) acc = __fma_rn(-lr[c], yb[c], acc);
+      }
+      __syncthreads();
+    }
+    if (diag) {
+      // unit lower solve of rows [r0, r1) by warp 0 (lane: rows r0 + lane, r0 + 32 + lane),
+      // the diagonal block staged in shared memory first
+      const int nr = (int)(r1 - r0);
+      if (row) sf_load_strip(L + i + r0 * m, m, nr, &Ls[t][0]);
+      yb[t] = acc;
+      __syncthreads();
+      if (t < 32) {
+        double a0 = yb[t], a1 = yb[t + 32];
+        for (int j = 0; j < nr; ++j) {
+          const double yj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
+          if (t > j && t < nr) a0 = __fma_rn(-Ls[t][j], yj, a0);
+          if (t + 32 > j && t + 32 < nr) a1 = __fma_rn(-Ls[t + 32][j], yj, a1);
+        }
+        if (t < nr) v[r0 + t] = a0;
+        if (t + 32 < nr) v[r0 + t + 32] = a1;
+      }
+      __threadfence();
+      __syncthreads();
+      if (t == 0) sf_st_release(&flags[b], 1);
+    } else if (row) {
+      atomicAdd(&w.x[sf_row(rows, perm, ne, fr.k, i - ne)], acc);
+    }
+  }
+}
+
+// z = D^-1 y for column c of a front (MixedDiagonal::solve_in_place,
+// diagonal.rs:312-360: zero pivots give 0, 2x2 blocks by Cramer's rule)
+__device__ __forceinline__ double sf_dinv(const DFront& fr, const Arenas& A, const double* y, int64_t c) {
+  const int8_t* dt = A.dtype + fr.dpos;
+  const double* dd = A.ddiag + fr.dpos;
+  const double* dof = A.doff + fr.dpos;
+  if (dt[c] == PT_1X1) {
+    const double d = dd[c];
+    return d == 0.0 ? 0.0 : __ddiv_rn(y[c], d);
+  }
+  const int64_t c0 = dt[c] == PT_2X2 ? c : c - 1;
+  const double a = dd[c0], b = dof[c0], cc = dd[c0 + 1];
+  const double det = __dsub_rn(__dmul_rn(a, cc), __dmul_rn(b, b));
+  const double r1 = y[c0], r2 = y[c0 + 1];
+  if (det == 0.0) return 0.0;
+  return c == c0 ? __ddiv_rn(__dsub_rn(__dmul_rn(cc, r1), __dmul_rn(b, r2)), det)
+                 : __ddiv_rn(__dsub_rn(__dmul_rn(a, r2), __dmul_rn(b, r1)), det);
+}
+
+__global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Arenas A) {
+  __shared__ int s_blk;
+  __shared__ double Ls[SF_B][SF_B + 1];
+  __shared__ double xs[SF_B];
+  const int t = threadIdx.x;
+  for (;;) {
+    if (t == 0) s_blk = atomicAdd(w.ticket, 1);
+    __syncthreads();
+    const int blk = s_blk;
+    __syncthreads();
+    if (blk >= w.nblk) break;
+    const SfFront sf = w.fr[sf_front(w, blk)];
+    const DFront fr = F[sf.s];
+    const int64_t m = fr.m, ne = fr.ne;
+    const double* L = A.panel + fr.panel;
+    const int32_t* rows = A.idx + fr.idx;
+    const int32_t* perm = rows + m;
+    const double* y = w.work + fr.scratch;  // forward results (rows < ne)
+    double* xf = w.work + fr.scratch + m;   // final values of this front's columns
+    int32_t* flags = w.flags + sf.blk0;
+    const int b = sf.nbd - 1 - (blk - sf.blk0);  // descending
+    const int64_t c0 = (int64_t)b * SF_B;
+    const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
+    const bool col = t < nc;
+    double acc = col ? sf_dinv(fr, A, y, c0 + t) : 0.0;
+    // rows of later blocks: L21 (parent's final values), then later diagonal blocks as they finish
+    const int nbr = (int)((m - ne + SF_B - 1) / SF_B);
+    for (int rb = -nbr; rb < sf.nbd - 1 - b; ++rb) {
+      int64_t i0;
+      const double* xsrc = nullptr;
+      bool l21 = rb < 0;
+      if (l21) {
+        i0 = ne + (int64_t)(nbr + rb) * SF_B;
+      } else {
+        const int r = sf.nbd - 1 - rb;  // later diagonal blocks, from the last one down
+        if (t == 0) sf_wait(&flags[sf.nbd - 1 - r], w.err);
+        i0 = (int64_t)r * SF_B;
+        xsrc = xf;
+      }
+      const int64_t iend = l21 ? m : ne;
+      const int nr = (int)((i0 + SF_B < iend ? i0 + SF_B : iend) - i0);
+      __syncthreads();
+      if (t < nr) {
+        const int64_t i = i0 + t;
+        xs[t] = l21 ? w.x[sf_row(rows, perm, ne, fr.k, i - ne)] : __ldcg(&xsrc[i]);
+        sf_load_strip(L + i + c0 * m, m, nc, &Ls[t][0]);
+      }
+      __syncthreads();
+      if (col)
+        for (int rr = 0; rr < nr; ++rr) acc = __fma_rn(-Ls[rr][t], xs[rr], acc);
+    }
+    // the diagonal block: x_c = acc_c - sum_{c < i < c0 + nc} L(i, c) x_i, from the bottom
+    __syncthreads();
+    if (t < nc) sf_load_strip(L + (c0 + t) + c0 * m, m, nc, &Ls[t][0]);  // Ls[row][col]
+    xs[t] = acc;
+    __syncthreads();
+    if (t < 32) {
+      double a0 = xs[t], a1 = xs[t + 32];
+      for (int j = nc - 1; j >= 0; --j) {
+        const double xj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
+        if (t < j) a0 = __fma_rn(-Ls[j][t], xj, a0);
+        if (t + 32 < j) a1 = __fma_rn(-Ls[j][t + 32], xj, a1);
+      }
+      if (t < nc) {
+        xf[c0 + t] = a0;
+        w.x[sf_col(rows, perm, c0 + t)] = a0;
+      }
+      if (t + 32 < nc) {
+        xf[c0 + t + 32] = a1;
+        w.x[sf_col(rows, perm, c0 + t + 32)] = a1;
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) sf_st_release(&flags[blk - sf.blk0], 1);
+  }
+}
+
+}  // namespace rvg
