@@ -210,6 +210,13 @@ enum {
 };
 rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable);
 rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* out);
+
+/* Self-test of the bounded device waits (no reference counterpart): runs one
+ * wait that nothing releases, on the handle's stream, and returns the status
+ * the host then reads: RVG_ERR_DEVICE_TIMEOUT when the wait ran out and was
+ * reported (the handle stays usable).  which = 0: a solve block's flag wait
+ * (1 s); which = 1: the mixed-form GEMM's pipeline wait (2 s). */
+rvg_status rvg_selftest_waits(rvg_handle* h, int32_t which);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 rvg_status rvg_stream(rvg_handle* h, void** stream);
 void rvg_destroy(rvg_handle* h);

@@ -96,8 +96,7 @@ __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
     if (i >= j) { double v = V(k + i, k + j); sh.T[i][j] = v; st->Tb[i][j] = v; }
   }
   __syncthreads();
-  if (tid < 32) warp_block_factor(sh, bs, A.o.small, tid);
-  __syncthreads();
+  cta_block_factor(sh, bs, A.o.small);
   const int bnelim = sh.bnelim;
   if (bnelim > 0) {
     for (int t = tid; t < bs * bs; t += NT) {
@@ -112,16 +111,20 @@ __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
         else bc += 1;
       }
     }
-    // row permutation of the view columns 0..k (step 5)
+    // row permutation of the view columns 0..k (step 5): all loads of a column
+    // before its stores
     for (int64_t c = tid; c < k; c += NT) {
       double buf[IBMAX];
-      for (int i = 0; i < bs; ++i) buf[i] = V(k + sh.bperm[i], c);
-      for (int i = 0; i < bs; ++i) V(k + i, c) = buf[i];
+#pragma unroll
+      for (int i = 0; i < IBMAX; ++i) buf[i] = i < bs ? V(k + sh.bperm[i], c) : 0.0;
+#pragma unroll
+      for (int i = 0; i < IBMAX; ++i)
+        if (i < bs) V(k + i, c) = buf[i];
     }
-    if (tid == 0) {  // column order (step 6)
-      int32_t ob[IBMAX];
-      for (int i = 0; i < bs; ++i) ob[i] = A.lp[k + i];
-      for (int i = 0; i < bs; ++i) A.lp[k + i] = ob[sh.bperm[i]];
+    if (tid < 32) {  // column order (step 6): lane i takes the entry of lane bperm[i]
+      const int32_t ob = tid < bs ? A.lp[k + tid] : 0;
+      const int32_t nbv = __shfl_sync(0xffffffffu, ob, sh.bperm[tid] & 31);
+      if (tid < bs) A.lp[k + tid] = nbv;
     }
     __syncthreads();
   }
@@ -138,6 +141,40 @@ __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
   if (tid == 0) { st->bs = bs; st->bnelim = bnelim; st->eff = bnelim; }
 }
 
+// One row of W = L D over pivots [0, n) (l(c) = l[c * ld]; D given by type,
+// diagonal and off-diagonal; the second column of a 2x2 is written with its
+// first), 16 columns at a time: the chunk's L and D values are loaded before
+// any W store, so the row's memory latency is not paid per column.
+__device__ __forceinline__ void lf_w_row(const double* l, int64_t ld, int n, const int8_t* dt, const double* dd,
+                                         const double* dof, double* w, int64_t wld) {
+  for (int c0 = 0; c0 < n; c0 += 16) {
+    double lv[17], dv[17], ov[16];
+    int8_t tv[16];
+#pragma unroll
+    for (int u = 0; u < 17; ++u) {
+      const bool in = c0 + u < n;
+      lv[u] = in ? l[(int64_t)(c0 + u) * ld] : 0.0;
+      dv[u] = in ? dd[c0 + u] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const bool in = c0 + u < n;
+      ov[u] = in ? dof[c0 + u] : 0.0;
+      tv[u] = in ? dt[c0 + u] : (int8_t)PT_DELAYED;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int64_t c = c0 + u;
+      if (tv[u] == PT_1X1) {
+        w[c * wld] = __dmul_rn(lv[u], dv[u]);
+      } else if (tv[u] == PT_2X2) {
+        w[c * wld] = __dadd_rn(__dmul_rn(lv[u], dv[u]), __dmul_rn(lv[u + 1], ov[u]));
+        w[(c + 1) * wld] = __dadd_rn(__dmul_rn(lv[u], ov[u]), __dmul_rn(lv[u + 1], dv[u + 1]));
+      }
+    }
+  }
+}
+
 // panel rows: backup, permute, TRSM, D^-1, threshold scan (grid over rows,
 // one row per thread, the row's 32 values in registers: every index into
 // them is a compile-time constant)
@@ -149,18 +186,34 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
   __shared__ double T[IBMAX][IBMAX + 1];
   __shared__ int bperm[IBMAX];
   __shared__ int8_t bdt[IBMAX];
-  __shared__ double bdd[IBMAX], bdo[IBMAX];
+  __shared__ double bdd[IBMAX], bdo[IBMAX], dinv[IBMAX];
   __shared__ int s_fail;
   const int bs = st->bs, k = st->k;
-  for (int t = threadIdx.x; t < bs * bs; t += blockDim.x) {
-    int i = t % bs, j = t / bs;
-    if (i >= j) T[i][j] = st->T[i][j];
+  {
+    // the factored block: thread t takes column t / 2 (rows of one half), all loads before the stores
+    const int j = threadIdx.x >> 1, h = threadIdx.x & 1;
+    double v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int i = h * 16 + u;
+      v[u] = (j < bs && i < bs && i >= j) ? st->T[i][j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) T[h * 16 + u][j] = v[u];
   }
   if (threadIdx.x < IBMAX) {
-    bperm[threadIdx.x] = st->bperm[threadIdx.x];
-    bdt[threadIdx.x] = st->bdt[threadIdx.x];
-    bdd[threadIdx.x] = st->bdd[threadIdx.x];
-    bdo[threadIdx.x] = st->bdo[threadIdx.x];
+    const int c = threadIdx.x;
+    bperm[c] = st->bperm[c];
+    const int8_t t = st->bdt[c];
+    const double d = st->bdd[c], o = st->bdo[c];
+    bdt[c] = t;
+    bdd[c] = d;
+    bdo[c] = o;
+    // the reciprocal each row's D^-1 step uses: 1 / d (1x1) or 1 / det (2x2 first column)
+    double r = 0.0;
+    if (c < bnelim && t == PT_1X1) r = 1.0 / d;
+    else if (c < bnelim && t == PT_2X2 && c + 1 < IBMAX) r = 1.0 / __dsub_rn(__dmul_rn(d, st->bdd[c + 1]), __dmul_rn(o, o));
+    dinv[c] = r;
   }
   if (threadIdx.x == 0) s_fail = bnelim;
   __syncthreads();
@@ -187,10 +240,10 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
     for (int c = 0; c < IBMAX; ++c) {
       if (c >= bnelim) continue;
       if (bdt[c] == PT_1X1) {
-        x[c] = __dmul_rn(x[c], 1.0 / bdd[c]);
+        x[c] = __dmul_rn(x[c], dinv[c]);
       } else if (bdt[c] == PT_2X2 && c + 1 < IBMAX) {
         const double A_ = bdd[c], B_ = bdo[c], C_ = bdd[c + 1];
-        const double inv_det = 1.0 / __dsub_rn(__dmul_rn(A_, C_), __dmul_rn(B_, B_));
+        const double inv_det = dinv[c];
         const double x1 = x[c], x2 = x[c + 1];
         x[c] = __dmul_rn(__dsub_rn(__dmul_rn(x1, C_), __dmul_rn(x2, B_)), inv_det);
         x[c + 1] = __dmul_rn(__dsub_rn(__dmul_rn(x2, A_), __dmul_rn(x1, B_)), inv_det);
@@ -260,21 +313,26 @@ __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
       V(k + nelim + i, k + nelim + j) = __dsub_rn(V(k + nelim + i, k + nelim + j), s);
     }
   }
-  if (tid == 0) {
+  if (tid < 32) {
+    // D entries, one pivot column per lane (the adjusted nelim never splits a 2x2)
     DRec VD{A.D.type + A.cs, A.D.diag + A.cs, A.D.off + A.cs};
-    int c = 0, n1 = 0, n2 = 0;
-    while (c < nelim) {
-      if (st->bdt[c] == PT_1X1) {
-        VD.type[k + c] = PT_1X1; VD.diag[k + c] = st->bdd[c]; VD.off[k + c] = 0.0; n1++; c += 1;
-      } else if (c + 1 < nelim) {
-        VD.type[k + c] = PT_2X2; VD.type[k + c + 1] = PT_2X2B;
-        VD.diag[k + c] = st->bdd[c]; VD.diag[k + c + 1] = st->bdd[c + 1];
-        VD.off[k + c] = st->bdo[c]; VD.off[k + c + 1] = 0.0; n2++; c += 2;
-      } else c += 1;
+    const int c = tid;
+    const int8_t t = c < nelim ? st->bdt[c] : (int8_t)PT_DELAYED;
+    const bool one = t == PT_1X1;
+    const bool first = t == PT_2X2 && c + 1 < nelim;
+    const bool second = t == PT_2X2B;
+    if (one || first || second) {
+      VD.type[k + c] = one ? PT_1X1 : (first ? PT_2X2 : PT_2X2B);
+      VD.diag[k + c] = st->bdd[c];
+      VD.off[k + c] = first ? st->bdo[c] : 0.0;
     }
-    st->n1 += n1; st->n2 += n2;
-    st->nelim = nelim;
-    st->eff = eff;
+    const int n1 = __popc(__ballot_sync(0xffffffffu, one));
+    const int n2 = __popc(__ballot_sync(0xffffffffu, first));
+    if (tid == 0) {
+      st->n1 += n1; st->n2 += n2;
+      st->nelim = nelim;
+      st->eff = eff;
+    }
   }
 }
 
@@ -315,19 +373,7 @@ __global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
     for (int j = eff; j < bs; ++j) V(i, k + j) = A.pb[i + (int64_t)bperm[j] * bm];
   if (nelim == 0) return;
   double* W = A.w + i;
-  const double* l = &V(i, k);
-  int c = 0;
-  while (c < nelim) {
-    if (bdt[c] == PT_1X1) {
-      W[(int64_t)c * bm] = __dmul_rn(l[c * A.m], bdd[c]);
-      c += 1;
-    } else {
-      const double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
-      W[(int64_t)c * bm] = __dadd_rn(__dmul_rn(l1, bdd[c]), __dmul_rn(l2, bdo[c]));
-      W[(int64_t)(c + 1) * bm] = __dadd_rn(__dmul_rn(l1, bdo[c]), __dmul_rn(l2, bdd[c + 1]));
-      c += 2;
-    }
-  }
+  lf_w_row(&V(i, k), A.m, nelim, bdt, bdd, bdo, W, bm);
   for (int jj = 0; jj < nf; ++jj) {
     double s = 0.0;
     for (int c2 = 0; c2 < nelim; ++c2) s = __dadd_rn(s, __dmul_rn(W[(int64_t)c2 * bm], Ls[jj][c2]));
@@ -390,7 +436,7 @@ __global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
 
 // W = L D for the rows below the outer block, over its bne eliminated
 // columns, appended to the pending window
-__global__ void k_lf_w(LFArgs A) {
+__global__ void __launch_bounds__(128) k_lf_w(LFArgs A) {
   const int bne = A.st->bne;
   const int64_t oe = A.cs + A.bcols;
   const int64_t i = oe + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -400,16 +446,7 @@ __global__ void k_lf_w(LFArgs A) {
   const double* dof = A.D.off + A.cs;
   const double* l = A.a + i + A.cs * A.m;
   double* w = A.wo + (i - A.wrow0) + A.wcol0 * A.wld;
-  int c = 0;
-  while (c < bne) {
-    if (dt[c] == PT_1X1) { w[c * A.wld] = __dmul_rn(l[c * A.m], dd[c]); c += 1; }
-    else {
-      double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
-      w[c * A.wld] = __dadd_rn(__dmul_rn(l1, dd[c]), __dmul_rn(l2, dof[c]));
-      w[(c + 1) * A.wld] = __dadd_rn(__dmul_rn(l1, dof[c]), __dmul_rn(l2, dd[c + 1]));
-      c += 2;
-    }
-  }
+  lf_w_row(l, A.m, bne, dt, dd, dof, w, A.wld);
 }
 
 // end of an outer block: column order, delays to the end of the remaining
@@ -419,12 +456,11 @@ __global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_
   const int tid = threadIdx.x;
   const int bne = st->bne;
   const int64_t cs = A.cs, bcols = A.bcols;
-  if (tid == 0) {
-    // perm[cs + i] = orig[lp[i]], via the inner W scratch as the copy buffer
-    int32_t* orig = (int32_t*)A.w;
-    for (int i = 0; i < bcols; ++i) orig[i] = A.perm[cs + i];
-    for (int i = 0; i < bcols; ++i) A.perm[cs + i] = orig[A.lp[i]];
-  }
+  // perm[cs + i] = orig[lp[i]], via the inner W scratch as the copy buffer
+  int32_t* orig = (int32_t*)A.w;
+  for (int i = tid; i < bcols; i += NT) orig[i] = A.perm[cs + i];
+  __syncthreads();
+  for (int i = tid; i < bcols; i += NT) A.perm[cs + i] = orig[A.lp[i]];
   __syncthreads();
   if (two_level && bne < bcols) {
     PanelView F{A.a, A.m};

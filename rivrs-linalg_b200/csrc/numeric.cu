@@ -193,118 +193,169 @@ struct CtaShared {
   double tmpd[NT];
 };
 
-// Complete pivoting on the bs x bs diagonal block held in shared memory,
-// executed by one warp (factor_block_diagonal, factor.rs:891-1153).
-__device__ void warp_block_factor(CtaShared& sh, int bs, double small, int lane) {
+// Complete pivoting on the bs x bs diagonal block held in shared memory
+// (factor_block_diagonal, factor.rs:891-1153).  Per pivot step, warp 0 finds
+// the pivot (lane = column, its rows in registers; the reduction keeps the
+// largest magnitude and, among equal ones, the smallest (column, row) key: the
+// reference's column-then-row scan with a strict >), performs the symmetric
+// swaps, the reciprocal and the scaling of the pivot column(s); then every
+// warp takes part in the rank-1 / rank-2 update (warps take columns, lanes
+// rows).  Two CTA barriers per step; every entry gets the same operations as
+// in the reference's loops.
+__device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
+  static_assert(NT == 256 && IBMAX == 32, "the update's column split assumes 8 warps and 32-column blocks");
   double(*T)[IBMAX + 1] = sh.T;
-  if (lane < IBMAX) { sh.bperm[lane] = lane; sh.bdt[lane] = PT_DELAYED; sh.bdd[lane] = 0; sh.bdo[lane] = 0; }
-  __syncwarp();
-  auto swp = [&](int i, int j) {  // swap_symmetric_block limited to the block
+  __shared__ int s_kind;
+  __shared__ double s_d[3];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < IBMAX) { sh.bperm[tid] = tid; sh.bdt[tid] = PT_DELAYED; sh.bdd[tid] = 0; sh.bdo[tid] = 0; }
+  __syncthreads();
+  // swap_symmetric_block limited to the block (warp 0)
+  auto swp = [&](int i, int j) {
     if (i == j) return;
     if (i > j) { int t = i; i = j; j = t; }
-    if (lane == 0) { double t = T[i][i]; T[i][i] = T[j][j]; T[j][j] = t; }
+    if (lane == 0) {
+      double t = T[i][i]; T[i][i] = T[j][j]; T[j][j] = t;
+      int p = sh.bperm[i]; sh.bperm[i] = sh.bperm[j]; sh.bperm[j] = p;
+    }
     if (lane < i) { double t = T[i][lane]; T[i][lane] = T[j][lane]; T[j][lane] = t; }
     if (lane > i && lane < j) { double t = T[lane][i]; T[lane][i] = T[j][lane]; T[j][lane] = t; }
     if (lane > j && lane < bs) { double t = T[lane][i]; T[lane][i] = T[lane][j]; T[lane][j] = t; }
-    if (lane == 0) { int t = sh.bperm[i]; sh.bperm[i] = sh.bperm[j]; sh.bperm[j] = t; }
     __syncwarp();
   };
   int k = 0;
-  while (k < bs) {
-    int cur = k;
-    int remaining = bs - k;
-    // arg-max over the lower triangle of [cur, bs)^2, scan order j then i
-    double bv = 0.0;
-    int64_t key = INT64_MAX;
-    if (lane >= cur && lane < bs) {
-      for (int i = lane; i < bs; ++i) {
-        double v = fabs(T[i][lane]);
-        if (v > bv) { bv = v; key = (int64_t)lane * 64 + i; }
-      }
-    }
-    warp_argmax(bv, key);
-    int mr = cur, mc = cur;
-    if (key != INT64_MAX) { mc = (int)(key / 64); mr = (int)(key % 64); }
-    double maxv = bv;
-    if (maxv < small) break;
-    if (mr == mc) {
-      swp(cur, mr);
-      double dkk = T[cur][cur], inv = 1.0 / dkk;
-      if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
-      __syncwarp();
-      if (lane > cur && lane < bs) {
-        for (int j = cur + 1; j <= lane; ++j) {
-          double ldl = __dmul_rn(T[j][cur], dkk);
-          T[lane][j] = __dsub_rn(T[lane][j], __dmul_rn(T[lane][cur], ldl));
+  for (;;) {
+    const int cur = k;
+    if (warp == 0) {
+      int kind = 0;  // 0 stop, 1 1x1 (+ rank-1 update), 2 2x2 (+ rank-2 update)
+      if (cur < bs) {
+        // arg-max over the lower triangle of [cur, bs)^2
+        double bv = 0.0;
+        unsigned key = 0xffffffffu;
+        if (lane >= cur && lane < bs) {
+          double col[IBMAX];
+#pragma unroll
+          for (int i = 0; i < IBMAX; ++i) col[i] = T[i][lane];
+#pragma unroll
+          for (int i = 0; i < IBMAX; ++i)
+            if (i >= lane && i < bs) {
+              const double v = fabs(col[i]);
+              if (v > bv) { bv = v; key = (unsigned)(lane * 64 + i); }
+            }
+        }
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(bv);  // bv >= 0: bits order as values
+        const unsigned hi = (unsigned)(bits >> 32), lo = (unsigned)bits;
+        const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+        const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+        key = __reduce_min_sync(0xffffffffu, (hi == mhi && lo == mlo) ? key : 0xffffffffu);
+        const double maxv = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+        int mr = cur, mc = cur;
+        if (key != 0xffffffffu) { mc = (int)(key / 64); mr = (int)(key % 64); }
+        if (maxv >= small) {
+          if (mr == mc) {
+            swp(cur, mr);
+            const double dkk = T[cur][cur], inv = 1.0 / dkk;
+            if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
+            if (lane == 0) { sh.bdt[cur] = PT_1X1; sh.bdd[cur] = dkk; s_d[0] = dkk; }
+            kind = 1;
+          } else {
+            const int t = mr, mi = mc;
+            const double amm = T[mi][mi], att = T[t][t], atm = T[t][mi];
+            const double delta = __dsub_rn(__dmul_rn(amm, att), __dmul_rn(atm, atm));
+            const int remaining = bs - cur;
+            if (remaining < 2) {
+              const int pp = fabs(amm) >= fabs(att) ? mi : t;
+              swp(cur, pp);
+              const double dkk = T[cur][cur];
+              if (!(fabs(dkk) < small)) {
+                const double inv = 1.0 / dkk;
+                if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
+                if (lane == 0) { sh.bdt[cur] = PT_1X1; sh.bdd[cur] = dkk; s_d[0] = dkk; }
+                kind = 1;  // the rank-1 update is empty here
+              }
+            } else if (fabs(delta) >= __dmul_rn(__dmul_rn(0.5, atm), atm)) {
+              swp(cur, mi);
+              const int nt = (t == cur) ? mi : t;
+              swp(cur + 1, nt);
+              const double a11 = T[cur][cur], a22 = T[cur + 1][cur + 1], a21 = T[cur + 1][cur];
+              const double det = __dsub_rn(__dmul_rn(a11, a22), __dmul_rn(a21, a21));
+              const double inv_det = 1.0 / det;
+              if (lane >= cur + 2 && lane < bs) {
+                const double ai1 = T[lane][cur], ai2 = T[lane][cur + 1];
+                T[lane][cur] = __dmul_rn(__dsub_rn(__dmul_rn(ai1, a22), __dmul_rn(ai2, a21)), inv_det);
+                T[lane][cur + 1] = __dmul_rn(__dsub_rn(__dmul_rn(ai2, a11), __dmul_rn(ai1, a21)), inv_det);
+              }
+              if (lane == 0) {
+                sh.bdt[cur] = PT_2X2; sh.bdt[cur + 1] = PT_2X2B;
+                sh.bdd[cur] = a11; sh.bdd[cur + 1] = a22; sh.bdo[cur] = a21;
+                s_d[0] = a11; s_d[1] = a21; s_d[2] = a22;
+              }
+              kind = 2;
+            } else {
+              const int pp = fabs(amm) >= fabs(att) ? mi : t;
+              swp(cur, pp);
+              const double dkk = T[cur][cur], inv = 1.0 / dkk;
+              if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
+              if (lane == 0) { sh.bdt[cur] = PT_1X1; sh.bdd[cur] = dkk; s_d[0] = dkk; }
+              kind = 1;
+            }
+          }
         }
       }
-      __syncwarp();
-      if (lane == 0) { sh.bdt[k] = PT_1X1; sh.bdd[k] = dkk; }
+      if (lane == 0) s_kind = kind;
+    }
+    __syncthreads();
+    const int kind = s_kind;
+    if (kind == 0) break;
+    const int i = lane;
+    if (kind == 1) {  // T[i][j] -= T[i][cur] (T[j][cur] d), cur < j <= i
+      const double dkk = s_d[0];
+      if (i > cur && i < bs) {
+        const double lc = T[i][cur];
+        double lj[IBMAX / 8], tij[IBMAX / 8];
+#pragma unroll
+        for (int q = 0; q < IBMAX / 8; ++q) {
+          const int j = cur + 1 + warp + 8 * q;
+          const bool in = j <= i;
+          lj[q] = in ? T[j][cur] : 0.0;
+          tij[q] = in ? T[i][j] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < IBMAX / 8; ++q) {
+          const int j = cur + 1 + warp + 8 * q;
+          if (j <= i) T[i][j] = __dsub_rn(tij[q], __dmul_rn(lc, __dmul_rn(lj[q], dkk)));
+        }
+      }
       k += 1;
-    } else {
-      int t = mr, mi = mc;
-      double amm = T[mi][mi], att = T[t][t], atm = T[t][mi];
-      double delta = __dsub_rn(__dmul_rn(amm, att), __dmul_rn(atm, atm));
-      if (remaining < 2) {
-        int pp = fabs(amm) >= fabs(att) ? mi : t;
-        swp(cur, pp);
-        double dkk = T[cur][cur];
-        if (fabs(dkk) < small) break;
-        double inv = 1.0 / dkk;
-        if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
-        __syncwarp();
-        if (lane == 0) { sh.bdt[k] = PT_1X1; sh.bdd[k] = dkk; }
-        k += 1;
-        continue;
-      }
-      if (fabs(delta) >= __dmul_rn(__dmul_rn(0.5, atm), atm)) {
-        swp(cur, mi);
-        int nt = (t == cur) ? mi : t;
-        swp(cur + 1, nt);
-        double a11 = T[cur][cur], a22 = T[cur + 1][cur + 1], a21 = T[cur + 1][cur];
-        double det = __dsub_rn(__dmul_rn(a11, a22), __dmul_rn(a21, a21));
-        double inv_det = 1.0 / det;
-        if (lane >= cur + 2 && lane < bs) {
-          double ai1 = T[lane][cur], ai2 = T[lane][cur + 1];
-          T[lane][cur] = __dmul_rn(__dsub_rn(__dmul_rn(ai1, a22), __dmul_rn(ai2, a21)), inv_det);
-          T[lane][cur + 1] = __dmul_rn(__dsub_rn(__dmul_rn(ai2, a11), __dmul_rn(ai1, a21)), inv_det);
+    } else {  // rank-2 over cur + 2 <= j <= i
+      const double a11 = s_d[0], a21 = s_d[1], a22 = s_d[2];
+      if (i >= cur + 2 && i < bs) {
+        const double c1 = T[i][cur], c2 = T[i][cur + 1];
+        double l1[IBMAX / 8], l2[IBMAX / 8], tij[IBMAX / 8];
+#pragma unroll
+        for (int q = 0; q < IBMAX / 8; ++q) {
+          const int j = cur + 2 + warp + 8 * q;
+          const bool in = j <= i;
+          l1[q] = in ? T[j][cur] : 0.0;
+          l2[q] = in ? T[j][cur + 1] : 0.0;
+          tij[q] = in ? T[i][j] : 0.0;
         }
-        __syncwarp();
-        if (lane >= cur + 2 && lane < bs) {
-          for (int j = cur + 2; j <= lane; ++j) {
-            double l1j = T[j][cur], l2j = T[j][cur + 1];
-            double w1 = __dadd_rn(__dmul_rn(l1j, a11), __dmul_rn(l2j, a21));
-            double w2 = __dadd_rn(__dmul_rn(l1j, a21), __dmul_rn(l2j, a22));
-            T[lane][j] = __dsub_rn(T[lane][j], __dadd_rn(__dmul_rn(T[lane][cur], w1), __dmul_rn(T[lane][cur + 1], w2)));
+#pragma unroll
+        for (int q = 0; q < IBMAX / 8; ++q) {
+          const int j = cur + 2 + warp + 8 * q;
+          if (j <= i) {
+            const double w1 = __dadd_rn(__dmul_rn(l1[q], a11), __dmul_rn(l2[q], a21));
+            const double w2 = __dadd_rn(__dmul_rn(l1[q], a21), __dmul_rn(l2[q], a22));
+            T[i][j] = __dsub_rn(tij[q], __dadd_rn(__dmul_rn(c1, w1), __dmul_rn(c2, w2)));
           }
         }
-        __syncwarp();
-        if (lane == 0) {
-          sh.bdt[k] = PT_2X2; sh.bdt[k + 1] = PT_2X2B;
-          sh.bdd[k] = a11; sh.bdd[k + 1] = a22; sh.bdo[k] = a21;
-        }
-        k += 2;
-      } else {
-        int pp = fabs(amm) >= fabs(att) ? mi : t;
-        swp(cur, pp);
-        double dkk = T[cur][cur], inv = 1.0 / dkk;
-        if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
-        __syncwarp();
-        if (lane > cur && lane < bs) {
-          for (int j = cur + 1; j <= lane; ++j) {
-            double ldl = __dmul_rn(T[j][cur], dkk);
-            T[lane][j] = __dsub_rn(T[lane][j], __dmul_rn(T[lane][cur], ldl));
-          }
-        }
-        __syncwarp();
-        if (lane == 0) { sh.bdt[k] = PT_1X1; sh.bdd[k] = dkk; }
-        k += 1;
       }
+      k += 2;
     }
-    __syncwarp();
+    __syncthreads();
   }
-  if (lane == 0) sh.bnelim = k;
-  __syncwarp();
+  if (tid == 0) sh.bnelim = k;
+  __syncthreads();
 }
 
 // Full symmetric swap of positions i, j inside a view of `rows` rows
@@ -355,14 +406,13 @@ __device__ int cta_factor_inner(CtaShared& sh, PanelView V, int64_t bm, int pl, 
     // 1. backup a[k..bm, k..k+bs]
     for (int j = 0; j < bs; ++j)
       for (int64_t i = tid; i < rows; i += NT) bk[i + j * ldb] = V(k + i, k + j);
-    // 2. load the diagonal block, factor it with one warp
+    // 2. load the diagonal block, factor it with the whole CTA
     for (int t = tid; t < bs * bs; t += NT) {
       int i = t % bs, j = t / bs;
       if (i >= j) sh.T[i][j] = V(k + i, k + j);
     }
     __syncthreads();
-    if (warp == 0) warp_block_factor(sh, bs, o.small, lane);
-    __syncthreads();
+    cta_block_factor(sh, bs, o.small);
     int bnelim = sh.bnelim;
     if (bnelim == 0) {
       for (int j = 0; j < bs; ++j)
@@ -1309,7 +1359,7 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
         a.wld = m - wrow;
         a.wrow0 = wrow;
         a.wcol0 = kadd;
-        k_lf_w<<<blocks_for(m - oe, 256), 256, 0, st>>>(a);
+        k_lf_w<<<blocks_for(m - oe, 128), 128, 0, st>>>(a);
         h->launches++;
         mark(h, RVG_PART_LF_W);
         // The next outer block is [g, g + min(rem - bcols, nb)); columns past
@@ -2122,6 +2172,35 @@ rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable) {
   if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
   h->profiling = enable != 0;
   return RVG_OK;
+}
+
+// A one-thread wait on a flag that nothing raises (the solve's flag wait).
+__global__ void k_wait_probe(const int32_t* flag, int32_t* err) { sf_wait(flag, err); }
+
+rvg_status rvg_selftest_waits(rvg_handle* h, int32_t which) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (which != 0 && which != 1) { set_error("which must be 0 (solve flag) or 1 (tensor-core pipeline)"); return RVG_ERR_INVALID_INPUT; }
+  CK(cudaSetDevice(h->device));
+  cudaStream_t st = h->st;
+  int rc = device_wait_status(h);  // start from a clean error word
+  if (rc) return (rvg_status)rc;
+  if ((rc = ensure(h->sf_sync, h->sf_sync_cap, 2, st))) return (rvg_status)rc;
+  CK(cudaMemsetAsync(h->sf_sync, 0, 2 * sizeof(int32_t), st));
+  if (which == 0) {
+    k_wait_probe<<<1, 1, 0, st>>>(h->sf_sync, h->d_err);
+  } else {
+    // one 128 x 128 tile, K = 32, operands never copied in: the MMA warp's wait runs out
+    double* c = nullptr;
+    float* p = nullptr;
+    CK(cudaMallocAsync((void**)&c, 128 * 128 * sizeof(double), st));
+    CK(cudaMallocAsync((void**)&p, 2 * (size_t)TC_BLOCK * sizeof(float), st));
+    TcArgs ta{c, 128, 0, 128, 0, 128, p, p + TC_BLOCK, 1, nullptr, 32, 1, 1, 1, h->d_err, nullptr, 0, 1};
+    k_syrk_tc<4><<<1, TC_THREADS, TC_SMEM, st>>>(ta);
+    CK(cudaFreeAsync(c, st));
+    CK(cudaFreeAsync(p, st));
+  }
+  CK(cudaGetLastError());
+  return (rvg_status)device_wait_status(h);
 }
 
 rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {

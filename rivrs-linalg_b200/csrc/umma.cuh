@@ -86,6 +86,7 @@ struct TcArgs {
   int32_t* err;
   const int32_t* cond;  // when set, the update runs only if *cond < cond_lt
   int32_t cond_lt;
+  int32_t stall;        // self-test of the bounded waits: the producer issues no copies
 };
 
 struct PackArgs {
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
     if (lane == 0) {
       int64_t g = 0, last_round[TC_STAGES];
       for (int s = 0; s < TC_STAGES; ++s) last_round[s] = -1;
-      for (int64_t t = blockIdx.x; t < a.ntiles && !abort_flag; t += gridDim.x) {
+      for (int64_t t = blockIdx.x; t < a.ntiles && !abort_flag && !a.stall; t += gridDim.x) {
         int64_t bx, by;
         tc_tile(a, t, bx, by);
         const float* A = a.Ap + by * a.Q * TC_BLOCK;
