@@ -317,6 +317,24 @@ def main():
     e2e = max_over_ranks(statistics.mean(e2e_times))
     bwd_e2e = rv.problems.backward_error(s, xh, b)
 
+    # blocked multi-RHS solve: 8 right-hand sides in one call against 8 single calls (device-resident)
+    stream = torch.cuda.ExternalStream(solver.stream())
+    rhs8 = torch.randn(8, s.n, dtype=torch.float64, device="cuda")  # 8 columns of length n, ld n
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        fn()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+    multi = {"nrhs": 8,
+             "blocked_ms": timed(lambda: solver.solve_device(rhs8.data_ptr(), 8, s.n)),
+             "one_at_a_time_ms": timed(lambda: [solver.solve_device(rhs8[r].data_ptr(), 1, s.n) for r in range(8)])}
+
     work = solver.work()
     dpeak = gemm_peak_tflops(torch, torch.float64)
     tpeak = gemm_peak_tflops(torch, torch.float32)
@@ -360,6 +378,7 @@ def main():
             "speedup_vs_plain_fp64": plain["t"] / t_step,
             "stats": stats, "factor_flops": full_flops,
             "factor_gflops": full_flops / t_step / 1e9,
+            "multi_rhs_solve": multi,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(s.values.nbytes + b.nbytes),
                     "d2h_bytes_per_step": int(b.nbytes)},
             "gpu_launches": int(launches // max(args.steps, 1)),

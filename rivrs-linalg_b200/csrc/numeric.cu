@@ -1875,10 +1875,12 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   if (n == 0 || nrhs == 0) return RVG_OK;
   int rc = ensure(h->d_x, h->x_cap, (size_t)(n * nrhs), st);
   if (rc) return rc;
-  // per-front solve workspace: forward results, then final values (m each)
+  // right-hand sides per launch (a power of two up to 8) and the per-front
+  // solve workspace: forward results, then final values (R x m each)
+  const int rmax = nrhs >= 8 ? 8 : nrhs >= 4 ? 4 : nrhs >= 2 ? 2 : 1;
   int64_t wneed = 0;
   std::vector<DFront> fr = h->h_fronts;
-  for (auto& f : fr) { f.scratch = wneed; wneed += 2 * (int64_t)f.m; }
+  for (auto& f : fr) { f.scratch = wneed; wneed += 2 * (int64_t)rmax * f.m; }
   if ((rc = ensure(h->solve_work, h->solve_work_cap, (size_t)std::max<int64_t>(wneed, 1), st))) return rc;
   CK(cudaMemcpyAsync(h->d_fronts, fr.data(), fr.size() * sizeof(DFront), cudaMemcpyHostToDevice, st));
   Arenas A{h->panel, h->idx, h->dtype, h->ddiag, h->doff, nullptr, h->cb_arena};
@@ -1923,23 +1925,45 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
     sw.ticket = h->sf_sync;
     sw.flags = h->sf_sync + 1;
     sw.x = h->d_x + rh * n;
+    sw.ldx = n;
     sw.work = h->solve_work;
     sw.err = h->d_err;
     return sw;
   };
-  for (int64_t rh = 0; rh < nrhs; ++rh) {
+  auto fwd = [&](int r, size_t w, const SfWave& sw) {
+    const unsigned g = (unsigned)std::min<int64_t>(nbf[w], 16LL * h->nsm);
+    switch (r) {
+      case 8: k_sf_fwd<8><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      case 4: k_sf_fwd<4><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      case 2: k_sf_fwd<2><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      default: k_sf_fwd<1><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+    }
+  };
+  auto bwd = [&](int r, size_t w, const SfWave& sw) {
+    const unsigned g = (unsigned)std::min<int64_t>(nbb[w], 6LL * h->nsm);
+    switch (r) {
+      case 8: k_sf_bwd<8><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      case 4: k_sf_bwd<4><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      case 2: k_sf_bwd<2><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      default: k_sf_bwd<1><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+    }
+  };
+  for (int64_t rh = 0; rh < nrhs;) {
+    const int64_t left = nrhs - rh;
+    const int r = left >= 8 ? 8 : left >= 4 ? 4 : left >= 2 ? 2 : 1;
     for (size_t w = 0; w < nw; ++w) {
       if (!nbf[w]) continue;
       CK(cudaMemsetAsync(h->sf_sync, 0, (size_t)(nbf[w] + 1) * 4, st));
-      k_sf_fwd<<<(unsigned)std::min<int64_t>(nbf[w], 16LL * h->nsm), SF_B, 0, st>>>(wave(w, true, rh), h->d_fronts, A);
+      fwd(r, w, wave(w, true, rh));
       launches++;
     }
     for (size_t w = nw; w-- > 0;) {
       if (!nbb[w]) continue;
       CK(cudaMemsetAsync(h->sf_sync, 0, (size_t)(nbb[w] + 1) * 4, st));
-      k_sf_bwd<<<(unsigned)std::min<int64_t>(nbb[w], 6LL * h->nsm), SF_B, 0, st>>>(wave(w, false, rh), h->d_fronts, A);
+      bwd(r, w, wave(w, false, rh));
       launches++;
     }
+    rh += r;
   }
   k_perm_scale_out<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_rhs, ldb, nrhs, h->d_x, n, h->d_pfwd,
                                                                   h->has_scaling ? h->d_scal : nullptr);

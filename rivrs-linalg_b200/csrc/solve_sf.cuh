@@ -25,7 +25,8 @@
 //   flag is up), then the unit upper solve (L11^T) of the diagonal block by
 //   one warp; x[col] = x_final; raise the flag.
 // Per row (forward) and per column (backward) the sums run in ascending
-// column / row order inside each 64-block.
+// column / row order inside each 64-block.  Up to 8 right-hand sides go
+// through one launch (template R), each L value read once for all of them.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -50,8 +51,9 @@ struct SfWave {
   int32_t nfr, nblk;
   int32_t* ticket;  // zeroed before the launch
   int32_t* flags;   // nblk entries, zeroed before the launch
-  double* x;        // solution vector (one RHS), permuted order
-  double* work;     // per-front work: v (m) then x_final (m), at DFront::scratch
+  double* x;        // solution vectors, permuted order: right-hand side r at x + r ldx
+  int64_t ldx;
+  double* work;     // per-front work at DFront::scratch: y (R x m) then x_final (R x m)
   int32_t* err;
 };
 
@@ -112,9 +114,11 @@ __device__ __forceinline__ void sf_load_strip(const double* src, int64_t m, int 
   }
 }
 
+// R right-hand sides at once: every L value read is used R times.
+template <int R>
 __global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Arenas A) {
   __shared__ int s_blk;
-  __shared__ double yb[SF_B];
+  __shared__ double yb[R][SF_B];
   __shared__ double Ls[SF_B][SF_B + 1];
   const int t = threadIdx.x;
   for (;;) {
@@ -129,7 +133,7 @@ __global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Aren
     const double* L = A.panel + fr.panel;
     const int32_t* rows = A.idx + fr.idx;
     const int32_t* perm = rows + m;
-    double* v = w.work + fr.scratch;
+    double* v = w.work + fr.scratch;  // y of right-hand side r at v + r m
     int32_t* flags = w.flags + sf.blk0;
     const int b = blk - sf.blk0;
     const bool diag = b < sf.nbd;
@@ -137,21 +141,35 @@ __global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Aren
     const int64_t r1 = diag ? (r0 + SF_B < ne ? r0 + SF_B : ne) : (r0 + SF_B < m ? r0 + SF_B : m);
     const int64_t i = r0 + t;
     const bool row = i < r1;
-    double acc = (diag && row) ? w.x[sf_col(rows, perm, i)] : 0.0;
+    double acc[R];
+    if (diag && row) {
+      const int32_t g = sf_col(rows, perm, i);
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] = w.x[r * w.ldx + g];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] = 0.0;
+    }
     const int ncb = diag ? b : sf.nbd;
     for (int cb = 0; cb < ncb; ++cb) {
       if (t == 0) sf_wait(&flags[cb], w.err);
       __syncthreads();
       const int64_t c0 = (int64_t)cb * SF_B;
       const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
-      if (t < nc) yb[t] = __ldcg(&v[c0 + t]);
+      if (t < nc) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) yb[r][t] = __ldcg(&v[r * m + c0 + t]);
+      }
       __syncthreads();
       if (row) {
         double lr[SF_B];
         sf_load_strip(L + i + c0 * m, m, nc, lr);
 #pragma unroll
         for (int c = 0; c < SF_B; ++c)
-          if (c < nc) acc = __fma_rn(-lr[c], yb[c], acc);
+          if (c < nc) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = __fma_rn(-lr[c], yb[r][c], acc[r]);
+          }
       }
       __syncthreads();
     }
@@ -160,23 +178,29 @@ __global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Aren
       // the diagonal block staged in shared memory first
       const int nr = (int)(r1 - r0);
       if (row) sf_load_strip(L + i + r0 * m, m, nr, &Ls[t][0]);
-      yb[t] = acc;
+#pragma unroll
+      for (int r = 0; r < R; ++r) yb[r][t] = acc[r];
       __syncthreads();
       if (t < 32) {
-        double a0 = yb[t], a1 = yb[t + 32];
-        for (int j = 0; j < nr; ++j) {
-          const double yj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
-          if (t > j && t < nr) a0 = __fma_rn(-Ls[t][j], yj, a0);
-          if (t + 32 > j && t + 32 < nr) a1 = __fma_rn(-Ls[t + 32][j], yj, a1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          double a0 = yb[r][t], a1 = yb[r][t + 32];
+          for (int j = 0; j < nr; ++j) {
+            const double yj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
+            if (t > j && t < nr) a0 = __fma_rn(-Ls[t][j], yj, a0);
+            if (t + 32 > j && t + 32 < nr) a1 = __fma_rn(-Ls[t + 32][j], yj, a1);
+          }
+          if (t < nr) v[r * m + r0 + t] = a0;
+          if (t + 32 < nr) v[r * m + r0 + t + 32] = a1;
         }
-        if (t < nr) v[r0 + t] = a0;
-        if (t + 32 < nr) v[r0 + t + 32] = a1;
       }
       __threadfence();
       __syncthreads();
       if (t == 0) sf_st_release(&flags[b], 1);
     } else if (row) {
-      atomicAdd(&w.x[sf_row(rows, perm, ne, fr.k, i - ne)], acc);
+      const int32_t g = sf_row(rows, perm, ne, fr.k, i - ne);
+#pragma unroll
+      for (int r = 0; r < R; ++r) atomicAdd(&w.x[r * w.ldx + g], acc[r]);
     }
   }
 }
@@ -200,10 +224,11 @@ __device__ __forceinline__ double sf_dinv(const DFront& fr, const Arenas& A, con
                  : __ddiv_rn(__dsub_rn(__dmul_rn(a, r2), __dmul_rn(b, r1)), det);
 }
 
+template <int R>
 __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Arenas A) {
   __shared__ int s_blk;
   __shared__ double Ls[SF_B][SF_B + 1];
-  __shared__ double xs[SF_B];
+  __shared__ double xs[R][SF_B];
   const int t = threadIdx.x;
   for (;;) {
     if (t == 0) s_blk = atomicAdd(w.ticket, 1);
@@ -217,59 +242,74 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
     const double* L = A.panel + fr.panel;
     const int32_t* rows = A.idx + fr.idx;
     const int32_t* perm = rows + m;
-    const double* y = w.work + fr.scratch;  // forward results (rows < ne)
-    double* xf = w.work + fr.scratch + m;   // final values of this front's columns
+    const double* y = w.work + fr.scratch;      // forward results of right-hand side r at y + r m
+    double* xf = w.work + fr.scratch + R * m;   // final values of this front's columns, at xf + r m
     int32_t* flags = w.flags + sf.blk0;
     const int b = sf.nbd - 1 - (blk - sf.blk0);  // descending
     const int64_t c0 = (int64_t)b * SF_B;
     const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
     const bool col = t < nc;
-    double acc = col ? sf_dinv(fr, A, y, c0 + t) : 0.0;
+    double acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = col ? sf_dinv(fr, A, y + r * m, c0 + t) : 0.0;
     // rows of later blocks: L21 (parent's final values), then later diagonal blocks as they finish
     const int nbr = (int)((m - ne + SF_B - 1) / SF_B);
     for (int rb = -nbr; rb < sf.nbd - 1 - b; ++rb) {
       int64_t i0;
-      const double* xsrc = nullptr;
-      bool l21 = rb < 0;
+      const bool l21 = rb < 0;
       if (l21) {
         i0 = ne + (int64_t)(nbr + rb) * SF_B;
       } else {
-        const int r = sf.nbd - 1 - rb;  // later diagonal blocks, from the last one down
-        if (t == 0) sf_wait(&flags[sf.nbd - 1 - r], w.err);
-        i0 = (int64_t)r * SF_B;
-        xsrc = xf;
+        const int rblk = sf.nbd - 1 - rb;  // later diagonal blocks, from the last one down
+        if (t == 0) sf_wait(&flags[sf.nbd - 1 - rblk], w.err);
+        i0 = (int64_t)rblk * SF_B;
       }
       const int64_t iend = l21 ? m : ne;
       const int nr = (int)((i0 + SF_B < iend ? i0 + SF_B : iend) - i0);
       __syncthreads();
       if (t < nr) {
         const int64_t i = i0 + t;
-        xs[t] = l21 ? w.x[sf_row(rows, perm, ne, fr.k, i - ne)] : __ldcg(&xsrc[i]);
+        if (l21) {
+          const int32_t g = sf_row(rows, perm, ne, fr.k, i - ne);
+#pragma unroll
+          for (int r = 0; r < R; ++r) xs[r][t] = w.x[r * w.ldx + g];
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i]);
+        }
         sf_load_strip(L + i + c0 * m, m, nc, &Ls[t][0]);
       }
       __syncthreads();
       if (col)
-        for (int rr = 0; rr < nr; ++rr) acc = __fma_rn(-Ls[rr][t], xs[rr], acc);
+        for (int rr = 0; rr < nr; ++rr) {
+          const double l = Ls[rr][t];
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc[r] = __fma_rn(-l, xs[r][rr], acc[r]);
+        }
     }
     // the diagonal block: x_c = acc_c - sum_{c < i < c0 + nc} L(i, c) x_i, from the bottom
     __syncthreads();
     if (t < nc) sf_load_strip(L + (c0 + t) + c0 * m, m, nc, &Ls[t][0]);  // Ls[row][col]
-    xs[t] = acc;
+#pragma unroll
+    for (int r = 0; r < R; ++r) xs[r][t] = acc[r];
     __syncthreads();
     if (t < 32) {
-      double a0 = xs[t], a1 = xs[t + 32];
-      for (int j = nc - 1; j >= 0; --j) {
-        const double xj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
-        if (t < j) a0 = __fma_rn(-Ls[j][t], xj, a0);
-        if (t + 32 < j) a1 = __fma_rn(-Ls[j][t + 32], xj, a1);
-      }
-      if (t < nc) {
-        xf[c0 + t] = a0;
-        w.x[sf_col(rows, perm, c0 + t)] = a0;
-      }
-      if (t + 32 < nc) {
-        xf[c0 + t + 32] = a1;
-        w.x[sf_col(rows, perm, c0 + t + 32)] = a1;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        double a0 = xs[r][t], a1 = xs[r][t + 32];
+        for (int j = nc - 1; j >= 0; --j) {
+          const double xj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
+          if (t < j) a0 = __fma_rn(-Ls[j][t], xj, a0);
+          if (t + 32 < j) a1 = __fma_rn(-Ls[j][t + 32], xj, a1);
+        }
+        if (t < nc) {
+          xf[r * m + c0 + t] = a0;
+          w.x[r * w.ldx + sf_col(rows, perm, c0 + t)] = a0;
+        }
+        if (t + 32 < nc) {
+          xf[r * m + c0 + t + 32] = a1;
+          w.x[r * w.ldx + sf_col(rows, perm, c0 + t + 32)] = a1;
+        }
       }
     }
     __threadfence();

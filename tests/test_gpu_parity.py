@@ -18,6 +18,9 @@ pytestmark = pytest.mark.gpu
 SOL_RTOL = 1e-10
 
 
+LARGE = dict(large_front_threshold=33)  # forces the multi-kernel large-front path onto small fronts
+
+
 def run_both(rv, orc, s, order=None, nrhs=1, seed=0, scaling=None, **opts):
     order = rv.ordering.default_order(s) if order is None else order
     solver = rv.SparseLDLT.analyze(s, rv.AnalyzeOptions(rv.OrderingStrategy.USER_SUPPLIED, order))
@@ -130,6 +133,20 @@ def test_multiple_rhs_and_refactor(rv, orc):
     del sv
 
 
+@pytest.mark.parametrize("nrhs", [2, 3, 8, 13])
+@pytest.mark.parametrize("large", [False, True])
+def test_blocked_multi_rhs(rv, orc, nrhs, large):
+    # right-hand sides go through the solve 8, 4, 2 or 1 at a time; each column must
+    # match the oracle's solve and the single-RHS solve of the same factor
+    s = rv.problems.kkt(8, seed=4)
+    solver, ref, b = run_both(rv, orc, s, nrhs=nrhs, **(LARGE if large else {}))
+    assert_parity(rv, s, solver, ref, b)
+    x = solver.solve(b)
+    for r in range(nrhs):
+        xr = solver.solve(np.ascontiguousarray(b[:, r]))
+        assert np.linalg.norm(x[:, r] - xr) <= SOL_RTOL * np.linalg.norm(xr)
+
+
 def test_scaling(rv, orc):
     s = rv.problems.shifted_laplacian(8, 0.1)
     sc = np.random.default_rng(7).uniform(0.5, 2.0, s.n)
@@ -149,7 +166,6 @@ def test_errors(rv):
 
 
 # ---- the multi-kernel large-front path, forced onto small fronts ----------
-LARGE = dict(large_front_threshold=33)
 
 
 @pytest.mark.parametrize("n", [48, 100, 257, 300, 520, 700])
