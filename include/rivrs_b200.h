@@ -211,6 +211,19 @@ enum {
 rvg_status rvg_set_profiling(rvg_handle* h, int32_t enable);
 rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* out);
 
+/* MC64 maximum-product matching and symmetric scaling (mc64_matching,
+ * sparse/src/ordering/matching.rs:121-248; Duff & Koster 2001, Duff & Pralet
+ * 2005), host code.  Input: a square symmetric matrix in CSC (either triangle
+ * or both; explicit zeros ignored), n > 0, finite values.  Output:
+ * matching[i] = column matched to row i (a permutation; unmatched rows take
+ * the free columns in increasing order), scaling[i] > 0 with
+ * |scaling[i] a_ij scaling[j]| <= 1 on every entry touching a matched index
+ * and a scaled entry of 1 in every nonzero matched row, *matched = number of
+ * matched rows (< n: structurally singular).  RVG_ERR_INVALID_INPUT for n == 0
+ * or non-finite entries (SparseError::InvalidInput). */
+rvg_status rvg_mc64(int64_t n, const int64_t* colptr, const int64_t* rowidx, const double* values,
+                    int64_t* matching, double* scaling, int64_t* matched);
+
 /* Self-test of the bounded device waits (no reference counterpart): runs one
  * wait that nothing releases, on the handle's stream, and returns the status
  * the host then reads: RVG_ERR_DEVICE_TIMEOUT when the wait ran out and was

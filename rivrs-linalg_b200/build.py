@@ -25,7 +25,7 @@ CU_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fP
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", os.path.join(ROOT, "include")]
 
 CU_SOURCES = ["numeric.cu", "noalloc.cu"]
-CXX_SOURCES = ["symbolic.cpp", "plan.cpp", "capi.cpp"]
+CXX_SOURCES = ["symbolic.cpp", "plan.cpp", "capi.cpp", "mc64.cpp"]
 
 
 def _run(cmd):

@@ -16,6 +16,8 @@ All functions return ``order`` with ``order[new] = old`` (int64).
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
 
@@ -85,3 +87,25 @@ def default_order(sysm) -> np.ndarray:
     if sysm.n <= 2:
         return natural_order(sysm.n)
     return rcm_order(sysm)
+
+
+def mc64(sysm):
+    """MC64 maximum-product matching and symmetric scaling (mc64_matching,
+    sparse/src/ordering/matching.rs:121-248), computed on the host by the
+    library (rvg_mc64).  Returns (matching, scaling, matched) in the system's
+    original index order: matching[i] is the column matched to row i,
+    scaling[i] the symmetric scaling factor, matched the number of matched
+    rows (n for structurally nonsingular matrices)."""
+    from . import _native as N
+    n = int(sysm.n)
+    colptr = N.as_i64(sysm.colptr)
+    rowidx = N.as_i64(sysm.rowidx)
+    vals = N.as_f64(sysm.values)
+    matching = np.zeros(max(n, 1), np.int64)
+    scaling = np.zeros(max(n, 1), np.float64)
+    matched = C.c_int64(0)
+    st = N.lib().rvg_mc64(n, N.ptr(colptr, N.i64p), N.ptr(rowidx, N.i64p), N.ptr(vals, N.dp),
+                          N.ptr(matching, N.i64p), N.ptr(scaling, N.dp), C.byref(matched))
+    if st != 0:
+        raise N.RvgError(st, N.lib().rvg_last_error().decode())
+    return matching[:n], scaling[:n], int(matched.value)

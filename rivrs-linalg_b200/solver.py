@@ -154,7 +154,15 @@ class SparseLDLT:
     @classmethod
     def analyze_with_matrix(cls, system, options: AnalyzeOptions | None = None, scaling: np.ndarray | None = None):
         """analyze plus scaling in ORIGINAL order, transformed to elimination order
-        (solver.rs:261-285)."""
+        (solver.rs:261-285).  With MATCH_ORDER_METIS the scaling is MC64's
+        (matching.rs:121-248); the fill-reducing order is the project's ordering
+        (METIS is not available)."""
+        options = options or AnalyzeOptions()
+        if scaling is None and options.ordering == OrderingStrategy.MATCH_ORDER_METIS:
+            try:
+                _, scaling, _ = orderings.mc64(system)
+            except N.RvgError as e:
+                raise InvalidInput(str(e)) from None
         s = cls.analyze(system, options)
         if scaling is not None:
             s._scaling = N.as_f64(np.asarray(scaling)[s.symbolic.perm_fwd])

@@ -147,6 +147,18 @@ def test_blocked_multi_rhs(rv, orc, nrhs, large):
         assert np.linalg.norm(x[:, r] - xr) <= SOL_RTOL * np.linalg.norm(xr)
 
 
+@pytest.mark.parametrize("large", [False, True])
+def test_mc64_scaled_factorization(rv, orc, large):
+    # MatchOrderMetis: MC64 scaling in elimination order, applied inside the factorization
+    for s in (rv.problems.shifted_laplacian(12, 0.1), rv.problems.kkt(8, seed=5)):
+        solver = rv.SparseLDLT.analyze_with_matrix(s, rv.AnalyzeOptions(rv.OrderingStrategy.MATCH_ORDER_METIS))
+        assert solver._scaling is not None
+        solver.factor(None, rv.FactorOptions(**(LARGE if large else {})))
+        ref = orc.OracleFactor(s, solver.symbolic, solver._scaling, orc.options())
+        assert solver.inertia() == s.inertia
+        assert_parity(rv, s, solver, ref, rv.problems.rhs_uniform(s.n, 0))
+
+
 def test_scaling(rv, orc):
     s = rv.problems.shifted_laplacian(8, 0.1)
     sc = np.random.default_rng(7).uniform(0.5, 2.0, s.n)
