@@ -91,9 +91,20 @@ __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
     if (tid == 0) { st->bs = 0; st->bnelim = 0; st->eff = 0; st->nelim = 0; }
     return;
   }
-  for (int t = tid; t < bs * bs; t += NT) {
-    int i = t % bs, j = t / bs;
-    if (i >= j) { double v = V(k + i, k + j); sh.T[i][j] = v; st->Tb[i][j] = v; }
+  {
+    // the block's loads before any global store (4 per thread)
+    constexpr int PER = IBMAX * IBMAX / NT;
+    double v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int t = tid + u * NT, i = t % IBMAX, j = t / IBMAX;
+      v[u] = (i < bs && j < bs && i >= j) ? V(k + i, k + j) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < PER; ++u) {
+      const int t = tid + u * NT, i = t % IBMAX, j = t / IBMAX;
+      if (i < bs && j < bs && i >= j) { sh.T[i][j] = v[u]; st->Tb[i][j] = v[u]; }
+    }
   }
   __syncthreads();
   cta_block_factor(sh, bs, A.o.small);
@@ -223,12 +234,17 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
   const int64_t be = k + bs;
   const double bound = 1.0 / A.o.threshold;
   if (r >= be && r < bm) {
-    double x[IBMAX];
+    // every load of the row before the first store: the backup may alias the
+    // panel as far as the compiler knows, so a load placed after a store
+    // would wait for it (one memory round trip per column)
+    double raw[IBMAX], x[IBMAX];
 #pragma unroll
-    for (int i = 0; i < IBMAX; ++i)
-      if (i < bs) A.pb[r + (int64_t)i * bm] = V(r, k + i);
+    for (int i = 0; i < IBMAX; ++i) raw[i] = i < bs ? V(r, k + i) : 0.0;
 #pragma unroll
     for (int i = 0; i < IBMAX; ++i) x[i] = i < bs ? V(r, k + bperm[i]) : 0.0;
+#pragma unroll
+    for (int i = 0; i < IBMAX; ++i)
+      if (i < bs) A.pb[r + (int64_t)i * bm] = raw[i];
 #pragma unroll
     for (int j = 1; j < IBMAX; ++j)
       if (j < bnelim) {

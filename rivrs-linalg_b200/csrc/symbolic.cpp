@@ -146,13 +146,71 @@ int symbolic_analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, co
     int64_t p = et[S.sup_end[s] - 1];
     S.sup_parent[s] = p == -1 ? -1 : snode_of[p];
   }
-  // 5. patterns: rows >= end of A's columns in s plus the children's
-  //    patterns; sizes are known from the column counts.
+  // 5. relaxed supernodes: merge a supernode into its parent when it ends
+  //    where the parent begins and the merged block keeps its explicit-zero
+  //    fraction under a size-dependent bound.  Only column counts are needed:
+  //    a fundamental supernode's pattern has cc(begin) - width rows, and
+  //    merging s into p keeps p's pattern (pattern(s) lies inside
+  //    cols(p) + pattern(p)), so each column of s gains
+  //    (k_p + |pat p| - |pat s|) stored entries.
+  std::vector<int64_t> gbeg(ns), gk(ns), gpat(ns);
+  std::vector<double> gzero(ns, 0.0), gstore(ns, 0.0);
+  for (int64_t s = 0; s < ns; ++s) {
+    gbeg[s] = S.sup_begin[s];
+    gk[s] = S.sup_end[s] - S.sup_begin[s];
+    gpat[s] = cc[S.sup_begin[s]] - gk[s];
+    double k = (double)gk[s];
+    gstore[s] = k * (k + 1) / 2 + k * (double)gpat[s];
+    double nz = 0;
+    for (int64_t j = S.sup_begin[s]; j < S.sup_end[s]; ++j) nz += (double)cc[j];
+    gzero[s] = gstore[s] - nz;
+  }
+  std::vector<char> absorbed(ns, 0);
+  for (int64_t s = 0; s < ns; ++s) {
+    int64_t p = S.sup_parent[s];
+    if (p < 0 || S.sup_end[s] != S.sup_begin[p]) continue;
+    double ks = (double)gk[s], kp = (double)gk[p];
+    double extra = ks * (kp + (double)gpat[p] - (double)gpat[s]);
+    double km = ks + kp;
+    double store = ks * (ks + 1) / 2 + ks * (kp + (double)gpat[p]) + gstore[p];
+    double zero = gzero[s] + gzero[p] + extra;
+    double lim = km <= 4 ? 1.0 : km <= 16 ? 0.8 : km <= 48 ? 0.1 : 0.05;
+    if (zero > lim * store) continue;
+    absorbed[s] = 1;
+    gbeg[p] = gbeg[s];
+    gk[p] += gk[s];
+    gstore[p] = store;
+    gzero[p] = zero;
+  }
+  {
+    int64_t nn = 0;
+    std::vector<int64_t> newid(ns, -1);
+    for (int64_t s = 0; s < ns; ++s) if (!absorbed[s]) newid[s] = nn++;
+    std::vector<int64_t> nb(nn), ne_(nn), np(nn, -1), npp(nn + 1, 0);
+    std::vector<int64_t> col_group(n, -1);
+    for (int64_t s = 0; s < ns; ++s)
+      if (!absorbed[s]) {
+        int64_t g = newid[s];
+        nb[g] = gbeg[s];
+        ne_[g] = S.sup_end[s];
+        for (int64_t j = nb[g]; j < ne_[g]; ++j) col_group[j] = g;
+        npp[g + 1] = npp[g] + gpat[s];
+      }
+    for (int64_t g = 0; g < nn; ++g) {
+      int64_t pc = et[ne_[g] - 1];
+      np[g] = pc < 0 ? -1 : col_group[pc];
+    }
+    S.sup_begin.swap(nb);
+    S.sup_end.swap(ne_);
+    S.sup_parent.swap(np);
+    S.pat_ptr.swap(npp);
+    ns = nn;
+  }
+  // 6. patterns of the relaxed supernodes: rows >= end of A's columns in s
+  //    plus the children's patterns (children precede their parent); the
+  //    sizes are known from the column counts.
   std::vector<std::vector<int64_t>> ch(ns);
   for (int64_t s = 0; s < ns; ++s) if (S.sup_parent[s] >= 0) ch[S.sup_parent[s]].push_back(s);
-  S.pat_ptr.assign(ns + 1, 0);
-  for (int64_t s = 0; s < ns; ++s)
-    S.pat_ptr[s + 1] = S.pat_ptr[s] + cc[S.sup_begin[s]] - (S.sup_end[s] - S.sup_begin[s]);
   S.pat_idx.resize(S.pat_ptr[ns]);
   std::vector<int64_t> mark(n, -1), P;
   for (int64_t s = 0; s < ns; ++s) {
@@ -174,73 +232,6 @@ int symbolic_analyze(int64_t n, const int64_t* colptr, const int64_t* rowidx, co
       return sym_fail(err, "internal: supernode pattern disagrees with column count");
     std::sort(P.begin(), P.end());
     std::copy(P.begin(), P.end(), S.pat_idx.begin() + S.pat_ptr[s]);
-  }
-  // 6. relaxed supernodes: merge a supernode into its parent when it ends
-  //    where the parent begins and the merged block keeps its explicit-zero
-  //    fraction under a size-dependent bound.  Merging s into p keeps p's
-  //    pattern (pattern(s) lies inside cols(p) + pattern(p)); each column of
-  //    s gains (k_p + |pat p| - |pat s|) stored entries.
-  {
-    std::vector<int64_t> gbeg(ns), gk(ns), gpat(ns);
-    std::vector<double> gzero(ns, 0.0), gstore(ns, 0.0);
-    std::vector<int64_t> top_of(ns);  // group id -> top member (the group is named by its top)
-    for (int64_t s = 0; s < ns; ++s) {
-      gbeg[s] = S.sup_begin[s];
-      gk[s] = S.sup_end[s] - S.sup_begin[s];
-      gpat[s] = S.pat_ptr[s + 1] - S.pat_ptr[s];
-      double k = (double)gk[s];
-      gstore[s] = k * (k + 1) / 2 + k * (double)gpat[s];
-      double nz = 0;
-      for (int64_t j = S.sup_begin[s]; j < S.sup_end[s]; ++j) nz += (double)cc[j];
-      gzero[s] = gstore[s] - nz;
-    }
-    std::vector<char> absorbed(ns, 0);
-    for (int64_t s = 0; s < ns; ++s) {
-      int64_t p = S.sup_parent[s];
-      if (p < 0 || S.sup_end[s] != S.sup_begin[p]) continue;
-      double ks = (double)gk[s], kp = (double)gk[p];
-      double extra = ks * (kp + (double)gpat[p] - (double)gpat[s]);
-      double km = ks + kp;
-      double store = ks * (ks + 1) / 2 + ks * (kp + (double)gpat[p]) + gstore[p];
-      double zero = gzero[s] + gzero[p] + extra;
-      double lim = km <= 4 ? 1.0 : km <= 16 ? 0.8 : km <= 48 ? 0.1 : 0.05;
-      if (zero > lim * store) continue;
-      absorbed[s] = 1;
-      gbeg[p] = gbeg[s];
-      gk[p] += gk[s];
-      gstore[p] = store;
-      gzero[p] = zero;
-    }
-    int64_t nn = 0;
-    std::vector<int64_t> newid(ns, -1);
-    for (int64_t s = 0; s < ns; ++s) if (!absorbed[s]) newid[s] = nn++;
-    if (nn != ns) {
-      std::vector<int64_t> nb(nn), ne_(nn), np(nn, -1), npp(nn + 1, 0), npi;
-      std::vector<int64_t> col_group(n, -1);
-      for (int64_t s = 0; s < ns; ++s)
-        if (!absorbed[s]) {
-          int64_t g = newid[s];
-          nb[g] = gbeg[s];
-          ne_[g] = S.sup_end[s];
-          for (int64_t j = nb[g]; j < ne_[g]; ++j) col_group[j] = g;
-        }
-      for (int64_t s = 0; s < ns; ++s)
-        if (!absorbed[s]) {
-          int64_t g = newid[s];
-          int64_t pc = et[ne_[g] - 1];
-          np[g] = pc < 0 ? -1 : col_group[pc];
-          npp[g + 1] = npp[g] + (S.pat_ptr[s + 1] - S.pat_ptr[s]);
-        }
-      npi.resize(npp[nn]);
-      for (int64_t s = 0; s < ns; ++s)
-        if (!absorbed[s]) std::copy(S.pat_idx.begin() + S.pat_ptr[s], S.pat_idx.begin() + S.pat_ptr[s + 1],
-                                    npi.begin() + npp[newid[s]]);
-      S.sup_begin.swap(nb);
-      S.sup_end.swap(ne_);
-      S.sup_parent.swap(np);
-      S.pat_ptr.swap(npp);
-      S.pat_idx.swap(npi);
-    }
   }
   S.colcount = std::move(cc);
   S.etree = std::move(et);
