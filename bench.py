@@ -41,6 +41,8 @@ CONFIGS = {
     "kkt60": ("kkt", 60, "kkt27_60^3: H 27-pt 60^3 + diag U[0,1e-2], J 54000x216000 (4/row), n=270000"),
     "lap16": ("lap", 16, "laplace7_16^3 shifted to 10% negative, n=4096"),
     "lap100": ("lap", 100, "laplace7_100^3 shifted to 5% negative, n=1000000"),
+    "batch64": ("batch", 64, "64 systems, n log-uniform in [5e3, 2e5] (seed 1), half shifted 7-pt Laplacians, "
+                "half KKT, 1-32 RHS each; then 20 refactorizations"),
 }
 METRIC = "factor+solve time to bwd err 1e-14, chosen form vs plain FP64 on 1 B200"
 
@@ -183,6 +185,157 @@ def gemm_peak_tflops(torch, dtype):
     return best
 
 
+def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local):
+    """The many-systems workload: 64 systems (n log-uniform in [5e3, 2e5],
+    half shifted Laplacians, half KKT, seed 1) with 1-32 right-hand sides each,
+    factored and solved as one block-diagonal union in plain FP64; a step is
+    the factorization of the batch plus the solve of all its right-hand sides.
+    Then refactorizations with every value scaled by 1 + 0.01 N(0,1)
+    (symmetric pairs alike), each followed by the solve."""
+    t0 = time.perf_counter()
+    fam = rv.problems.batch_family(count=64, seed=1)
+    systems, nrhs = [f[0] for f in fam], [f[1] for f in fam]
+    bl = rv.BatchLDLT(systems)
+    analyze_ms = (time.perf_counter() - t0) * 1e3
+    u = bl.union
+    flops = dense_flops(bl.solver.symbolic)
+    rhs = [rv.problems.rhs_normal(sy.n, 100 + i, r) for i, (sy, r) in enumerate(zip(systems, nrhs))]
+    big = bl.rhs_matrix(rhs)
+    R = big.shape[1]
+    opts = rv.FactorOptions(precision="fp64")
+    d_vals = torch.from_numpy(u.values).to("cuda")
+    d_scal = torch.from_numpy(bl.solver._scaling).to("cuda")
+    d_big = torch.from_numpy(np.ascontiguousarray(big.T)).to("cuda")  # R columns of length n, ld n
+    d_x = torch.empty_like(d_big)
+    # symmetric perturbation map on the device: entry -> its unordered pair
+    col = np.repeat(np.arange(u.n, dtype=np.int64), np.diff(u.colptr))
+    key = np.minimum(u.rowidx, col) * np.int64(u.n) + np.maximum(u.rowidx, col)
+    uniq, inv = np.unique(key, return_inverse=True)
+    d_inv = torch.from_numpy(inv.astype(np.int64)).to("cuda")
+    del col, key, inv
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(7)
+    d_pert = torch.empty_like(d_vals)
+    bl.solver._ensure_handle(opts)
+    bl.solver.set_profiling(True)
+    stream = torch.cuda.ExternalStream(bl.solver.stream())
+
+    def step(vals):
+        bl.solver.factor_device(vals.data_ptr(), d_scal.data_ptr(), opts)
+        with torch.cuda.stream(stream):  # the handle's stream orders the copy before the solve
+            d_x.copy_(d_big)
+        bl.solver.solve_device(d_x.data_ptr(), R, u.n)
+
+    def timed(vals):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        step(vals)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    for _ in range(args.warmup):
+        step(d_vals)
+    barrier()
+    clocks = ClockSampler()
+    times = [timed(d_vals) for _ in range(args.steps)]
+    prof = bl.solver.profile()
+    x = d_x.cpu().numpy().T
+    xs = bl.split(np.asfortranarray(x), rhs)
+    errs = []
+    for i, sy in enumerate(systems):
+        bb = rhs[i] if rhs[i].ndim == 2 else rhs[i][:, None]
+        xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
+        errs.append(max(rv.problems.backward_error(sy, xx[:, j], bb[:, j]) for j in range(bb.shape[1])))
+    inert_ok = all(a == sy.inertia for a, sy in zip(bl.inertias(), systems))
+    nref = 20
+    ref_times = []
+    for r in range(nref):
+        f = 1.0 + 0.01 * torch.randn(uniq.size, dtype=torch.float64, device="cuda", generator=gen)
+        torch.mul(d_vals, f[d_inv], out=d_pert)
+        del f
+        torch.cuda.synchronize()
+        ref_times.append(timed(d_pert))
+    clk = clocks.stop(local)
+    vals_last = d_pert.cpu().numpy()
+    x = d_x.cpu().numpy().T
+    xs = bl.split(np.asfortranarray(x), rhs)
+    errs_ref = []
+    for i, sy in enumerate(systems):
+        lo, hi = u.colptr[bl.offsets[i]], u.colptr[bl.offsets[i + 1]]
+        sv = rv.problems.System(name="p", n=sy.n, colptr=sy.colptr, rowidx=sy.rowidx, values=vals_last[lo:hi])
+        bb = rhs[i] if rhs[i].ndim == 2 else rhs[i][:, None]
+        xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
+        errs_ref.append(max(rv.problems.backward_error(sv, xx[:, j], bb[:, j]) for j in range(bb.shape[1])))
+    # end to end through the public API with host buffers: BatchLDLT.factor + solve
+    e2e_t = []
+    for _ in range(max(1, min(args.steps, 2))):
+        barrier()
+        t1 = time.perf_counter()
+        bl.factor(None, opts)
+        bl.solve(rhs)
+        torch.cuda.synchronize()
+        e2e_t.append(time.perf_counter() - t1)
+    t_step = max_over_ranks(statistics.mean(times))
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        orc = entry.load_oracle()
+        cb = batch_cpu_baseline(rv, orc, systems, flops)
+    if rank == 0:
+        ns = [sy.n for sy in systems]
+        line = {
+            "metric": "batch factor+solve time (64 systems, 1-32 RHS each), plain FP64 on 1 B200",
+            "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
+            "config": {"workload": CONFIGS["batch64"][2], "systems": len(systems), "n_total": int(u.n),
+                       "n_min": min(ns), "n_max": max(ns), "rhs_total": int(sum(nrhs)), "rhs_padded_to": R,
+                       "form": "plain FP64, one block-diagonal union, one handle and stream",
+                       "scaling": "MC64 per system (host analysis incl. ordering %.0f ms)" % analyze_ms,
+                       "l2": "working set far above L2 (126 MB); no flush needed",
+                       "parallelism": f"replicas x{world}"},
+            "bwd_err_max": max(errs), "inertia_exact": inert_ok,
+            "refactor": {"count": nref, "perturbation": "values x (1 + 0.01 N(0,1)), symmetric pairs alike",
+                         "s_per_refactor_mean": statistics.mean(ref_times), "s_min": min(ref_times),
+                         "s_max": max(ref_times), "bwd_err_max_last": max(errs_ref)},
+            "factor_flops": flops, "factor_gflops": flops / t_step / 1e9,
+            "e2e": {"value": max_over_ranks(statistics.mean(e2e_t)), "unit": "s",
+                    "h2d_bytes_per_step": int(u.values.nbytes + big.nbytes), "d2h_bytes_per_step": int(big.nbytes)},
+            "gpu_launches": int(prof["factor_launches"] + prof["solve_launches"]),
+            "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
+                                               "host_total_ms", "host_sync_ms")},
+            "parts_ms": prof["part_ms"], "work": bl.solver.work(), "stats": bl.solver.stats(),
+            "step_event_s": times, "peak_device_bytes": prof["peak_bytes"], "clocks": clk, "cpu_baseline": cb,
+        }
+        print(json.dumps(line), flush=True)
+    bl.close()
+
+
+def batch_cpu_baseline(rv, orc, systems, full_flops):
+    """The oracle on the first systems of the batch (a bounded sample, all host
+    cores), extrapolated to the whole batch by flops."""
+    threads = os.cpu_count() or 1
+    t, fl, used = 0.0, 0.0, 0
+    for sy in systems:
+        if t > 10.0:
+            break
+        an, _ = analyze(rv, sy)
+        b = rv.problems.rhs_normal(sy.n, 0)
+        t0 = time.perf_counter()
+        f = orc.OracleFactor(sy, an.symbolic, an._scaling, orc.options(), nthreads=threads)
+        f.solve(b)
+        t += time.perf_counter() - t0
+        f.close()
+        fl += dense_flops(an.symbolic)
+        used += 1
+    rate = fl / t
+    return dict(value=full_flops / rate, unit="s", cores=threads, kind="port",
+                sample=f"oracle factor+solve of the first {used} systems: {t:.2f} s for {fl:.3e} flops "
+                       f"({rate / 1e9:.1f} GFLOP/s), extrapolated to the batch's {full_flops:.3e} flops")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,12 +361,19 @@ def main():
         if rank != 0:
             return
         orc = entry.load_oracle()
-        s_full, _ = build_system(rv, args.config)
-        sym_full = rv.symbolic_analyze(s_full.n, s_full.colptr, s_full.rowidx, rv.ordering.default_order(s_full))
-        full = dense_flops(sym_full)
+        if args.config == "batch64":
+            systems = [f[0] for f in rv.problems.batch_family(count=64, seed=1)]
+            full = dense_flops(rv.BatchLDLT(systems).solver.symbolic)
+            sample = lambda: (batch_cpu_baseline(rv, orc, systems, full), None)
+        else:
+            s_full, _ = build_system(rv, args.config)
+            sym_full = rv.symbolic_analyze(s_full.n, s_full.colptr, s_full.rowidx,
+                                           rv.ordering.default_order(s_full))
+            full = dense_flops(sym_full)
+            sample = lambda: cpu_baseline(rv, orc, args.config, full)
         vals = []
         for i in range(args.warmup + args.steps):
-            cb, t = cpu_baseline(rv, orc, args.config, full)
+            cb, _ = sample()
             if i >= args.warmup:
                 vals.append(cb["value"])
         v = statistics.median(vals)
@@ -246,6 +406,12 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.config == "batch64":
+        run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     s, b = build_system(rv, args.config)
     solver, analyze_ms = analyze(rv, s)

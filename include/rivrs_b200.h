@@ -67,6 +67,12 @@ typedef struct {
    * Smaller is more accurate (the tensor cores accumulate FP32 with
    * truncation) and slower.  Default 4. */
   int32_t mixed_flush;
+  /* Mixed form with mixed_flush = 0 only: output columns per CTA tile of the
+   * tensor-core Schur GEMM, 128 or 256 (two 128-column tiles sharing one
+   * W tile in shared memory: a quarter fewer operand bytes per flop).  Results
+   * do not depend on it.  Default 256. */
+  int32_t mixed_tile_cols;
+  int32_t reserved;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */

@@ -4,11 +4,12 @@ A drop-in for the numeric half of rivrs-sparse (analyze -> factor -> solve):
 the host computes the ordering and symbolic structure; factorization and
 solve run as sm_100a CUDA kernels in librivrs_b200.so (include/rivrs_b200.h).
 """
-from . import ordering, problems
+from . import batch, ordering, problems
 from ._native import LIB_PATH, RvgError
+from .batch import BatchLDLT
 from .solver import (AnalyzeOptions, DimensionMismatch, FactorOptions, InvalidInput, OrderingStrategy,
                      SolveBeforeFactor, SparseError, SparseLDLT, SymbolicStructure, solve_full, symbolic_analyze)
 
 __all__ = ["AnalyzeOptions", "FactorOptions", "OrderingStrategy", "SparseLDLT", "SymbolicStructure", "SparseError",
            "DimensionMismatch", "InvalidInput", "SolveBeforeFactor", "RvgError", "solve_full", "symbolic_analyze",
-           "ordering", "problems", "LIB_PATH"]
+           "ordering", "problems", "batch", "BatchLDLT", "LIB_PATH"]

@@ -29,7 +29,8 @@ class Options(C.Structure):
     _fields_ = [("threshold", C.c_double), ("small", C.c_double), ("outer_block_size", i64),
                 ("inner_block_size", i64), ("nemin", i64), ("small_leaf_threshold", i64),
                 ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64),
-                ("precision", C.c_int32), ("mixed_flush", C.c_int32)]
+                ("precision", C.c_int32), ("mixed_flush", C.c_int32),
+                ("mixed_tile_cols", C.c_int32), ("reserved", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -1179,6 +1179,27 @@ int syrk_ev(rvg_handle* h) {
   return RVG_OK;
 }
 
+// The tensor-core Schur GEMM over a.ntiles 128 x 128 lower tiles: the flush
+// depth picks the k_syrk_tc instance; without flushing, 256-column CTA tiles
+// (k_syrk_tc_pair, over column-tile pairs) unless 128 is asked for.
+static void launch_tc(rvg_handle* h, TcArgs ta) {
+  cudaStream_t st = h->st;
+  if (h->opt.mixed_flush == 0 && h->opt.mixed_tile_cols == 256) {
+    ta.ntiles = tp_count_tiles(ta.nr, ta.nc, ta.r0, ta.c0);
+    const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
+    k_syrk_tc_pair<<<grid, TC_THREADS, TP_SMEM, st>>>(ta);
+    return;
+  }
+  const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
+  switch (h->opt.mixed_flush) {
+    case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 4: k_syrk_tc<4><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+  }
+}
+
 // The Schur update C -= W L^T (lower) of one contribution block.  kmax bounds
 // the device-side K (columns eliminated).
 int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
@@ -1196,15 +1217,8 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
       k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nr), 256, 0, st>>>(aw);
       k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nc), 256, 0, st>>>(al);
       TcArgs ta{ga.C, ga.ldc, ga.r0, ga.r1, ga.c0, ga.c1, h->pack, pl, Q, ga.Kdev, ga.K, nr, nc, ntiles, h->d_err};
-      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, h->nsm);
       if ((rc = syrk_ev(h))) return rc;
-      switch (h->opt.mixed_flush) {
-        case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-        case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-        case 4: k_syrk_tc<4><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-        case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-        default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-      }
+      launch_tc(h, ta);
       if ((rc = syrk_ev(h))) return rc;
       h->launches += 3;
       h->syrk_launches++;
@@ -1239,14 +1253,7 @@ int launch_window_gemm(rvg_handle* h, const LFArgs& a, int64_t m, int64_t c0, in
     const int64_t t0 = (c0 - wrow) / TC_BM;
     TcArgs ta{a.a, m, c0, m, c0, c1, pk_w + (size_t)t0 * Fq * TC_BLOCK, pk_l + (size_t)t0 * Fq * TC_BLOCK, Fq, kdev,
               kadd, nr, nc, ntiles, h->d_err, cond, cond_lt};
-    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, h->nsm);
-    switch (h->opt.mixed_flush) {
-      case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-      case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-      case 4: k_syrk_tc<4><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-      case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-      default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-    }
+    launch_tc(h, ta);
   } else {
     SyrkArgs ga{};
     ga.C = a.a;
@@ -1721,6 +1728,7 @@ void rvg_default_options(rvg_options* o) {
   o->large_front_threshold = 2048;
   o->precision = 0;
   o->mixed_flush = 4;
+  o->mixed_tile_cols = 256;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347
@@ -1738,6 +1746,10 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347
   if (o.precision != 0 && o.precision != 1) { set_error("precision must be 0 (FP64) or 1 (mixed)"); return RVG_ERR_INVALID_INPUT; }
   if (o.mixed_flush != 0 && o.mixed_flush != 1 && o.mixed_flush != 2 && o.mixed_flush != 4 && o.mixed_flush != 8) {
     set_error("mixed_flush must be 0, 1, 2, 4 or 8");
+    return RVG_ERR_INVALID_INPUT;
+  }
+  if (o.mixed_tile_cols != 128 && o.mixed_tile_cols != 256) {
+    set_error("mixed_tile_cols must be 128 or 256");
     return RVG_ERR_INVALID_INPUT;
   }
   return RVG_OK;
@@ -1805,6 +1817,7 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   CK(cudaFuncSetAttribute(k_syrk_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc<TC_NO_FLUSH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
   CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
   CK(cudaMallocAsync((void**)&h->d_err, sizeof(int32_t), st));
@@ -1903,9 +1916,9 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
       if (f.ne == 0) continue;
       const int32_t nbd = (f.ne + SF_B - 1) / SF_B, nbr = (f.m - f.ne + SF_B - 1) / SF_B;
       vf.push_back(SfFront{(int32_t)s, nbf[w], nbd, nbr});
-      vb.push_back(SfFront{(int32_t)s, nbb[w], nbd, 0});
+      vb.push_back(SfFront{(int32_t)s, nbb[w], nbd, nbr});
       nbf[w] += nbd + nbr;
-      nbb[w] += nbd;
+      nbb[w] += nbd + nbr;
     }
     nfr[w] = (int32_t)vf.size();
     offf[w] = pk.add(vf);

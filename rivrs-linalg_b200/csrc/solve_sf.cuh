@@ -18,7 +18,9 @@
 //     warp; publish y_r, raise flag r;
 //   L21 block (rows >= ne): -sum over all column blocks of L[rows, b] y_b,
 //     added atomically into x at the parent's rows (siblings share rows).
-// backward, per front (descending column blocks; x_final in v + m):
+// backward, per front (first the gather tickets: the parent's final values at
+// the L21 rows into v + m at rows >= ne; then descending column blocks;
+// x_final in v + m):
 //   z = D^-1 y on the block's columns (2x2 pairs may straddle blocks: y is
 //   still intact in v), minus L21^T x[row] (parent's final values), minus
 //   L[rows of later blocks, cols]^T x_final of those blocks (each once its
@@ -43,7 +45,7 @@ struct SfFront {
   int32_t s;     // supernode
   int32_t blk0;  // first ticket of the front
   int32_t nbd;   // diagonal blocks (ceil(ne / 64))
-  int32_t nbr;   // L21 blocks (forward only: ceil((m - ne) / 64))
+  int32_t nbr;   // L21 blocks (ceil((m - ne) / 64)): forward row blocks, backward gather tickets
 };
 
 struct SfWave {
@@ -245,23 +247,38 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
     const double* y = w.work + fr.scratch;      // forward results of right-hand side r at y + r m
     double* xf = w.work + fr.scratch + R * m;   // final values of this front's columns, at xf + r m
     int32_t* flags = w.flags + sf.blk0;
-    const int b = sf.nbd - 1 - (blk - sf.blk0);  // descending
+    const int nbr = sf.nbr;
+    if (blk - sf.blk0 < nbr) {
+      // gather ticket: the parent's final values at 64 rows of L21 into xf
+      const int64_t i = ne + (int64_t)(blk - sf.blk0) * SF_B + t;
+      if (i < m) {
+        const int32_t g = sf_row(rows, perm, ne, fr.k, i - ne);
+#pragma unroll
+        for (int r = 0; r < R; ++r) xf[r * m + i] = w.x[r * w.ldx + g];
+      }
+      __threadfence();
+      __syncthreads();
+      if (t == 0) sf_st_release(&flags[blk - sf.blk0], 1);
+      continue;
+    }
+    const int b = sf.nbd - 1 - (blk - sf.blk0 - nbr);  // descending
     const int64_t c0 = (int64_t)b * SF_B;
     const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
     const bool col = t < nc;
     double acc[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r] = col ? sf_dinv(fr, A, y + r * m, c0 + t) : 0.0;
-    // rows of later blocks: L21 (parent's final values), then later diagonal blocks as they finish
-    const int nbr = (int)((m - ne + SF_B - 1) / SF_B);
+    // rows of later blocks: L21 (the parent's final values, gathered into xf
+    // by the front's first tickets), then later diagonal blocks as they finish
     for (int rb = -nbr; rb < sf.nbd - 1 - b; ++rb) {
       int64_t i0;
       const bool l21 = rb < 0;
       if (l21) {
+        if (t == 0) sf_wait(&flags[nbr + rb], w.err);
         i0 = ne + (int64_t)(nbr + rb) * SF_B;
       } else {
         const int rblk = sf.nbd - 1 - rb;  // later diagonal blocks, from the last one down
-        if (t == 0) sf_wait(&flags[sf.nbd - 1 - rblk], w.err);
+        if (t == 0) sf_wait(&flags[nbr + sf.nbd - 1 - rblk], w.err);
         i0 = (int64_t)rblk * SF_B;
       }
       const int64_t iend = l21 ? m : ne;
@@ -269,14 +286,8 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
       __syncthreads();
       if (t < nr) {
         const int64_t i = i0 + t;
-        if (l21) {
-          const int32_t g = sf_row(rows, perm, ne, fr.k, i - ne);
 #pragma unroll
-          for (int r = 0; r < R; ++r) xs[r][t] = w.x[r * w.ldx + g];
-        } else {
-#pragma unroll
-          for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i]);
-        }
+        for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i]);
         sf_load_strip(L + i + c0 * m, m, nc, &Ls[t][0]);
       }
       __syncthreads();

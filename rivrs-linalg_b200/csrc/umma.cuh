@@ -444,4 +444,225 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TMEM_COLS) : "memory");
 }
 
+// ---------------------------------------------------------------- GEMM, column-tile pairs
+// The one-partial-sum form (no flush) with two 128-column output tiles per CTA
+// tile: both read the same 128-row W tile from shared memory, so a CTA brings
+// in 3 operand tiles per 2 output tiles instead of 4 (the update is bound by
+// the operand stream out of L2).  Stages hold half a packed chunk (16 deep:
+// the hi and lo halves of the W tile and of both L tiles, 48 KB, six
+// cp.async.bulk copies), four stages; tensor memory holds two 256-column
+// accumulators (tile 0 at columns [0, 128), tile 1 at [128, 256) of each).
+// Each output tile gets the same MMA sequence as in k_syrk_tc (per k-step
+// lo*hi, hi*lo, hi*hi, k-steps in order), and the epilogue does
+// C - (0 + partial) in FP64 like k_syrk_tc's one-group case, so the two
+// kernels give bit-identical results.  Epilogue warp e takes tile e / 4 of the
+// pair and its 32-row lane quarter, 16 columns at a time (tensor memory read,
+// then the C read-modify-write), and frees the accumulator after the tile.
+constexpr int TP_BK = 16;                                // K per stage
+constexpr int TP_STAGES = 4;
+constexpr uint32_t TP_HALF_BYTES = TC_PART * 4 / 2;      // 8 KB: half of one TF32 part of a block
+constexpr uint32_t TP_OPND_BYTES = 2 * TP_HALF_BYTES;    // hi + lo halves of one operand tile
+constexpr uint32_t TP_STAGE_BYTES = 3 * TP_OPND_BYTES;   // W tile + two L tiles: 48 KB
+constexpr size_t TP_SMEM = (size_t)TP_STAGES * TP_STAGE_BYTES + 1024 + 32768;
+constexpr uint32_t TP_TMEM_COLS = 512;
+
+// lower column-tile pairs (px: column tiles 2 px and 2 px + 1) in column order
+__host__ __device__ inline int64_t tp_count_tiles(int64_t nr, int64_t nc, int64_t r0, int64_t c0) {
+  int64_t n = 0;
+  for (int64_t px = 0; 2 * px < nc; ++px) {
+    const int64_t f = tc_first_row_tile(2 * px, r0, c0);
+    if (f < nr) n += nr - f;
+  }
+  return n;
+}
+__device__ inline void tp_tile(const TcArgs& a, int64_t t, int64_t& px, int64_t& by) {
+  for (px = 0; 2 * px < a.nc; ++px) {
+    const int64_t f = tc_first_row_tile(2 * px, a.r0, a.c0);
+    const int64_t cnt = f < a.nr ? a.nr - f : 0;
+    if (t < cnt) {
+      by = f + t;
+      return;
+    }
+    t -= cnt;
+  }
+  by = 0;  // not reached for t < ntiles
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc_pair(TcArgs a) {
+  extern __shared__ __align__(1024) uint8_t tc_smem[];
+  __shared__ __align__(8) uint64_t bars[2 * TP_STAGES + 5];
+  __shared__ uint32_t tslot;
+  __shared__ volatile int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (a.cond && *a.cond >= a.cond_lt) return;  // uniform over the CTA
+  int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
+  if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the packed chunks
+  if (K <= 0) return;
+  const int64_t nh = (K + TP_BK - 1) / TP_BK;  // half chunks
+  const uint32_t stage0 = (smem_u32(tc_smem) + 1023u) & ~1023u;
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[TP_STAGES + s]); };
+  auto pfull = [&](int b) { return smem_u32(&bars[2 * TP_STAGES + b]); };
+  auto pempty = [&](int b) { return smem_u32(&bars[2 * TP_STAGES + 2 + b]); };
+  const uint32_t fin = smem_u32(&bars[2 * TP_STAGES + 4]);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tslot)),
+                 "r"(TP_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < TP_STAGES; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(empty(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(pfull(b), 1);
+      mbar_init(pempty(b), TC_EPI_WARPS);
+    }
+    mbar_init(fin, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tslot;
+
+  if (warp == 0) {
+    // ---------------- producer
+    if (lane == 0) {
+      int64_t g = 0, last_round[TP_STAGES];
+      for (int s = 0; s < TP_STAGES; ++s) last_round[s] = -1;
+      for (int64_t t = blockIdx.x; t < a.ntiles && !abort_flag && !a.stall; t += gridDim.x) {
+        int64_t px, by;
+        tp_tile(a, t, px, by);
+        const bool two = 2 * px + 1 < a.nc;
+        const float* A = a.Ap + by * a.Q * TC_BLOCK;
+        const float* B0 = a.Bp + 2 * px * a.Q * TC_BLOCK;
+        const float* B1 = B0 + a.Q * TC_BLOCK;
+        for (int64_t h = 0; h < nh; ++h, ++g) {
+          const int s = (int)(g % TP_STAGES);
+          const int64_t r = g / TP_STAGES;
+          if (r > 0 && !mbar_wait(empty(s), (uint32_t)((r - 1) & 1), &abort_flag, a.err)) break;
+          const uint32_t dst = stage0 + (uint32_t)s * TP_STAGE_BYTES;
+          // hi half at +0, lo half at +TC_PART floats of the (tile, chunk) block
+          const int64_t off = (h >> 1) * TC_BLOCK + (h & 1) * (TC_PART / 2);
+          mbar_expect_tx(full(s), (two ? 3u : 2u) * TP_OPND_BYTES);
+          bulk_g2s(dst, A + off, TP_HALF_BYTES, full(s));
+          bulk_g2s(dst + TP_HALF_BYTES, A + off + TC_PART, TP_HALF_BYTES, full(s));
+          bulk_g2s(dst + TP_OPND_BYTES, B0 + off, TP_HALF_BYTES, full(s));
+          bulk_g2s(dst + TP_OPND_BYTES + TP_HALF_BYTES, B0 + off + TC_PART, TP_HALF_BYTES, full(s));
+          if (two) {
+            bulk_g2s(dst + 2 * TP_OPND_BYTES, B1 + off, TP_HALF_BYTES, full(s));
+            bulk_g2s(dst + 2 * TP_OPND_BYTES + TP_HALF_BYTES, B1 + off + TC_PART, TP_HALF_BYTES, full(s));
+          }
+          last_round[s] = r;
+        }
+      }
+      for (int s = 0; s < TP_STAGES; ++s) {
+        if (last_round[s] < 0) continue;
+        const uint64_t t0 = gtimer();
+        while (!mbar_try(full(s), (uint32_t)(last_round[s] & 1)) && gtimer() - t0 < TC_TIMEOUT_NS) {
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------- MMA issuer
+    if (lane == 0) {
+      int64_t g = 0, grp = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x, ++grp) {
+        int64_t px, by;
+        tp_tile(a, t, px, by);
+        const bool two = 2 * px + 1 < a.nc;
+        const int b = (int)(grp & 1);
+        const int64_t rb = grp >> 1;
+        if (rb > 0 && !mbar_wait(pempty(b), (uint32_t)((rb - 1) & 1), &abort_flag, a.err)) break;
+        tc_fence_after();
+        const uint32_t d0 = tbase + (uint32_t)(b * 2 * TC_BN), d1 = d0 + TC_BN;
+        for (int64_t h = 0; h < nh; ++h, ++g) {
+          const int s = (int)(g % TP_STAGES);
+          if (!mbar_wait(full(s), (uint32_t)((g / TP_STAGES) & 1), &abort_flag, a.err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t base = stage0 + (uint32_t)s * TP_STAGE_BYTES;
+#pragma unroll
+          for (int ks = 0; ks < TP_BK / 8; ++ks) {
+            const uint32_t ko = (uint32_t)ks * 2 * TC_LBO;
+            const uint64_t ah = tc_desc(base + ko), al = tc_desc(base + TP_HALF_BYTES + ko);
+            const uint32_t b0 = base + TP_OPND_BYTES, b1 = base + 2 * TP_OPND_BYTES;
+            const uint32_t acc = (h > 0 || ks > 0) ? 1u : 0u;
+            tc_mma(d0, al, tc_desc(b0 + ko), acc);
+            tc_mma(d0, ah, tc_desc(b0 + TP_HALF_BYTES + ko), 1u);
+            tc_mma(d0, ah, tc_desc(b0 + ko), 1u);
+            if (two) {
+              tc_mma(d1, al, tc_desc(b1 + ko), acc);
+              tc_mma(d1, ah, tc_desc(b1 + TP_HALF_BYTES + ko), 1u);
+              tc_mma(d1, ah, tc_desc(b1 + ko), 1u);
+            }
+          }
+          tc_commit(empty(s));
+        }
+        if (!ok) break;
+        tc_commit(pfull(b));
+      }
+      tc_commit(fin);
+      const uint64_t t0 = gtimer();
+      while (!mbar_try(fin, 0) && gtimer() - t0 < TC_TIMEOUT_NS) {
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue
+    const int e = warp - 2;
+    const int qd = warp & 3, ch = e >> 2;  // lane quarter, tile of the pair
+    const int64_t rl = 32 * qd + lane;
+    int64_t grp = 0;
+    for (int64_t t = blockIdx.x; t < a.ntiles; t += gridDim.x, ++grp) {
+      const int b = (int)(grp & 1);
+      int w = 1;
+      if (lane == 0) w = mbar_wait(pfull(b), (uint32_t)((grp >> 1) & 1), &abort_flag, a.err) ? 1 : 0;
+      if (__shfl_sync(0xffffffffu, w, 0) == 0) break;
+      tc_fence_after();
+      int64_t px, by;
+      tp_tile(a, t, px, by);
+      const int64_t i = a.r0 + by * TC_BM + rl;
+      const int64_t jb = a.c0 + (2 * px + ch) * TC_BN;
+      if (2 * px + ch < a.nc) {
+        double* col = a.C + i + jb * a.ldc;
+        for (int c0 = 0; c0 < TC_BN; c0 += 16) {
+          uint32_t v[16];
+          tc_ld16(tbase + ((uint32_t)(32 * qd) << 16) + (uint32_t)(b * 2 * TC_BN + ch * TC_BN + c0), v);
+          if (i < a.r1) {
+            double cv[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+              const int64_t j = jb + c0 + c;
+              cv[c] = (j < a.c1 && i >= j) ? col[(int64_t)(c0 + c) * a.ldc] : 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < 16; ++c) {
+              const int64_t j = jb + c0 + c;
+              if (j < a.c1 && i >= j) col[(int64_t)(c0 + c) * a.ldc] = cv[c] - (0.0 + (double)__uint_as_float(v[c]));
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(pempty(b));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TP_TMEM_COLS) : "memory");
+}
+
 }  // namespace rvg

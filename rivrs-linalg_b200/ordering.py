@@ -80,6 +80,9 @@ def natural_order(n: int) -> np.ndarray:
 
 
 def default_order(sysm) -> np.ndarray:
+    if "parts" in sysm.meta:  # block-diagonal union: each block's own order, blocks in sequence
+        offs = sysm.meta["offsets"]
+        return np.concatenate([default_order(p) + o for p, o in zip(sysm.meta["parts"], offs[:-1])])
     if sysm.grid is not None and sysm.n_h == 0:
         return nested_dissection_grid(sysm.grid)
     if sysm.grid is not None and sysm.n_h > 0:

@@ -145,6 +145,56 @@ def read_mtx(path: str) -> System:
     return from_scipy(path.rsplit("/", 1)[-1].replace(".mtx", ""), a)
 
 
+def batch_family(count: int = 64, seed: int = 1, n_lo: float = 5e3, n_hi: float = 2e5,
+                 max_rhs: int = 32) -> list:
+    """The many-systems workload: `count` systems with sizes drawn
+    log-uniform in [n_lo, n_hi] from `seed`; even slots are shifted 7-point
+    Laplacians (10% negative eigenvalues, g^3 nearest the drawn size), odd
+    slots KKT systems as kkt() (1.25 g^3 nearest the drawn size, seeded per
+    slot); each slot also draws its number of right-hand sides in
+    [1, max_rhs].  Returns [(System, nrhs)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = float(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
+        nrhs = int(rng.integers(1, max_rhs + 1))
+        if i % 2 == 0:
+            s = shifted_laplacian(max(2, int(round(n ** (1.0 / 3.0)))), 0.10)
+        else:
+            s = kkt(max(4, int(round((n / 1.25) ** (1.0 / 3.0)))), seed=seed * 1000 + i)
+        out.append((s, nrhs))
+    return out
+
+
+def block_diagonal(systems, name: str = "batch") -> System:
+    """One system holding `systems` as its diagonal blocks, in order.  Its
+    values are the blocks' values concatenated (column-major CSC keeps each
+    block's columns, and their entries, contiguous); meta['offsets'] holds the
+    first index of each block (and n), meta['parts'] the systems."""
+    a = sp.block_diag([s.to_scipy() for s in systems], format="csc")
+    inert = None
+    if all(s.inertia is not None for s in systems):
+        inert = tuple(int(sum(s.inertia[k] for s in systems)) for k in range(3))
+    out = from_scipy(name, a, inertia=inert)
+    if not np.array_equal(out.values, np.concatenate([s.values for s in systems])):
+        raise RuntimeError("block values are not contiguous")
+    out.meta.update(offsets=np.cumsum([0] + [s.n for s in systems]).astype(np.int64), parts=list(systems))
+    return out
+
+
+def perturb_symmetric(sysm: System, rel: float = 0.01, seed: int = 0) -> np.ndarray:
+    """Values of sysm scaled entrywise by 1 + rel * N(0,1), the two stored
+    copies (i, j) and (j, i) of an off-diagonal entry by the same factor, so
+    the matrix stays symmetric."""
+    rng = np.random.default_rng(seed)
+    col = np.repeat(np.arange(sysm.n, dtype=np.int64), np.diff(sysm.colptr))
+    row = sysm.rowidx
+    key = np.minimum(row, col) * np.int64(sysm.n) + np.maximum(row, col)
+    uniq, inv = np.unique(key, return_inverse=True)
+    f = 1.0 + rel * rng.standard_normal(uniq.size)
+    return sysm.values * f[inv]
+
+
 def rhs_uniform(n: int, seed: int = 0, nrhs: int = 1) -> np.ndarray:
     rng = np.random.default_rng(seed)
     b = rng.uniform(-1.0, 1.0, (nrhs, n))

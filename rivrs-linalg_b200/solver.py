@@ -52,6 +52,7 @@ class FactorOptions:
     large_front_threshold: int = 2048  # B200 scheduling only; results do not depend on it
     precision: str = "fp64"  # "fp64" (plain) or "mixed" (TF32 tensor-core Schur updates; pair with solve_refine)
     mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
+    mixed_tile_cols: int = 256  # mixed form, mixed_flush 0: Schur GEMM output columns per CTA tile (128, 256)
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
@@ -61,7 +62,7 @@ class FactorOptions:
                                  fallback_bk=int(self.fallback_bunch_kaufman),
                                  large_front_threshold=self.large_front_threshold,
                                  precision={"fp64": 0, "mixed": 1}[self.precision],
-                                 mixed_flush=self.mixed_flush)
+                                 mixed_flush=self.mixed_flush, mixed_tile_cols=self.mixed_tile_cols)
 
 
 class SparseError(RuntimeError):

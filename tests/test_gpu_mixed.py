@@ -82,3 +82,44 @@ def test_refine_errors(rv):
         solver.factor(None, rv.FactorOptions(precision="fp64", threshold=2.0))
     with pytest.raises(rv.InvalidInput):
         solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=3))
+
+
+@pytest.mark.parametrize("case", ["kkt", "dense_plain", "dense_delay", "dense_nb64"])
+def test_pair_tiles_bit_identical(rv, case):
+    # the no-flush Schur GEMM over 256-column CTA tiles (two 128-column tiles
+    # sharing the W tile) gives the same factor, bit for bit, as 128-column tiles
+    import scipy.sparse as sp
+    opts = dict(precision="mixed", mixed_flush=0)
+    if case == "kkt":
+        s = rv.problems.kkt(14, seed=4)
+        opts.update(large_front_threshold=64)
+    else:
+        n = 1500 if case != "dense_nb64" else 900
+        rng = np.random.default_rng(len(case))
+        a = rng.standard_normal((n, n))
+        a = a + a.T
+        if case == "dense_delay":
+            a[np.arange(n), np.arange(n)] *= 1e-6
+        s = rv.problems.from_scipy(case, sp.csc_matrix(a))
+        opts.update(large_front_threshold=33, outer_block_size=64 if case == "dense_nb64" else 256)
+    b = rv.problems.rhs_normal(s.n, 6)
+    out = []
+    for cols in (128, 256):
+        solver = rv.SparseLDLT.analyze(s)
+        solver.factor(None, rv.FactorOptions(mixed_tile_cols=cols, **opts))
+        out.append((solver.pivot_record(), solver.inertia(), solver.solve(b)))
+        solver.close()
+    (c0, k0, d0, o0), i0, x0 = out[0]
+    (c1, k1, d1, o1), i1, x1 = out[1]
+    assert i0 == i1
+    assert np.array_equal(c0, c1) and np.array_equal(k0, k1)
+    assert np.array_equal(d0, d1) and np.array_equal(o0, o1), "D differs"
+    # the solve adds sibling contributions with atomics: equal to rounding
+    assert np.linalg.norm(x0 - x1) <= 1e-13 * np.linalg.norm(x0)
+
+
+def test_pair_tiles_option_checked(rv):
+    s = rv.problems.shifted_laplacian(4, 0.1)
+    solver = rv.SparseLDLT.analyze(s)
+    with pytest.raises(rv.InvalidInput):
+        solver.factor(None, rv.FactorOptions(precision="mixed", mixed_tile_cols=192))
