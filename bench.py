@@ -188,96 +188,114 @@ def gemm_peak_tflops(torch, dtype):
 def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local):
     """The many-systems workload: 64 systems (n log-uniform in [5e3, 2e5],
     half shifted Laplacians, half KKT, seed 1) with 1-32 right-hand sides each,
-    factored and solved as one block-diagonal union in plain FP64; a step is
-    the factorization of the batch plus the solve of all its right-hand sides.
-    Then refactorizations with every value scaled by 1 + 0.01 N(0,1)
-    (symmetric pairs alike), each followed by the solve."""
+    in plain FP64.  The systems form block-diagonal unions sized to the device
+    memory (BatchLDLT groups); a step factors and solves every group in turn,
+    releasing each group's device memory before the next.  Then
+    refactorizations with every value scaled by 1 + 0.01 N(0,1) (symmetric
+    pairs alike), each followed by the solve."""
     t0 = time.perf_counter()
     fam = rv.problems.batch_family(count=64, seed=1)
     systems, nrhs = [f[0] for f in fam], [f[1] for f in fam]
     bl = rv.BatchLDLT(systems)
     analyze_ms = (time.perf_counter() - t0) * 1e3
-    u = bl.union
-    flops = dense_flops(bl.solver.symbolic)
+    flops = sum(dense_flops(g.solver.symbolic) for g in bl.groups)
     rhs = [rv.problems.rhs_normal(sy.n, 100 + i, r) for i, (sy, r) in enumerate(zip(systems, nrhs))]
-    big = bl.rhs_matrix(rhs)
-    R = big.shape[1]
     opts = rv.FactorOptions(precision="fp64")
-    d_vals = torch.from_numpy(u.values).to("cuda")
-    d_scal = torch.from_numpy(bl.solver._scaling).to("cuda")
-    d_big = torch.from_numpy(np.ascontiguousarray(big.T)).to("cuda")  # R columns of length n, ld n
-    d_x = torch.empty_like(d_big)
+    vals = bl.values()
+    d_vals = torch.from_numpy(vals).to("cuda")
+    G = []  # per group: scaling, right-hand sides (R columns of length n_g), solution buffer, stream
+    for g in bl.groups:
+        big = bl.rhs_matrix(rhs, g.first, g.count)
+        g.solver._ensure_handle(opts)
+        g.solver.trim(workspace=True, factor=True)  # creation sized the arenas: give them back until its turn
+        g.solver.set_profiling(True)
+        G.append(dict(g=g, scal=torch.from_numpy(g.solver._scaling).to("cuda"), R=big.shape[1],
+                      rhs=torch.from_numpy(np.ascontiguousarray(big.T)).to("cuda"),
+                      x=torch.empty(big.shape[1], big.shape[0], dtype=torch.float64, device="cuda"),
+                      stream=torch.cuda.ExternalStream(g.solver.stream()), voff=int(bl.voffsets[g.first])))
+    multi = len(bl.groups) > 1
     # symmetric perturbation map on the device: entry -> its unordered pair
-    col = np.repeat(np.arange(u.n, dtype=np.int64), np.diff(u.colptr))
-    key = np.minimum(u.rowidx, col) * np.int64(u.n) + np.maximum(u.rowidx, col)
-    uniq, inv = np.unique(key, return_inverse=True)
-    d_inv = torch.from_numpy(inv.astype(np.int64)).to("cuda")
-    del col, key, inv
+    invs, base = [], 0
+    for g in bl.groups:
+        u = g.union
+        col = np.repeat(np.arange(u.n, dtype=np.int64), np.diff(u.colptr))
+        key = np.minimum(u.rowidx, col) * np.int64(u.n) + np.maximum(u.rowidx, col)
+        uq, inv = np.unique(key, return_inverse=True)
+        invs.append(inv.astype(np.int64) + base)
+        base += uq.size
+    d_inv = torch.from_numpy(np.concatenate(invs)).to("cuda")
+    del invs
     gen = torch.Generator(device="cuda")
     gen.manual_seed(7)
     d_pert = torch.empty_like(d_vals)
-    bl.solver._ensure_handle(opts)
-    bl.solver.set_profiling(True)
-    stream = torch.cuda.ExternalStream(bl.solver.stream())
 
-    def step(vals):
-        bl.solver.factor_device(vals.data_ptr(), d_scal.data_ptr(), opts)
-        with torch.cuda.stream(stream):  # the handle's stream orders the copy before the solve
-            d_x.copy_(d_big)
-        bl.solver.solve_device(d_x.data_ptr(), R, u.n)
+    def step(dv):
+        for e in G:
+            g = e["g"]
+            g.solver.factor_device(dv.data_ptr() + 8 * e["voff"], e["scal"].data_ptr(), opts)
+            with torch.cuda.stream(e["stream"]):  # the handle's stream orders the copy before the solve
+                e["x"].copy_(e["rhs"])
+            g.solver.solve_device(e["x"].data_ptr(), e["R"], g.union.n)
+            if multi:
+                g.solver.trim(workspace=True, factor=True)
 
-    def timed(vals):
+    def timed(dv):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            e0.record(stream)
-        step(vals)
-        with torch.cuda.stream(stream):
-            e1.record(stream)
+        with torch.cuda.stream(G[0]["stream"]):
+            e0.record(G[0]["stream"])
+        step(dv)
+        with torch.cuda.stream(G[-1]["stream"]):
+            e1.record(G[-1]["stream"])
         e1.synchronize()
         return e0.elapsed_time(e1) * 1e-3
+
+    def check(values):
+        errs = []
+        for e in G:
+            g = e["g"]
+            xg = e["x"].cpu().numpy().T
+            xs = bl.split(np.asfortranarray(xg), rhs, g.first, g.count)
+            for i in range(g.count):
+                sy = systems[g.first + i]
+                lo, hi = bl.voffsets[g.first + i], bl.voffsets[g.first + i + 1]
+                sv = rv.problems.System(name="v", n=sy.n, colptr=sy.colptr, rowidx=sy.rowidx, values=values[lo:hi])
+                bb = rhs[g.first + i]
+                bb = bb if bb.ndim == 2 else bb[:, None]
+                xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
+                errs.append(max(rv.problems.backward_error(sv, xx[:, j], bb[:, j]) for j in range(bb.shape[1])))
+        return max(errs)
 
     for _ in range(args.warmup):
         step(d_vals)
     barrier()
     clocks = ClockSampler()
     times = [timed(d_vals) for _ in range(args.steps)]
-    prof = bl.solver.profile()
-    x = d_x.cpu().numpy().T
-    xs = bl.split(np.asfortranarray(x), rhs)
-    errs = []
-    for i, sy in enumerate(systems):
-        bb = rhs[i] if rhs[i].ndim == 2 else rhs[i][:, None]
-        xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
-        errs.append(max(rv.problems.backward_error(sy, xx[:, j], bb[:, j]) for j in range(bb.shape[1])))
-    inert_ok = all(a == sy.inertia for a, sy in zip(bl.inertias(), systems))
+    launches = sum(e["g"].solver.profile()["factor_launches"] + e["g"].solver.profile()["solve_launches"] for e in G)
+    parts = {}
+    for e in G:
+        for k, v in e["g"].solver.profile()["part_ms"].items():
+            parts[k] = parts.get(k, 0.0) + v
+    peak = max(e["g"].solver.profile()["peak_bytes"] for e in G)
+    bwd = check(vals)
     nref = 20
     ref_times = []
     for r in range(nref):
-        f = 1.0 + 0.01 * torch.randn(uniq.size, dtype=torch.float64, device="cuda", generator=gen)
+        f = 1.0 + 0.01 * torch.randn(base, dtype=torch.float64, device="cuda", generator=gen)
         torch.mul(d_vals, f[d_inv], out=d_pert)
         del f
         torch.cuda.synchronize()
         ref_times.append(timed(d_pert))
     clk = clocks.stop(local)
-    vals_last = d_pert.cpu().numpy()
-    x = d_x.cpu().numpy().T
-    xs = bl.split(np.asfortranarray(x), rhs)
-    errs_ref = []
-    for i, sy in enumerate(systems):
-        lo, hi = u.colptr[bl.offsets[i]], u.colptr[bl.offsets[i + 1]]
-        sv = rv.problems.System(name="p", n=sy.n, colptr=sy.colptr, rowidx=sy.rowidx, values=vals_last[lo:hi])
-        bb = rhs[i] if rhs[i].ndim == 2 else rhs[i][:, None]
-        xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
-        errs_ref.append(max(rv.problems.backward_error(sv, xx[:, j], bb[:, j]) for j in range(bb.shape[1])))
-    # end to end through the public API with host buffers: BatchLDLT.factor + solve
+    bwd_ref = check(d_pert.cpu().numpy())
+    # end to end through the public API with host buffers: BatchLDLT.factor_solve
     e2e_t = []
     for _ in range(max(1, min(args.steps, 2))):
         barrier()
         t1 = time.perf_counter()
-        bl.factor(None, opts)
-        bl.solve(rhs)
+        bl.factor_solve(None, rhs, opts)
         torch.cuda.synchronize()
         e2e_t.append(time.perf_counter() - t1)
+    inert_ok = bl.inertias() == [sy.inertia for sy in systems]
     t_step = max_over_ranks(statistics.mean(times))
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -285,29 +303,31 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
         cb = batch_cpu_baseline(rv, orc, systems, flops)
     if rank == 0:
         ns = [sy.n for sy in systems]
+        h2d = int(vals.nbytes + sum(e["rhs"].numel() * 8 for e in G))
         line = {
             "metric": "batch factor+solve time (64 systems, 1-32 RHS each), plain FP64 on 1 B200",
             "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
-            "config": {"workload": CONFIGS["batch64"][2], "systems": len(systems), "n_total": int(u.n),
-                       "n_min": min(ns), "n_max": max(ns), "rhs_total": int(sum(nrhs)), "rhs_padded_to": R,
-                       "form": "plain FP64, one block-diagonal union, one handle and stream",
+            "config": {"workload": CONFIGS["batch64"][2], "systems": len(systems), "n_total": int(bl.n),
+                       "n_min": min(ns), "n_max": max(ns), "rhs_total": int(sum(nrhs)),
+                       "groups": [g.count for g in bl.groups],
+                       "device_budget_gb": bl.device_budget / 1e9,
+                       "form": "plain FP64; block-diagonal unions (one handle each) factored, solved and "
+                               "released in turn",
                        "scaling": "MC64 per system (host analysis incl. ordering %.0f ms)" % analyze_ms,
                        "l2": "working set far above L2 (126 MB); no flush needed",
                        "parallelism": f"replicas x{world}"},
-            "bwd_err_max": max(errs), "inertia_exact": inert_ok,
+            "bwd_err_max": bwd, "inertia_exact": inert_ok,
             "refactor": {"count": nref, "perturbation": "values x (1 + 0.01 N(0,1)), symmetric pairs alike",
                          "s_per_refactor_mean": statistics.mean(ref_times), "s_min": min(ref_times),
-                         "s_max": max(ref_times), "bwd_err_max_last": max(errs_ref)},
+                         "s_max": max(ref_times), "bwd_err_max_last": bwd_ref},
             "factor_flops": flops, "factor_gflops": flops / t_step / 1e9,
             "e2e": {"value": max_over_ranks(statistics.mean(e2e_t)), "unit": "s",
-                    "h2d_bytes_per_step": int(u.values.nbytes + big.nbytes), "d2h_bytes_per_step": int(big.nbytes)},
-            "gpu_launches": int(prof["factor_launches"] + prof["solve_launches"]),
-            "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
-                                               "host_total_ms", "host_sync_ms")},
-            "parts_ms": prof["part_ms"], "work": bl.solver.work(), "stats": bl.solver.stats(),
-            "step_event_s": times, "peak_device_bytes": prof["peak_bytes"], "clocks": clk, "cpu_baseline": cb,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(sum(e["rhs"].numel() * 8 for e in G))},
+            "gpu_launches": int(launches),
+            "parts_ms": parts, "step_event_s": times, "peak_device_bytes": peak, "clocks": clk,
+            "cpu_baseline": cb,
         }
         print(json.dumps(line), flush=True)
     bl.close()
@@ -363,7 +383,7 @@ def main():
         orc = entry.load_oracle()
         if args.config == "batch64":
             systems = [f[0] for f in rv.problems.batch_family(count=64, seed=1)]
-            full = dense_flops(rv.BatchLDLT(systems).solver.symbolic)
+            full = sum(dense_flops(rv.SparseLDLT.analyze(sy).symbolic) for sy in systems)
             sample = lambda: (batch_cpu_baseline(rv, orc, systems, full), None)
         else:
             s_full, _ = build_system(rv, args.config)

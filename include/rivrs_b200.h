@@ -236,6 +236,17 @@ rvg_status rvg_mc64(int64_t n, const int64_t* colptr, const int64_t* rowidx, con
  * reported (the handle stays usable).  which = 0: a solve block's flag wait
  * (1 s); which = 1: the mixed-form GEMM's pipeline wait (2 s). */
 rvg_status rvg_selftest_waits(rvg_handle* h, int32_t which);
+/* Device memory release (no reference counterpart; the Rust numeric object
+ * is dropped whole, solver.rs:312-315).  what: bit 0 = the workspace of
+ * factor and solve (contribution and scratch arenas, packed operands, solve
+ * vectors), bit 1 = the factor itself (the handle is then unfactored:
+ * RVG_ERR_SOLVE_BEFORE_FACTOR until the next rvg_factor).  The analysis, the
+ * assembly maps and the other pattern data stay on the device; the next
+ * rvg_factor allocates the arenas again at their delay-free size.  Lets many
+ * handles take turns on one device. */
+rvg_status rvg_trim(rvg_handle* h, int32_t what);
+/* Free and total bytes of the current device (cudaMemGetInfo). */
+rvg_status rvg_mem_info(int64_t out2[2]);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 rvg_status rvg_stream(rvg_handle* h, void** stream);
 void rvg_destroy(rvg_handle* h);

@@ -97,6 +97,8 @@ SIGNATURES = {
     "rvg_set_profiling": (C.c_int, [vp, C.c_int32]),
     "rvg_get_profile": (C.c_int, [vp, C.POINTER(Profile)]),
     "rvg_selftest_waits": (C.c_int, [vp, C.c_int32]),
+    "rvg_trim": (C.c_int, [vp, C.c_int32]),
+    "rvg_mem_info": (C.c_int, [i64p]),
     "rvg_mc64": (C.c_int, [i64, i64p, i64p, dp, i64p, dp, i64p]),
     "rvg_dense_factor_noalloc": (C.c_int, [vp, i64, i64, C.POINTER(Options), vp, vp, vp, vp, vp, vp]),
     "rvg_destroy": (None, [vp]),

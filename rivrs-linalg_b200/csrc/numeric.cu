@@ -885,9 +885,11 @@ struct rvg_handle {
   float* wpack = nullptr; size_t wpack_cap = 0;      // the same for a large front's window of pending columns
   int32_t* d_err = nullptr;                          // set by a device wait that timed out
   int32_t* sf_sync = nullptr; size_t sf_sync_cap = 0; // solve: ticket counter and block flags of one wave
+  double* sf_part = nullptr; size_t sf_part_cap = 0;   // backward solve: partial sums of one wave
   int nsm = 0;                                       // SMs of the device (persistent grids)
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
   bool factored = false;
+  bool need_presize = false;                         // arenas released by rvg_trim
   // measurement
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -1830,9 +1832,14 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
 }
 
 static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
+  int rc;
+  if (h->need_presize) {  // after rvg_trim: the arenas at their delay-free size again
+    if ((rc = presize_arenas(h))) return rc;
+    h->need_presize = false;
+  }
   // the refinement needs the unfactored values and ||A||_F
   if (dv != h->d_vals && h->nnz) CK(cudaMemcpyAsync(h->d_vals, dv, h->nnz * 8, cudaMemcpyDeviceToDevice, h->st));
-  int rc = run_factor(h, h->d_vals, ds);
+  rc = run_factor(h, h->d_vals, ds);
   if (rc) return rc;
   double* d_acc = nullptr;
   CK(cudaMallocAsync((void**)&d_acc, 8, h->st));
@@ -1909,17 +1916,22 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   std::vector<size_t> offf(nw), offb(nw);
   std::vector<int32_t> nfr(nw, 0), nbf(nw, 0), nbb(nw, 0);
   int32_t maxblk = 1;
+  int64_t maxslots = 1;
   for (size_t w = 0; w < nw; ++w) {
     std::vector<SfFront> vf, vb;
+    int32_t slots = 0;
     for (int64_t s : P.waves[w]) {
       const DFront& f = fr[s];
       if (f.ne == 0) continue;
       const int32_t nbd = (f.ne + SF_B - 1) / SF_B, nbr = (f.m - f.ne + SF_B - 1) / SF_B;
-      vf.push_back(SfFront{(int32_t)s, nbf[w], nbd, nbr});
-      vb.push_back(SfFront{(int32_t)s, nbb[w], nbd, nbr});
+      const int32_t ngrp = (nbr + SF_PG - 1) / SF_PG;
+      vf.push_back(SfFront{(int32_t)s, nbf[w], nbd, nbr, 0, 0});
+      vb.push_back(SfFront{(int32_t)s, nbb[w], nbd, nbr, ngrp, slots});
       nbf[w] += nbd + nbr;
-      nbb[w] += nbd + nbr;
+      nbb[w] += nbr + nbd * ngrp + nbd;  // gathers, partial sums, column blocks
+      slots += nbd * ngrp;
     }
+    maxslots = std::max<int64_t>(maxslots, slots);
     nfr[w] = (int32_t)vf.size();
     offf[w] = pk.add(vf);
     offb[w] = pk.add(vb);
@@ -1930,8 +1942,10 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
   std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
   CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
   if ((rc = ensure(h->sf_sync, h->sf_sync_cap, (size_t)maxblk + 1, st))) return rc;
+  if ((rc = ensure_nocopy(h->sf_part, h->sf_part_cap, (size_t)maxslots * 8 * SF_B, st))) return rc;
   auto wave = [&](size_t w, bool fwd, int64_t rh) {
     SfWave sw;
+    sw.part = h->sf_part;
     sw.fr = (const SfFront*)(h->d_stage + (fwd ? offf[w] : offb[w]));
     sw.nfr = nfr[w];
     sw.nblk = fwd ? nbf[w] : nbb[w];
@@ -2260,6 +2274,58 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
   return RVG_OK;
 }
 
+static int trim_buf(void* p, cudaStream_t st) {
+  if (p) CK(cudaFreeAsync(p, st));
+  return RVG_OK;
+}
+
+rvg_status rvg_trim(rvg_handle* h, int32_t what) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (what & ~3) { set_error("what: bit 0 = workspace, bit 1 = factor"); return RVG_ERR_INVALID_INPUT; }
+  CK(cudaSetDevice(h->device));
+  cudaStream_t st = h->st;
+  int rc;
+#define RVG_TRIM(p, cap)                              \
+  do {                                                \
+    if ((rc = trim_buf(p, st))) return (rvg_status)rc; \
+    p = nullptr;                                      \
+    cap = 0;                                          \
+  } while (0)
+  if (what & 1) {
+    RVG_TRIM(h->scratch, h->scratch_cap);
+    RVG_TRIM(h->cb_arena, h->cb_cap);
+    RVG_TRIM(h->pack, h->pack_cap);
+    RVG_TRIM(h->wpack, h->wpack_cap);
+    RVG_TRIM(h->solve_work, h->solve_work_cap);
+    RVG_TRIM(h->sf_part, h->sf_part_cap);
+    RVG_TRIM(h->d_x, h->x_cap);
+    RVG_TRIM(h->d_ref, h->ref_cap);
+    RVG_TRIM(h->d_stage, h->stage_cap);
+    h->cb_free.clear();
+  }
+  if (what & 2) {
+    RVG_TRIM(h->panel, h->panel_cap);
+    RVG_TRIM(h->idx, h->idx_cap);
+    if ((rc = trim_buf(h->dtype, st)) || (rc = trim_buf(h->ddiag, st)) || (rc = trim_buf(h->doff, st)))
+      return (rvg_status)rc;
+    h->dtype = nullptr; h->ddiag = nullptr; h->doff = nullptr; h->d_cap = 0;
+    h->factored = false;
+  }
+#undef RVG_TRIM
+  if (what) h->need_presize = true;
+  CK(cudaStreamSynchronize(st));  // the memory is back in the pool when this returns
+  return RVG_OK;
+}
+
+rvg_status rvg_mem_info(int64_t out2[2]) {
+  if (!out2) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  size_t f = 0, t = 0;
+  CK(cudaMemGetInfo(&f, &t));
+  out2[0] = (int64_t)f;
+  out2[1] = (int64_t)t;
+  return RVG_OK;
+}
+
 rvg_status rvg_stream(rvg_handle* h, void** s) {
   if (!h || !s) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
   *s = (void*)h->st;
@@ -2274,7 +2340,7 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part);
   fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }

@@ -18,14 +18,19 @@
 //     warp; publish y_r, raise flag r;
 //   L21 block (rows >= ne): -sum over all column blocks of L[rows, b] y_b,
 //     added atomically into x at the parent's rows (siblings share rows).
-// backward, per front (first the gather tickets: the parent's final values at
-// the L21 rows into v + m at rows >= ne; then descending column blocks;
-// x_final in v + m):
-//   z = D^-1 y on the block's columns (2x2 pairs may straddle blocks: y is
-//   still intact in v), minus L21^T x[row] (parent's final values), minus
-//   L[rows of later blocks, cols]^T x_final of those blocks (each once its
-//   flag is up), then the unit upper solve (L11^T) of the diagonal block by
-//   one warp; x[col] = x_final; raise the flag.
+// backward, per front, in ticket order:
+//   gather tickets: the parent's final values at 64 rows of L21 into v + m
+//     (rows >= ne);
+//   partial-sum tickets: for a column block and a group of up to 8 L21 row
+//     blocks, the sums L[rows, cols]^T x[rows] over the group, into a slot of
+//     the wave's partial-sum buffer (the L21 reduction of one column block is
+//     spread over CTAs, as the forward pass spreads its rows);
+//   column blocks, descending (x_final in v + m): z = D^-1 y on the block's
+//     columns (2x2 pairs may straddle blocks: y is still intact in v), minus
+//     the block's partial sums in group order, minus L[rows of later blocks,
+//     cols]^T x_final of those blocks (each once its flag is up), then the
+//     unit upper solve (L11^T) of the diagonal block by one warp;
+//     x[col] = x_final; raise the flag.
 // Per row (forward) and per column (backward) the sums run in ascending
 // column / row order inside each 64-block.  Up to 8 right-hand sides go
 // through one launch (template R), each L value read once for all of them.
@@ -41,15 +46,20 @@ constexpr int SF_B = 64;                            // block rows / columns
 constexpr uint64_t SF_TIMEOUT_NS = 1000000000ull;   // 1 s per wait
 
 // one front of a wave: its first ticket and its block counts
+constexpr int SF_PG = 8;  // backward: L21 row blocks per partial-sum ticket (512 rows)
+
 struct SfFront {
-  int32_t s;     // supernode
-  int32_t blk0;  // first ticket of the front
-  int32_t nbd;   // diagonal blocks (ceil(ne / 64))
-  int32_t nbr;   // L21 blocks (ceil((m - ne) / 64)): forward row blocks, backward gather tickets
+  int32_t s;      // supernode
+  int32_t blk0;   // first ticket of the front
+  int32_t nbd;    // diagonal blocks (ceil(ne / 64))
+  int32_t nbr;    // L21 blocks (ceil((m - ne) / 64)): forward row blocks, backward gather tickets
+  int32_t ngrp;   // backward: partial-sum tickets per column block (ceil(nbr / SF_PG))
+  int32_t pslot;  // backward: the front's first partial-sum slot (R x 64 values each)
 };
 
 struct SfWave {
   const SfFront* fr;
+  double* part;     // backward partial sums: slot q at part + q R 64
   int32_t nfr, nblk;
   int32_t* ticket;  // zeroed before the launch
   int32_t* flags;   // nblk entries, zeroed before the launch
@@ -247,10 +257,12 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
     const double* y = w.work + fr.scratch;      // forward results of right-hand side r at y + r m
     double* xf = w.work + fr.scratch + R * m;   // final values of this front's columns, at xf + r m
     int32_t* flags = w.flags + sf.blk0;
-    const int nbr = sf.nbr;
-    if (blk - sf.blk0 < nbr) {
+    const int nbr = sf.nbr, ngrp = sf.ngrp;
+    const int lt = blk - sf.blk0;  // ticket within the front
+    const int npart = sf.nbd * ngrp;
+    if (lt < nbr) {
       // gather ticket: the parent's final values at 64 rows of L21 into xf
-      const int64_t i = ne + (int64_t)(blk - sf.blk0) * SF_B + t;
+      const int64_t i = ne + (int64_t)lt * SF_B + t;
       if (i < m) {
         const int32_t g = sf_row(rows, perm, ne, fr.k, i - ne);
 #pragma unroll
@@ -258,37 +270,73 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
       }
       __threadfence();
       __syncthreads();
-      if (t == 0) sf_st_release(&flags[blk - sf.blk0], 1);
+      if (t == 0) sf_st_release(&flags[lt], 1);
       continue;
     }
-    const int b = sf.nbd - 1 - (blk - sf.blk0 - nbr);  // descending
+    if (lt < nbr + npart) {
+      // partial-sum ticket (column blocks descending, groups ascending)
+      const int pq = lt - nbr;
+      const int b = sf.nbd - 1 - pq / ngrp, gi = pq % ngrp;
+      const int64_t c0 = (int64_t)b * SF_B;
+      const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
+      double ps[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) ps[r] = 0.0;
+      const int rb1 = (gi + 1) * SF_PG < nbr ? (gi + 1) * SF_PG : nbr;
+      for (int rb = gi * SF_PG; rb < rb1; ++rb) {
+        if (t == 0) sf_wait(&flags[rb], w.err);
+        const int64_t i0 = ne + (int64_t)rb * SF_B;
+        const int nr = (int)((i0 + SF_B < m ? i0 + SF_B : m) - i0);
+        __syncthreads();
+        if (t < nr) {
+#pragma unroll
+          for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i0 + t]);
+          sf_load_strip(L + i0 + t + c0 * m, m, nc, &Ls[t][0]);
+        }
+        __syncthreads();
+        if (t < nc)
+          for (int rr = 0; rr < nr; ++rr) {
+            const double l = Ls[rr][t];
+#pragma unroll
+            for (int r = 0; r < R; ++r) ps[r] = __fma_rn(l, xs[r][rr], ps[r]);
+          }
+      }
+      double* slot = w.part + ((int64_t)sf.pslot + pq) * R * SF_B;
+#pragma unroll
+      for (int r = 0; r < R; ++r) slot[r * SF_B + t] = ps[r];
+      __threadfence();
+      __syncthreads();
+      if (t == 0) sf_st_release(&flags[lt], 1);
+      continue;
+    }
+    const int q = lt - nbr - npart;  // column blocks, descending
+    const int b = sf.nbd - 1 - q;
     const int64_t c0 = (int64_t)b * SF_B;
     const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
     const bool col = t < nc;
     double acc[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r] = col ? sf_dinv(fr, A, y + r * m, c0 + t) : 0.0;
-    // rows of later blocks: L21 (the parent's final values, gathered into xf
-    // by the front's first tickets), then later diagonal blocks as they finish
-    for (int rb = -nbr; rb < sf.nbd - 1 - b; ++rb) {
-      int64_t i0;
-      const bool l21 = rb < 0;
-      if (l21) {
-        if (t == 0) sf_wait(&flags[nbr + rb], w.err);
-        i0 = ne + (int64_t)(nbr + rb) * SF_B;
-      } else {
-        const int rblk = sf.nbd - 1 - rb;  // later diagonal blocks, from the last one down
-        if (t == 0) sf_wait(&flags[nbr + sf.nbd - 1 - rblk], w.err);
-        i0 = (int64_t)rblk * SF_B;
-      }
-      const int64_t iend = l21 ? m : ne;
-      const int nr = (int)((i0 + SF_B < iend ? i0 + SF_B : iend) - i0);
+    // the block's L21 partial sums, in group order
+    for (int gi = 0; gi < ngrp; ++gi) {
+      const int pq = q * ngrp + gi;
+      if (t == 0) sf_wait(&flags[nbr + pq], w.err);
+      __syncthreads();
+      const double* slot = w.part + ((int64_t)sf.pslot + pq) * R * SF_B;
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] = __dsub_rn(acc[r], __ldcg(&slot[r * SF_B + t]));
+    }
+    // rows of later diagonal blocks, from the last one down, as they finish
+    const int cb0 = nbr + npart;  // flag of column block q' at flags[cb0 + q']
+    for (int rblk = sf.nbd - 1; rblk > b; --rblk) {
+      if (t == 0) sf_wait(&flags[cb0 + (sf.nbd - 1 - rblk)], w.err);
+      const int64_t i0 = (int64_t)rblk * SF_B;
+      const int nr = (int)((i0 + SF_B < ne ? i0 + SF_B : ne) - i0);
       __syncthreads();
       if (t < nr) {
-        const int64_t i = i0 + t;
 #pragma unroll
-        for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i]);
-        sf_load_strip(L + i + c0 * m, m, nc, &Ls[t][0]);
+        for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i0 + t]);
+        sf_load_strip(L + i0 + t + c0 * m, m, nc, &Ls[t][0]);
       }
       __syncthreads();
       if (col)

@@ -302,6 +302,15 @@ class SparseLDLT:
         _check(N.lib().rvg_timings(self._handle, N.ptr(out, N.dp)))
         return dict(assembly_ms=out[0], kernel_ms=out[1], gemm_ms=out[2], factor_ms=out[3], solve_ms=out[4])
 
+    def trim(self, workspace: bool = True, factor: bool = False):
+        """Release device memory: the factor/solve workspace and, with
+        factor=True, the factor too (solve then needs a new factor())."""
+        if self._handle is None:
+            return
+        _check(N.lib().rvg_trim(self._handle, (1 if workspace else 0) | (2 if factor else 0)))
+        if factor:
+            self._factored = False
+
     def set_profiling(self, enable: bool = True):
         if self._handle is None:
             self._ensure_handle(self._opts or FactorOptions())

@@ -38,23 +38,25 @@ def test_block_diagonal_union(rv):
 
 def test_union_analysis_is_the_systems_side_by_side(rv):
     systems, _ = small_family(rv)
-    bl = rv.BatchLDLT(systems, scaling=False)
+    bl = rv.BatchLDLT(systems, scaling=False, device_budget=0)
+    assert len(bl.groups) == 1
     offs = bl.offsets
-    perm = bl.solver.symbolic.perm_fwd
+    perm = bl.groups[0].solver.symbolic.perm_fwd
     # each system's indices stay contiguous in elimination order
     sysid = np.searchsorted(offs, perm, side="right") - 1
     assert np.all(np.diff(sysid) >= 0)
     nsup = 0
     for s in systems:
         nsup += rv.SparseLDLT.analyze(s).symbolic.sup_begin.size
-    assert bl.solver.symbolic.sup_begin.size == nsup
+    assert bl.groups[0].solver.symbolic.sup_begin.size == nsup
 
 
 def test_union_scaling_is_per_system_mc64(rv):
     systems, _ = small_family(rv)
-    bl = rv.BatchLDLT(systems)
+    bl = rv.BatchLDLT(systems, device_budget=0)
+    g = bl.groups[0]
     sc = np.empty(bl.n)
-    sc[bl.solver.symbolic.perm_fwd] = bl.solver._scaling
+    sc[g.solver.symbolic.perm_fwd] = g.solver._scaling
     for i, s in enumerate(systems):
         _, si, _ = rv.ordering.mc64(s)
         assert np.allclose(sc[bl.offsets[i]:bl.offsets[i + 1]], si, rtol=1e-12, atol=0)
@@ -62,7 +64,7 @@ def test_union_scaling_is_per_system_mc64(rv):
 
 def test_rhs_packing(rv):
     systems, nrhs = small_family(rv)
-    bl = rv.BatchLDLT(systems, scaling=False)
+    bl = rv.BatchLDLT(systems, scaling=False, device_budget=0)
     rhs = [rv.problems.rhs_normal(s.n, i, r) for i, (s, r) in enumerate(zip(systems, nrhs))]
     big = bl.rhs_matrix(rhs)
     assert big.shape == (bl.n, max(nrhs))
@@ -80,4 +82,36 @@ def test_perturbation_keeps_symmetry(rv):
     assert np.max(np.abs(d)) == 0.0
     assert not np.array_equal(v, s.values)
     with pytest.raises(rv.InvalidInput):
-        rv.BatchLDLT(systems=[], scaling=False)
+        rv.BatchLDLT(systems=[], scaling=False, device_budget=0)
+
+
+def test_groups_follow_the_memory_budget(rv):
+    systems, nrhs = small_family(rv)
+    est = [sum(rv.batch.memory_estimate(rv.SparseLDLT.analyze(s).symbolic)) for s in systems]
+    budget = int(1.1 * (max(est) + sorted(est)[-2]) + 1)
+    bl = rv.BatchLDLT(systems, scaling=False, device_budget=budget)
+    assert len(bl.groups) > 1
+    assert sum(g.count for g in bl.groups) == len(systems)
+    nxt = 0
+    for g in bl.groups:
+        assert g.first == nxt
+        nxt += g.count
+        assert 1.1 * sum(est[g.first:g.first + g.count]) <= budget or g.count == 1
+        assert g.union.n == sum(s.n for s in systems[g.first:g.first + g.count])
+    # a group's right-hand sides and values are its systems' slices
+    rhs = [rv.problems.rhs_normal(s.n, i, r) for i, (s, r) in enumerate(zip(systems, nrhs))]
+    vals = bl.values()
+    for g in bl.groups:
+        assert np.array_equal(bl.group_values(g, vals), g.union.values)
+        big = bl.rhs_matrix(rhs, g.first, g.count)
+        back = bl.split(big, rhs, g.first, g.count)
+        for a, b in zip(back, rhs[g.first:g.first + g.count]):
+            assert np.array_equal(a, b)
+
+
+def test_memory_estimate_bounds_the_factor(rv):
+    s = rv.problems.kkt(10, seed=1)
+    sym = rv.SparseLDLT.analyze(s).symbolic
+    f, w = rv.batch.memory_estimate(sym)
+    assert f >= 8 * sym.predicted_nnz
+    assert w > 0

@@ -13,17 +13,13 @@ def family(rv, count=6, seed=3):
     return [s for s, _ in fam], [r for _, r in fam]
 
 
-def per_system_record(bl, i):
-    col, code, dd, do = bl.solver.pivot_record()
-    sel = bl._sys_of_pos[col] == i
-    return col[sel] - col[sel].min(), code[sel], dd[sel], do[sel]
-
-
 def separate(rv, bl, i, values, opts):
     s = bl.systems[i]
-    sc = np.empty(bl.n)
-    sc[bl.solver.symbolic.perm_fwd] = bl.solver._scaling
-    solver = rv.SparseLDLT.analyze_with_matrix(s, scaling=sc[bl.offsets[i]:bl.offsets[i + 1]])
+    g = next(g for g in bl.groups if g.first <= i < g.first + g.count)
+    sc = np.empty(g.union.n)
+    sc[g.solver.symbolic.perm_fwd] = g.solver._scaling
+    lo = bl.offsets[i] - bl.offsets[g.first]
+    solver = rv.SparseLDLT.analyze_with_matrix(s, scaling=sc[lo:lo + s.n])
     solver.factor(values, opts)
     return solver
 
@@ -32,7 +28,7 @@ def separate(rv, bl, i, values, opts):
 def test_union_matches_separate_factorizations(rv, precision):
     systems, nrhs = family(rv)
     opts = rv.FactorOptions(precision=precision, mixed_flush=0, large_front_threshold=256)
-    bl = rv.BatchLDLT(systems)
+    bl = rv.BatchLDLT(systems, device_budget=0)
     for rnd in range(2):  # factor, then a refactorization with perturbed values
         vals = [None if rnd == 0 else rv.problems.perturb_symmetric(s, 0.01, seed=10 + i)
                 for i, s in enumerate(systems)]
@@ -44,7 +40,7 @@ def test_union_matches_separate_factorizations(rv, precision):
             if rnd == 0:
                 assert inert[i] == s.inertia
             one = separate(rv, bl, i, vals[i], opts)
-            c0, k0, d0, o0 = per_system_record(bl, i)
+            c0, k0, d0, o0 = bl.system_record(i)
             c1, k1, d1, o1 = one.pivot_record()
             assert np.array_equal(c0, c1 - c1.min()) and np.array_equal(k0, k1)
             assert np.array_equal(d0, d1) and np.array_equal(o0, o1), ("D differs", i)
@@ -67,10 +63,48 @@ def test_union_matches_separate_factorizations(rv, precision):
 
 def test_union_refined_solve(rv):
     systems, _ = family(rv, count=4, seed=5)
-    bl = rv.BatchLDLT(systems)
+    bl = rv.BatchLDLT(systems, device_budget=0)
     bl.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=0, large_front_threshold=256))
+    g = bl.groups[0]
     b = rv.problems.rhs_normal(bl.n, 1)
-    x, iters, err = bl.solver.solve_refine(b, tol=1e-14, max_iter=10)
+    x, iters, err = g.solver.solve_refine(b, tol=1e-14, max_iter=10)
     assert err <= 1e-14
-    assert bl.solver.inertia() == bl.union.inertia
+    assert g.solver.inertia() == g.union.inertia
     bl.close()
+
+
+def test_groups_and_trim_match_one_union(rv):
+    # a budget that forces several groups: factor_solve (each group factored,
+    # solved and released in turn) gives every system the same D and solution
+    # as one union holding all of them; a second round reuses the trimmed handles
+    systems, nrhs = family(rv, count=6, seed=7)
+    opts = rv.FactorOptions(precision="fp64", large_front_threshold=256)
+    one = rv.BatchLDLT(systems, device_budget=0)
+    est = [sum(rv.batch.memory_estimate(rv.SparseLDLT.analyze(s).symbolic)) for s in systems]
+    many = rv.BatchLDLT(systems, device_budget=int(1.1 * 2 * max(est)) + 1)
+    assert len(many.groups) > 1
+    rhs = [rv.problems.rhs_normal(s.n, i, r) for i, (s, r) in enumerate(zip(systems, nrhs))]
+    one.factor(None, opts)
+    x1 = one.solve(rhs)
+    for rnd in range(2):
+        xs = many.factor_solve(None, rhs, opts)
+        assert many.inertias() == one.inertias() == [s.inertia for s in systems]
+        for a, b in zip(xs, x1):
+            assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b)
+    # factor + solve with every group's factor kept (workspace trimmed between groups)
+    many.factor(None, opts)
+    for i in range(len(systems)):
+        c0, k0, d0, o0 = one.system_record(i)
+        c1, k1, d1, o1 = many.system_record(i)
+        assert np.array_equal(c0, c1) and np.array_equal(k0, k1)
+        assert np.array_equal(d0, d1) and np.array_equal(o0, o1)
+    xs = many.solve(rhs)
+    for a, b in zip(xs, x1):
+        assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(b)
+    # the trimmed handle refuses to solve until it is factored again
+    g = many.groups[0]
+    g.solver.trim(workspace=True, factor=True)
+    with pytest.raises(rv.SolveBeforeFactor):
+        g.solver.solve(np.zeros(g.union.n))
+    one.close()
+    many.close()
