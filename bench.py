@@ -366,6 +366,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-flush", default="4,0",
                     help="comma list of mixed-form flush depths to time (32-deep K chunks per FP32 partial sum; 0 = all K)")
+    ap.add_argument("--bf16-flush", default="0",
+                    help="the same for the mixed form with BF16 operand parts")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -441,22 +443,25 @@ def main():
     d_b = torch.from_numpy(b).to("cuda")
     d_x = torch.empty_like(d_b)
 
-    def run_form(precision, flush=4):
-        """W warm-up + K timed steps of one form: factor + (refined) solve, inputs in HBM."""
-        opts = rv.FactorOptions(precision=precision, mixed_flush=flush)
+    def run_form(precision, flush=4, ops="tf32", method="ir"):
+        """W warm-up + K timed steps of one form: factor + (refined) solve, inputs in HBM.
+        method: "ir" (iterative refinement) or "gmres" (GMRES-IR) back to FP64 accuracy."""
+        opts = rv.FactorOptions(precision=precision, mixed_flush=flush, mixed_operands=ops)
         solver._ensure_handle(opts)
-        solver.set_profiling(True)
+        solver.set_profiling(False)  # timed steps without the per-launch events
         stream = torch.cuda.ExternalStream(solver.stream())
 
         def step():
             solver.factor_device(d_vals.data_ptr(), d_scal.data_ptr() if d_scal is not None else None, opts)
+            if method == "gmres":
+                return solver.solve_gmres_device(d_b.data_ptr(), d_x.data_ptr(), tol=1e-14, max_iter=100, restart=30)
             return solver.solve_refine_device(d_b.data_ptr(), d_x.data_ptr(), tol=1e-14, max_iter=10)
 
         for _ in range(args.warmup):
             step()
         barrier()
         clocks = ClockSampler()
-        times, walls, syrk_ms, syrk_flops, syrk_launch, launches, its = [], [], 0.0, 0.0, 0, 0, []
+        times, walls, launches, its = [], [], 0, []
         for _ in range(args.steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             with torch.cuda.stream(stream):
@@ -469,23 +474,28 @@ def main():
             e1.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
             pr = solver.profile()
-            syrk_ms += pr["syrk_ms"]
-            syrk_flops += pr["syrk_flops"]
-            syrk_launch += pr["syrk_launches"]
             launches += pr["factor_launches"] + pr["solve_launches"] * (1 + it)
             its.append(it)
         barrier()
         clk = clocks.stop(local)
+        # one more step with the per-launch events on: where the time goes, the Schur GEMM's rate
+        solver.set_profiling(True)
+        step()
+        pr = solver.profile()
+        solver.set_profiling(False)
+        syrk_ms, syrk_flops, syrk_launch = pr["syrk_ms"], pr["syrk_flops"], pr["syrk_launches"]
         x = d_x.cpu().numpy()
         return dict(t=max_over_ranks(statistics.mean(times)), times=times, walls=walls, clk=clk,
                     bwd=rv.problems.backward_error(s, x, b), inertia=solver.inertia(), stats=solver.stats(),
                     prof=solver.profile(), syrk_ms=syrk_ms, syrk_flops=syrk_flops, syrk_launch=syrk_launch,
-                    launches=launches, refine_iters=its, opts=opts)
+                    launches=launches, refine_iters=its, opts=opts, method=method)
 
     plain = run_form("fp64")
     forms = {"plain_fp64": plain}
     for fl in [int(v) for v in args.mixed_flush.split(",") if v.strip()]:
         forms[f"mixed_flush{fl}"] = run_form("mixed", fl)
+    for fl in [int(v) for v in args.bf16_flush.split(",") if v.strip()]:
+        forms[f"mixed_bf16_flush{fl}_gmres"] = run_form("mixed", fl, "bf16", "gmres")
     # the chosen form: the fastest that reaches the accuracy target (plain always does)
     chosen_key = min((k for k, f in forms.items() if f["bwd"] <= 1e-14 or k == "plain_fp64"),
                      key=lambda k: forms[k]["t"])
@@ -507,7 +517,10 @@ def main():
         barrier()
         t0 = time.perf_counter()
         solver.factor(s.values, opts)
-        xh, _, _ = solver.solve_refine(b, tol=1e-14, max_iter=10)
+        if chosen["method"] == "gmres":
+            xh, _, _ = solver.solve_gmres(b, tol=1e-14, max_iter=100, restart=30)
+        else:
+            xh, _, _ = solver.solve_refine(b, tol=1e-14, max_iter=10)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
     e2e = max_over_ranks(statistics.mean(e2e_times))
@@ -532,14 +545,40 @@ def main():
              "one_at_a_time_ms": timed(lambda: [solver.solve_device(rhs8[r].data_ptr(), 1, s.n) for r in range(8)])}
 
     work = solver.work()
+    # the HBM-bound parts against the measured copy bandwidth: one solve (multi_rhs_solve's single-RHS
+    # calls; the solve reads the factor once per RHS) and the assembly of the chosen form's profiled step
+    hbm = None
+    mp = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    if os.path.exists(mp):
+        hbm = json.load(open(mp)).get("hbm_gbs")
+    t_solve1 = multi["one_at_a_time_ms"] / 8 * 1e-3
+    solve_gbs = work["bytes_solve_per_rhs"] / t_solve1 / 1e9
+    asm_gbs = work["bytes_assembly"] / (prof["assembly_ms"] * 1e-3) / 1e9 if prof["assembly_ms"] > 0 else None
+    hbm_parts = {"peak_gbs": hbm, "peak_source": "measured-peaks file (copy)" if hbm else None,
+                 "solve": {"bytes_per_rhs": work["bytes_solve_per_rhs"], "ms_per_rhs": t_solve1 * 1e3,
+                           "gbs": solve_gbs, "frac": solve_gbs / hbm if hbm else None},
+                 "assembly": {"bytes": work["bytes_assembly"], "ms": prof["assembly_ms"], "gbs": asm_gbs,
+                              "frac": asm_gbs / hbm if (hbm and asm_gbs) else None}}
     dpeak = gemm_peak_tflops(torch, torch.float64)
     tpeak = gemm_peak_tflops(torch, torch.float32)
     if chosen_name == "mixed":
         # TF32 tensor flops the kernel executes: three products per FP64-equivalent term
         syrk_ms, syrk_flops, syrk_launch = chosen["syrk_ms"], 3.0 * chosen["syrk_flops"], chosen["syrk_launch"]
         peak = tpeak
-        rl_kernel = "k_syrk_tc (mixed-form Schur GEMM: tcgen05 kind::tf32, operands split hi+lo, 3 products per term)"
-        rl_source = "cuBLAS TF32 GEMM 8192^3 (FP32 inputs, TF32 tensor math) measured in this run"
+        if chosen["opts"].mixed_operands == "bf16":
+            mp = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+            if os.path.exists(mp):
+                peak = json.load(open(mp))["bf16_tflops_sustained"]
+                rl_source = "measured-peaks file: cuBLAS bf16 GEMM, sustained (the kernel runs inside a long step)"
+            else:
+                peak = gemm_peak_tflops(torch, torch.bfloat16)
+                rl_source = "cuBLAS BF16 GEMM 8192^3 measured in this run"
+            rl_kernel = ("k_syrk_tc%s (mixed-form Schur GEMM: tcgen05 kind::f16, operands split into BF16 hi+lo, "
+                         "3 products per term)" % ("_pair" if chosen["opts"].mixed_flush == 0 else ""))
+        else:
+            rl_kernel = ("k_syrk_tc%s (mixed-form Schur GEMM: tcgen05 kind::tf32, operands split hi+lo, 3 products "
+                         "per term)" % ("_pair" if chosen["opts"].mixed_flush == 0 else ""))
+            rl_source = "cuBLAS TF32 GEMM 8192^3 (FP32 inputs, TF32 tensor math) measured in this run"
     else:
         peak = dpeak
         rl_kernel = "k_syrk_dmma (FP64 Schur-complement GEMM, plain form)"
@@ -566,16 +605,19 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "bwd_err": bwd, "bwd_err_e2e": bwd_e2e, "inertia": list(inertia), "inertia_expected": list(s.inertia),
             "forms": {k: {"s_per_step": f["t"], "bwd_err": f["bwd"], "refine_corrections": f["refine_iters"],
+                          "accuracy_method": "GMRES-IR (FP64 FGMRES, factor as preconditioner)"
+                          if f["method"] == "gmres" else "iterative refinement",
                           "inertia": list(f["inertia"]),
                           "syrk_tflops_fp64_equiv": (f["syrk_flops"] / (f["syrk_ms"] * 1e-3) / 1e12)
                           if f["syrk_ms"] > 0 else None,
-                          "syrk_share": (f["syrk_ms"] / args.steps * 1e-3) / f["t"] if f["t"] else None}
+                          "syrk_share": (f["syrk_ms"] * 1e-3) / f["t"] if f["t"] else None}
                       for k, f in forms.items()},
             "chosen_form": chosen_key,
             "speedup_vs_plain_fp64": plain["t"] / t_step,
             "stats": stats, "factor_flops": full_flops,
             "factor_gflops": full_flops / t_step / 1e9,
             "multi_rhs_solve": multi,
+            "hbm_bound_parts": hbm_parts,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(s.values.nbytes + b.nbytes),
                     "d2h_bytes_per_step": int(b.nbytes)},
             "gpu_launches": int(launches // max(args.steps, 1)),
@@ -583,8 +625,8 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
                          "peak_source": rl_source, "dgemm_peak": dpeak, "tf32_gemm_peak": tpeak,
-                         "launches_per_step": syrk_launch // max(args.steps, 1),
-                         "share_of_step": (syrk_ms / args.steps * 1e-3) / t_step if t_step else None},
+                         "launches_per_step": syrk_launch,
+                         "share_of_step": (syrk_ms * 1e-3) / t_step if t_step else None},
             "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
                                                "host_total_ms", "host_alloc_ms", "host_sync_ms")},
             "parts_ms": prof["part_ms"],

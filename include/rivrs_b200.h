@@ -72,7 +72,11 @@ typedef struct {
    * W tile in shared memory: a quarter fewer operand bytes per flop).  Results
    * do not depend on it.  Default 256. */
   int32_t mixed_tile_cols;
-  int32_t reserved;
+  /* Mixed form: the parts each FP64 operand is split into, 0 = two TF32 parts
+   * (kind::tf32, about 22 significant bits per product), 1 = two BF16 parts
+   * (kind::f16, about 16 bits: half the operand bytes and twice the tensor
+   * rate, so more refinement steps).  Default 0. */
+  int32_t mixed_operands;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */
@@ -151,6 +155,25 @@ rvg_status rvg_solve_refine(rvg_handle* h, const double* rhs, double* x, double 
                             int32_t* iters, double* bwd_err);
 rvg_status rvg_solve_refine_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
                                    int32_t* iters, double* bwd_err);
+/* The same for nrhs right-hand sides (columns at stride ldb >= n), host
+ * (rvg_solve_refine_nrhs) or device (_device) arrays: every solve is blocked
+ * over the columns, corrections continue until every column's scaled
+ * backward error is <= tol; bwd_err receives nrhs values, *iters the
+ * corrections made (the same for all columns). */
+/* GMRES-IR (no reference counterpart; the mixed form's way back to full
+ * accuracy where plain refinement stalls, e.g. BF16 operand parts on an
+ * ill-conditioned matrix): restarted flexible GMRES in FP64 on A x = b with
+ * the factor as right preconditioner, `restart` basis vectors (1..200), until
+ * the scaled backward error (as rvg_solve_refine) is <= tol or after
+ * `max_iter` preconditioned products (one solve each, reported in *iters). */
+rvg_status rvg_solve_gmres(rvg_handle* h, const double* rhs, double* x, double tol, int32_t max_iter,
+                           int32_t restart, int32_t* iters, double* bwd_err);
+rvg_status rvg_solve_gmres_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
+                                  int32_t restart, int32_t* iters, double* bwd_err);
+rvg_status rvg_solve_refine_nrhs(rvg_handle* h, const double* rhs, double* x, int64_t nrhs, int64_t ldb, double tol,
+                                 int32_t max_iter, int32_t* iters, double* bwd_err);
+rvg_status rvg_solve_refine_nrhs_device(rvg_handle* h, const double* d_rhs, double* d_x, int64_t nrhs, int64_t ldb,
+                                        double tol, int32_t max_iter, int32_t* iters, double* bwd_err);
 
 /* SparseLDLT::inertia (solver.rs:504-519): [positive, negative, zero]. */
 rvg_status rvg_inertia(rvg_handle* h, int64_t out3[3]);

@@ -30,7 +30,7 @@ class Options(C.Structure):
                 ("inner_block_size", i64), ("nemin", i64), ("small_leaf_threshold", i64),
                 ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64),
                 ("precision", C.c_int32), ("mixed_flush", C.c_int32),
-                ("mixed_tile_cols", C.c_int32), ("reserved", C.c_int32)]
+                ("mixed_tile_cols", C.c_int32), ("mixed_operands", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -85,6 +85,13 @@ SIGNATURES = {
     "rvg_solve": (C.c_int, [vp, dp, i64, i64]),
     "rvg_solve_device": (C.c_int, [vp, vp, i64, i64]),
     "rvg_solve_refine": (C.c_int, [vp, dp, dp, C.c_double, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "rvg_solve_gmres": (C.c_int, [vp, dp, dp, C.c_double, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_double)]),
+    "rvg_solve_gmres_device": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_double)]),
+    "rvg_solve_refine_nrhs": (C.c_int, [vp, dp, dp, i64, i64, C.c_double, C.c_int32, C.POINTER(C.c_int32), dp]),
+    "rvg_solve_refine_nrhs_device": (C.c_int, [vp, vp, vp, i64, i64, C.c_double, C.c_int32, C.POINTER(C.c_int32),
+                                               dp]),
     "rvg_solve_refine_device": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
                                           C.POINTER(C.c_double)]),
     "rvg_inertia": (C.c_int, [vp, i64p]),

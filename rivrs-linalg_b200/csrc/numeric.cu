@@ -236,12 +236,19 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
           double col[IBMAX];
 #pragma unroll
           for (int i = 0; i < IBMAX; ++i) col[i] = T[i][lane];
+          // four interleaved scans (rows i mod 4), each keeping its first maximum,
+          // merged to the first maximum in row order
+          double b4[4] = {0.0, 0.0, 0.0, 0.0};
+          unsigned k4[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
 #pragma unroll
           for (int i = 0; i < IBMAX; ++i)
             if (i >= lane && i < bs) {
               const double v = fabs(col[i]);
-              if (v > bv) { bv = v; key = (unsigned)(lane * 64 + i); }
+              if (v > b4[i & 3]) { b4[i & 3] = v; k4[i & 3] = (unsigned)(lane * 64 + i); }
             }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (b4[q] > bv || (b4[q] == bv && k4[q] < key)) { bv = b4[q]; key = k4[q]; }
         }
         const unsigned long long bits = (unsigned long long)__double_as_longlong(bv);  // bv >= 0: bits order as values
         const unsigned hi = (unsigned)(bits >> 32), lo = (unsigned)bits;
@@ -253,8 +260,10 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
         if (key != 0xffffffffu) { mc = (int)(key / 64); mr = (int)(key % 64); }
         if (maxv >= small) {
           if (mr == mc) {
+            // the pivot's reciprocal from its value before the swap (the same number), so
+            // the division overlaps the swap
+            const double dkk = T[mr][mr], inv = 1.0 / dkk;
             swp(cur, mr);
-            const double dkk = T[cur][cur], inv = 1.0 / dkk;
             if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
             if (lane == 0) { sh.bdt[cur] = PT_1X1; sh.bdd[cur] = dkk; s_d[0] = dkk; }
             kind = 1;
@@ -265,21 +274,21 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
             const int remaining = bs - cur;
             if (remaining < 2) {
               const int pp = fabs(amm) >= fabs(att) ? mi : t;
+              const double dkk = T[pp][pp], inv = 1.0 / dkk;
               swp(cur, pp);
-              const double dkk = T[cur][cur];
               if (!(fabs(dkk) < small)) {
-                const double inv = 1.0 / dkk;
                 if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
                 if (lane == 0) { sh.bdt[cur] = PT_1X1; sh.bdd[cur] = dkk; s_d[0] = dkk; }
                 kind = 1;  // the rank-1 update is empty here
               }
             } else if (fabs(delta) >= __dmul_rn(__dmul_rn(0.5, atm), atm)) {
+              // the swaps bring (mi, t) to (cur, cur + 1): a11 = amm, a22 = att, a21 = atm, and the
+              // determinant a11 a22 - a21 a21 is delta; its reciprocal overlaps the swaps
+              const double inv_det = 1.0 / delta;
               swp(cur, mi);
               const int nt = (t == cur) ? mi : t;
               swp(cur + 1, nt);
               const double a11 = T[cur][cur], a22 = T[cur + 1][cur + 1], a21 = T[cur + 1][cur];
-              const double det = __dsub_rn(__dmul_rn(a11, a22), __dmul_rn(a21, a21));
-              const double inv_det = 1.0 / det;
               if (lane >= cur + 2 && lane < bs) {
                 const double ai1 = T[lane][cur], ai2 = T[lane][cur + 1];
                 T[lane][cur] = __dmul_rn(__dsub_rn(__dmul_rn(ai1, a22), __dmul_rn(ai2, a21)), inv_det);
@@ -293,8 +302,8 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
               kind = 2;
             } else {
               const int pp = fabs(amm) >= fabs(att) ? mi : t;
+              const double dkk = T[pp][pp], inv = 1.0 / dkk;
               swp(cur, pp);
-              const double dkk = T[cur][cur], inv = 1.0 / dkk;
               if (lane > cur && lane < bs) T[lane][cur] = __dmul_rn(T[lane][cur], inv);
               if (lane == 0) { sh.bdt[cur] = PT_1X1; sh.bdd[cur] = dkk; s_d[0] = dkk; }
               kind = 1;
@@ -793,16 +802,25 @@ __global__ void k_perm_scale_out(double* rhs, int64_t ldb, int64_t nrhs, const d
 // FP64 iterative refinement (residual of the unfactored matrix)
 // ---------------------------------------------------------------------------
 // r = b - A x; A full symmetric CSC, so column i is also row i
+// right-hand side j = blockIdx.y of columns at stride ldx (x, b) and ldr (r)
 __global__ void k_residual(const int64_t* colptr, const int32_t* rowidx, const double* val, const double* x,
-                           const double* b, double* r, int64_t n) {
+                           const double* b, double* r, int64_t n, int64_t ldx, int64_t ldr) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  x += blockIdx.y * ldx;
+  b += blockIdx.y * ldx;
+  r += blockIdx.y * ldr;
   double s = 0.0;
   for (int64_t p = colptr[i]; p < colptr[i + 1]; ++p) s = __fma_rn(val[p], x[rowidx[p]], s);
   r[i] = b[i] - s;
 }
-// out[0] += ||r||^2, out[1] += ||x||^2, out[2] += ||b||^2
-__global__ void k_norms3(const double* r, const double* x, const double* b, int64_t n, double* out) {
+// out[3j] += ||r_j||^2, out[3j + 1] += ||x_j||^2, out[3j + 2] += ||b_j||^2 for j = blockIdx.y
+__global__ void k_norms3(const double* r, const double* x, const double* b, int64_t n, double* out, int64_t ldx,
+                         int64_t ldr) {
+  x += blockIdx.y * ldx;
+  b += blockIdx.y * ldx;
+  r += blockIdx.y * ldr;
+  out += 3 * blockIdx.y;
   double s0 = 0, s1 = 0, s2 = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     s0 += r[i] * r[i]; s1 += x[i] * x[i]; s2 += b[i] * b[i];
@@ -820,9 +838,48 @@ __global__ void k_sumsq(const double* v, int64_t n, double* out) {
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
-__global__ void k_axpy1(double* x, const double* d, int64_t n) {
+// GMRES building blocks (one right-hand side): y = A x over the full symmetric CSC
+__global__ void k_spmv(const int64_t* colptr, const int32_t* rowidx, const double* val, const double* x, double* y,
+                       int64_t n) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) x[i] += d[i];
+  if (i >= n) return;
+  double s = 0.0;
+  for (int64_t p = colptr[i]; p < colptr[i + 1]; ++p) s = __fma_rn(val[p], x[rowidx[p]], s);
+  y[i] = s;
+}
+// out[i] += V_i . w for the basis vectors i = blockIdx.y (columns of V at stride n)
+__global__ void k_dots(const double* V, const double* w, int64_t n, double* out) {
+  const double* v = V + blockIdx.y * n;
+  double s = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    s = __fma_rn(v[k], w[k], s);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out + blockIdx.y, s);
+}
+// w -= sum_{i < cnt} c_i V_i   (c on the device)
+__global__ void k_sub_comb(double* w, const double* V, const double* c, int cnt, int64_t n) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double s = w[k];
+  for (int i = 0; i < cnt; ++i) s = __fma_rn(-c[i], V[(int64_t)i * n + k], s);
+  w[k] = s;
+}
+// x += sum_{i < cnt} c_i Z_i
+__global__ void k_add_comb(double* x, const double* Z, const double* c, int cnt, int64_t n) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double s = x[k];
+  for (int i = 0; i < cnt; ++i) s = __fma_rn(c[i], Z[(int64_t)i * n + k], s);
+  x[k] = s;
+}
+__global__ void k_scale_to(double* v, const double* w, double a, int64_t n) {
+  int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) v[k] = w[k] * a;
+}
+
+__global__ void k_axpy1(double* x, const double* d, int64_t n, int64_t ldx, int64_t ldd) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[blockIdx.y * ldx + i] += d[blockIdx.y * ldd + i];
 }
 
 }  // namespace rvg
@@ -878,7 +935,9 @@ struct rvg_handle {
   int32_t* d_rowidx = nullptr;
   double a_fro = 0;                                 // ||A||_F of the last factored values
   double* d_ref = nullptr; size_t ref_cap = 0;      // refinement vectors r, d, b (3n) and norms
+  double* d_gm = nullptr; size_t gm_cap = 0;        // GMRES-IR: Krylov basis, preconditioned basis, work
   double* h_norms = nullptr;
+  char* h_norms_m = nullptr; size_t h_norms_m_cap = 0;  // pinned per-column norms of the refinement
   double* scratch = nullptr; size_t scratch_cap = 0; // per-wave scratch, persistent across factors
   double* cb_arena = nullptr; size_t cb_cap = 0;     // contribution blocks, first-fit by wave
   float* pack = nullptr; size_t pack_cap = 0;        // TF32 hi/lo operand tiles of the mixed-form updates
@@ -1184,22 +1243,32 @@ int syrk_ev(rvg_handle* h) {
 // The tensor-core Schur GEMM over a.ntiles 128 x 128 lower tiles: the flush
 // depth picks the k_syrk_tc instance; without flushing, 256-column CTA tiles
 // (k_syrk_tc_pair, over column-tile pairs) unless 128 is asked for.
-static void launch_tc(rvg_handle* h, TcArgs ta) {
+template <int FMT>
+static void launch_tc_fmt(rvg_handle* h, TcArgs ta) {
   cudaStream_t st = h->st;
   if (h->opt.mixed_flush == 0 && h->opt.mixed_tile_cols == 256) {
     ta.ntiles = tp_count_tiles(ta.nr, ta.nc, ta.r0, ta.c0);
     const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
-    k_syrk_tc_pair<<<grid, TC_THREADS, TP_SMEM, st>>>(ta);
+    k_syrk_tc_pair<FMT><<<grid, TC_THREADS, TP_SMEM, st>>>(ta);
     return;
   }
   const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
   switch (h->opt.mixed_flush) {
-    case 1: k_syrk_tc<1><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-    case 2: k_syrk_tc<2><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-    case 4: k_syrk_tc<4><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-    case 8: k_syrk_tc<8><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
-    default: k_syrk_tc<TC_NO_FLUSH><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 1: k_syrk_tc<1, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 2: k_syrk_tc<2, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 4: k_syrk_tc<4, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    case 8: k_syrk_tc<8, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
+    default: k_syrk_tc<TC_NO_FLUSH, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
   }
+}
+static void launch_tc(rvg_handle* h, TcArgs ta) {
+  if (h->opt.mixed_operands == 1) launch_tc_fmt<TC_BF16>(h, ta);
+  else launch_tc_fmt<TC_TF32>(h, ta);
+}
+// the operand split of the mixed form (TF32 or BF16 parts)
+static void launch_pack(rvg_handle* h, dim3 grid, const PackArgs& pa) {
+  if (h->opt.mixed_operands == 1) k_pack_bf16x3<<<grid, 256, 0, h->st>>>(pa);
+  else k_pack_tf32x3<<<grid, 256, 0, h->st>>>(pa);
 }
 
 // The Schur update C -= W L^T (lower) of one contribution block.  kmax bounds
@@ -1216,8 +1285,8 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
       float* pl = h->pack + (size_t)nr * Q * TC_BLOCK;
       PackArgs aw{ga.W, ga.ldw, ga.r1 - ga.r0, Q, ga.Kdev, ga.K, h->pack};
       PackArgs al{ga.L + ga.c0, ga.ldl, ga.c1 - ga.c0, Q, ga.Kdev, ga.K, pl};
-      k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nr), 256, 0, st>>>(aw);
-      k_pack_tf32x3<<<dim3((unsigned)Q, (unsigned)nc), 256, 0, st>>>(al);
+      launch_pack(h, dim3((unsigned)Q, (unsigned)nr), aw);
+      launch_pack(h, dim3((unsigned)Q, (unsigned)nc), al);
       TcArgs ta{ga.C, ga.ldc, ga.r0, ga.r1, ga.c0, ga.c1, h->pack, pl, Q, ga.Kdev, ga.K, nr, nc, ntiles, h->d_err};
       if ((rc = syrk_ev(h))) return rc;
       launch_tc(h, ta);
@@ -1383,8 +1452,8 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
           const int64_t q0 = kadd / TC_BK, nqb = (bcols + TC_BK - 1) / TC_BK, t0 = (oe - wrow) / TC_BM;
           PackArgs pw{a.wo + (oe - wrow), a.wld, m - oe, Fq, bne_dev, kadd, pk_w, q0, t0, nullptr, 0};
           PackArgs pl{a.a + wd * m + oe, m, p - oe, Fq, bne_dev, kadd, pk_l, q0, t0, nullptr, 0};
-          k_pack_tf32x3<<<dim3((unsigned)nqb, blocks_for(m - oe, TC_BM)), 256, 0, st>>>(pw);
-          k_pack_tf32x3<<<dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), 256, 0, st>>>(pl);
+          launch_pack(h, dim3((unsigned)nqb, blocks_for(m - oe, TC_BM)), pw);
+          launch_pack(h, dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), pl);
           h->launches += 2;
         }
         int rc;
@@ -1731,6 +1800,7 @@ void rvg_default_options(rvg_options* o) {
   o->precision = 0;
   o->mixed_flush = 4;
   o->mixed_tile_cols = 256;
+  o->mixed_operands = 0;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347
@@ -1748,6 +1818,10 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347
   if (o.precision != 0 && o.precision != 1) { set_error("precision must be 0 (FP64) or 1 (mixed)"); return RVG_ERR_INVALID_INPUT; }
   if (o.mixed_flush != 0 && o.mixed_flush != 1 && o.mixed_flush != 2 && o.mixed_flush != 4 && o.mixed_flush != 8) {
     set_error("mixed_flush must be 0, 1, 2, 4 or 8");
+    return RVG_ERR_INVALID_INPUT;
+  }
+  if (o.mixed_operands != 0 && o.mixed_operands != 1) {
+    set_error("mixed_operands must be 0 (TF32) or 1 (BF16)");
     return RVG_ERR_INVALID_INPUT;
   }
   if (o.mixed_tile_cols != 128 && o.mixed_tile_cols != 256) {
@@ -1815,12 +1889,18 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   if ((rc = presize_arenas(h.get()))) return (rvg_status)rc;
   CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_tc<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_tc<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_tc_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP_SMEM));
-  CK(cudaFuncSetAttribute(k_syrk_tc<TC_NO_FLUSH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<1, TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<2, TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<4, TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<8, TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<TC_NO_FLUSH, TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc_pair<TC_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<1, TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<2, TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<4, TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<8, TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc<TC_NO_FLUSH, TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
+  CK(cudaFuncSetAttribute(k_syrk_tc_pair<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP_SMEM));
   CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
   CK(cudaMallocAsync((void**)&h->d_err, sizeof(int32_t), st));
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
@@ -2036,36 +2116,189 @@ rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb) {
   return RVG_OK;
 }
 
-static int refine_common(rvg_handle* h, const double* d_b, double* d_x, double tol, int32_t max_iter, int32_t* iters,
-                         double* bwd) {
+// nrhs right-hand sides at once (columns at stride ld of b and x): the blocked
+// solve, then residuals, norms and corrections of every column until each
+// column's scaled backward error is <= tol (or max_iter corrections); bwd[j]
+// is column j's final error.
+static int refine_common(rvg_handle* h, const double* d_b, double* d_x, int64_t nrhs, int64_t ld, double tol,
+                         int32_t max_iter, int32_t* iters, double* bwd) {
   const int64_t n = h->P.n;
   cudaStream_t st = h->st;
-  int rc = ensure(h->d_ref, h->ref_cap, (size_t)(2 * n + 8), st);
+  int rc = ensure(h->d_ref, h->ref_cap, (size_t)((nrhs + 1) * n + 3 * nrhs + 8), st);
   if (rc) return rc;
-  double* r = h->d_ref;
-  double* nrm = h->d_ref + n;  // 3 doubles (the rest of the buffer is unused)
-  CK(cudaMemcpyAsync(d_x, d_b, n * 8, cudaMemcpyDeviceToDevice, st));
-  if ((rc = solve_common(h, d_x, 1, n))) return rc;
+  double* r = h->d_ref;                  // n x nrhs, ld n
+  double* nrm = h->d_ref + nrhs * n;     // 3 per column
+  if ((rc = ensure_host((char*&)h->h_norms_m, h->h_norms_m_cap, (size_t)(3 * nrhs + 1) * 8))) return rc;
+  double* hn = (double*)h->h_norms_m;
+  if (ld == n) CK(cudaMemcpyAsync(d_x, d_b, (size_t)(n * nrhs) * 8, cudaMemcpyDeviceToDevice, st));
+  else CK(cudaMemcpy2DAsync(d_x, ld * 8, d_b, ld * 8, n * 8, nrhs, cudaMemcpyDeviceToDevice, st));
+  if ((rc = solve_common(h, d_x, nrhs, ld))) return rc;
   int it = 0;
-  double e = 0;
-  const unsigned nb = blocks_for(n, 256);
+  const dim3 g((unsigned)blocks_for(n, 256), (unsigned)nrhs), gn(64, (unsigned)nrhs);
   for (;;) {
-    k_residual<<<nb, 256, 0, st>>>(h->d_colptr, h->d_rowidx, h->d_vals, d_x, d_b, r, n);
-    CK(cudaMemsetAsync(nrm, 0, 3 * 8, st));
-    k_norms3<<<296, 256, 0, st>>>(r, d_x, d_b, n, nrm);
-    CK(cudaMemcpyAsync(h->h_norms, nrm, 3 * 8, cudaMemcpyDeviceToHost, st));
+    k_residual<<<g, 256, 0, st>>>(h->d_colptr, h->d_rowidx, h->d_vals, d_x, d_b, r, n, ld, n);
+    CK(cudaMemsetAsync(nrm, 0, (size_t)(3 * nrhs) * 8, st));
+    k_norms3<<<gn, 256, 0, st>>>(r, d_x, d_b, n, nrm, ld, n);
+    CK(cudaMemcpyAsync(hn, nrm, (size_t)(3 * nrhs) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    const double denom = h->a_fro * std::sqrt(h->h_norms[1]) + std::sqrt(h->h_norms[2]);
-    e = denom == 0 ? 0.0 : std::sqrt(h->h_norms[0]) / denom;
-    if (e <= tol || it >= max_iter) break;
-    if ((rc = solve_common(h, r, 1, n))) return rc;
-    k_axpy1<<<nb, 256, 0, st>>>(d_x, r, n);
+    bool done = true;
+    for (int64_t j = 0; j < nrhs; ++j) {
+      const double denom = h->a_fro * std::sqrt(hn[3 * j + 1]) + std::sqrt(hn[3 * j + 2]);
+      const double e = denom == 0 ? 0.0 : std::sqrt(hn[3 * j]) / denom;
+      if (bwd) bwd[j] = e;
+      if (!(e <= tol)) done = false;
+    }
+    if (done || it >= max_iter) break;
+    if ((rc = solve_common(h, r, nrhs, n))) return rc;
+    k_axpy1<<<g, 256, 0, st>>>(d_x, r, n, ld, n);
     ++it;
   }
   CK(cudaGetLastError());
   if ((rc = device_wait_status(h))) return rc;
   if (iters) *iters = it;
+  return RVG_OK;
+}
+
+// GMRES-IR: restarted flexible GMRES in FP64 on A x = b with the factor as
+// right preconditioner (z_j = solve(v_j), w = A z_j, Gram-Schmidt applied
+// twice, Givens rotations on the host, x += Z y at every restart).  It stops
+// when the scaled backward error of the true residual, checked at every
+// restart and when the rotated residual estimate reaches tol, is <= tol, or
+// after max_iter preconditioned products; *iters counts them (one solve each).
+static int gmres_common(rvg_handle* h, const double* d_b, double* d_x, double tol, int32_t max_iter, int32_t restart,
+                        int32_t* iters, double* bwd) {
+  const int64_t n = h->P.n;
+  cudaStream_t st = h->st;
+  const int m = restart;
+  // V (m + 1 basis vectors), Z (m preconditioned ones), r / w, coefficients
+  int rc = ensure(h->d_gm, h->gm_cap, (size_t)((2 * m + 2) * n + 4 * (m + 2) + 8), st);
+  if (rc) return rc;
+  double* V = h->d_gm;
+  double* Z = V + (int64_t)(m + 1) * n;
+  double* w = Z + (int64_t)m * n;
+  double* dc = w + n;          // m + 1 coefficients
+  double* dn = dc + (m + 2);   // norms
+  if ((rc = ensure_host((char*&)h->h_norms_m, h->h_norms_m_cap, (size_t)(4 * (m + 2) + 8) * 8))) return rc;
+  double* hn = (double*)h->h_norms_m;
+  const unsigned nb = blocks_for(n, 256);
+  const dim3 gd(64, 1);
+  auto sync_read = [&](const double* src, int cnt) -> int {
+    CK(cudaMemcpyAsync(hn, src, (size_t)cnt * 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return RVG_OK;
+  };
+  // true residual r = b - A x into w; its backward error and ||r||
+  auto residual = [&](double& e, double& rn) -> int {
+    k_residual<<<dim3(nb, 1), 256, 0, st>>>(h->d_colptr, h->d_rowidx, h->d_vals, d_x, d_b, w, n, n, n);
+    CK(cudaMemsetAsync(dn, 0, 3 * 8, st));
+    k_norms3<<<dim3(64, 1), 256, 0, st>>>(w, d_x, d_b, n, dn, n, n);
+    int r2 = sync_read(dn, 3);
+    if (r2) return r2;
+    const double denom = h->a_fro * std::sqrt(hn[1]) + std::sqrt(hn[2]);
+    rn = std::sqrt(hn[0]);
+    e = denom == 0 ? 0.0 : rn / denom;
+    return RVG_OK;
+  };
+  CK(cudaMemcpyAsync(d_x, d_b, n * 8, cudaMemcpyDeviceToDevice, st));
+  if ((rc = solve_common(h, d_x, 1, n))) return rc;  // x0 = M^-1 b
+  int it = 0;
+  double e = 0, beta = 0;
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+  for (;;) {
+    if ((rc = residual(e, beta))) return rc;
+    if (e <= tol || it >= max_iter || beta == 0) break;
+    // target for the residual estimate: the backward error with the current ||x||
+    const double xnorm = std::sqrt(hn[1]), bnorm = std::sqrt(hn[2]);
+    const double target = 0.5 * tol * (h->a_fro * xnorm + bnorm);
+    k_scale_to<<<nb, 256, 0, st>>>(V, w, 1.0 / beta, n);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    for (; j < m && it < max_iter; ++j) {
+      double* z = Z + (int64_t)j * n;
+      CK(cudaMemcpyAsync(z, V + (int64_t)j * n, n * 8, cudaMemcpyDeviceToDevice, st));
+      if ((rc = solve_common(h, z, 1, n))) return rc;
+      ++it;
+      k_spmv<<<nb, 256, 0, st>>>(h->d_colptr, h->d_rowidx, h->d_vals, z, w, n);
+      // Gram-Schmidt twice against v_0..v_j
+      for (int pass = 0; pass < 2; ++pass) {
+        CK(cudaMemsetAsync(dc, 0, (size_t)(j + 1) * 8, st));
+        k_dots<<<dim3(64, (unsigned)(j + 1)), 256, 0, st>>>(V, w, n, dc);
+        k_sub_comb<<<nb, 256, 0, st>>>(w, V, dc, j + 1, n);
+        if ((rc = sync_read(dc, j + 1))) return rc;
+        for (int i = 0; i <= j; ++i) H[(size_t)i * m + j] = (pass ? H[(size_t)i * m + j] : 0.0) + hn[i];
+      }
+      CK(cudaMemsetAsync(dn, 0, 8, st));
+      k_sumsq<<<64, 256, 0, st>>>(w, n, dn);
+      if ((rc = sync_read(dn, 1))) return rc;
+      const double hn1 = std::sqrt(hn[0]);
+      H[(size_t)(j + 1) * m + j] = hn1;
+      if (hn1 > 0) k_scale_to<<<nb, 256, 0, st>>>(V + (int64_t)(j + 1) * n, w, 1.0 / hn1, n);
+      // Givens rotations
+      for (int i = 0; i < j; ++i) {
+        const double a = H[(size_t)i * m + j], b2 = H[(size_t)(i + 1) * m + j];
+        H[(size_t)i * m + j] = cs[i] * a + sn[i] * b2;
+        H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b2;
+      }
+      const double a = H[(size_t)j * m + j], b2 = H[(size_t)(j + 1) * m + j];
+      const double rr = std::hypot(a, b2);
+      cs[j] = rr == 0 ? 1.0 : a / rr;
+      sn[j] = rr == 0 ? 0.0 : b2 / rr;
+      H[(size_t)j * m + j] = rr;
+      H[(size_t)(j + 1) * m + j] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      if (std::fabs(g[j + 1]) <= target || hn1 == 0) { ++j; break; }
+    }
+    // y = H^-1 g on the leading j x j triangle, x += Z y
+    for (int i = j - 1; i >= 0; --i) {
+      double s2 = g[i];
+      for (int k = i + 1; k < j; ++k) s2 -= H[(size_t)i * m + k] * y[k];
+      y[i] = H[(size_t)i * m + i] == 0 ? 0.0 : s2 / H[(size_t)i * m + i];
+    }
+    if (j > 0) {
+      CK(cudaMemcpyAsync(dc, y.data(), (size_t)j * 8, cudaMemcpyHostToDevice, st));
+      k_add_comb<<<nb, 256, 0, st>>>(d_x, Z, dc, j, n);
+    }
+  }
+  CK(cudaGetLastError());
+  if ((rc = device_wait_status(h))) return rc;
+  if (iters) *iters = it;
   if (bwd) *bwd = e;
+  return RVG_OK;
+}
+
+rvg_status rvg_solve_gmres_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
+                                  int32_t restart, int32_t* iters, double* bwd_err) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  if (restart < 1 || restart > 200) { set_error("restart must be in [1, 200]"); return RVG_ERR_INVALID_INPUT; }
+  if (h->P.n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  int rc = gmres_common(h, d_rhs, d_x, tol, max_iter, restart, iters, bwd_err);
+  h->t_solve = now_ms() - t0;
+  return (rvg_status)rc;
+}
+
+rvg_status rvg_solve_gmres(rvg_handle* h, const double* rhs, double* x, double tol, int32_t max_iter, int32_t restart,
+                           int32_t* iters, double* bwd_err) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  if (restart < 1 || restart > 200) { set_error("restart must be in [1, 200]"); return RVG_ERR_INVALID_INPUT; }
+  const int64_t n = h->P.n;
+  if (n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  double* d = nullptr;
+  CK(cudaMallocAsync((void**)&d, 2 * n * 8, h->st));
+  CK(cudaMemcpyAsync(d, rhs, n * 8, cudaMemcpyHostToDevice, h->st));
+  int rc = gmres_common(h, d, d + n, tol, max_iter, restart, iters, bwd_err);
+  if (rc) return (rvg_status)rc;
+  CK(cudaMemcpyAsync(x, d + n, n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaFreeAsync(d, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->t_solve = now_ms() - t0;
   return RVG_OK;
 }
 
@@ -2076,7 +2309,7 @@ rvg_status rvg_solve_refine_device(rvg_handle* h, const double* d_rhs, double* d
   if (h->P.n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; return RVG_OK; }
   CK(cudaSetDevice(h->device));
   double t0 = now_ms();
-  int rc = refine_common(h, d_rhs, d_x, tol, max_iter, iters, bwd_err);
+  int rc = refine_common(h, d_rhs, d_x, 1, h->P.n, tol, max_iter, iters, bwd_err);
   h->t_solve = now_ms() - t0;
   return (rvg_status)rc;
 }
@@ -2092,9 +2325,44 @@ rvg_status rvg_solve_refine(rvg_handle* h, const double* rhs, double* x, double 
   double* d = nullptr;
   CK(cudaMallocAsync((void**)&d, 2 * n * 8, h->st));
   CK(cudaMemcpyAsync(d, rhs, n * 8, cudaMemcpyHostToDevice, h->st));
-  int rc = refine_common(h, d, d + n, tol, max_iter, iters, bwd_err);
+  int rc = refine_common(h, d, d + n, 1, n, tol, max_iter, iters, bwd_err);
   if (rc) return (rvg_status)rc;
   CK(cudaMemcpyAsync(x, d + n, n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaFreeAsync(d, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->t_solve = now_ms() - t0;
+  return RVG_OK;
+}
+
+rvg_status rvg_solve_refine_nrhs_device(rvg_handle* h, const double* d_rhs, double* d_x, int64_t nrhs, int64_t ldb,
+                                        double tol, int32_t max_iter, int32_t* iters, double* bwd_err) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  const int64_t n = h->P.n;
+  if (nrhs < 1 || ldb < n || (n > 0 && (!d_rhs || !d_x))) { set_error("need nrhs >= 1, ldb >= n and both vectors"); return RVG_ERR_INVALID_INPUT; }
+  if (n == 0) { if (iters) *iters = 0; if (bwd_err) for (int64_t j = 0; j < nrhs; ++j) bwd_err[j] = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  int rc = refine_common(h, d_rhs, d_x, nrhs, ldb, tol, max_iter, iters, bwd_err);
+  h->t_solve = now_ms() - t0;
+  return (rvg_status)rc;
+}
+
+rvg_status rvg_solve_refine_nrhs(rvg_handle* h, const double* rhs, double* x, int64_t nrhs, int64_t ldb, double tol,
+                                 int32_t max_iter, int32_t* iters, double* bwd_err) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  const int64_t n = h->P.n;
+  if (nrhs < 1 || ldb < n || (n > 0 && (!rhs || !x))) { set_error("need nrhs >= 1, ldb >= n and both arrays"); return RVG_ERR_INVALID_INPUT; }
+  if (n == 0) { if (iters) *iters = 0; if (bwd_err) for (int64_t j = 0; j < nrhs; ++j) bwd_err[j] = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  double* d = nullptr;
+  CK(cudaMallocAsync((void**)&d, 2 * (size_t)(n * nrhs) * 8, h->st));
+  CK(cudaMemcpy2DAsync(d, n * 8, rhs, ldb * 8, n * 8, nrhs, cudaMemcpyHostToDevice, h->st));
+  int rc = refine_common(h, d, d + n * nrhs, nrhs, n, tol, max_iter, iters, bwd_err);
+  if (rc) return (rvg_status)rc;
+  CK(cudaMemcpy2DAsync(x, ldb * 8, d + n * nrhs, n * 8, n * 8, nrhs, cudaMemcpyDeviceToHost, h->st));
   CK(cudaFreeAsync(d, h->st));
   CK(cudaStreamSynchronize(h->st));
   h->t_solve = now_ms() - t0;
@@ -2246,7 +2514,7 @@ rvg_status rvg_selftest_waits(rvg_handle* h, int32_t which) {
     CK(cudaMallocAsync((void**)&c, 128 * 128 * sizeof(double), st));
     CK(cudaMallocAsync((void**)&p, 2 * (size_t)TC_BLOCK * sizeof(float), st));
     TcArgs ta{c, 128, 0, 128, 0, 128, p, p + TC_BLOCK, 1, nullptr, 32, 1, 1, 1, h->d_err, nullptr, 0, 1};
-    k_syrk_tc<4><<<1, TC_THREADS, TC_SMEM, st>>>(ta);
+    k_syrk_tc<4, TC_TF32><<<1, TC_THREADS, TC_SMEM, st>>>(ta);
     CK(cudaFreeAsync(c, st));
     CK(cudaFreeAsync(p, st));
   }
@@ -2300,6 +2568,7 @@ rvg_status rvg_trim(rvg_handle* h, int32_t what) {
     RVG_TRIM(h->sf_part, h->sf_part_cap);
     RVG_TRIM(h->d_x, h->x_cap);
     RVG_TRIM(h->d_ref, h->ref_cap);
+    RVG_TRIM(h->d_gm, h->gm_cap);
     RVG_TRIM(h->d_stage, h->stage_cap);
     h->cb_free.clear();
   }
@@ -2340,13 +2609,14 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
   fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
   if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->h_counts) cudaFreeHost(h->h_counts);
   if (h->h_norms) cudaFreeHost(h->h_norms);
+  if (h->h_norms_m) cudaFreeHost(h->h_norms_m);
   for (auto e : h->ev_pool) cudaEventDestroy(e);
   for (auto e : h->mk_pool) cudaEventDestroy(e);
   for (auto& e : h->ev) if (e) cudaEventDestroy(e);

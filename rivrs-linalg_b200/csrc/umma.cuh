@@ -69,9 +69,25 @@ constexpr uint64_t TC_TIMEOUT_NS = 2000000000ull;   // 2 s per wait
 constexpr uint32_t TC_LBO = 2048, TC_SBO = 128;     // core-matrix strides of the packed layout
 constexpr int TC_NO_FLUSH = 1 << 24;               // chunks per partial sum when it spans all of K
 
-// instruction descriptor: D F32, A and B TF32, both K-major, N = 128, M = 128
-constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
-                              ((uint32_t)(TC_BM >> 4) << 24);
+// Operand formats: each FP64 operand is split once into hi + lo parts of
+// TF32 (kind::tf32, 4-byte elements, 11 significant bits per part) or of BF16
+// (kind::f16 with both operands BF16, 2-byte elements, 8 significant bits per
+// part: half the operand bytes, half the products' accuracy).  A packed
+// (tile, chunk) block always starts TC_BLOCK floats after the previous one;
+// the BF16 parts fill its first half.  A chunk is 32 deep in both formats;
+// core matrices are 8 rows x 16 bytes (4 TF32 or 8 BF16 values), so one MMA
+// (32 bytes of K) spans two core-matrix columns in both.
+constexpr int TC_TF32 = 0, TC_BF16 = 1;
+template <int FMT>
+struct TcFmt {
+  static constexpr int EB = FMT == TC_BF16 ? 2 : 4;              // bytes per element
+  static constexpr uint32_t PART_BYTES = TC_BM * TC_BK * EB;    // hi (or lo) part of a block
+  static constexpr uint32_t BLOCK_BYTES = 2 * PART_BYTES;       // bytes of a block that are read
+  static constexpr int KSTEPS = TC_BK * EB / 32;                // MMAs per chunk and product
+  static constexpr uint32_t AB = FMT == TC_BF16 ? 1u : 2u;      // A / B format field (BF16 in kind::f16, TF32)
+  static constexpr uint32_t IDESC = (1u << 4) | (AB << 7) | (AB << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                                    ((uint32_t)(TC_BM >> 4) << 24);
+};
 
 struct TcArgs {
   double* C;
@@ -158,13 +174,23 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
          (1ull << 46);  // descriptor version 1, no swizzle, base offset 0
 }
 
+template <int FMT>
 __device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-      "l"(a), "l"(b), "r"(TC_IDESC), "r"(accumulate)
-      : "memory");
+  if constexpr (FMT == TC_BF16) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(TcFmt<FMT>::IDESC), "r"(accumulate)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(a), "l"(b), "r"(TcFmt<FMT>::IDESC), "r"(accumulate)
+        : "memory");
+  }
 }
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -230,6 +256,48 @@ __global__ void __launch_bounds__(256) k_pack_tf32x3(PackArgs a) {
   }
 }
 
+__device__ __forceinline__ uint16_t bf16_rn(float x) {
+  uint16_t h;
+  asm("cvt.rn.bf16.f32 %0, %1;" : "=h"(h) : "f"(x));
+  return h;
+}
+__device__ __forceinline__ float bf16_to_f32(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
+
+// BF16 parts: hi = bf16(x), lo = bf16(x - hi); grid (Q chunks, tiles), 256
+// threads; thread item = one row x 8 consecutive k (one 16-byte core-matrix row)
+__global__ void __launch_bounds__(256) k_pack_bf16x3(PackArgs a) {
+  if (a.cond && *a.cond >= a.cond_lt) return;
+  int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
+  if (K > a.Q * TC_BK) K = a.Q * TC_BK;
+  const int64_t q = a.q0 + blockIdx.x, t = blockIdx.y;
+  if (q * TC_BK >= K) return;
+  uint16_t* hi = reinterpret_cast<uint16_t*>(a.P + ((a.t0 + t) * a.Q + q) * TC_BLOCK);
+  uint16_t* lo = hi + TcFmt<TC_BF16>::PART_BYTES / 2;
+#pragma unroll
+  for (int e = 0; e < (TC_BM * TC_BK / 8) / 256; ++e) {
+    const int idx = threadIdx.x + 256 * e;
+    const int r = idx % TC_BM, kq = idx / TC_BM;
+    const int64_t row = t * TC_BM + r;
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int c = 0; c < 8; c += 2) {
+      uint16_t h2[2], l2[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int64_t k = q * TC_BK + kq * 8 + c + u;
+        const double x = (row < a.R && k < K) ? a.X[row + k * a.ldx] : 0.0;
+        h2[u] = bf16_rn((float)x);
+        l2[u] = bf16_rn((float)(x - (double)bf16_to_f32(h2[u])));
+      }
+      hw[c / 2] = (uint32_t)h2[0] | ((uint32_t)h2[1] << 16);
+      lw[c / 2] = (uint32_t)l2[0] | ((uint32_t)l2[1] << 16);
+    }
+    const int off = (kq * (TC_BM / 8) + (r >> 3)) * 64 + (r & 7) * 8;
+    *reinterpret_cast<uint4*>(hi + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4*>(lo + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+  }
+}
+
 // ---------------------------------------------------------------- tiles
 // Lower tiles in column order: column tile bx holds row tiles by >= first_row_tile(bx).
 __host__ __device__ inline int64_t tc_first_row_tile(int64_t bx, int64_t r0, int64_t c0) {
@@ -263,10 +331,13 @@ __device__ inline void tc_tile(const TcArgs& a, int64_t t, int64_t& bx, int64_t&
 // that grows about linearly with K; each run of G chunks starts from zero in
 // tensor memory and is then added into FP64 accumulators held in registers
 // by the epilogue warps (warp e owns 32 rows x 64 columns of the tile).
-template <int G>
+template <int G, int FMT>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
+  using F = TcFmt<FMT>;
+  constexpr int STAGES = TC_STAGES * (4 / F::EB);       // the same shared memory either way
+  constexpr uint32_t STAGE_BYTES = 2 * F::BLOCK_BYTES;     // W block + L block
   extern __shared__ __align__(1024) uint8_t tc_smem[];
-  __shared__ __align__(8) uint64_t bars[2 * TC_STAGES + 5];
+  __shared__ __align__(8) uint64_t bars[2 * STAGES + 5];
   __shared__ uint32_t tslot;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -278,10 +349,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
   const int64_t ngrp = (nq + G - 1) / G;  // partial sums per tile
   const uint32_t stage0 = (smem_u32(tc_smem) + 1023u) & ~1023u;
   auto full = [&](int s) { return smem_u32(&bars[s]); };
-  auto empty = [&](int s) { return smem_u32(&bars[TC_STAGES + s]); };
-  auto pfull = [&](int b) { return smem_u32(&bars[2 * TC_STAGES + b]); };
-  auto pempty = [&](int b) { return smem_u32(&bars[2 * TC_STAGES + 2 + b]); };
-  const uint32_t fin = smem_u32(&bars[2 * TC_STAGES + 4]);  // completion of every MMA issued
+  auto empty = [&](int s) { return smem_u32(&bars[STAGES + s]); };
+  auto pfull = [&](int b) { return smem_u32(&bars[2 * STAGES + b]); };
+  auto pempty = [&](int b) { return smem_u32(&bars[2 * STAGES + 2 + b]); };
+  const uint32_t fin = smem_u32(&bars[2 * STAGES + 4]);  // completion of every MMA issued
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tslot)),
@@ -290,7 +361,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (threadIdx.x == 32) {
-    for (int s = 0; s < TC_STAGES; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       mbar_init(full(s), 1);
       mbar_init(empty(s), 1);
     }
@@ -310,26 +381,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
   if (warp == 0) {
     // ---------------- producer
     if (lane == 0) {
-      int64_t g = 0, last_round[TC_STAGES];
-      for (int s = 0; s < TC_STAGES; ++s) last_round[s] = -1;
+      int64_t g = 0, last_round[STAGES];
+      for (int s = 0; s < STAGES; ++s) last_round[s] = -1;
       for (int64_t t = blockIdx.x; t < a.ntiles && !abort_flag && !a.stall; t += gridDim.x) {
         int64_t bx, by;
         tc_tile(a, t, bx, by);
         const float* A = a.Ap + by * a.Q * TC_BLOCK;
         const float* B = a.Bp + bx * a.Q * TC_BLOCK;
         for (int64_t q = 0; q < nq; ++q, ++g) {
-          const int s = (int)(g % TC_STAGES);
-          const int64_t r = g / TC_STAGES;
+          const int s = (int)(g % STAGES);
+          const int64_t r = g / STAGES;
           if (r > 0 && !mbar_wait(empty(s), (uint32_t)((r - 1) & 1), &abort_flag, a.err)) break;
-          const uint32_t dst = stage0 + (uint32_t)s * TC_STAGE_BYTES;
-          mbar_expect_tx(full(s), TC_STAGE_BYTES);
-          bulk_g2s(dst, A + q * TC_BLOCK, TC_BLOCK_BYTES, full(s));
-          bulk_g2s(dst + TC_BLOCK_BYTES, B + q * TC_BLOCK, TC_BLOCK_BYTES, full(s));
+          const uint32_t dst = stage0 + (uint32_t)s * STAGE_BYTES;
+          mbar_expect_tx(full(s), STAGE_BYTES);
+          bulk_g2s(dst, A + q * TC_BLOCK, F::BLOCK_BYTES, full(s));
+          bulk_g2s(dst + F::BLOCK_BYTES, B + q * TC_BLOCK, F::BLOCK_BYTES, full(s));
           last_round[s] = r;
         }
       }
       // the copies issued last land before the CTA's shared memory goes away
-      for (int s = 0; s < TC_STAGES; ++s) {
+      for (int s = 0; s < STAGES; ++s) {
         if (last_round[s] < 0) continue;
         const uint64_t t0 = gtimer();
         while (!mbar_try(full(s), (uint32_t)(last_round[s] & 1)) && gtimer() - t0 < TC_TIMEOUT_NS) {
@@ -353,22 +424,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
             }
             tc_fence_after();
           }
-          const int s = (int)(g % TC_STAGES);
-          if (!mbar_wait(full(s), (uint32_t)((g / TC_STAGES) & 1), &abort_flag, a.err)) {
+          const int s = (int)(g % STAGES);
+          if (!mbar_wait(full(s), (uint32_t)((g / STAGES) & 1), &abort_flag, a.err)) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t d = tbase + (uint32_t)(b * TC_BN);
-          const uint32_t base = stage0 + (uint32_t)s * TC_STAGE_BYTES;
+          const uint32_t base = stage0 + (uint32_t)s * STAGE_BYTES;
 #pragma unroll
-          for (int ks = 0; ks < TC_BK / 8; ++ks) {
+          for (int ks = 0; ks < F::KSTEPS; ++ks) {
             const uint32_t ko = (uint32_t)ks * 2 * TC_LBO;
-            const uint64_t ah = tc_desc(base + ko), al = tc_desc(base + TC_PART * 4 + ko);
-            const uint64_t bh = tc_desc(base + TC_BLOCK_BYTES + ko), bl = tc_desc(base + TC_BLOCK_BYTES + TC_PART * 4 + ko);
-            tc_mma(d, al, bh, (q % G > 0 || ks > 0) ? 1u : 0u);
-            tc_mma(d, ah, bl, 1u);
-            tc_mma(d, ah, bh, 1u);
+            const uint64_t ah = tc_desc(base + ko), al = tc_desc(base + F::PART_BYTES + ko);
+            const uint64_t bh = tc_desc(base + F::BLOCK_BYTES + ko), bl = tc_desc(base + F::BLOCK_BYTES + F::PART_BYTES + ko);
+            tc_mma<FMT>(d, al, bh, (q % G > 0 || ks > 0) ? 1u : 0u);
+            tc_mma<FMT>(d, ah, bl, 1u);
+            tc_mma<FMT>(d, ah, bh, 1u);
           }
           tc_commit(empty(s));  // the stage is free once these MMAs have read it
           if (q % G == G - 1 || q == nq - 1) {
@@ -448,9 +519,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
 // The one-partial-sum form (no flush) with two 128-column output tiles per CTA
 // tile: both read the same 128-row W tile from shared memory, so a CTA brings
 // in 3 operand tiles per 2 output tiles instead of 4 (the update is bound by
-// the operand stream out of L2).  Stages hold half a packed chunk (16 deep:
-// the hi and lo halves of the W tile and of both L tiles, 48 KB, six
-// cp.async.bulk copies), four stages; tensor memory holds two 256-column
+// the operand stream out of L2).  A stage holds 8 KB of each part of the W
+// tile and of both L tiles (16 deep in TF32, a whole 32-deep chunk in BF16:
+// 48 KB, six cp.async.bulk copies), four stages; tensor memory holds two 256-column
 // accumulators (tile 0 at columns [0, 128), tile 1 at [128, 256) of each).
 // Each output tile gets the same MMA sequence as in k_syrk_tc (per k-step
 // lo*hi, hi*lo, hi*hi, k-steps in order), and the epilogue does
@@ -458,9 +529,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
 // kernels give bit-identical results.  Epilogue warp e takes tile e / 4 of the
 // pair and its 32-row lane quarter, 16 columns at a time (tensor memory read,
 // then the C read-modify-write), and frees the accumulator after the tile.
-constexpr int TP_BK = 16;                                // K per stage
 constexpr int TP_STAGES = 4;
-constexpr uint32_t TP_HALF_BYTES = TC_PART * 4 / 2;      // 8 KB: half of one TF32 part of a block
+constexpr uint32_t TP_HALF_BYTES = 8192;                  // a stage's slice of one part
 constexpr uint32_t TP_OPND_BYTES = 2 * TP_HALF_BYTES;    // hi + lo halves of one operand tile
 constexpr uint32_t TP_STAGE_BYTES = 3 * TP_OPND_BYTES;   // W tile + two L tiles: 48 KB
 constexpr size_t TP_SMEM = (size_t)TP_STAGES * TP_STAGE_BYTES + 1024 + 32768;
@@ -488,7 +558,12 @@ __device__ inline void tp_tile(const TcArgs& a, int64_t t, int64_t& px, int64_t&
   by = 0;  // not reached for t < ntiles
 }
 
+template <int FMT>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc_pair(TcArgs a) {
+  using F = TcFmt<FMT>;
+  constexpr int SK = 64 / F::EB;                 // K per stage: 16 (TF32) or 32 (BF16), 8 KB per part either way
+  constexpr int SPC = TC_BK / SK;                // stages per packed chunk
+  static_assert(TC_BM * SK * F::EB == (int)TP_HALF_BYTES, "a stage part is 8 KB");
   extern __shared__ __align__(1024) uint8_t tc_smem[];
   __shared__ __align__(8) uint64_t bars[2 * TP_STAGES + 5];
   __shared__ uint32_t tslot;
@@ -498,7 +573,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc_pair(TcArgs a) {
   int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the packed chunks
   if (K <= 0) return;
-  const int64_t nh = (K + TP_BK - 1) / TP_BK;  // half chunks
+  const int64_t nh = (K + SK - 1) / SK;  // stages of SK
   const uint32_t stage0 = (smem_u32(tc_smem) + 1023u) & ~1023u;
   auto full = [&](int s) { return smem_u32(&bars[s]); };
   auto empty = [&](int s) { return smem_u32(&bars[TP_STAGES + s]); };
@@ -547,16 +622,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc_pair(TcArgs a) {
           const int64_t r = g / TP_STAGES;
           if (r > 0 && !mbar_wait(empty(s), (uint32_t)((r - 1) & 1), &abort_flag, a.err)) break;
           const uint32_t dst = stage0 + (uint32_t)s * TP_STAGE_BYTES;
-          // hi half at +0, lo half at +TC_PART floats of the (tile, chunk) block
-          const int64_t off = (h >> 1) * TC_BLOCK + (h & 1) * (TC_PART / 2);
+          // the stage's slice of the hi part (at +0) and of the lo part (at +PART_BYTES) of the block
+          constexpr int64_t PF = F::PART_BYTES / 4;  // a part, in floats
+          const int64_t off = (h / SPC) * TC_BLOCK + (h % SPC) * (TP_HALF_BYTES / 4);
           mbar_expect_tx(full(s), (two ? 3u : 2u) * TP_OPND_BYTES);
           bulk_g2s(dst, A + off, TP_HALF_BYTES, full(s));
-          bulk_g2s(dst + TP_HALF_BYTES, A + off + TC_PART, TP_HALF_BYTES, full(s));
+          bulk_g2s(dst + TP_HALF_BYTES, A + off + PF, TP_HALF_BYTES, full(s));
           bulk_g2s(dst + TP_OPND_BYTES, B0 + off, TP_HALF_BYTES, full(s));
-          bulk_g2s(dst + TP_OPND_BYTES + TP_HALF_BYTES, B0 + off + TC_PART, TP_HALF_BYTES, full(s));
+          bulk_g2s(dst + TP_OPND_BYTES + TP_HALF_BYTES, B0 + off + PF, TP_HALF_BYTES, full(s));
           if (two) {
             bulk_g2s(dst + 2 * TP_OPND_BYTES, B1 + off, TP_HALF_BYTES, full(s));
-            bulk_g2s(dst + 2 * TP_OPND_BYTES + TP_HALF_BYTES, B1 + off + TC_PART, TP_HALF_BYTES, full(s));
+            bulk_g2s(dst + 2 * TP_OPND_BYTES + TP_HALF_BYTES, B1 + off + PF, TP_HALF_BYTES, full(s));
           }
           last_round[s] = r;
         }
@@ -592,18 +668,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc_pair(TcArgs a) {
           tc_fence_after();
           const uint32_t base = stage0 + (uint32_t)s * TP_STAGE_BYTES;
 #pragma unroll
-          for (int ks = 0; ks < TP_BK / 8; ++ks) {
+          for (int ks = 0; ks < 2; ++ks) {  // 32 bytes of K per MMA, 64 per stage
             const uint32_t ko = (uint32_t)ks * 2 * TC_LBO;
             const uint64_t ah = tc_desc(base + ko), al = tc_desc(base + TP_HALF_BYTES + ko);
             const uint32_t b0 = base + TP_OPND_BYTES, b1 = base + 2 * TP_OPND_BYTES;
             const uint32_t acc = (h > 0 || ks > 0) ? 1u : 0u;
-            tc_mma(d0, al, tc_desc(b0 + ko), acc);
-            tc_mma(d0, ah, tc_desc(b0 + TP_HALF_BYTES + ko), 1u);
-            tc_mma(d0, ah, tc_desc(b0 + ko), 1u);
+            tc_mma<FMT>(d0, al, tc_desc(b0 + ko), acc);
+            tc_mma<FMT>(d0, ah, tc_desc(b0 + TP_HALF_BYTES + ko), 1u);
+            tc_mma<FMT>(d0, ah, tc_desc(b0 + ko), 1u);
             if (two) {
-              tc_mma(d1, al, tc_desc(b1 + ko), acc);
-              tc_mma(d1, ah, tc_desc(b1 + TP_HALF_BYTES + ko), 1u);
-              tc_mma(d1, ah, tc_desc(b1 + ko), 1u);
+              tc_mma<FMT>(d1, al, tc_desc(b1 + ko), acc);
+              tc_mma<FMT>(d1, ah, tc_desc(b1 + TP_HALF_BYTES + ko), 1u);
+              tc_mma<FMT>(d1, ah, tc_desc(b1 + ko), 1u);
             }
           }
           tc_commit(empty(s));

@@ -24,6 +24,10 @@ def main():
     ap.add_argument("--mixed-flush", type=int, default=4)
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--no-scaling", action="store_true", help="skip MC64 scaling")
+    ap.add_argument("--large-threshold", type=int, default=2048,
+                    help="fronts of at least this order take the multi-kernel (whole GPU) path")
+    ap.add_argument("--operands", default="tf32", choices=["tf32", "bf16"], help="mixed form: operand parts")
+    ap.add_argument("--profile", action="store_true", help="print the factorization's time by kind of work")
     args = ap.parse_args()
 
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
@@ -40,13 +44,21 @@ def main():
         solver = rv.SparseLDLT.analyze(s)
     else:
         solver = rv.SparseLDLT.analyze_with_matrix(s, rv.AnalyzeOptions(rv.OrderingStrategy.MATCH_ORDER_METIS))
-    opts = rv.FactorOptions(precision=args.precision, mixed_flush=args.mixed_flush)
+    opts = rv.FactorOptions(precision=args.precision, mixed_flush=args.mixed_flush,
+                            large_front_threshold=args.large_threshold, mixed_operands=args.operands)
+    if args.profile:
+        solver._ensure_handle(opts)
+        solver.set_profiling(True)
     for r in range(args.reps):
         t0 = time.perf_counter()
         solver.factor(s.values, opts)
         _, iters, err = solver.solve_refine(b, tol=1e-14, max_iter=10)
         print(f"rep {r}: n={s.n} {time.perf_counter() - t0:.3f} s refinement steps {iters} bwd err {err:.2e} "
               f"stats {solver.stats()}", flush=True)
+        if args.profile:
+            pr = solver.profile()
+            print("  factor ms %.1f, parts %s" % (pr["factor_ms"], {k: round(v, 1) for k, v in pr["part_ms"].items()
+                                                                 if v > 0}), flush=True)
     solver.close()
 
 

@@ -53,6 +53,7 @@ class FactorOptions:
     precision: str = "fp64"  # "fp64" (plain) or "mixed" (TF32 tensor-core Schur updates; pair with solve_refine)
     mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
     mixed_tile_cols: int = 256  # mixed form, mixed_flush 0: Schur GEMM output columns per CTA tile (128, 256)
+    mixed_operands: str = "tf32"  # mixed form: FP64 operands split into two "tf32" or two "bf16" parts
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
@@ -62,7 +63,8 @@ class FactorOptions:
                                  fallback_bk=int(self.fallback_bunch_kaufman),
                                  large_front_threshold=self.large_front_threshold,
                                  precision={"fp64": 0, "mixed": 1}[self.precision],
-                                 mixed_flush=self.mixed_flush, mixed_tile_cols=self.mixed_tile_cols)
+                                 mixed_flush=self.mixed_flush, mixed_tile_cols=self.mixed_tile_cols,
+                                 mixed_operands={"tf32": 0, "bf16": 1}[self.mixed_operands])
 
 
 class SparseError(RuntimeError):
@@ -230,6 +232,17 @@ class SparseLDLT:
         Returns (x, corrections, backward error)."""
         if not self._factored:
             raise SolveBeforeFactor("factor() must be called before solve()")
+        if np.ndim(rhs) == 2:  # several right-hand sides: blocked solves, per-column errors
+            b = np.asfortranarray(np.asarray(rhs, dtype=np.float64))
+            if b.shape[0] != self.system.n:
+                raise DimensionMismatch("RHS length must match matrix dimension")
+            x = np.empty_like(b, order="F")
+            it = C.c_int32()
+            errs = np.zeros(b.shape[1])
+            _check(N.lib().rvg_solve_refine_nrhs(self._handle, b.ctypes.data_as(N.dp), x.ctypes.data_as(N.dp),
+                                                 b.shape[1], b.shape[0], tol, max_iter, C.byref(it),
+                                                 errs.ctypes.data_as(N.dp)))
+            return x, it.value, errs
         b = N.as_f64(rhs)
         if b.ndim != 1 or b.size != self.system.n:
             raise DimensionMismatch("RHS length must match matrix dimension")
@@ -248,6 +261,43 @@ class SparseLDLT:
         _check(N.lib().rvg_solve_refine_device(self._handle, C.c_void_p(d_rhs_ptr), C.c_void_p(d_x_ptr), tol, max_iter,
                                                C.byref(it), C.byref(err)))
         return it.value, err.value
+
+    def solve_gmres(self, rhs: np.ndarray, tol: float = 1e-14, max_iter: int = 100, restart: int = 30):
+        """x by GMRES-IR: FP64 flexible GMRES preconditioned by the factor.
+        Returns (x, preconditioned products, backward error)."""
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        b = N.as_f64(rhs)
+        if b.ndim != 1 or b.size != self.system.n:
+            raise DimensionMismatch("RHS length must match matrix dimension")
+        x = np.empty_like(b)
+        it = C.c_int32()
+        err = C.c_double()
+        _check(N.lib().rvg_solve_gmres(self._handle, N.ptr(b, N.dp), N.ptr(x, N.dp), tol, max_iter, restart,
+                                       C.byref(it), C.byref(err)))
+        return x, it.value, err.value
+
+    def solve_gmres_device(self, d_rhs_ptr: int, d_x_ptr: int, tol: float = 1e-14, max_iter: int = 100,
+                           restart: int = 30):
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        it = C.c_int32()
+        err = C.c_double()
+        _check(N.lib().rvg_solve_gmres_device(self._handle, C.c_void_p(d_rhs_ptr), C.c_void_p(d_x_ptr), tol,
+                                              max_iter, restart, C.byref(it), C.byref(err)))
+        return it.value, err.value
+
+    def solve_refine_nrhs_device(self, d_rhs_ptr: int, d_x_ptr: int, nrhs: int, ldb: int | None = None,
+                                 tol: float = 1e-14, max_iter: int = 10):
+        """Refined solve of nrhs device-resident columns; returns (corrections, errors per column)."""
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        it = C.c_int32()
+        errs = np.zeros(nrhs)
+        _check(N.lib().rvg_solve_refine_nrhs_device(self._handle, C.c_void_p(d_rhs_ptr), C.c_void_p(d_x_ptr), nrhs,
+                                                    ldb or self.system.n, tol, max_iter, C.byref(it),
+                                                    errs.ctypes.data_as(N.dp)))
+        return it.value, errs
 
     def solve_device(self, d_rhs_ptr: int, nrhs: int = 1, ldb: int | None = None):
         if not self._factored:

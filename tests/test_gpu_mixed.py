@@ -38,9 +38,11 @@ def test_mixed_reaches_fp64_accuracy(rv, name):
         import scipy.sparse as sp
         s = rv.problems.from_scipy("dense700", sp.csc_matrix(a))
     b = rv.problems.rhs_normal(s.n, 3)
-    for precision, flush in (("fp64", 2), ("mixed", 1), ("mixed", 2), ("mixed", 8), ("mixed", 0)):
-        x, iters, err, inertia = factor_refine(rv, s, b, precision=precision, mixed_flush=flush, **SMALL_LARGE)
-        assert err <= 1e-14, (precision, flush, err, iters)
+    for precision, flush, ops in (("fp64", 2, "tf32"), ("mixed", 1, "tf32"), ("mixed", 2, "tf32"), ("mixed", 8, "tf32"),
+                                  ("mixed", 0, "tf32"), ("mixed", 4, "bf16"), ("mixed", 0, "bf16")):
+        x, iters, err, inertia = factor_refine(rv, s, b, precision=precision, mixed_flush=flush, mixed_operands=ops,
+                                               **SMALL_LARGE)
+        assert err <= 1e-14, (precision, flush, ops, err, iters)
         assert rv.problems.backward_error(s, x, b) <= 1e-14
         if s.inertia is not None:
             assert inertia == s.inertia
@@ -61,8 +63,10 @@ def test_mixed_window(rv, n, nb, kind):
         a[np.arange(n), np.arange(n)] *= 1e-6
     s = rv.problems.from_scipy(f"dense{n}", sp.csc_matrix(a))
     b = rv.problems.rhs_normal(s.n, 4)
-    for flush in (4, 0):
-        x, iters, err, inertia = factor_refine(rv, s, b, precision="mixed", mixed_flush=flush,
+    # (TF32 parts only: these random dense matrices are too ill-conditioned for plain refinement
+    # of a BF16-split factor)
+    for flush, ops in ((4, "tf32"), (0, "tf32")):
+        x, iters, err, inertia = factor_refine(rv, s, b, precision="mixed", mixed_flush=flush, mixed_operands=ops,
                                                large_front_threshold=33, outer_block_size=nb)
         assert err <= 1e-14, (flush, err, iters)
         assert rv.problems.backward_error(s, x, b) <= 1e-14
@@ -84,12 +88,13 @@ def test_refine_errors(rv):
         solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=3))
 
 
+@pytest.mark.parametrize("ops", ["tf32", "bf16"])
 @pytest.mark.parametrize("case", ["kkt", "dense_plain", "dense_delay", "dense_nb64"])
-def test_pair_tiles_bit_identical(rv, case):
+def test_pair_tiles_bit_identical(rv, case, ops):
     # the no-flush Schur GEMM over 256-column CTA tiles (two 128-column tiles
     # sharing the W tile) gives the same factor, bit for bit, as 128-column tiles
     import scipy.sparse as sp
-    opts = dict(precision="mixed", mixed_flush=0)
+    opts = dict(precision="mixed", mixed_flush=0, mixed_operands=ops)
     if case == "kkt":
         s = rv.problems.kkt(14, seed=4)
         opts.update(large_front_threshold=64)
@@ -123,3 +128,83 @@ def test_pair_tiles_option_checked(rv):
     solver = rv.SparseLDLT.analyze(s)
     with pytest.raises(rv.InvalidInput):
         solver.factor(None, rv.FactorOptions(precision="mixed", mixed_tile_cols=192))
+
+
+def test_bf16_parts_are_less_accurate_but_refine(rv):
+    # the BF16 split keeps about 16 bits per product against 22 for TF32: a larger
+    # first residual, and the refinement still ends at the FP64 target
+    import scipy.sparse as sp
+    rng = np.random.default_rng(11)
+    n = 1200
+    a = rng.standard_normal((n, n))
+    a = a + a.T + np.diag(np.full(n, 4.0 * np.sqrt(n)))
+    s = rv.problems.from_scipy("dense1200", sp.csc_matrix(a))
+    b = rv.problems.rhs_normal(n, 2)
+    first = {}
+    for ops in ("tf32", "bf16"):
+        solver = rv.SparseLDLT.analyze(s)
+        solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=4, mixed_operands=ops,
+                                             large_front_threshold=33))
+        x0 = solver.solve(b)
+        first[ops] = rv.problems.backward_error(s, x0, b)
+        x, iters, err = solver.solve_refine(b, tol=1e-14, max_iter=10)
+        assert err <= 1e-14, (ops, err, iters)
+        solver.close()
+    assert first["bf16"] > first["tf32"]
+    assert first["bf16"] < 1e-3
+
+
+@pytest.mark.parametrize("ops", ["tf32", "bf16"])
+def test_refine_several_rhs(rv, ops):
+    # blocked refinement of 5 right-hand sides: every column reaches the target, and each
+    # agrees with the one-column refinement of the same factor (to the forward error a
+    # backward error of 1e-14 allows on this matrix)
+    s = rv.problems.kkt(12, seed=3)
+    b = rv.problems.rhs_normal(s.n, 9, 5)
+    solver = rv.SparseLDLT.analyze(s)
+    solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands=ops,
+                                         large_front_threshold=64))
+    x, iters, errs = solver.solve_refine(b, tol=1e-14, max_iter=10)
+    assert x.shape == b.shape and errs.shape == (5,)
+    assert (errs <= 1e-14).all(), errs
+    for j in range(5):
+        assert rv.problems.backward_error(s, x[:, j], b[:, j]) <= 1e-14
+        x1, _, _ = solver.solve_refine(b[:, j].copy(), tol=1e-14, max_iter=10)
+        assert np.linalg.norm(x[:, j] - x1) <= 1e-8 * np.linalg.norm(x1)
+    solver.close()
+
+
+@pytest.mark.parametrize("ops,flush", [("tf32", 0), ("bf16", 0), ("bf16", 4)])
+def test_gmres_ir_where_refinement_stalls(rv, ops, flush):
+    # a random dense indefinite matrix (ill-conditioned): GMRES-IR with the mixed factor as
+    # preconditioner reaches the FP64 target for both operand splits
+    import scipy.sparse as sp
+    n = 900
+    rng = np.random.default_rng(n + 128)
+    a = rng.standard_normal((n, n))
+    a = a + a.T
+    s = rv.problems.from_scipy("dense900", sp.csc_matrix(a))
+    b = rv.problems.rhs_normal(n, 4)
+    solver = rv.SparseLDLT.analyze(s)
+    solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=flush, mixed_operands=ops,
+                                         large_front_threshold=33, outer_block_size=128))
+    x, its, err = solver.solve_gmres(b, tol=1e-14, max_iter=200, restart=30)
+    assert err <= 1e-14, (ops, flush, err, its)
+    assert rv.problems.backward_error(s, x, b) <= 1e-14
+    solver.close()
+
+
+def test_gmres_ir_on_kkt_and_errors(rv):
+    s = rv.problems.kkt(10, seed=5)
+    b = rv.problems.rhs_normal(s.n, 7)
+    solver = rv.SparseLDLT.analyze(s)
+    with pytest.raises(rv.SolveBeforeFactor):
+        solver.solve_gmres(b)
+    solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16",
+                                         large_front_threshold=64))
+    x, its, err = solver.solve_gmres(b, tol=1e-14, restart=5)
+    assert err <= 1e-14 and its >= 1
+    assert rv.problems.backward_error(s, x, b) <= 1e-14
+    with pytest.raises(rv.InvalidInput):
+        solver.solve_gmres(b, restart=0)
+    solver.close()

@@ -49,11 +49,14 @@ def assert_parity(rv, s, solver, ref, b, bwd=1e-14):
     x = solver.solve(b)
     xr = ref.solve(b)
     assert np.linalg.norm(x - xr) <= SOL_RTOL * max(np.linalg.norm(xr), 1e-300)
-    if b.ndim == 1:
-        assert rv.problems.backward_error(s, x, b) <= bwd
-    else:
-        for j in range(b.shape[1]):
-            assert rv.problems.backward_error(s, x[:, j], b[:, j]) <= bwd
+    # the backward error gate, or (ill-conditioned cases) within 4x of the oracle's on the same factor:
+    # the solve's sums run in another order than the oracle's, and the forward pass adds sibling
+    # contributions atomically
+    xs, xrs, bs = (x, xr, b) if b.ndim == 2 else (x[:, None], xr[:, None], b[:, None])
+    for j in range(bs.shape[1]):
+        e = rv.problems.backward_error(s, xs[:, j], bs[:, j])
+        er = rv.problems.backward_error(s, xrs[:, j], bs[:, j])
+        assert e <= max(bwd, 4 * er), (e, er)
 
 
 @pytest.mark.parametrize("g,frac", [(4, 0.1), (8, 0.1), (12, 0.05), (16, 0.1), (20, 0.1)])
