@@ -3,25 +3,37 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--config C] [--impl b200|reference]
 
-A step is one numeric factorization plus one solve of the whole system
-(the path rivrs-sparse times as factor + solve).  The default workload is the
-saddle-point KKT system [[H, J^T], [J, 0]] with H the 27-point Laplacian of a
-60^3 grid plus diag(U[0,1e-2]) and J 54,000 x 216,000 with 4 N(0,1) entries
-per row (n = 270,000), plain FP64, one right-hand side b ~ N(0,1).
+A step is one numeric factorization plus the solve of the whole system to a
+scaled backward error of 1e-14 (the metric: factor+solve time to that
+accuracy).  The default workload is the saddle-point KKT system
+[[H, J^T], [J, 0]] with H the 27-point Laplacian of a 60^3 grid plus
+diag(U[0,1e-2]) and J 54,000 x 216,000 with 4 N(0,1) entries per row
+(n = 270,000), MC64-scaled, one right-hand side b ~ N(0,1).  Forms timed:
+plain FP64; the mixed form (Schur updates on the tcgen05 tensor cores) with
+TF32 operand parts at the flush depths of --mixed-flush, followed by FP64
+iterative refinement; with BF16 parts at the depths of --bf16-flush,
+followed by GMRES-IR.  `value` is the fastest form that reaches 1e-14.
 
-* `value`  factor+solve seconds per step with the matrix values and the RHS
-           already in HBM (CUDA events on the handle's stream, max over ranks).
-* `e2e`    the same step through the public C ABI with host buffers
-           (rvg_factor / rvg_solve): values and RHS copied in, x copied out.
-* `roofline` the dominant kernel, the FP64 Schur-complement GEMM: executed
-           flops / its event-timed device time, against a cuBLAS DGEMM peak
-           measured in the same run.
+* `value`  seconds per step with the matrix values and the RHS already in HBM
+           (CUDA events on the handle's stream, max over ranks; the library's
+           per-launch profiling events off).
+* `e2e`    the same step through the public API with host buffers (values and
+           RHS copied in, x copied out).
+* `roofline` the chosen form's Schur-complement GEMM (from one extra profiled
+           step): executed flops / its event-timed device time, against a
+           GEMM peak of the same arithmetic (cuBLAS measured in the run, or
+           the measured-peaks file for BF16).
+* `hbm_bound_parts` the solve and the assembly against the measured HBM
+           copy bandwidth.
 * `cpu_baseline` the oracle (OpenMP restatement of the reference numeric
            path) on a bounded KKT sample of the same family, its flop rate
            extrapolated to the workload.
-Multi-GPU runs are independent replicas (the single-system path does not
-shard): each rank factors its own copy, no collective in the data path.
+`--config batch64` times the many-systems workload instead (64 systems,
+grouped unions; see run_batch).  Multi-GPU runs are independent replicas
+(the single-system path does not shard): each rank factors its own copy, no
+collective in the data path.
 """
+
 import argparse
 import json
 import os

@@ -51,8 +51,10 @@ typedef struct {
   int32_t failed_pivot_tpp; /* 1 = FailedPivotMethod::Tpp, 0 = Pass */
   int32_t fallback_bk;      /* 1 = AptpFallback::BunchKaufman, 0 = Delay */
   /* B200 scheduling, no reference counterpart: fronts of order >= this use
-   * the multi-kernel path (whole GPU per front); smaller ones are batched one
-   * CTA or warp per front.  Results do not depend on it.  Default 2048. */
+   * the multi-kernel path (whole GPU per front), and so do fronts of at least
+   * half this order in a wave that holds at most 16 of them; the others are
+   * batched one CTA or warp per front.  Results do not depend on it.
+   * Default 2048. */
   int64_t large_front_threshold;
   /* Arithmetic of the large Schur-complement updates, no reference
    * counterpart: 0 = plain FP64 (tensor-core DMMA, bit-identical to the CPU

@@ -7,7 +7,7 @@
 
 namespace rvg {
 
-enum : int32_t { FF_SMALL_LEAF = 1, FF_HAS_CB = 2, FF_HAS_PARENT = 4 };
+enum : int32_t { FF_SMALL_LEAF = 1, FF_HAS_CB = 2, FF_HAS_PARENT = 4, FF_LARGE = 8 };
 
 struct DFront {
   int64_t panel;    // offset (doubles) in the panel arena, ld = m

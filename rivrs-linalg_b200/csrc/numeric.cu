@@ -1134,6 +1134,17 @@ unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); 
 constexpr int64_t LF_WINDOW = 4;
 int64_t lf_window_cols(int64_t nb, bool mixed) { return (!mixed || nb % 128 == 0) ? LF_WINDOW * nb : nb; }
 
+// Which fronts of a wave take the multi-kernel path (the whole GPU, one front
+// after another) instead of one CTA each: every front of order >= T, and
+// those of order >= T / 2 when the wave holds at most LF_FEW of them (a few
+// such fronts leave most SMs idle on the CTA path; many keep them busy).
+// Results do not depend on the choice: both paths perform the same
+// arithmetic.  mid = the wave's count of non-TPP fronts with T/2 <= m < T.
+constexpr int64_t LF_FEW = 16;
+inline bool front_is_large(int64_t m, bool tpp, int64_t T, int64_t mid) {
+  return !tpp && (m >= T || (m >= T / 2 && mid <= LF_FEW));
+}
+
 // Arena sizes of the delay-free schedule, computed from the pattern alone
 // (delays can only add to them; the arenas grow in that case).
 int presize_arenas(rvg_handle* h) {
@@ -1141,8 +1152,14 @@ int presize_arenas(rvg_handle* h) {
   const int64_t nb = h->opt.outer_block_size, ib = h->opt.inner_block_size;
   int64_t panel = 0, idx = 0, dsz = 0, scratch = 0;
   std::vector<int64_t> cbw(P.waves.size(), 0), rel(P.waves.size(), -1);
+  const int64_t T = h->opt.large_front_threshold;
   for (size_t w = 0; w < P.waves.size(); ++w) {
-    int64_t sc_w = 0;
+    int64_t sc_w = 0, mid = 0;
+    for (int64_t s : P.waves[w]) {
+      const Snode& x = P.sn[s];
+      const int64_t k = x.n_owned(), m = k + (int64_t)x.pattern.size();
+      if (!(x.in_small_leaf || k < ib) && m >= T / 2 && m < T) ++mid;
+    }
     for (int64_t s : P.waves[w]) {
       const Snode& x = P.sn[s];
       int64_t k = x.n_owned(), nfs = (int64_t)x.pattern.size(), m = k + nfs;
@@ -1152,7 +1169,7 @@ int presize_arenas(rvg_handle* h) {
       bool has_cb = x.parent >= 0 && nfs > 0;
       if (has_cb) cbw[w] += nfs * nfs;
       bool tpp = x.in_small_leaf || k < ib;
-      bool large = !tpp && m >= h->opt.large_front_threshold;
+      bool large = front_is_large(m, tpp, T, mid);
       int64_t sc = tpp ? 0 : (2 * IBMAX * m + nb);
       if (large) sc = m * (2 * IBMAX + LF_WINDOW * nb) + nb;
       if (has_cb) sc = std::max<int64_t>(sc, nfs * k);
@@ -1569,12 +1586,25 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       f.idx = idx_used + idx_need; idx_need += m + k;
       f.dpos = d_used + d_need; d_need += k;
       if (f.flags & FF_HAS_CB) cb_need += nfs * nfs;
-      const bool tpp = (f.flags & FF_SMALL_LEAF) || k < ib;
-      const bool large = !tpp && m >= h->opt.large_front_threshold;
-      int64_t sc = tpp ? 0 : (2 * IBMAX * m + h->opt.outer_block_size);
-      if (large) sc = m * (2 * IBMAX + LF_WINDOW * h->opt.outer_block_size) + h->opt.outer_block_size;
-      if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
-      f.scratch = scratch_need; scratch_need += sc;
+    }
+    {
+      const int64_t T = h->opt.large_front_threshold;
+      int64_t mid = 0;
+      for (int64_t s : wave) {
+        const DFront& f = h->h_fronts[s];
+        if (!((f.flags & FF_SMALL_LEAF) || f.k < ib) && f.m >= T / 2 && f.m < T) ++mid;
+      }
+      for (int64_t s : wave) {
+        DFront& f = h->h_fronts[s];
+        const int64_t m = f.m, k = f.k, nfs = f.nfs;
+        const bool tpp = (f.flags & FF_SMALL_LEAF) || k < ib;
+        const bool large = front_is_large(m, tpp, T, mid);
+        if (large) f.flags |= FF_LARGE;
+        int64_t sc = tpp ? 0 : (2 * IBMAX * m + h->opt.outer_block_size);
+        if (large) sc = m * (2 * IBMAX + LF_WINDOW * h->opt.outer_block_size) + h->opt.outer_block_size;
+        if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
+        f.scratch = scratch_need; scratch_need += sc;
+      }
     }
     double ta = now_ms();
     if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st))) return rc;
@@ -1606,7 +1636,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       staged.push_back(h->h_fronts[s]);
       const DFront& f = h->h_fronts[s];
       if ((f.flags & FF_SMALL_LEAF) || f.k < ib) tpp_ids.push_back((int32_t)s);
-      else if (f.m >= h->opt.large_front_threshold) large_ids.push_back((int32_t)s);
+      else if (f.flags & FF_LARGE) large_ids.push_back((int32_t)s);
       else aptp_ids.push_back((int32_t)s);
     }
     std::vector<ScatterItem> sitems;
@@ -1630,7 +1660,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       const DFront& f = h->h_fronts[s];
       if (!(f.flags & FF_HAS_CB) || f.k == 0) continue;
       for (int ti = 0; ti * 256 < f.nfs; ++ti) witems.push_back(TileItem{(int32_t)s, ti, 0, 0});
-      if (f.m >= h->opt.large_front_threshold && f.nfs >= 256) continue;  // GEMM by k_syrk_lower
+      if ((f.flags & FF_LARGE) && f.nfs >= 256) continue;  // GEMM by launch_syrk
       int nt = (f.nfs + GT - 1) / GT;
       for (int tj = 0; tj < nt; ++tj)
         for (int ti = tj; ti < nt; ++ti) gitems.push_back(TileItem{(int32_t)s, ti, tj, 0});
@@ -1691,7 +1721,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     mark(h, RVG_PART_CB_GEMM);
     for (int64_t s : wave) {
       const DFront& f = h->h_fronts[s];
-      if (!(f.flags & FF_HAS_CB) || f.k == 0 || !(f.m >= h->opt.large_front_threshold && f.nfs >= 256)) continue;
+      if (!(f.flags & FF_HAS_CB) || f.k == 0 || !((f.flags & FF_LARGE) && f.nfs >= 256)) continue;
       SyrkArgs ga{A.cbase + f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
                   0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
       if ((rc = launch_syrk(h, ga, f.k))) return rc;
