@@ -197,21 +197,27 @@ def gemm_peak_tflops(torch, dtype):
     return best
 
 
-def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local):
+def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local, dist=None):
     """The many-systems workload: 64 systems (n log-uniform in [5e3, 2e5],
     half shifted Laplacians, half KKT, seed 1) with 1-32 right-hand sides each,
     in plain FP64.  The systems form block-diagonal unions sized to the device
     memory (BatchLDLT groups); a step factors and solves every group in turn,
     releasing each group's device memory before the next.  Then
     refactorizations with every value scaled by 1 + 0.01 N(0,1) (symmetric
-    pairs alike), each followed by the solve."""
+    pairs alike), each followed by the solve.  On N GPUs the 64 systems are
+    split between the ranks (balanced by flops, no collective in the data
+    path): the total work is fixed, the time is the slowest rank's."""
     t0 = time.perf_counter()
     fam = rv.problems.batch_family(count=64, seed=1)
-    systems, nrhs = [f[0] for f in fam], [f[1] for f in fam]
+    mine = list(range(len(fam)))
+    if world > 1:
+        weights = [dense_flops(rv.SparseLDLT.analyze(f[0]).symbolic) for f in fam]
+        mine = rv.replicas.shard(weights, rank, world)
+    systems, nrhs = [fam[i][0] for i in mine], [fam[i][1] for i in mine]
     bl = rv.BatchLDLT(systems)
     analyze_ms = (time.perf_counter() - t0) * 1e3
     flops = sum(dense_flops(g.solver.symbolic) for g in bl.groups)
-    rhs = [rv.problems.rhs_normal(sy.n, 100 + i, r) for i, (sy, r) in enumerate(zip(systems, nrhs))]
+    rhs = [rv.problems.rhs_normal(sy.n, 100 + i, r) for i, sy, r in zip(mine, systems, nrhs)]
     opts = rv.FactorOptions(precision="fp64")
     vals = bl.values()
     d_vals = torch.from_numpy(vals).to("cuda")
@@ -309,6 +315,10 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
         e2e_t.append(time.perf_counter() - t1)
     inert_ok = bl.inertias() == [sy.inertia for sy in systems]
     t_step = max_over_ranks(statistics.mean(times))
+    t_ref = max_over_ranks(statistics.mean(ref_times))
+    e2e_v = max_over_ranks(statistics.mean(e2e_t))
+    flops_all = rv.replicas.sum_over_ranks(flops, dist, device="cuda")
+    n_all = int(rv.replicas.sum_over_ranks(bl.n, dist, device="cuda"))
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         orc = entry.load_oracle()
@@ -317,11 +327,13 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
         ns = [sy.n for sy in systems]
         h2d = int(vals.nbytes + sum(e["rhs"].numel() * 8 for e in G))
         line = {
-            "metric": "batch factor+solve time (64 systems, 1-32 RHS each), plain FP64 on 1 B200",
+            "metric": "batch factor+solve time (64 systems, 1-32 RHS each), plain FP64",
             "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": t_step * 1e3, "higher_is_better": False,
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
-            "config": {"workload": CONFIGS["batch64"][2], "systems": len(systems), "n_total": int(bl.n),
+            "config": {"workload": CONFIGS["batch64"][2], "systems": len(fam), "systems_rank0": len(systems),
+                       "n_total": n_all,
                        "n_min": min(ns), "n_max": max(ns), "rhs_total": int(sum(nrhs)),
                        "groups": [g.count for g in bl.groups],
                        "device_budget_gb": bl.device_budget / 1e9,
@@ -329,13 +341,13 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
                                "released in turn",
                        "scaling": "MC64 per system (host analysis incl. ordering %.0f ms)" % analyze_ms,
                        "l2": "working set far above L2 (126 MB); no flush needed",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"systems split over {world} GPUs" if world > 1 else "one GPU"},
             "bwd_err_max": bwd, "inertia_exact": inert_ok,
             "refactor": {"count": nref, "perturbation": "values x (1 + 0.01 N(0,1)), symmetric pairs alike",
-                         "s_per_refactor_mean": statistics.mean(ref_times), "s_min": min(ref_times),
+                         "s_per_refactor_mean": t_ref, "s_min": min(ref_times),
                          "s_max": max(ref_times), "bwd_err_max_last": bwd_ref},
-            "factor_flops": flops, "factor_gflops": flops / t_step / 1e9,
-            "e2e": {"value": max_over_ranks(statistics.mean(e2e_t)), "unit": "s",
+            "factor_flops": flops_all, "factor_gflops": flops_all / t_step / 1e9,
+            "e2e": {"value": e2e_v, "unit": "s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(sum(e["rhs"].numel() * 8 for e in G))},
             "gpu_launches": int(launches),
             "parts_ms": parts, "step_event_s": times, "peak_device_bytes": peak, "clocks": clk,
@@ -442,7 +454,7 @@ def main():
         return float(t.item())
 
     if args.config == "batch64":
-        run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local)
+        run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local, dist)
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -596,6 +608,16 @@ def main():
         rl_kernel = "k_syrk_dmma (FP64 Schur-complement GEMM, plain form)"
         rl_source = "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in the measured-peaks file)"
     achieved = (syrk_flops / (syrk_ms * 1e-3) / 1e12) if syrk_ms > 0 else None
+    # DRAM traffic of the chosen kernel per launch: the ncu capture of its longest launch on the KKT 36^3
+    # (profiles/k_syrk_tc_pair_bf16_kkt36.md: 1,569.6 MB for 148.1 GFLOP FP64-equivalent at K = 1024) scaled
+    # to this run's average launch by its flops (C traffic grows with the entries, operands with K x rows)
+    traffic = traffic_src = None
+    if chosen_name == "mixed" and chosen["opts"].mixed_operands == "bf16" and chosen["opts"].mixed_flush == 0 \
+            and chosen["syrk_launch"]:
+        fp64_flops_per_launch = chosen["syrk_flops"] / chosen["syrk_launch"]
+        traffic = 1569.6e6 / 148.1e9 * fp64_flops_per_launch
+        traffic_src = ("ncu dram__bytes_read+write of one k_syrk_tc_pair<BF16> launch (KKT 36^3, K = 1024), "
+                       "scaled by FP64-equivalent flops to this run's average launch")
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         orc = entry.load_oracle()
@@ -635,7 +657,8 @@ def main():
             "gpu_launches": int(launches // max(args.steps, 1)),
             "roofline": {"kernel": rl_kernel, "bound": "tensor",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "traffic_unit": "bytes per launch", "traffic_source": traffic_src,
                          "peak_source": rl_source, "dgemm_peak": dpeak, "tf32_gemm_peak": tpeak,
                          "launches_per_step": syrk_launch,
                          "share_of_step": (syrk_ms * 1e-3) / t_step if t_step else None},
