@@ -471,6 +471,7 @@ def main():
         """W warm-up + K timed steps of one form: factor + (refined) solve, inputs in HBM.
         method: "ir" (iterative refinement) or "gmres" (GMRES-IR) back to FP64 accuracy."""
         opts = rv.FactorOptions(precision=precision, mixed_flush=flush, mixed_operands=ops)
+        used = set()
         solver._ensure_handle(opts)
         solver.set_profiling(False)  # timed steps without the per-launch events
         stream = torch.cuda.ExternalStream(solver.stream())
@@ -479,6 +480,10 @@ def main():
             solver.factor_device(d_vals.data_ptr(), d_scal.data_ptr() if d_scal is not None else None, opts)
             if method == "gmres":
                 return solver.solve_gmres_device(d_b.data_ptr(), d_x.data_ptr(), tol=1e-14, max_iter=100, restart=30)
+            if method == "auto":
+                it, e, how = solver.solve_auto_device(d_b.data_ptr(), d_x.data_ptr(), tol=1e-14, max_iter=100)
+                used.add(how)
+                return it, e
             return solver.solve_refine_device(d_b.data_ptr(), d_x.data_ptr(), tol=1e-14, max_iter=10)
 
         for _ in range(args.warmup):
@@ -512,14 +517,14 @@ def main():
         return dict(t=max_over_ranks(statistics.mean(times)), times=times, walls=walls, clk=clk,
                     bwd=rv.problems.backward_error(s, x, b), inertia=solver.inertia(), stats=solver.stats(),
                     prof=solver.profile(), syrk_ms=syrk_ms, syrk_flops=syrk_flops, syrk_launch=syrk_launch,
-                    launches=launches, refine_iters=its, opts=opts, method=method)
+                    launches=launches, refine_iters=its, opts=opts, method=method, used=sorted(used))
 
     plain = run_form("fp64")
     forms = {"plain_fp64": plain}
     for fl in [int(v) for v in args.mixed_flush.split(",") if v.strip()]:
-        forms[f"mixed_flush{fl}"] = run_form("mixed", fl)
+        forms[f"mixed_flush{fl}"] = run_form("mixed", fl, "tf32", "auto")
     for fl in [int(v) for v in args.bf16_flush.split(",") if v.strip()]:
-        forms[f"mixed_bf16_flush{fl}_gmres"] = run_form("mixed", fl, "bf16", "gmres")
+        forms[f"mixed_bf16_flush{fl}"] = run_form("mixed", fl, "bf16", "auto")
     # the chosen form: the fastest that reaches the accuracy target (plain always does)
     chosen_key = min((k for k, f in forms.items() if f["bwd"] <= 1e-14 or k == "plain_fp64"),
                      key=lambda k: forms[k]["t"])
@@ -543,6 +548,8 @@ def main():
         solver.factor(s.values, opts)
         if chosen["method"] == "gmres":
             xh, _, _ = solver.solve_gmres(b, tol=1e-14, max_iter=100, restart=30)
+        elif chosen["method"] == "auto":
+            xh, _, _, _ = solver.solve_auto(b, tol=1e-14, max_iter=100)
         else:
             xh, _, _ = solver.solve_refine(b, tol=1e-14, max_iter=10)
         torch.cuda.synchronize()
@@ -629,9 +636,11 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
             "config": {"workload": CONFIGS[args.config][2],
-                       "form": (f"{chosen_key}: " + ("Schur updates on tcgen05 TF32 tensor cores (operands split "
-                                "hi+lo, FP32 partial sums added in FP64), FP64 pivoting/storage, FP64 iterative "
-                                "refinement" if chosen_name == "mixed" else "plain FP64 (DMMA)")
+                       "form": (f"{chosen_key}: " + (("Schur updates on tcgen05 tensor cores (FP64 operands split "
+                                "into %s hi+lo, FP32 accumulation added in FP64), FP64 pivoting/storage; FP64 "
+                                "iterative refinement escalating to GMRES-IR (used: %s)"
+                                % (chosen["opts"].mixed_operands.upper(), ", ".join(chosen["used"])))
+                                if chosen_name == "mixed" else "plain FP64 (DMMA)")
                                 + "; APTP u=0.01, nb=256, ib=32, nemin=32"),
                        "ordering": "geometric nested dissection, constraints last", "rhs": 1,
                        "scaling": "MC64 (host analysis incl. ordering %.0f ms, outside the timed region)" % analyze_ms,
@@ -639,8 +648,11 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "bwd_err": bwd, "bwd_err_e2e": bwd_e2e, "inertia": list(inertia), "inertia_expected": list(s.inertia),
             "forms": {k: {"s_per_step": f["t"], "bwd_err": f["bwd"], "refine_corrections": f["refine_iters"],
-                          "accuracy_method": "GMRES-IR (FP64 FGMRES, factor as preconditioner)"
-                          if f["method"] == "gmres" else "iterative refinement",
+                          "accuracy_method": {"gmres": "GMRES-IR (FP64 FGMRES, factor as preconditioner)",
+                                              "auto": "iterative refinement, escalating to GMRES-IR when it stalls "
+                                                      "(used: %s)" % ", ".join(f["used"]),
+                                              "ir": "iterative refinement"}[f["method"]],
+                          "solves_after_first": f["refine_iters"],
                           "inertia": list(f["inertia"]),
                           "syrk_tflops_fp64_equiv": (f["syrk_flops"] / (f["syrk_ms"] * 1e-3) / 1e12)
                           if f["syrk_ms"] > 0 else None,

@@ -172,6 +172,15 @@ rvg_status rvg_solve_gmres(rvg_handle* h, const double* rhs, double* x, double t
                            int32_t restart, int32_t* iters, double* bwd_err);
 rvg_status rvg_solve_gmres_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
                                   int32_t restart, int32_t* iters, double* bwd_err);
+/* Refinement that escalates (no reference counterpart): FP64 iterative
+ * refinement while every correction at least halves the backward error, then
+ * GMRES-IR (restart 30) from the refined x until tol or max_iter solves after
+ * the first.  *method = 0 if refinement alone reached the result, 1 if it
+ * escalated to GMRES-IR. */
+rvg_status rvg_solve_auto(rvg_handle* h, const double* rhs, double* x, double tol, int32_t max_iter, int32_t* iters,
+                          double* bwd_err, int32_t* method);
+rvg_status rvg_solve_auto_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
+                                 int32_t* iters, double* bwd_err, int32_t* method);
 rvg_status rvg_solve_refine_nrhs(rvg_handle* h, const double* rhs, double* x, int64_t nrhs, int64_t ldb, double tol,
                                  int32_t max_iter, int32_t* iters, double* bwd_err);
 rvg_status rvg_solve_refine_nrhs_device(rvg_handle* h, const double* d_rhs, double* d_x, int64_t nrhs, int64_t ldb,

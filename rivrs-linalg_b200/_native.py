@@ -89,6 +89,10 @@ SIGNATURES = {
                                   C.POINTER(C.c_double)]),
     "rvg_solve_gmres_device": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
                                          C.POINTER(C.c_double)]),
+    "rvg_solve_auto": (C.c_int, [vp, dp, dp, C.c_double, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                 C.POINTER(C.c_int32)]),
+    "rvg_solve_auto_device": (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
     "rvg_solve_refine_nrhs": (C.c_int, [vp, dp, dp, i64, i64, C.c_double, C.c_int32, C.POINTER(C.c_int32), dp]),
     "rvg_solve_refine_nrhs_device": (C.c_int, [vp, vp, vp, i64, i64, C.c_double, C.c_int32, C.POINTER(C.c_int32),
                                                dp]),

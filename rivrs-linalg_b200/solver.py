@@ -277,6 +277,28 @@ class SparseLDLT:
                                        C.byref(it), C.byref(err)))
         return x, it.value, err.value
 
+    def solve_auto(self, rhs: np.ndarray, tol: float = 1e-14, max_iter: int = 100):
+        """x by iterative refinement, escalating to GMRES-IR when it stalls.
+        Returns (x, solves after the first, backward error, "ir" or "gmres")."""
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        b = N.as_f64(rhs)
+        if b.ndim != 1 or b.size != self.system.n:
+            raise DimensionMismatch("RHS length must match matrix dimension")
+        x = np.empty_like(b)
+        it, err, meth = C.c_int32(), C.c_double(), C.c_int32()
+        _check(N.lib().rvg_solve_auto(self._handle, N.ptr(b, N.dp), N.ptr(x, N.dp), tol, max_iter, C.byref(it),
+                                      C.byref(err), C.byref(meth)))
+        return x, it.value, err.value, ("gmres" if meth.value else "ir")
+
+    def solve_auto_device(self, d_rhs_ptr: int, d_x_ptr: int, tol: float = 1e-14, max_iter: int = 100):
+        if not self._factored:
+            raise SolveBeforeFactor("factor() must be called before solve()")
+        it, err, meth = C.c_int32(), C.c_double(), C.c_int32()
+        _check(N.lib().rvg_solve_auto_device(self._handle, C.c_void_p(d_rhs_ptr), C.c_void_p(d_x_ptr), tol, max_iter,
+                                             C.byref(it), C.byref(err), C.byref(meth)))
+        return it.value, err.value, ("gmres" if meth.value else "ir")
+
     def solve_gmres_device(self, d_rhs_ptr: int, d_x_ptr: int, tol: float = 1e-14, max_iter: int = 100,
                            restart: int = 30):
         if not self._factored:

@@ -208,3 +208,29 @@ def test_gmres_ir_on_kkt_and_errors(rv):
     with pytest.raises(rv.InvalidInput):
         solver.solve_gmres(b, restart=0)
     solver.close()
+
+
+def test_auto_refinement_escalates_only_when_needed(rv):
+    import scipy.sparse as sp
+    # well conditioned: refinement alone
+    s = rv.problems.kkt(10, seed=6)
+    b = rv.problems.rhs_normal(s.n, 3)
+    solver = rv.SparseLDLT.analyze(s)
+    solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=4, large_front_threshold=64))
+    x, its, err, how = solver.solve_auto(b)
+    assert err <= 1e-14 and how == "ir"
+    solver.close()
+    # ill conditioned with a BF16-split factor: refinement stalls, GMRES-IR finishes
+    n = 900
+    rng = np.random.default_rng(n + 128)
+    a = rng.standard_normal((n, n))
+    a = a + a.T
+    s = rv.problems.from_scipy("dense900", sp.csc_matrix(a))
+    b = rv.problems.rhs_normal(n, 4)
+    solver = rv.SparseLDLT.analyze(s)
+    solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16",
+                                         large_front_threshold=33, outer_block_size=128))
+    x, its, err, how = solver.solve_auto(b, max_iter=200)
+    assert err <= 1e-14 and how == "gmres", (err, its, how)
+    assert rv.problems.backward_error(s, x, b) <= 1e-14
+    solver.close()
