@@ -36,7 +36,10 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
+
+#include <thread>
 
 #include "dense.cuh"
 #include "front.cuh"
@@ -907,6 +910,21 @@ __global__ void k_get_counts(const int32_t* ids, int n, const DFront* F, int32_t
 
 using namespace rvg;
 
+// One large front in flight: the stream its launches go to, its pivot state
+// on the device and the packed window of its mixed-form updates.  Context 0
+// is the handle's own stream; the others let the large fronts of one wave run
+// side by side (one host thread each).
+struct LfCtx {
+  cudaStream_t st = nullptr;
+  LFState* lf = nullptr;
+  float* wpack = nullptr; size_t wpack_cap = 0;
+  bool own = false;        // stream and state created for this context
+  bool marks = false;      // profiling marks (only one front in flight, on the handle's stream)
+  int64_t launches = 0;
+  double sync_ms = 0, syrk_flops = 0;
+};
+constexpr int LF_CONCURRENT = 8;  // large fronts of a wave in flight at once
+
 struct rvg_handle {
   Plan P;
   rvg_options opt;
@@ -931,6 +949,7 @@ struct rvg_handle {
   char* h_stage = nullptr; size_t h_stage_cap = 0; // pinned host mirror
   int32_t* h_counts = nullptr; size_t h_counts_cap = 0;
   LFState* d_lf = nullptr;                          // state of the large-front path
+  std::vector<LfCtx> lfx;                            // concurrent large-front contexts 1.. (0 = the handle's)
   int64_t* d_colptr = nullptr;                      // matrix pattern (full symmetric CSC = its own CSR)
   int32_t* d_rowidx = nullptr;
   double a_fro = 0;                                 // ||A||_F of the last factored values
@@ -1244,8 +1263,8 @@ double lower_entries(int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
 
 // CUDA events around each Schur GEMM launch (profiling): their sum is the
 // GEMM time the measured rate is based on.
-int syrk_ev(rvg_handle* h) {
-  if (!h->profiling) return RVG_OK;
+int syrk_ev(rvg_handle* h, bool on = true) {
+  if (!h->profiling || !on) return RVG_OK;
   if (h->ev_used + 1 > h->ev_pool.size()) {
     for (int i = 0; i < 64; ++i) {
       cudaEvent_t e;
@@ -1261,8 +1280,7 @@ int syrk_ev(rvg_handle* h) {
 // depth picks the k_syrk_tc instance; without flushing, 256-column CTA tiles
 // (k_syrk_tc_pair, over column-tile pairs) unless 128 is asked for.
 template <int FMT>
-static void launch_tc_fmt(rvg_handle* h, TcArgs ta) {
-  cudaStream_t st = h->st;
+static void launch_tc_fmt(rvg_handle* h, cudaStream_t st, TcArgs ta) {
   if (h->opt.mixed_flush == 0 && h->opt.mixed_tile_cols == 256) {
     ta.ntiles = tp_count_tiles(ta.nr, ta.nc, ta.r0, ta.c0);
     const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
@@ -1278,14 +1296,14 @@ static void launch_tc_fmt(rvg_handle* h, TcArgs ta) {
     default: k_syrk_tc<TC_NO_FLUSH, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
   }
 }
-static void launch_tc(rvg_handle* h, TcArgs ta) {
-  if (h->opt.mixed_operands == 1) launch_tc_fmt<TC_BF16>(h, ta);
-  else launch_tc_fmt<TC_TF32>(h, ta);
+static void launch_tc(rvg_handle* h, cudaStream_t st, TcArgs ta) {
+  if (h->opt.mixed_operands == 1) launch_tc_fmt<TC_BF16>(h, st, ta);
+  else launch_tc_fmt<TC_TF32>(h, st, ta);
 }
 // the operand split of the mixed form (TF32 or BF16 parts)
-static void launch_pack(rvg_handle* h, dim3 grid, const PackArgs& pa) {
-  if (h->opt.mixed_operands == 1) k_pack_bf16x3<<<grid, 256, 0, h->st>>>(pa);
-  else k_pack_tf32x3<<<grid, 256, 0, h->st>>>(pa);
+static void launch_pack(rvg_handle* h, cudaStream_t st, dim3 grid, const PackArgs& pa) {
+  if (h->opt.mixed_operands == 1) k_pack_bf16x3<<<grid, 256, 0, st>>>(pa);
+  else k_pack_tf32x3<<<grid, 256, 0, st>>>(pa);
 }
 
 // The Schur update C -= W L^T (lower) of one contribution block.  kmax bounds
@@ -1302,11 +1320,11 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
       float* pl = h->pack + (size_t)nr * Q * TC_BLOCK;
       PackArgs aw{ga.W, ga.ldw, ga.r1 - ga.r0, Q, ga.Kdev, ga.K, h->pack};
       PackArgs al{ga.L + ga.c0, ga.ldl, ga.c1 - ga.c0, Q, ga.Kdev, ga.K, pl};
-      launch_pack(h, dim3((unsigned)Q, (unsigned)nr), aw);
-      launch_pack(h, dim3((unsigned)Q, (unsigned)nc), al);
+      launch_pack(h, st, dim3((unsigned)Q, (unsigned)nr), aw);
+      launch_pack(h, st, dim3((unsigned)Q, (unsigned)nc), al);
       TcArgs ta{ga.C, ga.ldc, ga.r0, ga.r1, ga.c0, ga.c1, h->pack, pl, Q, ga.Kdev, ga.K, nr, nc, ntiles, h->d_err};
       if ((rc = syrk_ev(h))) return rc;
-      launch_tc(h, ta);
+      launch_tc(h, st, ta);
       if ((rc = syrk_ev(h))) return rc;
       h->launches += 3;
       h->syrk_launches++;
@@ -1327,12 +1345,12 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
 // (ld m - wrow), L is the panel itself; the mixed form reads the packed
 // window (tile 0 = rows [wrow, wrow + 128), F / 32 chunks per tile).  With
 // cond set the launch only acts if *cond < cond_lt.
-int launch_window_gemm(rvg_handle* h, const LFArgs& a, int64_t m, int64_t c0, int64_t c1, int64_t wd, int64_t wrow,
-                       int64_t F, const float* pk_w, const float* pk_l, int64_t kadd, const int32_t* kdev,
-                       const int32_t* cond, int32_t cond_lt) {
-  cudaStream_t st = h->st;
+int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int64_t c0, int64_t c1, int64_t wd,
+                       int64_t wrow, int64_t F, const float* pk_w, const float* pk_l, int64_t kadd,
+                       const int32_t* kdev, const int32_t* cond, int32_t cond_lt) {
+  cudaStream_t st = cx.st;
   if (c1 <= c0) return RVG_OK;
-  int rc = syrk_ev(h);
+  int rc = syrk_ev(h, cx.marks);
   if (rc) return rc;
   if (h->opt.precision == 1) {
     const int64_t Fq = F / TC_BK;
@@ -1341,7 +1359,7 @@ int launch_window_gemm(rvg_handle* h, const LFArgs& a, int64_t m, int64_t c0, in
     const int64_t t0 = (c0 - wrow) / TC_BM;
     TcArgs ta{a.a, m, c0, m, c0, c1, pk_w + (size_t)t0 * Fq * TC_BLOCK, pk_l + (size_t)t0 * Fq * TC_BLOCK, Fq, kdev,
               kadd, nr, nc, ntiles, h->d_err, cond, cond_lt};
-    launch_tc(h, ta);
+    launch_tc(h, st, ta);
   } else {
     SyrkArgs ga{};
     ga.C = a.a;
@@ -1360,17 +1378,18 @@ int launch_window_gemm(rvg_handle* h, const LFArgs& a, int64_t m, int64_t c0, in
     ga.cond_lt = cond_lt;
     k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
   }
-  if ((rc = syrk_ev(h))) return rc;
-  h->launches++;
-  h->syrk_launches++;
+  if ((rc = syrk_ev(h, cx.marks))) return rc;
+  cx.launches++;
+  if (cx.marks) h->syrk_launches++;
   return RVG_OK;
 }
 
 // One large front on the whole GPU: the launch sequence of large.cuh, with
 // one host synchronisation per 256-column outer block (its start column
 // depends on the delays of the previous block).
-int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts& dop) {
-  cudaStream_t st = h->st;
+int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, const DevOpts& dop) {
+  cudaStream_t st = cx.st;
+  auto mk = [&](int kind) { if (cx.marks) mark(h, kind); };
   const DFront& f = h->h_fronts[s];
   const int64_t m = f.m, p = f.k, nb = h->opt.outer_block_size, ib = h->opt.inner_block_size;
   LFArgs a{};
@@ -1379,7 +1398,7 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
   a.p = p;
   a.perm = Ar.idx + f.idx + m;
   a.D = DRec{Ar.dtype + f.dpos, Ar.ddiag + f.dpos, Ar.doff + f.dpos};
-  a.st = h->d_lf;
+  a.st = cx.lf;
   double* sc = Ar.scratch + f.scratch;
   a.pb = sc;
   a.w = sc + m * IBMAX;
@@ -1396,21 +1415,21 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
   float *pk_w = nullptr, *pk_l = nullptr;
   if (mixed && two_level) {
     const int64_t tiles = (m + TC_BM - 1) / TC_BM;
-    int rc = ensure_nocopy(h->wpack, h->wpack_cap, (size_t)2 * tiles * Fq * TC_BLOCK, st);
+    int rc = ensure_nocopy(cx.wpack, cx.wpack_cap, (size_t)2 * tiles * Fq * TC_BLOCK, st);
     if (rc) return rc;
-    pk_w = h->wpack;
-    pk_l = h->wpack + (size_t)tiles * Fq * TC_BLOCK;
+    pk_w = cx.wpack;
+    pk_l = cx.wpack + (size_t)tiles * Fq * TC_BLOCK;
   }
-  mark(h, -1);
+  mk(-1);
   k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
-  h->launches++;
+  cx.launches++;
   int64_t rem = p, gne = 0;
   while (rem > 0) {
     const int64_t bcols = std::min(rem, nb), cs = gne, bm = m - cs, oe = cs + bcols;
     a.cs = cs;
     a.bcols = bcols;
     k_lf_begin_outer<<<1, 256, 0, st>>>(a);
-    mark(h, RVG_PART_LF_SETUP);
+    mk(RVG_PART_LF_SETUP);
     const int64_t ninner = (bcols + ib - 1) / ib;
     // the inner block's trailing update: rows and columns from ts = k + bs
     // (device values) within the outer block's view
@@ -1428,25 +1447,25 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
     gi.dbs = &a.st->bs;
     for (int64_t it = 0; it < ninner; ++it) {
       k_lf_block<<<1, NT, 0, st>>>(a);
-      mark(h, RVG_PART_LF_BLOCK);
+      mk(RVG_PART_LF_BLOCK);
       k_lf_panel<<<blocks_for(bm, LF_PANEL_T), LF_PANEL_T, 0, st>>>(a);
-      mark(h, RVG_PART_LF_PANEL);
+      mk(RVG_PART_LF_PANEL);
       k_lf_post<<<1, 256, 0, st>>>(a);
-      mark(h, RVG_PART_LF_POST);
+      mk(RVG_PART_LF_POST);
       k_lf_wi<<<blocks_for(bm, 256), 256, 0, st>>>(a);
       k_syrk_inner<<<syrk_grid(gi), G_T, G_SMEM, st>>>(gi);
-      mark(h, RVG_PART_LF_UPDATE);
+      mk(RVG_PART_LF_UPDATE);
       k_lf_delay<<<1, NT, 0, st>>>(a);
-      mark(h, RVG_PART_LF_DELAY);
+      mk(RVG_PART_LF_DELAY);
     }
-    h->launches += 1 + 6 * ninner;
+    cx.launches += 1 + 6 * ninner;
     bool flush = false;
     int64_t kadd = 0, ncol = 0;
     if (two_level) {
       if (cs > 0) {
         k_lf_prop<<<(unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256, (size_t)bcols * LF_PROP_COLS * 8, st>>>(a);
-        h->launches++;
-        mark(h, RVG_PART_LF_PROP);
+        cx.launches++;
+        mk(RVG_PART_LF_PROP);
       }
       if (oe < p) {
         // this block's W joins the window [wd, gne + bne)
@@ -1455,8 +1474,8 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
         a.wrow0 = wrow;
         a.wcol0 = kadd;
         k_lf_w<<<blocks_for(m - oe, 128), 128, 0, st>>>(a);
-        h->launches++;
-        mark(h, RVG_PART_LF_W);
+        cx.launches++;
+        mk(RVG_PART_LF_W);
         // The next outer block is [g, g + min(rem - bcols, nb)); columns past
         // rem (delayed ones parked at the end) belong to no later block.  The
         // window is applied everywhere when it is full, or when the next block
@@ -1469,51 +1488,51 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
           const int64_t q0 = kadd / TC_BK, nqb = (bcols + TC_BK - 1) / TC_BK, t0 = (oe - wrow) / TC_BM;
           PackArgs pw{a.wo + (oe - wrow), a.wld, m - oe, Fq, bne_dev, kadd, pk_w, q0, t0, nullptr, 0};
           PackArgs pl{a.a + wd * m + oe, m, p - oe, Fq, bne_dev, kadd, pk_l, q0, t0, nullptr, 0};
-          launch_pack(h, dim3((unsigned)nqb, blocks_for(m - oe, TC_BM)), pw);
-          launch_pack(h, dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), pl);
-          h->launches += 2;
+          launch_pack(h, st, dim3((unsigned)nqb, blocks_for(m - oe, TC_BM)), pw);
+          launch_pack(h, st, dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), pl);
+          cx.launches += 2;
         }
         int rc;
         if (flush) {
           // the window is full: every trailing column takes it (one GEMM)
-          rc = launch_window_gemm(h, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
+          rc = launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
           if (rc) return rc;
         } else {
           // near field: the next outer block's columns (oe + nb <= p here) take the whole window
-          rc = launch_window_gemm(h, a, m, oe, oe + ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
+          rc = launch_window_gemm(h, cx, a, m, oe, oe + ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
           if (rc) return rc;
           // far field: only if this block delayed columns (decided on the device)
           if (oe + nb < p) {
-            rc = launch_window_gemm(h, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, bne_dev,
+            rc = launch_window_gemm(h, cx, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, bne_dev,
                                     (int32_t)bcols);
             if (rc) return rc;
           }
         }
-        mark(h, RVG_PART_LF_SYRK);
+        mk(RVG_PART_LF_SYRK);
       }
     }
     k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level);
-    h->launches++;
-    mark(h, RVG_PART_LF_OUTER);
+    cx.launches++;
+    mk(RVG_PART_LF_OUTER);
     CK(cudaGetLastError());
     int32_t g = 0;
     CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
     {
       double ts0 = now_ms();
       CK(cudaStreamSynchronize(st));
-      h->host_sync_ms += now_ms() - ts0;
+      cx.sync_ms += now_ms() - ts0;
     }
-    mark_flush(h);
-    mark(h, -1);
+    if (cx.marks) mark_flush(h);
+    mk(-1);
     const int64_t bne = g - gne;
     if (two_level && oe < p) {
       const bool delayed = bne < bcols;
       const double K = (double)(kadd + bne);
       if (flush) {
-        h->syrk_flops += 2.0 * K * lower_entries(oe, m, oe, p);
+        cx.syrk_flops += 2.0 * K * lower_entries(oe, m, oe, p);
       } else {
-        h->syrk_flops += 2.0 * K * lower_entries(oe, m, oe, oe + ncol);
-        if (oe + nb < p && delayed) h->syrk_flops += 2.0 * K * lower_entries(oe + nb, m, oe + nb, p);
+        cx.syrk_flops += 2.0 * K * lower_entries(oe, m, oe, oe + ncol);
+        if (oe + nb < p && delayed) cx.syrk_flops += 2.0 * K * lower_entries(oe + nb, m, oe + nb, p);
       }
       if (flush || delayed) {  // every column is up to date: a new, empty window
         wd = g;
@@ -1524,10 +1543,78 @@ int factor_large_front(rvg_handle* h, int32_t s, const Arenas& Ar, const DevOpts
     rem -= bcols;
   }
   k_lf_finish<<<1, 32, 0, st>>>(a, h->d_fronts, s);
-  h->launches++;
-  mark(h, RVG_PART_LF_SETUP);
+  cx.launches++;
+  mk(RVG_PART_LF_SETUP);
   CK(cudaGetLastError());
   return RVG_OK;
+}
+
+// The large fronts of one wave: one after another on the handle's stream when
+// there is one (profiling marks on), otherwise up to LF_CONCURRENT at a time,
+// each context's fronts in turn on its own host thread and stream, ordered
+// after the wave's assembly and before what follows by events.
+int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Arenas& A, const DevOpts& dop) {
+  if (ids.empty()) return RVG_OK;
+  if (h->lfx.empty()) {
+    h->lfx.resize(1);
+    h->lfx[0].st = h->st;
+    h->lfx[0].lf = h->d_lf;
+  }
+  auto fold = [&](LfCtx& c) {
+    h->launches += c.launches;
+    h->host_sync_ms += c.sync_ms;
+    h->syrk_flops += c.syrk_flops;
+    c.launches = 0; c.sync_ms = 0; c.syrk_flops = 0;
+  };
+  const int nc = (int)std::min<size_t>(ids.size(), LF_CONCURRENT);
+  while ((int)h->lfx.size() < nc) {  // grown before any reference into lfx is taken
+    LfCtx c;
+    c.own = true;
+    CK(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
+    CK(cudaMalloc((void**)&c.lf, sizeof(LFState)));
+    h->lfx.push_back(c);
+  }
+  LfCtx& c0 = h->lfx[0];
+  c0.wpack = h->wpack; c0.wpack_cap = h->wpack_cap;
+  int rc = RVG_OK;
+  if (nc == 1) {
+    c0.marks = true;
+    for (int32_t s : ids)
+      if ((rc = factor_large_front(h, c0, s, A, dop))) break;
+    h->wpack = c0.wpack; h->wpack_cap = c0.wpack_cap;
+    fold(c0);
+    return rc;
+  }
+  mark(h, -1);
+  cudaEvent_t ready;
+  CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  CK(cudaEventRecord(ready, h->st));
+  for (int t = 1; t < nc; ++t) CK(cudaStreamWaitEvent(h->lfx[t].st, ready, 0));
+  std::vector<int> rcs(nc, RVG_OK);
+  std::vector<std::string> errs(nc);
+  auto work = [&](int t) {
+    cudaSetDevice(h->device);
+    LfCtx& c = h->lfx[t];
+    c.marks = false;
+    for (size_t i = t; i < ids.size(); i += nc)
+      if ((rcs[t] = factor_large_front(h, c, ids[i], A, dop))) { errs[t] = g_err; break; }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nc; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto& x : th) x.join();
+  h->wpack = c0.wpack; h->wpack_cap = c0.wpack_cap;
+  for (int t = 1; t < nc; ++t) {
+    CK(cudaEventRecord(ready, h->lfx[t].st));
+    CK(cudaStreamWaitEvent(h->st, ready, 0));
+  }
+  CK(cudaEventDestroy(ready));
+  mark(h, RVG_PART_OTHER);
+  for (int t = 0; t < nc; ++t) {
+    fold(h->lfx[t]);
+    if (rcs[t] && !rc) { rc = rcs[t]; set_error(errs[t]); }
+  }
+  return rc;
 }
 
 // The numeric factorization proper: the level-set schedule of
@@ -1708,8 +1795,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       k_aptp<<<(unsigned)aptp_ids.size(), NT, 0, st>>>((const int32_t*)(D + o_aptp), (int)aptp_ids.size(),
                                                         h->d_fronts, A, dop);
     mark(h, RVG_PART_APTP);
-    for (int32_t s : large_ids)
-      if ((rc = factor_large_front(h, s, A, dop))) return rc;
+    if ((rc = factor_large_fronts(h, large_ids, A, dop))) return rc;
     CK(cudaEventRecord(h->ev[3], st));
     // ---- contribution GEMM (fronts with nothing eliminated skip inside)
     mark(h, -1);
@@ -2151,7 +2237,7 @@ rvg_status rvg_solve(rvg_handle* h, double* rhs, int64_t nrhs, int64_t ldb) {
 // column's scaled backward error is <= tol (or max_iter corrections); bwd[j]
 // is column j's final error.
 static int refine_common(rvg_handle* h, const double* d_b, double* d_x, int64_t nrhs, int64_t ld, double tol,
-                         int32_t max_iter, int32_t* iters, double* bwd) {
+                         int32_t max_iter, int32_t* iters, double* bwd, bool* stalled = nullptr) {
   const int64_t n = h->P.n;
   cudaStream_t st = h->st;
   int rc = ensure(h->d_ref, h->ref_cap, (size_t)((nrhs + 1) * n + 3 * nrhs + 8), st);
@@ -2164,6 +2250,8 @@ static int refine_common(rvg_handle* h, const double* d_b, double* d_x, int64_t 
   else CK(cudaMemcpy2DAsync(d_x, ld * 8, d_b, ld * 8, n * 8, nrhs, cudaMemcpyDeviceToDevice, st));
   if ((rc = solve_common(h, d_x, nrhs, ld))) return rc;
   int it = 0;
+  double prev_worst = 0;
+  if (stalled) *stalled = false;
   const dim3 g((unsigned)blocks_for(n, 256), (unsigned)nrhs), gn(64, (unsigned)nrhs);
   for (;;) {
     k_residual<<<g, 256, 0, st>>>(h->d_colptr, h->d_rowidx, h->d_vals, d_x, d_b, r, n, ld, n);
@@ -2172,13 +2260,18 @@ static int refine_common(rvg_handle* h, const double* d_b, double* d_x, int64_t 
     CK(cudaMemcpyAsync(hn, nrm, (size_t)(3 * nrhs) * 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     bool done = true;
+    double worst = 0;
     for (int64_t j = 0; j < nrhs; ++j) {
       const double denom = h->a_fro * std::sqrt(hn[3 * j + 1]) + std::sqrt(hn[3 * j + 2]);
       const double e = denom == 0 ? 0.0 : std::sqrt(hn[3 * j]) / denom;
       if (bwd) bwd[j] = e;
       if (!(e <= tol)) done = false;
+      worst = std::max(worst, e);
     }
     if (done || it >= max_iter) break;
+    // with `stalled` given: stop once a correction no longer halves the error
+    if (stalled && it > 0 && !(worst <= 0.5 * prev_worst)) { *stalled = true; break; }
+    prev_worst = worst;
     if ((rc = solve_common(h, r, nrhs, n))) return rc;
     k_axpy1<<<g, 256, 0, st>>>(d_x, r, n, ld, n);
     ++it;
@@ -2196,7 +2289,7 @@ static int refine_common(rvg_handle* h, const double* d_b, double* d_x, int64_t 
 // restart and when the rotated residual estimate reaches tol, is <= tol, or
 // after max_iter preconditioned products; *iters counts them (one solve each).
 static int gmres_common(rvg_handle* h, const double* d_b, double* d_x, double tol, int32_t max_iter, int32_t restart,
-                        int32_t* iters, double* bwd) {
+                        int32_t* iters, double* bwd, bool x_given = false) {
   const int64_t n = h->P.n;
   cudaStream_t st = h->st;
   const int m = restart;
@@ -2229,8 +2322,10 @@ static int gmres_common(rvg_handle* h, const double* d_b, double* d_x, double to
     e = denom == 0 ? 0.0 : rn / denom;
     return RVG_OK;
   };
-  CK(cudaMemcpyAsync(d_x, d_b, n * 8, cudaMemcpyDeviceToDevice, st));
-  if ((rc = solve_common(h, d_x, 1, n))) return rc;  // x0 = M^-1 b
+  if (!x_given) {
+    CK(cudaMemcpyAsync(d_x, d_b, n * 8, cudaMemcpyDeviceToDevice, st));
+    if ((rc = solve_common(h, d_x, 1, n))) return rc;  // x0 = M^-1 b
+  }
   int it = 0;
   double e = 0, beta = 0;
   std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
@@ -2295,6 +2390,60 @@ static int gmres_common(rvg_handle* h, const double* d_b, double* d_x, double to
   if ((rc = device_wait_status(h))) return rc;
   if (iters) *iters = it;
   if (bwd) *bwd = e;
+  return RVG_OK;
+}
+
+// Iterative refinement while every correction at least halves the backward
+// error, then GMRES-IR from the refined x: the cheap method when it converges,
+// the robust one when the factor's error times the condition number is too
+// large for it.  *method: 0 refinement alone, 1 escalated to GMRES-IR;
+// *iters: the solves after the first one (corrections + GMRES products).
+static int auto_common(rvg_handle* h, const double* d_b, double* d_x, double tol, int32_t max_iter, int32_t* iters,
+                       double* bwd, int32_t* method) {
+  bool stalled = false;
+  int32_t it1 = 0, it2 = 0;
+  double e = 0;
+  int rc = refine_common(h, d_b, d_x, 1, h->P.n, tol, std::min<int32_t>(max_iter, 10), &it1, &e, &stalled);
+  if (rc) return rc;
+  if (method) *method = 0;
+  if (!(e <= tol) && it1 < max_iter) {
+    if ((rc = gmres_common(h, d_b, d_x, tol, max_iter - it1, 30, &it2, &e, true))) return rc;
+    if (method) *method = 1;
+  }
+  if (iters) *iters = it1 + it2;
+  if (bwd) *bwd = e;
+  return RVG_OK;
+}
+
+rvg_status rvg_solve_auto_device(rvg_handle* h, const double* d_rhs, double* d_x, double tol, int32_t max_iter,
+                                 int32_t* iters, double* bwd_err, int32_t* method) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  if (h->P.n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; if (method) *method = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  int rc = auto_common(h, d_rhs, d_x, tol, max_iter, iters, bwd_err, method);
+  h->t_solve = now_ms() - t0;
+  return (rvg_status)rc;
+}
+
+rvg_status rvg_solve_auto(rvg_handle* h, const double* rhs, double* x, double tol, int32_t max_iter, int32_t* iters,
+                          double* bwd_err, int32_t* method) {
+  if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored) { set_error("factor() must be called before solve()"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  const int64_t n = h->P.n;
+  if (n == 0) { if (iters) *iters = 0; if (bwd_err) *bwd_err = 0; if (method) *method = 0; return RVG_OK; }
+  CK(cudaSetDevice(h->device));
+  double t0 = now_ms();
+  double* d = nullptr;
+  CK(cudaMallocAsync((void**)&d, 2 * n * 8, h->st));
+  CK(cudaMemcpyAsync(d, rhs, n * 8, cudaMemcpyHostToDevice, h->st));
+  int rc = auto_common(h, d, d + n, tol, max_iter, iters, bwd_err, method);
+  if (rc) return (rvg_status)rc;
+  CK(cudaMemcpyAsync(x, d + n, n * 8, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaFreeAsync(d, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->t_solve = now_ms() - t0;
   return RVG_OK;
 }
 
@@ -2599,6 +2748,8 @@ rvg_status rvg_trim(rvg_handle* h, int32_t what) {
     RVG_TRIM(h->d_x, h->x_cap);
     RVG_TRIM(h->d_ref, h->ref_cap);
     RVG_TRIM(h->d_gm, h->gm_cap);
+    for (size_t t = 1; t < h->lfx.size(); ++t) RVG_TRIM(h->lfx[t].wpack, h->lfx[t].wpack_cap);
+    if (!h->lfx.empty()) { h->lfx[0].wpack = nullptr; h->lfx[0].wpack_cap = 0; }
     RVG_TRIM(h->d_stage, h->stage_cap);
     h->cb_free.clear();
   }
@@ -2640,6 +2791,12 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
   fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
+  for (size_t t = 1; t < h->lfx.size(); ++t) {
+    LfCtx& c = h->lfx[t];
+    fr(c.wpack);
+    if (c.lf) cudaFree(c.lf);
+    if (c.own && c.st) { cudaStreamSynchronize(c.st); cudaStreamDestroy(c.st); }
+  }
   fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
@@ -2651,6 +2808,7 @@ void rvg_destroy(rvg_handle* h) {
   for (auto e : h->mk_pool) cudaEventDestroy(e);
   for (auto& e : h->ev) if (e) cudaEventDestroy(e);
   delete h;
+  cudaGetLastError();  // nothing of this handle's teardown is left for the caller's next call to report
 }
 
 }  // extern "C"
