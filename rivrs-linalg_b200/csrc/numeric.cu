@@ -210,6 +210,9 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
   double(*T)[IBMAX + 1] = sh.T;
   __shared__ int s_kind;
   __shared__ double s_d[3];
+  // column maxima of the trailing triangle after each update (bits of |v| and the (column, row) key of the
+  // first maximum in row order), left by the updating warps for the next step's pivot search
+  __shared__ unsigned s_chi[IBMAX], s_clo[IBMAX], s_ckey[IBMAX];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid < IBMAX) { sh.bperm[tid] = tid; sh.bdt[tid] = PT_DELAYED; sh.bdd[tid] = 0; sh.bdo[tid] = 0; }
   __syncthreads();
@@ -226,35 +229,62 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
     if (lane > j && lane < bs) { double t = T[lane][i]; T[lane][i] = T[lane][j]; T[lane][j] = t; }
     __syncwarp();
   };
+  // each updated column j0 + 8q of this warp: the maximum of |T[i][j]| over rows j <= i < bs (the lanes'
+  // new values) and the smallest row holding it, as the scan in row order finds them (entries that are not
+  // > 0, NaN included, never count)
+  auto col_maxima = [&](int j0, int i, const double* nvq) {
+#pragma unroll
+    for (int q = 0; q < IBMAX / 8; ++q) {
+      const int j = j0 + 8 * q;
+      if (j < bs) {  // uniform over the warp
+        const double a = (i >= j && i < bs) ? fabs(nvq[q]) : 0.0;
+        const bool pos = a > 0.0;
+        const unsigned long long bits = pos ? (unsigned long long)__double_as_longlong(a) : 0ull;
+        const unsigned h1 = (unsigned)(bits >> 32), l1 = (unsigned)bits;
+        const unsigned mh = __reduce_max_sync(0xffffffffu, h1);
+        const unsigned ml = __reduce_max_sync(0xffffffffu, h1 == mh ? l1 : 0u);
+        const unsigned kk = __reduce_min_sync(0xffffffffu, (pos && h1 == mh && l1 == ml) ? (unsigned)(j * 64 + i)
+                                                                                          : 0xffffffffu);
+        if (lane == 0) { s_chi[j] = mh; s_clo[j] = ml; s_ckey[j] = kk; }
+      }
+    }
+  };
   int k = 0;
   for (;;) {
     const int cur = k;
     if (warp == 0) {
       int kind = 0;  // 0 stop, 1 1x1 (+ rank-1 update), 2 2x2 (+ rank-2 update)
       if (cur < bs) {
-        // arg-max over the lower triangle of [cur, bs)^2
-        double bv = 0.0;
-        unsigned key = 0xffffffffu;
+        // arg-max over the lower triangle of [cur, bs)^2: lane = column, its first maximum in row order
+        unsigned hi = 0, lo = 0, key = 0xffffffffu;
         if (lane >= cur && lane < bs) {
-          double col[IBMAX];
+          if (cur == 0) {  // the first step scans the block
+            double col[IBMAX];
 #pragma unroll
-          for (int i = 0; i < IBMAX; ++i) col[i] = T[i][lane];
-          // four interleaved scans (rows i mod 4), each keeping its first maximum,
-          // merged to the first maximum in row order
-          double b4[4] = {0.0, 0.0, 0.0, 0.0};
-          unsigned k4[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+            for (int i = 0; i < IBMAX; ++i) col[i] = T[i][lane];
+            // four interleaved scans (rows i mod 4), each keeping its first maximum,
+            // merged to the first maximum in row order
+            double b4[4] = {0.0, 0.0, 0.0, 0.0};
+            unsigned k4[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
 #pragma unroll
-          for (int i = 0; i < IBMAX; ++i)
-            if (i >= lane && i < bs) {
-              const double v = fabs(col[i]);
-              if (v > b4[i & 3]) { b4[i & 3] = v; k4[i & 3] = (unsigned)(lane * 64 + i); }
-            }
+            for (int i = 0; i < IBMAX; ++i)
+              if (i >= lane && i < bs) {
+                const double v = fabs(col[i]);
+                if (v > b4[i & 3]) { b4[i & 3] = v; k4[i & 3] = (unsigned)(lane * 64 + i); }
+              }
+            double bv = 0.0;
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (b4[q] > bv || (b4[q] == bv && k4[q] < key)) { bv = b4[q]; key = k4[q]; }
+            for (int q = 0; q < 4; ++q)
+              if (b4[q] > bv || (b4[q] == bv && k4[q] < key)) { bv = b4[q]; key = k4[q]; }
+            const unsigned long long bits = (unsigned long long)__double_as_longlong(bv);  // bv >= 0
+            hi = (unsigned)(bits >> 32);
+            lo = (unsigned)bits;
+          } else {  // left by the previous step's update
+            hi = s_chi[lane];
+            lo = s_clo[lane];
+            key = s_ckey[lane];
+          }
         }
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(bv);  // bv >= 0: bits order as values
-        const unsigned hi = (unsigned)(bits >> 32), lo = (unsigned)bits;
         const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
         const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
         key = __reduce_min_sync(0xffffffffu, (hi == mhi && lo == mlo) ? key : 0xffffffffu);
@@ -320,6 +350,7 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
     const int kind = s_kind;
     if (kind == 0) break;
     const int i = lane;
+    double nv[IBMAX / 8] = {};  // the lane's (row's) new entries in the warp's columns
     if (kind == 1) {  // T[i][j] -= T[i][cur] (T[j][cur] d), cur < j <= i
       const double dkk = s_d[0];
       if (i > cur && i < bs) {
@@ -335,9 +366,13 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
 #pragma unroll
         for (int q = 0; q < IBMAX / 8; ++q) {
           const int j = cur + 1 + warp + 8 * q;
-          if (j <= i) T[i][j] = __dsub_rn(tij[q], __dmul_rn(lc, __dmul_rn(lj[q], dkk)));
+          if (j <= i) {
+            nv[q] = __dsub_rn(tij[q], __dmul_rn(lc, __dmul_rn(lj[q], dkk)));
+            T[i][j] = nv[q];
+          }
         }
       }
+      col_maxima(cur + 1 + warp, i, nv);
       k += 1;
     } else {  // rank-2 over cur + 2 <= j <= i
       const double a11 = s_d[0], a21 = s_d[1], a22 = s_d[2];
@@ -358,10 +393,12 @@ __device__ void cta_block_factor(CtaShared& sh, int bs, double small) {
           if (j <= i) {
             const double w1 = __dadd_rn(__dmul_rn(l1[q], a11), __dmul_rn(l2[q], a21));
             const double w2 = __dadd_rn(__dmul_rn(l1[q], a21), __dmul_rn(l2[q], a22));
-            T[i][j] = __dsub_rn(tij[q], __dadd_rn(__dmul_rn(c1, w1), __dmul_rn(c2, w2)));
+            nv[q] = __dsub_rn(tij[q], __dadd_rn(__dmul_rn(c1, w1), __dmul_rn(c2, w2)));
+            T[i][j] = nv[q];
           }
         }
       }
+      col_maxima(cur + 2 + warp, i, nv);
       k += 2;
     }
     __syncthreads();

@@ -218,3 +218,44 @@ def test_large_front_path_nfs_gemm(rv, orc):
     solver, ref, b = run_both(rv, orc, s, large_front_threshold=300)
     assert solver.inertia() == s.inertia
     assert_parity(rv, s, solver, ref, b)
+
+
+@pytest.mark.parametrize("case", ["one_pos", "one_neg", "zero2", "zero40", "diag100", "offdiag_only"])
+def test_edge_cases(rv, orc, case):
+    # tiny, zero and structurally trivial matrices: the same pivots, D and inertia as the oracle
+    import scipy.sparse as sp
+    if case == "one_pos":
+        a = sp.csc_matrix(np.array([[4.0]]))
+    elif case == "one_neg":
+        a = sp.csc_matrix(np.array([[-2.5]]))
+    elif case == "zero2":
+        a = sp.csc_matrix((np.zeros(4), (np.array([0, 1, 0, 1]), np.array([0, 0, 1, 1]))), shape=(2, 2))
+    elif case == "zero40":
+        i = np.arange(40)
+        a = sp.csc_matrix((np.zeros(40), (i, i)), shape=(40, 40)) + sp.csc_matrix(
+            (np.zeros(39), (i[1:], i[:-1])), shape=(40, 40))
+        a = a + a.T
+    elif case == "diag100":
+        d = np.random.default_rng(1).standard_normal(100)
+        a = sp.diags(d).tocsc()
+    else:
+        # pure 2x2 coupling, zero diagonal: every pivot a 2x2 block
+        n = 30
+        r = np.arange(0, n, 2)
+        a = sp.csc_matrix((np.ones(n // 2), (r, r + 1)), shape=(n, n))
+        a = a + a.T
+    s = rv.problems.from_scipy(case, a)
+    solver, ref, b = run_both(rv, orc, s)
+    assert_parity(rv, s, solver, ref, b)
+    solver.close()
+
+
+def test_empty_system(rv):
+    import scipy.sparse as sp
+    s = rv.problems.from_scipy("empty", sp.csc_matrix((0, 0)))
+    solver = rv.SparseLDLT.analyze(s)
+    solver.factor()
+    x = solver.solve(np.zeros(0))
+    assert x.shape == (0,)
+    assert solver.inertia() == (0, 0, 0)
+    solver.close()
