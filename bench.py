@@ -575,6 +575,28 @@ def main():
              "blocked_ms": timed(lambda: solver.solve_device(rhs8.data_ptr(), 8, s.n)),
              "one_at_a_time_ms": timed(lambda: [solver.solve_device(rhs8[r].data_ptr(), 1, s.n) for r in range(8)])}
 
+    # refactorization (factor only, same pattern and values): dynamic against replayed as one CUDA graph
+    def factor_times(o, reps):
+        solver._ensure_handle(o)  # other options: a new handle, with a stream of its own
+        fst = torch.cuda.ExternalStream(solver.stream())
+        out, launches = [], []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(fst)
+            solver.factor_device(d_vals.data_ptr(), d_scal.data_ptr() if d_scal is not None else None, o)
+            e1.record(fst)
+            e1.synchronize()
+            out.append(e0.elapsed_time(e1) * 1e-3)
+            launches.append(solver.profile()["factor_launches"])
+        return out, launches
+    import dataclasses
+    o_dyn = chosen["opts"]
+    t_dyn, l_dyn = factor_times(o_dyn, 3)
+    t_rep, l_rep = factor_times(dataclasses.replace(o_dyn, graph_refactor=True), 5)  # records, captures, replays
+    graph_refactor = {"form": chosen_key, "dynamic_factor_s": statistics.mean(t_dyn),
+                      "dynamic_launches": l_dyn[-1], "replay_factor_s": statistics.mean(t_rep[2:]),
+                      "first_capture_s": t_rep[1], "replayed": all(x == 1 for x in l_rep[2:])}
+    solver._ensure_handle(o_dyn)
     work = solver.work()
     # the HBM-bound parts against the measured copy bandwidth: one solve (multi_rhs_solve's single-RHS
     # calls; the solve reads the factor once per RHS) and the assembly of the chosen form's profiled step
@@ -664,6 +686,7 @@ def main():
             "factor_gflops": full_flops / t_step / 1e9,
             "multi_rhs_solve": multi,
             "hbm_bound_parts": hbm_parts,
+            "graph_refactor": graph_refactor,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(s.values.nbytes + b.nbytes),
                     "d2h_bytes_per_step": int(b.nbytes)},
             "gpu_launches": int(launches // max(args.steps, 1)),

@@ -79,6 +79,17 @@ typedef struct {
    * (kind::f16, about 16 bits: half the operand bytes and twice the tensor
    * rate, so more refinement steps).  Default 0. */
   int32_t mixed_operands;
+  /* Refactorization as one CUDA graph launch, no reference counterpart
+   * (the reference's refactor, solver.rs:335-341, reruns the numeric phase).
+   * 1 = a factorization of the same handle after a dynamic one captures the
+   * whole numeric phase, with the host decisions (front sizes, eliminated
+   * counts, large fronts' progress per outer block) taken from the dynamic
+   * one, into a CUDA graph, and later factorizations launch that graph.  Checks
+   * on the device compare the pivoting the new values give with the recorded
+   * one; when they differ (other delays or 2x2 pivots) the factorization is
+   * redone dynamically, which records anew.  Results are the dynamic path's,
+   * bit for bit.  Default 0. */
+  int32_t graph_refactor;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */

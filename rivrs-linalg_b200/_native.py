@@ -30,7 +30,8 @@ class Options(C.Structure):
                 ("inner_block_size", i64), ("nemin", i64), ("small_leaf_threshold", i64),
                 ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64),
                 ("precision", C.c_int32), ("mixed_flush", C.c_int32),
-                ("mixed_tile_cols", C.c_int32), ("mixed_operands", C.c_int32)]
+                ("mixed_tile_cols", C.c_int32), ("mixed_operands", C.c_int32),
+                ("graph_refactor", C.c_int32)]
 
 
 class Stats(C.Structure):

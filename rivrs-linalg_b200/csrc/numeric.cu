@@ -942,6 +942,29 @@ __global__ void k_get_counts(const int32_t* ids, int n, const DFront* F, int32_t
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) { const DFront& f = F[ids[i]]; out[3 * i] = f.ne; out[3 * i + 1] = f.n1; out[3 * i + 2] = f.n2; }
 }
+// Refactorization replay checks: the counts (and a large front's progress)
+// the captured schedule assumed.  On a difference the flag is raised and the
+// recorded value put in place of the computed one, so that every later launch
+// of the graph indexes the fronts exactly as the recorded factorization did
+// (the parents' sizes and delayed-row offsets were laid out from the record);
+// the factor is then discarded and recomputed dynamically.
+__global__ void k_check_counts(const int32_t* ids, int n, DFront* F, const int32_t* rec, int32_t* mismatch) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int s = ids[i];
+  DFront& f = F[s];
+  const int32_t* r = rec + 3 * (int64_t)s;
+  if (f.ne != r[0] || f.n1 != r[1] || f.n2 != r[2]) {
+    atomicExch(mismatch, 1);
+    f.ne = r[0]; f.n1 = r[1]; f.n2 = r[2];
+  }
+}
+__global__ void k_check_gne(LFState* st, int32_t expect, int32_t* mismatch) {
+  if (threadIdx.x == 0 && st->gne != expect) {
+    atomicExch(mismatch, 1);
+    st->gne = expect;
+  }
+}
 
 }  // namespace rvg
 
@@ -1005,6 +1028,20 @@ struct rvg_handle {
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
   bool factored = false;
   bool need_presize = false;                         // arenas released by rvg_trim
+  // refactorization replay (graph_refactor): the host's decisions in the last dynamic factorization
+  bool rec_ok = false;                               // a complete record is available
+  std::vector<int32_t> rec_cnt;                      // per front: eliminated, 1x1 and 2x2 counts
+  std::vector<std::vector<int32_t>> rec_g;           // per large front: eliminated count after each outer block
+  std::vector<size_t> rec_stage;                     // per wave: bytes of the packed launch data
+  int64_t rec_d_used = 0;                            // D entries used
+  bool replay = false;                               // run_factor is being captured into the graph
+  int32_t* d_rec = nullptr; size_t d_rec_cap = 0;    // rec_cnt on the device (for the checks)
+  int32_t* d_mismatch = nullptr;                     // set by a check that sees another decision
+  char* h_stage_all = nullptr; size_t h_stage_all_cap = 0;  // pinned launch data of every wave (replay)
+  std::vector<size_t> stage_off;                     // per wave: its offset in h_stage_all
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  const double* graph_ds = nullptr;                  // the scaling pointer the graph reads
   // measurement
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -1032,7 +1069,7 @@ double now_ms() {
 // to the later mark's kind (a kind < 0 starts a new segment).  Read back
 // after each stream synchronisation.
 void mark(rvg_handle* h, int kind) {
-  if (!h->profiling) return;
+  if (!h->profiling || h->replay) return;
   if (h->mk_used == h->mk_pool.size()) {
     cudaEvent_t e;
     if (cudaEventCreate(&e) != cudaSuccess) return;
@@ -1051,9 +1088,19 @@ void mark_flush(rvg_handle* h) {
   h->mk_used = 0;
 }
 
+// Set while a refactorization graph is captured: every buffer must already be
+// large enough (the capture replays the sizes of the last factorization), so a
+// growth request aborts the capture and the factorization runs dynamically.
+thread_local bool tl_no_alloc = false;
+static int no_alloc_fail() {
+  set_error("refactorization replay would allocate");
+  return RVG_ERR_DEVICE;
+}
+
 template <class T>
 int ensure(T*& p, size_t& cap, size_t need, cudaStream_t st) {
   if (need <= cap && p) return RVG_OK;
+  if (tl_no_alloc) return no_alloc_fail();
   size_t nc = std::max(need, cap + cap / 2);
   if (nc == 0) nc = 1;
   T* np = nullptr;
@@ -1069,6 +1116,7 @@ int ensure(T*& p, size_t& cap, size_t need, cudaStream_t st) {
 
 int ensure_host(char*& p, size_t& cap, size_t need) {
   if (need <= cap && p) return RVG_OK;
+  if (tl_no_alloc) return no_alloc_fail();
   size_t nc = std::max(need, cap + cap / 2);
   if (p) CK(cudaFreeHost(p));
   p = nullptr;
@@ -1079,6 +1127,7 @@ int ensure_host(char*& p, size_t& cap, size_t need) {
 
 int ensure_d_arrays(rvg_handle* h, size_t need) {  // type / diag / off share one capacity
   if (need <= h->d_cap && h->dtype) return RVG_OK;
+  if (tl_no_alloc) return no_alloc_fail();
   size_t nc = std::max(need, h->d_cap + h->d_cap / 2);
   int8_t* t; double *a, *b;
   CK(cudaMallocAsync((void**)&t, nc, h->st));
@@ -1097,6 +1146,7 @@ int ensure_d_arrays(rvg_handle* h, size_t need) {  // type / diag / off share on
 template <class T>
 int ensure_nocopy(T*& p, size_t& cap, size_t need, cudaStream_t st) {
   if (need <= cap && p) return RVG_OK;
+  if (tl_no_alloc) return no_alloc_fail();
   size_t nc = std::max(need, cap + cap / 4);
   if (nc == 0) nc = 1;
   if (p) CK(cudaFreeAsync(p, st));
@@ -1118,6 +1168,7 @@ int cb_alloc(rvg_handle* h, int64_t len, int64_t* off) {
       return RVG_OK;
     }
   }
+  if (tl_no_alloc) return no_alloc_fail();
   // grow: new capacity covers the old one plus the request
   size_t old = h->cb_cap;
   size_t nc = std::max(old + (size_t)len, old + old / 4);
@@ -1301,7 +1352,7 @@ double lower_entries(int64_t r0, int64_t r1, int64_t c0, int64_t c1) {
 // CUDA events around each Schur GEMM launch (profiling): their sum is the
 // GEMM time the measured rate is based on.
 int syrk_ev(rvg_handle* h, bool on = true) {
-  if (!h->profiling || !on) return RVG_OK;
+  if (!h->profiling || !on || h->replay) return RVG_OK;
   if (h->ev_used + 1 > h->ev_pool.size()) {
     for (int i = 0; i < 64; ++i) {
       cudaEvent_t e;
@@ -1461,6 +1512,8 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
   cx.launches++;
   int64_t rem = p, gne = 0;
+  size_t outer = 0;
+  if (!h->replay) h->rec_g[s].clear();
   while (rem > 0) {
     const int64_t bcols = std::min(rem, nb), cs = gne, bm = m - cs, oe = cs + bcols;
     a.cs = cs;
@@ -1553,12 +1606,19 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     mk(RVG_PART_LF_OUTER);
     CK(cudaGetLastError());
     int32_t g = 0;
-    CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
-    {
+    if (h->replay) {  // the progress of the recorded factorization, checked on the device
+      const std::vector<int32_t>& rg = h->rec_g[s];
+      if (outer >= rg.size()) { set_error("refactorization replay: record too short"); return RVG_ERR_DEVICE; }
+      g = rg[outer];
+      k_check_gne<<<1, 32, 0, st>>>(a.st, g, h->d_mismatch);
+    } else {
+      CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
       double ts0 = now_ms();
       CK(cudaStreamSynchronize(st));
       cx.sync_ms += now_ms() - ts0;
+      h->rec_g[s].push_back(g);
     }
+    ++outer;
     if (cx.marks) mark_flush(h);
     mk(-1);
     const int64_t bne = g - gne;
@@ -1603,8 +1663,11 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
     h->syrk_flops += c.syrk_flops;
     c.launches = 0; c.sync_ms = 0; c.syrk_flops = 0;
   };
+  // (a capture forks into the same contexts with the fronts dealt the same way:
+  // the replayed graph runs them concurrently on the buffers the dynamic run sized)
   const int nc = (int)std::min<size_t>(ids.size(), LF_CONCURRENT);
   while ((int)h->lfx.size() < nc) {  // grown before any reference into lfx is taken
+    if (tl_no_alloc) return no_alloc_fail();
     LfCtx c;
     c.own = true;
     CK(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
@@ -1629,12 +1692,16 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
   for (int t = 1; t < nc; ++t) CK(cudaStreamWaitEvent(h->lfx[t].st, ready, 0));
   std::vector<int> rcs(nc, RVG_OK);
   std::vector<std::string> errs(nc);
+  const bool no_alloc = tl_no_alloc;
   auto work = [&](int t) {
     cudaSetDevice(h->device);
+    const bool was = tl_no_alloc;
+    tl_no_alloc = no_alloc;
     LfCtx& c = h->lfx[t];
     c.marks = false;
     for (size_t i = t; i < ids.size(); i += nc)
       if ((rcs[t] = factor_large_front(h, c, ids[i], A, dop))) { errs[t] = g_err; break; }
+    tl_no_alloc = was;
   };
   std::vector<std::thread> th;
   for (int t = 1; t < nc; ++t) th.emplace_back(work, t);
@@ -1653,6 +1720,8 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
   }
   return rc;
 }
+
+int finish_factor(rvg_handle* h, int64_t d_used);
 
 // The numeric factorization proper: the level-set schedule of
 // factor_tree_levelset (numeric.rs:1957-2163) with every front of a wave
@@ -1683,6 +1752,11 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   h->syrk_launches = 0;
   h->launches = 0;
   h->peak_bytes = 0;
+  if (!h->replay) {
+    h->rec_ok = false;
+    h->rec_g.assign(ns, {});
+    h->rec_stage.assign(P.waves.size(), 0);
+  }
   CK(cudaEventRecord(h->ev[0], st));
   for (size_t w = 0; w < P.waves.size(); ++w) {
     const std::vector<int64_t>& wave = P.waves[w];
@@ -1797,9 +1871,17 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     size_t o_w = pk.add(witems), o_g = pk.add(gitems);
     size_t o_cnt = pk.add(std::vector<int32_t>(3 * (size_t)nw + 4, 0));
     if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size(), st))) return rc;
-    if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size()))) return rc;
-    std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
-    CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
+    char* hs;
+    if (h->replay) {  // a slice of its own: the graph copies from it at every replay
+      if (pk.buf.size() != h->rec_stage[w]) { set_error("refactorization replay: launch data differ"); return RVG_ERR_DEVICE; }
+      hs = h->h_stage_all + h->stage_off[w];
+    } else {
+      if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size()))) return rc;
+      hs = h->h_stage;
+      h->rec_stage[w] = pk.buf.size();
+    }
+    std::memcpy(hs, pk.buf.data(), pk.buf.size());
+    CK(cudaMemcpyAsync(h->d_stage, hs, pk.buf.size(), cudaMemcpyHostToDevice, st));
     char* D = h->d_stage;
     const int32_t* d_ids = (const int32_t*)(D + o_ids);
     // ---- descriptors
@@ -1853,7 +1935,25 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     }
     CK(cudaEventRecord(h->ev[4], st));
     CK(cudaGetLastError());
-    // ---- eliminated counts back to the host
+    // ---- eliminated counts back to the host (replay: the recorded ones, checked on the device)
+    if (h->replay) {
+      k_check_counts<<<blocks_for(nw, 128), 128, 0, st>>>(d_ids, nw, h->d_fronts, h->d_rec, h->d_mismatch);
+      CK(cudaGetLastError());
+      for (int i = 0; i < nw; ++i) {
+        DFront& f = h->h_fronts[wave[i]];
+        const int32_t* r = &h->rec_cnt[3 * (size_t)wave[i]];
+        f.ne = r[0]; f.n1 = r[1]; f.n2 = r[2];
+      }
+      for (int64_t s : cb_syrk_fronts) {
+        const DFront& f = h->h_fronts[s];
+        h->syrk_flops += 2.0 * (double)f.ne * (double)f.nfs * (double)(f.nfs + 1) / 2.0;
+      }
+      int64_t last = -1;
+      for (int64_t s : wave) if (P.sn[s].parent >= 0) last = std::max(last, P.height[P.sn[s].parent]);
+      cb_release_at[w] = last;
+      panel_used += panel_need; idx_used += idx_need; d_used += d_need;
+      continue;
+    }
     k_get_counts<<<blocks_for(nw, 128), 128, 0, st>>>(d_ids, nw, h->d_fronts, (int32_t*)(D + o_cnt));
     if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4) * 4))) return rc;
     CK(cudaMemcpyAsync(h->h_counts, D + o_cnt, (size_t)3 * nw * 4, cudaMemcpyDeviceToHost, st));
@@ -1899,12 +1999,34 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   for (size_t w = 0; w < cb_block.size(); ++w)
     if (cb_block[w] >= 0) { cb_release(h, cb_block[w], cb_len[w]); cb_block[w] = -1; }
   CK(cudaEventRecord(h->ev[5], st));
+  if (h->replay) {
+    if (d_used != h->rec_d_used) { set_error("refactorization replay: sizes differ"); return RVG_ERR_DEVICE; }
+    return RVG_OK;  // captured; the statistics follow each replay (finish_factor)
+  }
+  h->factor_launches = h->launches;
+  h->host_total_ms = now_ms() - t_start;
+  h->rec_cnt.assign(3 * ns, 0);
+  for (int64_t s = 0; s < ns; ++s) {
+    const DFront& f = h->h_fronts[s];
+    h->rec_cnt[3 * s] = f.ne; h->rec_cnt[3 * s + 1] = f.n1; h->rec_cnt[3 * s + 2] = f.n2;
+  }
+  h->rec_d_used = d_used;
+  h->t_assembly = t_asm; h->t_kernel = t_ker; h->t_gemm = t_gem;
+  rc = finish_factor(h, d_used);
+  if (rc) return rc;
+  h->rec_ok = true;
+  return RVG_OK;
+}
+
+// Host side of the end of a factorization (dynamic or replayed): the total
+// time, the Schur GEMM time of the profiling events, the aggregate statistics.
+int finish_factor(rvg_handle* h, int64_t d_used) {
+  cudaStream_t st = h->st;
+  const int64_t ns = (int64_t)h->P.sn.size();
   CK(cudaStreamSynchronize(st));
   float tot = 0;
   cudaEventElapsedTime(&tot, h->ev[0], h->ev[5]);
-  h->t_assembly = t_asm; h->t_kernel = t_ker; h->t_gemm = t_gem; h->t_factor = tot;
-  h->factor_launches = h->launches;
-  h->host_total_ms = now_ms() - t_start;
+  h->t_factor = tot;
   if (h->profiling)
     for (size_t e = 0; e + 1 < h->ev_used; e += 2) {
       float ms = 0;
@@ -1954,6 +2076,7 @@ void rvg_default_options(rvg_options* o) {
   o->mixed_flush = 4;
   o->mixed_tile_cols = 256;
   o->mixed_operands = 0;
+  o->graph_refactor = 0;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347
@@ -2064,6 +2187,89 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   return RVG_OK;
 }
 
+static int device_wait_status(rvg_handle* h);
+
+static void drop_graph(rvg_handle* h) {
+  if (h->gexec) cudaGraphExecDestroy(h->gexec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->gexec = nullptr;
+  h->graph = nullptr;
+}
+
+// Refactorization as one CUDA graph launch.  The first call after a dynamic
+// factorization captures run_factor with every host decision taken from that
+// factorization's record (front sizes, eliminated counts, the large fronts'
+// progress per outer block) and the launch data of each wave in a pinned slice
+// of its own; device checks compare what the replayed factorization actually
+// eliminated with the record.  Later calls launch the graph.  *done = false
+// (and the graph dropped) when the checks saw another decision, when a buffer
+// would have to grow, or when capture fails: the caller then factors
+// dynamically, which records again.  The results are the dynamic path's.
+static int replay_factor(rvg_handle* h, const double* ds, bool* done) {
+  *done = false;
+  cudaStream_t st = h->st;
+  if (h->gexec && h->graph_ds != ds) drop_graph(h);
+  if (!h->gexec) {
+    // device copy of the recorded counts, the mismatch word, the pinned launch data
+    const size_t nc = h->rec_cnt.size();
+    int rc;
+    if ((rc = ensure(h->d_rec, h->d_rec_cap, std::max<size_t>(nc, 1), st))) return rc;
+    if (!h->d_mismatch) CK(cudaMalloc((void**)&h->d_mismatch, sizeof(int32_t)));
+    if (nc) CK(cudaMemcpyAsync(h->d_rec, h->rec_cnt.data(), nc * 4, cudaMemcpyHostToDevice, st));
+    h->stage_off.assign(h->rec_stage.size(), 0);
+    size_t tot = 0;
+    for (size_t w = 0; w < h->rec_stage.size(); ++w) { h->stage_off[w] = tot; tot += (h->rec_stage[w] + 255) & ~size_t(255); }
+    if ((rc = ensure_host(h->h_stage_all, h->h_stage_all_cap, std::max<size_t>(tot, 1)))) return rc;
+    CK(cudaStreamSynchronize(st));
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    h->replay = true;
+    tl_no_alloc = true;
+    rc = run_factor(h, h->d_vals, ds);
+    tl_no_alloc = false;
+    h->replay = false;
+    const cudaError_t ec = cudaStreamEndCapture(st, &g);
+    if (rc || ec != cudaSuccess || !g) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      h->rec_ok = false;
+      return RVG_OK;  // not replayable: factor dynamically
+    }
+    if (cudaGraphInstantiate(&h->gexec, g, 0) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      cudaGetLastError();
+      h->gexec = nullptr;
+      h->rec_ok = false;
+      return RVG_OK;
+    }
+    h->graph = g;
+    h->graph_ds = ds;
+  }
+  CK(cudaMemsetAsync(h->d_mismatch, 0, sizeof(int32_t), st));
+  const double t0 = now_ms();
+  h->ev_used = 0;  // no per-launch events inside the graph
+  CK(cudaEventRecord(h->ev[0], st));  // (the records inside the capture only ordered the capture)
+  CK(cudaGraphLaunch(h->gexec, st));
+  CK(cudaEventRecord(h->ev[5], st));
+  int32_t mis = 0;
+  CK(cudaMemcpyAsync(&mis, h->d_mismatch, 4, cudaMemcpyDeviceToHost, st));
+  int rc = finish_factor(h, h->rec_d_used);  // synchronises
+  if (rc) return rc;
+  if ((rc = device_wait_status(h))) return rc;
+  h->host_total_ms = now_ms() - t0;
+  for (double& v : h->part_ms) v = 0;
+  if (mis) {  // another decision than the recorded one: this factor is not valid
+    h->factored = false;
+    drop_graph(h);
+    h->rec_ok = false;
+    return RVG_OK;
+  }
+  h->factor_launches = 1;
+  h->host_sync_ms = 0;
+  *done = true;
+  return RVG_OK;
+}
+
 static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
   int rc;
   if (h->need_presize) {  // after rvg_trim: the arenas at their delay-free size again
@@ -2072,8 +2278,15 @@ static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
   }
   // the refinement needs the unfactored values and ||A||_F
   if (dv != h->d_vals && h->nnz) CK(cudaMemcpyAsync(h->d_vals, dv, h->nnz * 8, cudaMemcpyDeviceToDevice, h->st));
-  rc = run_factor(h, h->d_vals, ds);
-  if (rc) return rc;
+  bool done = false;
+  if (h->opt.graph_refactor && h->rec_ok) {
+    if ((rc = replay_factor(h, ds, &done))) return rc;
+  }
+  if (!done) {
+    drop_graph(h);  // a dynamic run may move buffers: the next refactorization captures anew
+    rc = run_factor(h, h->d_vals, ds);
+    if (rc) return rc;
+  }
   double* d_acc = nullptr;
   CK(cudaMallocAsync((void**)&d_acc, 8, h->st));
   CK(cudaMemsetAsync(d_acc, 0, 8, h->st));
@@ -2799,7 +3012,10 @@ rvg_status rvg_trim(rvg_handle* h, int32_t what) {
     h->factored = false;
   }
 #undef RVG_TRIM
-  if (what) h->need_presize = true;
+  if (what) {
+    h->need_presize = true;
+    drop_graph(h);  // it holds the addresses of the released buffers
+  }
   CK(cudaStreamSynchronize(st));  // the memory is back in the pool when this returns
   return RVG_OK;
 }
@@ -2828,6 +3044,10 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
   fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
+  drop_graph(h);
+  fr(h->d_rec);
+  if (h->d_mismatch) cudaFree(h->d_mismatch);
+  if (h->h_stage_all) cudaFreeHost(h->h_stage_all);
   for (size_t t = 1; t < h->lfx.size(); ++t) {
     LfCtx& c = h->lfx[t];
     fr(c.wpack);

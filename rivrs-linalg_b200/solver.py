@@ -54,6 +54,7 @@ class FactorOptions:
     mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
     mixed_tile_cols: int = 256  # mixed form, mixed_flush 0: Schur GEMM output columns per CTA tile (128, 256)
     mixed_operands: str = "tf32"  # mixed form: FP64 operands split into two "tf32" or two "bf16" parts
+    graph_refactor: bool = False  # refactorizations of one handle replayed as one CUDA graph (same pivoting)
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
@@ -64,7 +65,8 @@ class FactorOptions:
                                  large_front_threshold=self.large_front_threshold,
                                  precision={"fp64": 0, "mixed": 1}[self.precision],
                                  mixed_flush=self.mixed_flush, mixed_tile_cols=self.mixed_tile_cols,
-                                 mixed_operands={"tf32": 0, "bf16": 1}[self.mixed_operands])
+                                 mixed_operands={"tf32": 0, "bf16": 1}[self.mixed_operands],
+                                 graph_refactor=int(self.graph_refactor))
 
 
 class SparseError(RuntimeError):
