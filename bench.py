@@ -55,7 +55,11 @@ CONFIGS = {
     "lap100": ("lap", 100, "laplace7_100^3 shifted to 5% negative, n=1000000"),
     "batch64": ("batch", 64, "64 systems, n log-uniform in [5e3, 2e5] (seed 1), half shifted 7-pt Laplacians, "
                 "half KKT, 1-32 RHS each; then 20 refactorizations"),
+    "learned": ("learned", 0, "per-front precision selector: trained on 200 generated matrices (shift U[1%,20%], "
+                "KKT regularisation 10^U[-8,-2], grids 20^3-60^3), evaluated on held-out matrices: laplace7_100^3 "
+                "at 5% negative (n=1e6) and a kkt27_60^3 with a held-out seed (n=270000)"),
 }
+SELECTOR = os.path.join(ROOT, "rivrs-linalg_b200", "data", "selector_bf16.npz")
 METRIC = "factor+solve time to bwd err 1e-14, chosen form vs plain FP64 on 1 B200"
 
 
@@ -380,6 +384,95 @@ def batch_cpu_baseline(rv, orc, systems, full_flops):
                        f"({rate / 1e9:.1f} GFLOP/s), extrapolated to the batch's {full_flops:.3e} flops")
 
 
+def time_form(rv, torch, solver, s, b, opts, warmup, steps):
+    """Factor + solve to 1e-14 (refinement escalating to GMRES-IR) with the
+    values, scaling and right-hand side resident on the device; CUDA events on
+    the handle's stream around each step.  Returns the mean step time and the
+    last step's accuracy figures."""
+    solver._ensure_handle(opts)
+    st = torch.cuda.ExternalStream(solver.stream())
+    d_vals = torch.from_numpy(s.values).to("cuda")
+    d_scal = torch.from_numpy(solver._scaling).to("cuda") if solver._scaling is not None else None
+    d_b = torch.from_numpy(b).to("cuda")
+    d_x = torch.empty_like(d_b)
+    out = {}
+
+    def step():
+        solver.factor_device(d_vals.data_ptr(), d_scal.data_ptr() if d_scal is not None else None, opts)
+        return solver.solve_auto_device(d_b.data_ptr(), d_x.data_ptr(), tol=1e-14, max_iter=100)
+
+    for _ in range(warmup):
+        step()
+    times, its, used = [], [], set()
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        it, err, how = step()
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1) * 1e-3)
+        its.append(it)
+        used.add(how)
+    out.update(s_per_step=statistics.mean(times), times=times, solves_after_first=its, methods=sorted(used),
+               bwd_err=rv.problems.backward_error(s, d_x.cpu().numpy(), b), inertia=list(solver.inertia()))
+    if opts.precision == "learned":
+        out["selector"] = solver.selector_stats()
+    return out
+
+
+def run_learned(args, rv, torch):
+    """The selector workload: label the generated training family on the GPU
+    (every matrix factored with all large fronts in FP64 and all in the mixed
+    form), train the network with the library's kernels, then time plain
+    FP64, the mixed form and the learned form on held-out matrices."""
+    S = rv.selector
+    t0 = time.perf_counter()
+    fam = S.c5_family(args.train_count, 11, 20, 60)
+    lab_opts = rv.FactorOptions(large_front_threshold=256, mixed_flush=0, mixed_operands="bf16")
+    data = S.label_family(fam, 1e-3, lab_opts)
+    t_label = time.perf_counter() - t0
+    sel = S.PrecisionSelector(seed=11)
+    sel.fit_normalisation(data.X)
+    t1 = time.perf_counter()
+    hist = sel.train(data.X, data.y, weights=S.sample_weights(data, 0.5), steps=3000, lr=3e-3)
+    t_train = time.perf_counter() - t1
+    held = [rv.problems.shifted_laplacian(100, 0.05),
+            rv.problems.kkt(60, seed=20261203, reg_hi=10.0 ** -5)]
+    rows, clocks = [], ClockSampler()
+    for s in held:
+        solver, an_ms = analyze(rv, s)
+        solver.set_selector(sel)
+        b = rv.problems.rhs_normal(s.n, seed=1)
+        r = {"matrix": s.name, "n": s.n, "analyze_ms": an_ms}
+        for form in ("fp64", "mixed", "learned"):
+            o = rv.FactorOptions(precision=form, mixed_flush=0, mixed_operands="bf16")
+            r[form] = time_form(rv, torch, solver, s, b, o, args.warmup, args.steps)
+        solver.close()
+        X, y, err, m = S.label_fronts(s, 1e-3, rv.FactorOptions(mixed_flush=0, mixed_operands="bf16"))
+        r["misprediction"] = S.misprediction(sel, S.Labelled(X, y, err, m, [0] * y.size))
+        rows.append(r)
+        torch.cuda.empty_cache()
+    clk = clocks.stop(0)
+    t_l = sum(r["learned"]["s_per_step"] for r in rows)
+    t_p = sum(r["fp64"]["s_per_step"] for r in rows)
+    t_m = sum(r["mixed"]["s_per_step"] for r in rows)
+    line = {"metric": METRIC, "value": t_l, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_l * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded generators; held-out seeds for evaluation)",
+            "config": {"workload": CONFIGS["learned"][2], "form": "learned: BF16-part tensor-core Schur updates on "
+                       "the fronts the selector predicts safe, plain FP64 elsewhere; refinement escalating to "
+                       "GMRES-IR", "value": "sum over the held-out matrices of factor+solve time to 1e-14",
+                       "l2": "working sets far above L2 (126 MB); no flush needed"},
+            "sum_fp64_s": t_p, "sum_mixed_s": t_m, "speedup_vs_plain_fp64": t_p / t_l,
+            "speedup_vs_all_mixed": t_m / t_l, "held_out": rows,
+            "training": {"matrices": len(fam), "fronts": int(data.y.size), "safe_fraction": float(data.y.mean()),
+                         "tau": 1e-3, "label_s": t_label, "train_s": t_train, "adam_steps": 3000,
+                         "loss_first": hist[0][1], "loss_last": hist[-1][1],
+                         "train_misprediction": S.misprediction(sel, data)},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,6 +481,8 @@ def main():
     ap.add_argument("--config", default="kkt60", choices=sorted(CONFIGS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-precision form")
+    ap.add_argument("--train-count", type=int, default=200, help="learned config: generated training matrices")
     ap.add_argument("--mixed-flush", default="4,0",
                     help="comma list of mixed-form flush depths to time (32-deep K chunks per FP32 partial sum; 0 = all K)")
     ap.add_argument("--bf16-flush", default="0",
@@ -411,6 +506,20 @@ def main():
             systems = [f[0] for f in rv.problems.batch_family(count=64, seed=1)]
             full = sum(dense_flops(rv.SparseLDLT.analyze(sy).symbolic) for sy in systems)
             sample = lambda: (batch_cpu_baseline(rv, orc, systems, full), None)
+        elif args.config == "learned":
+            # the held-out pair in plain FP64 on the host: each extrapolated from a bounded sample of its family
+            fulls = {}
+            for cfg in ("lap100", "kkt60"):
+                sf, _ = build_system(rv, cfg)
+                fulls[cfg] = dense_flops(rv.symbolic_analyze(sf.n, sf.colptr, sf.rowidx,
+                                                             rv.ordering.default_order(sf)))
+
+            def sample():
+                parts = [cpu_baseline(rv, orc, cfg, fulls[cfg])[0] for cfg in ("lap100", "kkt60")]
+                cb = dict(parts[1])
+                cb["value"] = parts[0]["value"] + parts[1]["value"]
+                cb["sample"] = "; ".join(p["sample"] for p in parts) + " (sum of the two)"
+                return cb, None
         else:
             s_full, _ = build_system(rv, args.config)
             sym_full = rv.symbolic_analyze(s_full.n, s_full.colptr, s_full.rowidx,
@@ -453,6 +562,12 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.config == "learned":
+        if rank == 0:
+            run_learned(args, rv, torch)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     if args.config == "batch64":
         run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, local, dist)
         if dist is not None:
@@ -467,10 +582,10 @@ def main():
     d_b = torch.from_numpy(b).to("cuda")
     d_x = torch.empty_like(d_b)
 
-    def run_form(precision, flush=4, ops="tf32", method="ir"):
+    def run_form(precision, flush=4, ops="tf32", method="ir", **extra):
         """W warm-up + K timed steps of one form: factor + (refined) solve, inputs in HBM.
         method: "ir" (iterative refinement) or "gmres" (GMRES-IR) back to FP64 accuracy."""
-        opts = rv.FactorOptions(precision=precision, mixed_flush=flush, mixed_operands=ops)
+        opts = rv.FactorOptions(precision=precision, mixed_flush=flush, mixed_operands=ops, **extra)
         used = set()
         solver._ensure_handle(opts)
         solver.set_profiling(False)  # timed steps without the per-launch events
@@ -523,8 +638,22 @@ def main():
     forms = {"plain_fp64": plain}
     for fl in [int(v) for v in args.mixed_flush.split(",") if v.strip()]:
         forms[f"mixed_flush{fl}"] = run_form("mixed", fl, "tf32", "auto")
+    # the scheduling options of the BF16 form tuned on this pattern (results do not depend on them)
+    tuned, tune_table = rv.autotune.autotune(solver, d_vals.data_ptr(), d_scal.data_ptr() if d_scal is not None else None,
+                                             rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16"),
+                                             reps=1)
+    autotune_rep = {"candidates": [dict(c, factor_s=s_) for c, s_ in tune_table],
+                    "chosen": {"large_front_threshold": tuned.large_front_threshold,
+                               "mixed_tile_cols": tuned.mixed_tile_cols}}
     for fl in [int(v) for v in args.bf16_flush.split(",") if v.strip()]:
-        forms[f"mixed_bf16_flush{fl}"] = run_form("mixed", fl, "bf16", "auto")
+        extra = ({"large_front_threshold": tuned.large_front_threshold, "mixed_tile_cols": tuned.mixed_tile_cols}
+                 if fl == 0 else {})
+        forms[f"mixed_bf16_flush{fl}"] = run_form("mixed", fl, "bf16", "auto", **extra)
+    if os.path.exists(SELECTOR) and not args.no_learned:
+        # the shipped selector picks the form per large front (BF16 parts where it predicts safe, FP64 elsewhere)
+        solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
+        forms["learned_bf16_flush0"] = run_form("learned", 0, "bf16", "auto")
+        forms["learned_bf16_flush0"]["selector"] = solver.selector_stats()
     # the chosen form: the fastest that reaches the accuracy target (plain always does)
     chosen_key = min((k for k, f in forms.items() if f["bwd"] <= 1e-14 or k == "plain_fp64"),
                      key=lambda k: forms[k]["t"])
@@ -678,7 +807,8 @@ def main():
                           "inertia": list(f["inertia"]),
                           "syrk_tflops_fp64_equiv": (f["syrk_flops"] / (f["syrk_ms"] * 1e-3) / 1e12)
                           if f["syrk_ms"] > 0 else None,
-                          "syrk_share": (f["syrk_ms"] * 1e-3) / f["t"] if f["t"] else None}
+                          "syrk_share": (f["syrk_ms"] * 1e-3) / f["t"] if f["t"] else None,
+                          "selector": f.get("selector")}
                       for k, f in forms.items()},
             "chosen_form": chosen_key,
             "speedup_vs_plain_fp64": plain["t"] / t_step,
@@ -687,6 +817,7 @@ def main():
             "multi_rhs_solve": multi,
             "hbm_bound_parts": hbm_parts,
             "graph_refactor": graph_refactor,
+            "autotune": autotune_rep,
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(s.values.nbytes + b.nbytes),
                     "d2h_bytes_per_step": int(b.nbytes)},
             "gpu_launches": int(launches // max(args.steps, 1)),

@@ -62,7 +62,11 @@ typedef struct {
    * with each FP64 operand split once into two TF32 parts (three products per
    * term, FP32-level products), FP32 partial sums added into FP64; pivot
    * tests, 2x2 inversions, TRSM and storage stay FP64.  Pair the mixed form
-   * with rvg_solve_refine. */
+   * with rvg_solve_refine.  2 = learned: each large front takes the mixed
+   * form or plain FP64 as the per-front selector (rvg_set_selector) predicts
+   * from the features of the assembled front; a mixed front whose pivots grow
+   * past the selector's bound makes the whole factorization run again in
+   * FP64 (rvg_selector_stats). */
   int32_t precision;
   /* Mixed form only: 32-deep K chunks per FP32 partial sum before it is
    * added in FP64 (1, 2, 4 or 8; 0 = one partial sum over the whole K range).
@@ -292,6 +296,53 @@ rvg_status rvg_selftest_waits(rvg_handle* h, int32_t which);
 rvg_status rvg_trim(rvg_handle* h, int32_t what);
 /* Free and total bytes of the current device (cudaMemGetInfo). */
 rvg_status rvg_mem_info(int64_t out2[2]);
+
+/* ---- learned per-front precision (no reference counterpart) ------------
+ * The selector is a 12-64-64-1 perceptron (ReLU, sigmoid output) on float32
+ * parameters: W1 (64 x 12, row major), b1, W2 (64 x 64), b2, W3 (64), b3
+ * (rvg_mlp_trained_count() values), then the per-feature mean and standard
+ * deviation the inputs are normalised with (rvg_mlp_param_count() in all).
+ * Its output is the probability that a front's tensor-core Schur updates keep
+ * its pivots within bound. */
+#define RVG_MLP_FEATURES 12
+#define RVG_FRONT_FEATURE_COLS 22
+int64_t rvg_mlp_param_count(void);
+int64_t rvg_mlp_trained_count(void);
+/* Floats of the work buffer rvg_mlp_grad needs for n samples. */
+int64_t rvg_mlp_work_floats(int64_t n);
+/* Probabilities of n samples (features n x 12, row major); device pointers,
+ * enqueued on `stream` (a cudaStream_t or NULL). */
+rvg_status rvg_mlp_forward(const float* d_params, const float* d_x, int64_t n, float* d_prob, void* stream);
+/* Loss sum_i w_i (softplus(z_i) - y_i z_i) / norm and its gradient with
+ * respect to the trained parameters (d_grad: rvg_mlp_trained_count() floats,
+ * d_loss: one float, may be NULL); d_weight may be NULL (all 1).  The result
+ * is deterministic (fixed summation order).  Allocates nothing: d_work holds
+ * rvg_mlp_work_floats(n) floats. */
+rvg_status rvg_mlp_grad(const float* d_params, const float* d_x, const float* d_y, const float* d_weight, int64_t n,
+                        double norm, float* d_grad, float* d_loss, float* d_work, int64_t work_floats, void* stream);
+/* One Adam step (t = step >= 1) with decoupled weight decay on the trained
+ * parameters; d_m and d_v are the moment estimates (same length, start 0). */
+rvg_status rvg_mlp_adam(float* d_params, const float* d_grad, float* d_m, float* d_v, int64_t step, float lr,
+                        float beta1, float beta2, float eps, float weight_decay, void* stream);
+/* Installs a selector on a handle (host parameters, copied): fronts whose
+ * probability is >= threshold take the mixed form; a mixed front whose
+ * largest |D| entry exceeds growth_bound times its largest assembled |a|
+ * triggers the FP64 refactorization. */
+rvg_status rvg_set_selector(rvg_handle* h, const float* params, int64_t nparams, float threshold,
+                            double growth_bound);
+/* The large fronts of the last learned-precision factorization, one row of
+ * RVG_FRONT_FEATURE_COLS doubles each: supernode, m, k, eliminated, 1x1 and
+ * 2x2 pivots, route (1 = mixed), probability, max |a| of the assembled
+ * fully-summed columns, max |D|, then the 12 features: log2 m, log2 k, k/m,
+ * log2(1 + delayed rows in), delayed rows in / k, log10 max |a|, log10 of
+ * max |a_jj| / max |a|, log10 of min |a_jj| / max |a|, log10 of the smallest
+ * column ratio |a_jj| / max_{i>j} |a_ij|, the fractions of columns with that
+ * ratio below the pivot threshold, with a negative and with a zero diagonal.
+ * out == NULL: *nrows only. */
+rvg_status rvg_front_features(rvg_handle* h, double* out, int64_t cap_rows, int64_t* nrows);
+/* [large fronts, fronts the selector sent to the mixed form, mixed fronts
+ * over the growth bound, 1 if the factor in place is the FP64 rerun]. */
+rvg_status rvg_selector_stats(rvg_handle* h, int64_t out4[4]);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 rvg_status rvg_stream(rvg_handle* h, void** stream);
 void rvg_destroy(rvg_handle* h);

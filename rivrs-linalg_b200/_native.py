@@ -113,6 +113,15 @@ SIGNATURES = {
     "rvg_mem_info": (C.c_int, [i64p]),
     "rvg_mc64": (C.c_int, [i64, i64p, i64p, dp, i64p, dp, i64p]),
     "rvg_dense_factor_noalloc": (C.c_int, [vp, i64, i64, C.POINTER(Options), vp, vp, vp, vp, vp, vp]),
+    "rvg_mlp_param_count": (i64, []),
+    "rvg_mlp_trained_count": (i64, []),
+    "rvg_mlp_work_floats": (i64, [i64]),
+    "rvg_mlp_forward": (C.c_int, [vp, vp, i64, vp, vp]),
+    "rvg_mlp_grad": (C.c_int, [vp, vp, vp, vp, i64, C.c_double, vp, vp, vp, i64, vp]),
+    "rvg_mlp_adam": (C.c_int, [vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, vp]),
+    "rvg_set_selector": (C.c_int, [vp, C.POINTER(C.c_float), i64, C.c_float, C.c_double]),
+    "rvg_front_features": (C.c_int, [vp, dp, i64, i64p]),
+    "rvg_selector_stats": (C.c_int, [vp, i64p]),
     "rvg_destroy": (None, [vp]),
 }
 

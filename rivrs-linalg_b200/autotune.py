@@ -1,0 +1,95 @@
+"""Autotuner for the scheduling options of one sparsity pattern.
+
+Two options only schedule the work: the large-front cutoff
+(`large_front_threshold`: fronts at or above it take the whole GPU one after
+another, the others are batched one CTA or warp per front) and, in the mixed
+form without flushing, the Schur GEMM's tile width (`mixed_tile_cols`: 128, or
+256 = two 128-column tiles sharing one W tile).  In the plain form neither
+changes a result; the tile width changes none in the mixed form either, but
+there the cutoff also decides which fronts take the tensor-core updates, so
+the refined solution is checked by the caller as for any mixed factor.  Their
+best values depend on the pattern (how many large fronts a wave holds, how
+large).  `autotune` times
+the candidates on the caller's own matrix with device-resident values (CUDA
+events on the handle's stream, best of `reps` after one warm-up) and returns
+the fastest; with `cache` set, results are kept in a JSON file keyed by the
+pattern's fingerprint, the precision and the device, so a pattern is tuned once.
+There is no counterpart in the reference (its CPU path has no such options).
+"""
+from __future__ import annotations
+
+import dataclasses
+import hashlib
+import json
+import os
+
+import numpy as np
+
+from .solver import FactorOptions, SparseLDLT
+
+DEFAULT_THRESHOLDS = (1024, 2048, 4096)
+DEFAULT_TILE_COLS = (128, 256)
+
+
+def fingerprint(solver: SparseLDLT) -> str:
+    """Hash of the analysed structure (supernode ranges, patterns, parents)."""
+    sym = solver.symbolic
+    h = hashlib.sha256()
+    for a in (sym.sup_begin, sym.sup_end, sym.sup_parent, np.diff(sym.pat_ptr)):
+        h.update(np.ascontiguousarray(a, np.int64).tobytes())
+    h.update(str(solver.system.n).encode())
+    return h.hexdigest()[:24]
+
+
+def candidates(base: FactorOptions, thresholds=DEFAULT_THRESHOLDS, tile_cols=DEFAULT_TILE_COLS) -> list:
+    out = []
+    tiles = tile_cols if (base.precision != "fp64" and base.mixed_flush == 0) else (base.mixed_tile_cols,)
+    for t in thresholds:
+        for c in tiles:
+            out.append(dataclasses.replace(base, large_front_threshold=int(t), mixed_tile_cols=int(c)))
+    return out
+
+
+def _key(solver, base, device_name):
+    return "|".join([fingerprint(solver), base.precision, base.mixed_operands, str(base.mixed_flush), device_name])
+
+
+def autotune(solver: SparseLDLT, d_vals_ptr: int, d_scal_ptr: int | None, base: FactorOptions, reps: int = 2,
+             thresholds=DEFAULT_THRESHOLDS, tile_cols=DEFAULT_TILE_COLS, cache: str | None = None):
+    """(best options, [(candidate options as a dict, seconds)]) for factoring
+    the values at d_vals_ptr (device) with the solver's pattern."""
+    import torch
+    dev = torch.cuda.get_device_name()
+    key = _key(solver, base, dev)
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            got = json.load(f).get(key)
+        if got:
+            return dataclasses.replace(base, **got["best"]), [(c, t) for c, t in got["table"]]
+    table = []
+    for o in candidates(base, thresholds, tile_cols):
+        solver._ensure_handle(o)
+        st = torch.cuda.ExternalStream(solver.stream())
+        solver.factor_device(d_vals_ptr, d_scal_ptr, o)  # warm-up (sizes the arenas)
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            solver.factor_device(d_vals_ptr, d_scal_ptr, o)
+            e1.record(st)
+            e1.synchronize()
+            t = e0.elapsed_time(e1) * 1e-3
+            best = t if best is None else min(best, t)
+        table.append(({"large_front_threshold": o.large_front_threshold, "mixed_tile_cols": o.mixed_tile_cols}, best))
+    choice = min(table, key=lambda r: r[1])[0]
+    if cache:
+        data = {}
+        if os.path.exists(cache):
+            with open(cache) as f:
+                data = json.load(f)
+        data[key] = {"best": choice, "table": table}
+        tmp = cache + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(data, f, indent=1)
+        os.replace(tmp, cache)
+    return dataclasses.replace(base, **choice), table

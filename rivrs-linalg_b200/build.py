@@ -24,7 +24,7 @@ CU_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fP
             "-I", os.path.join(ROOT, "include")] + ARCH
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", os.path.join(ROOT, "include")]
 
-CU_SOURCES = ["numeric.cu", "noalloc.cu"]
+CU_SOURCES = ["numeric.cu", "noalloc.cu", "mlp.cu"]
 CXX_SOURCES = ["symbolic.cpp", "plan.cpp", "capi.cpp", "mc64.cpp"]
 
 

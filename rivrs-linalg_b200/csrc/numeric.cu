@@ -43,6 +43,7 @@
 
 #include "dense.cuh"
 #include "front.cuh"
+#include "mlp.cuh"
 #include "rvg_internal.h"
 
 namespace rvg {
@@ -966,6 +967,139 @@ __global__ void k_check_gne(LFState* st, int32_t expect, int32_t* mismatch) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// learned precision (precision = 2): per large front, features of the
+// assembled front, the selector's decision, and the observed pivot growth.
+// Row of a front in the feature table (FEAT_STRIDE 32-bit words):
+//   0 max |a| over the fully-summed columns (lower part), 1 max |a_jj|,
+//   2 min |a_jj|, 3 min over columns of |a_jj| / max_{i>j} |a_ij|, 4 columns
+//   with that ratio < u, 5 negative diagonals, 6 zero diagonals (as counts),
+//   7 max |D| after the factorization; 8..19 the 12 features; 20 the
+//   selector's probability that the mixed form is safe; 21 the route (1 =
+//   mixed).  Maxima, minima and counts combine by atomics whose result does
+//   not depend on their order, so features and routes are reproducible.
+// ---------------------------------------------------------------------------
+constexpr int FEAT_STRIDE = 32;
+constexpr unsigned F_POS_INF = 0x7f800000u;
+
+__global__ void k_feat_init(const int32_t* ids, int n, unsigned* feat) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    unsigned* r = feat + (size_t)ids[i] * FEAT_STRIDE;
+    r[0] = 0u; r[1] = 0u; r[2] = F_POS_INF; r[3] = F_POS_INF; r[4] = 0u; r[5] = 0u; r[6] = 0u; r[7] = 0u;
+  }
+}
+
+__device__ __forceinline__ unsigned fbits(double v) { return __float_as_uint((float)v); }
+
+// grid (column chunks of 8, fronts): warp w of chunk x reads column 8x + w
+// of the front's fully-summed block from its diagonal down.
+__global__ void __launch_bounds__(256) k_front_features(const int32_t* ids, const DFront* F, Arenas A, double u,
+                                                        unsigned* feat) {
+  const int s = ids[blockIdx.y];
+  const DFront f = F[s];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t j = (int64_t)blockIdx.x * 8 + warp;
+  __shared__ unsigned sv[8][7];
+  unsigned v[7] = {0u, 0u, F_POS_INF, F_POS_INF, 0u, 0u, 0u};
+  if (j < f.k) {
+    const double* col = A.panel + f.panel + j * (int64_t)f.m;
+    double cm = 0.0;
+    for (int64_t i = j + 1 + lane; i < f.m; i += 32) cm = fmax(cm, fabs(col[i]));
+    for (int o = 16; o > 0; o >>= 1) cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+    const double d = col[j], ad = fabs(d);
+    v[0] = fbits(fmax(cm, ad));
+    v[1] = fbits(ad);
+    v[2] = fbits(ad);
+    const double ratio = cm > 0.0 ? ad / cm : INFINITY;
+    v[3] = fbits(ratio);
+    v[4] = ratio < u ? 1u : 0u;
+    v[5] = d < 0.0 ? 1u : 0u;
+    v[6] = d == 0.0 ? 1u : 0u;
+  }
+  if (lane == 0)
+    for (int q = 0; q < 7; ++q) sv[warp][q] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if ((int64_t)blockIdx.x * 8 >= f.k) return;
+    unsigned r[7] = {0u, 0u, F_POS_INF, F_POS_INF, 0u, 0u, 0u};
+    for (int w = 0; w < 8; ++w) {
+      r[0] = max(r[0], sv[w][0]); r[1] = max(r[1], sv[w][1]);
+      r[2] = min(r[2], sv[w][2]); r[3] = min(r[3], sv[w][3]);
+      r[4] += sv[w][4]; r[5] += sv[w][5]; r[6] += sv[w][6];
+    }
+    unsigned* row = feat + (size_t)s * FEAT_STRIDE;
+    atomicMax(row + 0, r[0]); atomicMax(row + 1, r[1]);
+    atomicMin(row + 2, r[2]); atomicMin(row + 3, r[3]);
+    if (r[4]) atomicAdd(row + 4, r[4]);
+    if (r[5]) atomicAdd(row + 5, r[5]);
+    if (r[6]) atomicAdd(row + 6, r[6]);
+  }
+}
+
+// One warp per front: the 12 features, the network, the route.
+__global__ void k_mlp_route(const int32_t* ids, int n, const DFront* F, const float* P, float thresh, int force_fp64,
+                            unsigned* feat, int32_t* route_out) {
+  __shared__ MlpAct act;
+  __shared__ float fx[MLP_IN];
+  const int i = blockIdx.x, lane = threadIdx.x;
+  if (i >= n) return;
+  const int s = ids[i];
+  const DFront f = F[s];
+  unsigned* row = feat + (size_t)s * FEAT_STRIDE;
+  if (lane == 0) {
+    const float lo = 1e-30f;
+    const float mx = fmaxf(__uint_as_float(row[0]), lo);
+    const float k = (float)max(f.k, 1), m = (float)max(f.m, 1);
+    fx[0] = log2f(m);
+    fx[1] = log2f(k);
+    fx[2] = k / m;
+    fx[3] = log2f(1.f + (float)f.ndin);
+    fx[4] = (float)f.ndin / k;
+    fx[5] = log10f(mx);
+    fx[6] = log10f(fmaxf(__uint_as_float(row[1]) / mx, lo));
+    fx[7] = log10f(fmaxf(__uint_as_float(row[2]) / mx, lo));
+    fx[8] = log10f(fminf(fmaxf(__uint_as_float(row[3]), lo), 1e10f));
+    fx[9] = (float)row[4] / k;
+    fx[10] = (float)row[5] / k;
+    fx[11] = (float)row[6] / k;
+  }
+  __syncwarp();
+  const float xin = lane < MLP_IN ? fx[lane] : 0.f;
+  const float z = mlp_forward_warp(P, xin, act);
+  if (lane < MLP_IN) row[8 + lane] = __float_as_uint(fx[lane]);
+  if (lane == 0) {
+    const float pr = mlp_sigmoid(z);
+    const int r = (!force_fp64 && pr >= thresh) ? 1 : 0;
+    row[20] = __float_as_uint(pr);
+    row[21] = __float_as_uint((float)r);
+    route_out[i] = r;
+  }
+}
+
+// After the wave's factorization: max |D| of each large front; a front that
+// took the mixed form and whose max |D| exceeds bound * max |a| raises flag.
+__global__ void k_front_growth(const int32_t* ids, const DFront* F, Arenas A, double bound, unsigned* feat,
+                               int32_t* flag) {
+  const int s = ids[blockIdx.x];
+  const DFront f = F[s];
+  __shared__ double sm[8];
+  double mx = 0.0;
+  for (int c = threadIdx.x; c < f.ne; c += blockDim.x) {
+    const int64_t q = f.dpos + c;
+    mx = fmax(mx, A.dtype[q] == PT_2X2 ? fmax(fabs(A.ddiag[q]), fabs(A.doff[q])) : fabs(A.ddiag[q]));
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, sm[w]);
+    unsigned* row = feat + (size_t)s * FEAT_STRIDE;
+    row[7] = fbits(mx);
+    const double amax = (double)__uint_as_float(row[0]);
+    if (__uint_as_float(row[21]) == 1.f && mx > bound * amax) atomicAdd(flag, 1);
+  }
+}
+
 }  // namespace rvg
 
 using namespace rvg;
@@ -1042,6 +1176,16 @@ struct rvg_handle {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   const double* graph_ds = nullptr;                  // the scaling pointer the graph reads
+  // learned precision (precision = 2)
+  float* d_sel = nullptr;                            // selector parameters (MLP_NPARAM floats)
+  float sel_thresh = 0.5f;                           // probability at or above which a front takes the mixed form
+  double sel_bound = 1e6;                            // growth bound: max |D| <= bound * max |a| for a mixed front
+  unsigned* d_feat = nullptr; size_t d_feat_cap = 0; // feature table, FEAT_STRIDE words per front
+  int32_t* d_sel_flag = nullptr;                     // mixed fronts over the growth bound in the last run
+  std::vector<int8_t> route;                         // per front: 1 = mixed form (decided on the device)
+  std::vector<int32_t> sel_large;                    // the large fronts of the last factorization
+  bool sel_force_fp64 = false;                       // the FP64 refactorization after a growth flag
+  int64_t sel_routed = 0, sel_flagged = 0, sel_fallback = 0;
   // measurement
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -1396,9 +1540,17 @@ static void launch_pack(rvg_handle* h, cudaStream_t st, dim3 grid, const PackArg
 
 // The Schur update C -= W L^T (lower) of one contribution block.  kmax bounds
 // the device-side K (columns eliminated).
-int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
+// Whether front s takes the mixed form's tensor-core updates: every large
+// front with precision = 1, the selector's choice with precision = 2.
+bool front_mixed(const rvg_handle* h, int64_t s) {
+  if (h->opt.precision == 1) return true;
+  if (h->opt.precision != 2 || h->sel_force_fp64) return false;
+  return s >= 0 && s < (int64_t)h->route.size() && h->route[s] != 0;
+}
+
+int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax, bool mixed) {
   cudaStream_t st = h->st;
-  if (h->opt.precision == 1) {
+  if (mixed) {
     const int64_t nr = (ga.r1 - ga.r0 + TC_BM - 1) / TC_BM, nc = (ga.c1 - ga.c0 + TC_BN - 1) / TC_BN;
     const int64_t Q = (kmax + TC_BK - 1) / TC_BK;
     const int64_t ntiles = (nr > 0 && nc > 0) ? tc_count_tiles(nr, nc, ga.r0, ga.c0) : 0;
@@ -1435,12 +1587,12 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax) {
 // cond set the launch only acts if *cond < cond_lt.
 int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int64_t c0, int64_t c1, int64_t wd,
                        int64_t wrow, int64_t F, const float* pk_w, const float* pk_l, int64_t kadd,
-                       const int32_t* kdev, const int32_t* cond, int32_t cond_lt) {
+                       const int32_t* kdev, const int32_t* cond, int32_t cond_lt, bool mixed) {
   cudaStream_t st = cx.st;
   if (c1 <= c0) return RVG_OK;
   int rc = syrk_ev(h, cx.marks);
   if (rc) return rc;
-  if (h->opt.precision == 1) {
+  if (mixed) {
     const int64_t Fq = F / TC_BK;
     const int64_t nr = (m - c0 + TC_BM - 1) / TC_BM, nc = (c1 - c0 + TC_BN - 1) / TC_BN;
     const int64_t ntiles = tc_count_tiles(nr, nc, c0, c0);
@@ -1491,14 +1643,14 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   a.pb = sc;
   a.w = sc + m * IBMAX;
   a.wo = sc + 2 * m * IBMAX;
-  const int64_t F = lf_window_cols(nb, h->opt.precision == 1);
+  const bool mixed = front_mixed(h, s);
+  const int64_t F = lf_window_cols(nb, mixed);
   a.lp = (int32_t*)(sc + m * (2 * IBMAX + LF_WINDOW * nb));
   a.nfsb = p;
   a.o = dop;
   const int two_level = p > nb;
   // window of pending columns [wd, gne) of the deferred updates; its W rows start at wrow
   int64_t wd = 0, wrow = std::min(p, nb);
-  const bool mixed = h->opt.precision == 1;
   const int64_t Fq = F / TC_BK;
   float *pk_w = nullptr, *pk_l = nullptr;
   if (mixed && two_level) {
@@ -1585,16 +1737,16 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         int rc;
         if (flush) {
           // the window is full: every trailing column takes it (one GEMM)
-          rc = launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
+          rc = launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0, mixed);
           if (rc) return rc;
         } else {
           // near field: the next outer block's columns (oe + nb <= p here) take the whole window
-          rc = launch_window_gemm(h, cx, a, m, oe, oe + ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0);
+          rc = launch_window_gemm(h, cx, a, m, oe, oe + ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0, mixed);
           if (rc) return rc;
           // far field: only if this block delayed columns (decided on the device)
           if (oe + nb < p) {
             rc = launch_window_gemm(h, cx, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, bne_dev,
-                                    (int32_t)bcols);
+                                    (int32_t)bcols, mixed);
             if (rc) return rc;
           }
         }
@@ -1752,6 +1904,15 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   h->syrk_launches = 0;
   h->launches = 0;
   h->peak_bytes = 0;
+  if (h->opt.precision == 2) {
+    if (!h->d_sel) { set_error("precision = 2 (learned) needs a selector: call rvg_set_selector first"); return RVG_ERR_INVALID_INPUT; }
+    if ((rc = ensure(h->d_feat, h->d_feat_cap, (size_t)std::max<int64_t>(ns, 1) * FEAT_STRIDE, st))) return rc;
+    if (!h->d_sel_flag) CK(cudaMalloc((void**)&h->d_sel_flag, sizeof(int32_t)));
+    CK(cudaMemsetAsync(h->d_sel_flag, 0, sizeof(int32_t), st));
+    h->route.assign(ns, 0);
+    h->sel_large.clear();
+    h->sel_routed = 0;
+  }
   if (!h->replay) {
     h->rec_ok = false;
     h->rec_g.assign(ns, {});
@@ -1870,6 +2031,12 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     for (size_t q = 0; q < maxch; ++q) o_e[q] = pk.add(eitems[q]);
     size_t o_w = pk.add(witems), o_g = pk.add(gitems);
     size_t o_cnt = pk.add(std::vector<int32_t>(3 * (size_t)nw + 4, 0));
+    const bool learned = h->opt.precision == 2 && !large_ids.empty();
+    size_t o_lg = 0, o_rt = 0;
+    if (learned) {
+      o_lg = pk.add(large_ids);
+      o_rt = pk.add(std::vector<int32_t>(large_ids.size(), 0));
+    }
     if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size(), st))) return rc;
     char* hs;
     if (h->replay) {  // a slice of its own: the graph copies from it at every replay
@@ -1904,6 +2071,30 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     // contribution blocks whose parents are now all assembled
     for (size_t w2 = 0; w2 < w; ++w2)
       if (cb_block[w2] >= 0 && cb_release_at[w2] == (int64_t)w) { cb_release(h, cb_block[w2], cb_len[w2]); cb_block[w2] = -1; }
+    // ---- learned precision: features of the assembled large fronts, the
+    // selector's route for each (read back: it picks the launches below)
+    if (learned) {
+      const int nl = (int)large_ids.size();
+      const int32_t* d_lg = (const int32_t*)(D + o_lg);
+      int32_t* d_rt = (int32_t*)(D + o_rt);
+      int64_t kmax = 0;
+      for (int32_t s : large_ids) kmax = std::max<int64_t>(kmax, h->h_fronts[s].k);
+      k_feat_init<<<1, 256, 0, st>>>(d_lg, nl, h->d_feat);
+      k_front_features<<<dim3((unsigned)((kmax + 7) / 8), (unsigned)nl), 256, 0, st>>>(d_lg, h->d_fronts, A,
+                                                                                     h->opt.threshold, h->d_feat);
+      k_mlp_route<<<nl, 32, 0, st>>>(d_lg, nl, h->d_fronts, h->d_sel, h->sel_thresh, h->sel_force_fp64 ? 1 : 0,
+                                    h->d_feat, d_rt);
+      CK(cudaGetLastError());
+      if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(std::max(3 * nw + 4, nl)) * 4))) return rc;
+      CK(cudaMemcpyAsync(h->h_counts, d_rt, (size_t)nl * 4, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      for (int i = 0; i < nl; ++i) {
+        h->route[large_ids[i]] = (int8_t)(h->h_counts[i] != 0);
+        h->sel_routed += h->h_counts[i] != 0;
+      }
+      h->sel_large.insert(h->sel_large.end(), large_ids.begin(), large_ids.end());
+      h->launches += 3;
+    }
     // ---- dense factorization
     mark(h, -1);
     if (!tpp_ids.empty())
@@ -1929,9 +2120,14 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       if (!(f.flags & FF_HAS_CB) || f.k == 0 || !((f.flags & FF_LARGE) && f.nfs >= 256)) continue;
       SyrkArgs ga{A.cbase + f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
                   0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
-      if ((rc = launch_syrk(h, ga, f.k))) return rc;
+      if ((rc = launch_syrk(h, ga, f.k, front_mixed(h, s)))) return rc;
       mark(h, RVG_PART_CB_SYRK);
       cb_syrk_fronts.push_back(s);
+    }
+    if (learned) {
+      k_front_growth<<<(unsigned)large_ids.size(), 256, 0, st>>>((const int32_t*)(D + o_lg), h->d_fronts, A,
+                                                                 h->sel_bound, h->d_feat, h->d_sel_flag);
+      h->launches++;
     }
     CK(cudaEventRecord(h->ev[4], st));
     CK(cudaGetLastError());
@@ -2079,7 +2275,7 @@ void rvg_default_options(rvg_options* o) {
   o->graph_refactor = 0;
 }
 
-static int check_opts(const rvg_options& o) {  // factor.rs:307-347
+static int check_opts(const rvg_options& o) {  // factor.rs:307-347 (precision and below: no counterpart)
   if (!(o.threshold > 0.0 && o.threshold <= 1.0)) { set_error("threshold must be in (0, 1]"); return RVG_ERR_INVALID_INPUT; }
   if (!(o.small >= 0.0)) { set_error("small must be >= 0.0"); return RVG_ERR_INVALID_INPUT; }
   if (o.outer_block_size <= 0) { set_error("outer_block_size must be > 0"); return RVG_ERR_INVALID_INPUT; }
@@ -2091,7 +2287,7 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347
   if (o.inner_block_size > IBMAX) { set_error("inner_block_size above 32 is not supported by the B200 kernels"); return RVG_ERR_INVALID_INPUT; }
   if (o.nemin < 1) { set_error("nemin must be >= 1"); return RVG_ERR_INVALID_INPUT; }
   if (o.large_front_threshold < 1) { set_error("large_front_threshold must be >= 1"); return RVG_ERR_INVALID_INPUT; }
-  if (o.precision != 0 && o.precision != 1) { set_error("precision must be 0 (FP64) or 1 (mixed)"); return RVG_ERR_INVALID_INPUT; }
+  if (o.precision < 0 || o.precision > 2) { set_error("precision must be 0 (FP64), 1 (mixed) or 2 (learned)"); return RVG_ERR_INVALID_INPUT; }
   if (o.mixed_flush != 0 && o.mixed_flush != 1 && o.mixed_flush != 2 && o.mixed_flush != 4 && o.mixed_flush != 8) {
     set_error("mixed_flush must be 0, 1, 2, 4 or 8");
     return RVG_ERR_INVALID_INPUT;
@@ -2279,13 +2475,31 @@ static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
   // the refinement needs the unfactored values and ||A||_F
   if (dv != h->d_vals && h->nnz) CK(cudaMemcpyAsync(h->d_vals, dv, h->nnz * 8, cudaMemcpyDeviceToDevice, h->st));
   bool done = false;
-  if (h->opt.graph_refactor && h->rec_ok) {
+  if (h->opt.graph_refactor && h->rec_ok && h->opt.precision != 2) {
     if ((rc = replay_factor(h, ds, &done))) return rc;
   }
   if (!done) {
     drop_graph(h);  // a dynamic run may move buffers: the next refactorization captures anew
     rc = run_factor(h, h->d_vals, ds);
     if (rc) return rc;
+  }
+  if (h->opt.precision == 2) {
+    // a front that took the mixed form and grew past the bound: the whole
+    // factorization again in FP64 (the plain form is the selector's fallback)
+    int32_t flagged = 0;
+    CK(cudaMemcpyAsync(&flagged, h->d_sel_flag, 4, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->sel_flagged = flagged;
+    h->sel_fallback = 0;
+    if (flagged) {
+      const int64_t routed = h->sel_routed;
+      h->sel_force_fp64 = true;
+      rc = run_factor(h, h->d_vals, ds);
+      h->sel_force_fp64 = false;
+      if (rc) return rc;
+      h->sel_routed = routed;  // what the selector chose (the factor in place is FP64)
+      h->sel_fallback = 1;
+    }
   }
   double* d_acc = nullptr;
   CK(cudaMallocAsync((void**)&d_acc, 8, h->st));
@@ -2976,6 +3190,60 @@ static int trim_buf(void* p, cudaStream_t st) {
   return RVG_OK;
 }
 
+static float ubits(unsigned u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+rvg_status rvg_set_selector(rvg_handle* h, const float* params, int64_t nparams, float threshold,
+                            double growth_bound) {
+  if (!h || !params) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  if (nparams != MLP_NPARAM) { set_error("selector parameters: expected rvg_mlp_param_count() floats"); return RVG_ERR_DIMENSION_MISMATCH; }
+  for (int c = 0; c < MLP_IN; ++c)
+    if (!(params[MLP_SD + c] > 0.f)) { set_error("selector normalisation: standard deviations must be positive"); return RVG_ERR_INVALID_INPUT; }
+  if (!(growth_bound > 0)) { set_error("growth bound must be positive"); return RVG_ERR_INVALID_INPUT; }
+  CK(cudaSetDevice(h->device));
+  if (!h->d_sel) CK(cudaMalloc((void**)&h->d_sel, MLP_NPARAM * sizeof(float)));
+  CK(cudaMemcpyAsync(h->d_sel, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->sel_thresh = threshold;
+  h->sel_bound = growth_bound;
+  return RVG_OK;
+}
+
+rvg_status rvg_front_features(rvg_handle* h, double* out, int64_t cap_rows, int64_t* nrows) {
+  if (!h || !nrows) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  if (!h->factored || h->opt.precision != 2) { set_error("no learned-precision factorization to report"); return RVG_ERR_SOLVE_BEFORE_FACTOR; }
+  *nrows = (int64_t)h->sel_large.size();
+  if (!out) return RVG_OK;
+  if (cap_rows < *nrows) { set_error("feature table: too few rows"); return RVG_ERR_DIMENSION_MISMATCH; }
+  std::vector<unsigned> rows((size_t)h->P.sn.size() * FEAT_STRIDE);
+  if (!rows.empty()) CK(cudaMemcpy(rows.data(), h->d_feat, rows.size() * 4, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < h->sel_large.size(); ++i) {
+    const int32_t s = h->sel_large[i];
+    const DFront& f = h->h_fronts[s];
+    const unsigned* r = rows.data() + (size_t)s * FEAT_STRIDE;
+    double* o = out + i * RVG_FRONT_FEATURE_COLS;
+    o[0] = s; o[1] = f.m; o[2] = f.k; o[3] = f.ne; o[4] = f.n1; o[5] = f.n2;
+    o[6] = ubits(r[21]);  // route
+    o[7] = ubits(r[20]);  // probability
+    o[8] = ubits(r[0]);   // max |a|
+    o[9] = ubits(r[7]);   // max |D|
+    for (int c = 0; c < MLP_IN; ++c) o[10 + c] = ubits(r[8 + c]);
+  }
+  return RVG_OK;
+}
+
+rvg_status rvg_selector_stats(rvg_handle* h, int64_t out4[4]) {
+  if (!h || !out4) { set_error("null argument"); return RVG_ERR_INVALID_INPUT; }
+  out4[0] = (int64_t)h->sel_large.size();
+  out4[1] = h->sel_routed;
+  out4[2] = h->sel_flagged;
+  out4[3] = h->sel_fallback;
+  return RVG_OK;
+}
+
 rvg_status rvg_trim(rvg_handle* h, int32_t what) {
   if (!h) { set_error("null handle"); return RVG_ERR_INVALID_INPUT; }
   if (what & ~3) { set_error("what: bit 0 = workspace, bit 1 = factor"); return RVG_ERR_INVALID_INPUT; }
@@ -3046,6 +3314,9 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
   drop_graph(h);
   fr(h->d_rec);
+  if (h->d_sel) cudaFree(h->d_sel);
+  fr(h->d_feat);
+  if (h->d_sel_flag) cudaFree(h->d_sel_flag);
   if (h->d_mismatch) cudaFree(h->d_mismatch);
   if (h->h_stage_all) cudaFreeHost(h->h_stage_all);
   for (size_t t = 1; t < h->lfx.size(); ++t) {

@@ -50,7 +50,8 @@ class FactorOptions:
     failed_pivot_tpp: bool = True
     fallback_bunch_kaufman: bool = True
     large_front_threshold: int = 2048  # B200 scheduling only; results do not depend on it
-    precision: str = "fp64"  # "fp64" (plain) or "mixed" (TF32 tensor-core Schur updates; pair with solve_refine)
+    precision: str = "fp64"  # "fp64" (plain), "mixed" (tensor-core Schur updates; pair with solve_refine/solve_auto)
+    # or "learned" (per front, as the selector installed with set_selector predicts)
     mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
     mixed_tile_cols: int = 256  # mixed form, mixed_flush 0: Schur GEMM output columns per CTA tile (128, 256)
     mixed_operands: str = "tf32"  # mixed form: FP64 operands split into two "tf32" or two "bf16" parts
@@ -63,7 +64,7 @@ class FactorOptions:
                                  failed_pivot_tpp=int(self.failed_pivot_tpp),
                                  fallback_bk=int(self.fallback_bunch_kaufman),
                                  large_front_threshold=self.large_front_threshold,
-                                 precision={"fp64": 0, "mixed": 1}[self.precision],
+                                 precision={"fp64": 0, "mixed": 1, "learned": 2}[self.precision],
                                  mixed_flush=self.mixed_flush, mixed_tile_cols=self.mixed_tile_cols,
                                  mixed_operands={"tf32": 0, "bf16": 1}[self.mixed_operands],
                                  graph_refactor=int(self.graph_refactor))
@@ -142,6 +143,7 @@ class SparseLDLT:
         self._handle = None
         self._factored = False
         self._opts = None
+        self._selector = None
 
     # -- analyze -----------------------------------------------------------
     @classmethod
@@ -188,6 +190,8 @@ class SparseLDLT:
                                   C.byref(o), C.byref(h)))
         self._handle = h
         self._opts = options
+        if self._selector is not None:
+            self._install_selector()
 
     def factor(self, values=None, options: FactorOptions | None = None):
         """SparseLDLT::factor (solver.rs:296-324); `values` default to the
@@ -364,6 +368,37 @@ class SparseLDLT:
         out = np.zeros(9 * max(ns.value, 1), np.int64)
         _check(N.lib().rvg_front_info(self._handle, N.ptr(out, N.i64p), C.byref(ns)))
         return out[:9 * ns.value].reshape(ns.value, 9)
+
+    # -- learned per-front precision ----------------------------------------
+    def set_selector(self, selector, threshold: float | None = None, growth_bound: float | None = None):
+        """Installs a trained selector (selector.PrecisionSelector) for
+        factorizations with precision="learned"."""
+        self._selector = (selector, selector.threshold if threshold is None else threshold,
+                          selector.growth_bound if growth_bound is None else growth_bound)
+        if self._handle is not None:
+            self._install_selector()
+
+    def _install_selector(self):
+        sel, thr, bound = self._selector
+        p = np.ascontiguousarray(sel.params, dtype=np.float32)
+        _check(N.lib().rvg_set_selector(self._handle, p.ctypes.data_as(C.POINTER(C.c_float)), p.size,
+                                        float(thr), float(bound)))
+
+    def front_features(self) -> np.ndarray:
+        """Rows (RVG_FRONT_FEATURE_COLS) of the large fronts of the last
+        learned-precision factorization: supernode, m, k, eliminated, 1x1, 2x2,
+        route, probability, max|a|, max|D|, then the 12 features."""
+        nr = C.c_int64()
+        _check(N.lib().rvg_front_features(self._handle, None, 0, C.byref(nr)))
+        out = np.zeros((max(nr.value, 1), 22))
+        _check(N.lib().rvg_front_features(self._handle, N.ptr(out, N.dp), nr.value, C.byref(nr)))
+        return out[:nr.value]
+
+    def selector_stats(self) -> dict:
+        out = np.zeros(4, np.int64)
+        _check(N.lib().rvg_selector_stats(self._handle, N.ptr(out, N.i64p)))
+        return dict(large_fronts=int(out[0]), routed_mixed=int(out[1]), over_bound=int(out[2]),
+                    fp64_rerun=bool(out[3]))
 
     def work(self):
         out = np.zeros(6)

@@ -36,6 +36,16 @@ def orc():
 
 
 @pytest.fixture(scope="session")
+def mlp_oracle():
+    """The float64 oracle of the precision selector's network (checker only)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("rvg_mlp_oracle", os.path.join(ROOT, "oracle", "mlp_oracle.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="session")
 def golden():
     import json
     with open(os.path.join(ROOT, "tests", "golden", "hand_constructed.json")) as f:
