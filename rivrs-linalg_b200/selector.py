@@ -264,10 +264,15 @@ def misprediction(selector: PrecisionSelector, data: Labelled) -> dict:
     """Rates on labelled fronts: unsafe fronts sent to the mixed form (the
     costly mistake), safe fronts kept in FP64 (lost speed), and overall."""
     p = selector.predict_proba(data.X) if data.y.size else np.zeros(0)
-    route = p >= selector.threshold
-    safe = data.y > 0.5
-    n = max(data.y.size, 1)
-    return dict(fronts=int(data.y.size), safe=int(safe.sum()), routed_mixed=int(route.sum()),
+    return misprediction_of(p, selector.threshold, data.y)
+
+
+def misprediction_of(p: np.ndarray, threshold: float, y: np.ndarray) -> dict:
+    """misprediction() from the probabilities themselves."""
+    route = np.asarray(p) >= threshold
+    safe = np.asarray(y) > 0.5
+    n = max(safe.size, 1)
+    return dict(fronts=int(safe.size), safe=int(safe.sum()), routed_mixed=int(route.sum()),
                 unsafe_sent_mixed=int((route & ~safe).sum()), safe_kept_fp64=int((~route & safe).sum()),
                 rate=float(((route & ~safe) | (~route & safe)).sum() / n))
 
