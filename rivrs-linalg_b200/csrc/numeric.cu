@@ -635,12 +635,12 @@ __device__ int cta_factor_inner(CtaShared& sh, PanelView V, int64_t bm, int pl, 
 // One CTA per front: aptp_factor_in_place (factor.rs:301-404) for fronts with
 // k >= ib outside small-leaf subtrees: factor_inner (k <= nb) or
 // two_level_factor (k > nb), then the TPP fallback on the leftover columns.
-__global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* F, Arenas A, DevOpts o) {
-  if ((int)blockIdx.x >= n) return;
-  __shared__ CtaShared sh;
-  __shared__ int tpp_cnt[2];
+// One front by the whole CTA (aptp_factor_in_place, factor.rs:301-404).
+// Every thread reaches every barrier; the CTA's shared state is free again
+// when it returns.
+__device__ __forceinline__ void cta_aptp_front(CtaShared& sh, int* tpp_cnt, int s, DFront* F, const Arenas& A,
+                                               const DevOpts& o) {
   const int tid = threadIdx.x;
-  const int s = ids[blockIdx.x];
   const DFront fr = F[s];
   const int64_t m = fr.m;
   const int p = fr.k;
@@ -720,6 +720,35 @@ __global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* 
     n2 += tpp_cnt[1];
   }
   if (tid == 0) { F[s].ne = gne; F[s].n1 = n1; F[s].n2 = n2; }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* F, Arenas A, DevOpts o) {
+  if ((int)blockIdx.x >= n) return;
+  __shared__ CtaShared sh;
+  __shared__ int tpp_cnt[2];
+  cta_aptp_front(sh, tpp_cnt, ids[blockIdx.x], F, A, o);
+}
+
+// The medium fronts of a wave (across every system of a union) as one
+// persistent launch: a grid of at most the resident CTAs, each taking the
+// next front from a work queue (*next, zero at launch) until the list is
+// done.  The host lists the fronts largest first, so the long ones start
+// early and the short ones fill in behind them.  Which CTA factors a front
+// changes nothing in its result.
+__global__ void __launch_bounds__(NT) k_aptp_queue(const int32_t* ids, int n, int32_t* next, DFront* F, Arenas A,
+                                                   DevOpts o) {
+  __shared__ CtaShared sh;
+  __shared__ int tpp_cnt[2];
+  __shared__ int s_i;
+  for (;;) {
+    if (threadIdx.x == 0) s_i = atomicAdd(next, 1);
+    __syncthreads();
+    const int i = s_i;
+    __syncthreads();  // every thread has read s_i before thread 0 takes the next item
+    if (i >= n) break;
+    cta_aptp_front(sh, tpp_cnt, ids[i], F, A, o);
+  }
 }
 
 }  // namespace rvg
@@ -1185,6 +1214,7 @@ struct rvg_handle {
   std::vector<int8_t> route;                         // per front: 1 = mixed form (decided on the device)
   std::vector<int32_t> sel_large;                    // the large fronts of the last factorization
   bool sel_force_fp64 = false;                       // the FP64 refactorization after a growth flag
+  int aptp_ctas = 0;                                 // resident CTAs of the medium fronts' queue kernel
   int64_t sel_routed = 0, sel_flagged = 0, sel_fallback = 0;
   // measurement
   bool profiling = false;
@@ -1998,6 +2028,11 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       else if (f.flags & FF_LARGE) large_ids.push_back((int32_t)s);
       else aptp_ids.push_back((int32_t)s);
     }
+    // medium fronts largest first (dense work ~ k m^2): the persistent launch starts the long ones early
+    std::stable_sort(aptp_ids.begin(), aptp_ids.end(), [&](int32_t a, int32_t b) {
+      const DFront &fa = h->h_fronts[a], &fb = h->h_fronts[b];
+      return (double)fa.k * fa.m * fa.m > (double)fb.k * fb.m * fb.m;
+    });
     std::vector<ScatterItem> sitems;
     for (int64_t s : wave)
       for (int64_t e = P.amap_ptr[s]; e < P.amap_ptr[s + 1]; e += 256) sitems.push_back(ScatterItem{(int32_t)s, 0, e});
@@ -2031,6 +2066,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     for (size_t q = 0; q < maxch; ++q) o_e[q] = pk.add(eitems[q]);
     size_t o_w = pk.add(witems), o_g = pk.add(gitems);
     size_t o_cnt = pk.add(std::vector<int32_t>(3 * (size_t)nw + 4, 0));
+    size_t o_q = pk.add(std::vector<int32_t>(4, 0));  // work-queue counter of the medium fronts' launch
     const bool learned = h->opt.precision == 2 && !large_ids.empty();
     size_t o_lg = 0, o_rt = 0;
     if (learned) {
@@ -2101,9 +2137,17 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       k_tpp<<<blocks_for(tpp_ids.size(), 8), 256, 0, st>>>((const int32_t*)(D + o_tpp), (int)tpp_ids.size(),
                                                             h->d_fronts, A, dop);
     mark(h, RVG_PART_TPP);
-    if (!aptp_ids.empty())
-      k_aptp<<<(unsigned)aptp_ids.size(), NT, 0, st>>>((const int32_t*)(D + o_aptp), (int)aptp_ids.size(),
-                                                        h->d_fronts, A, dop);
+    if (!aptp_ids.empty()) {
+      if (!h->aptp_ctas) {  // resident CTAs of the queue kernel on this device
+        int occ = 0, sms = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_aptp_queue, NT, 0));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+        h->aptp_ctas = std::max(1, occ) * std::max(1, sms);
+      }
+      const int na = (int)aptp_ids.size();
+      k_aptp_queue<<<(unsigned)std::min(na, h->aptp_ctas), NT, 0, st>>>((const int32_t*)(D + o_aptp), na,
+                                                                        (int32_t*)(D + o_q), h->d_fronts, A, dop);
+    }
     mark(h, RVG_PART_APTP);
     if ((rc = factor_large_fronts(h, large_ids, A, dop))) return rc;
     CK(cudaEventRecord(h->ev[3], st));
