@@ -54,23 +54,16 @@ def _key(solver, base, device_name):
     return "|".join([fingerprint(solver), base.precision, base.mixed_operands, str(base.mixed_flush), device_name])
 
 
-def autotune(solver: SparseLDLT, d_vals_ptr: int, d_scal_ptr: int | None, base: FactorOptions, reps: int = 2,
-             thresholds=DEFAULT_THRESHOLDS, tile_cols=DEFAULT_TILE_COLS, cache: str | None = None):
-    """(best options, [(candidate options as a dict, seconds)]) for factoring
-    the values at d_vals_ptr (device) with the solver's pattern."""
+def _event_timer(solver: SparseLDLT, d_vals_ptr: int, d_scal_ptr: int | None, reps: int):
+    """Seconds of one factorization with options o: one untimed run (sizes the
+    arenas), then the best of `reps` runs timed by CUDA events on the handle's
+    stream."""
     import torch
-    dev = torch.cuda.get_device_name()
-    key = _key(solver, base, dev)
-    if cache and os.path.exists(cache):
-        with open(cache) as f:
-            got = json.load(f).get(key)
-        if got:
-            return dataclasses.replace(base, **got["best"]), [(c, t) for c, t in got["table"]]
-    table = []
-    for o in candidates(base, thresholds, tile_cols):
+
+    def run(o: FactorOptions) -> float:
         solver._ensure_handle(o)
         st = torch.cuda.ExternalStream(solver.stream())
-        solver.factor_device(d_vals_ptr, d_scal_ptr, o)  # warm-up (sizes the arenas)
+        solver.factor_device(d_vals_ptr, d_scal_ptr, o)
         best = None
         for _ in range(reps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -80,7 +73,31 @@ def autotune(solver: SparseLDLT, d_vals_ptr: int, d_scal_ptr: int | None, base: 
             e1.synchronize()
             t = e0.elapsed_time(e1) * 1e-3
             best = t if best is None else min(best, t)
-        table.append(({"large_front_threshold": o.large_front_threshold, "mixed_tile_cols": o.mixed_tile_cols}, best))
+        return best
+    return run
+
+
+def autotune(solver: SparseLDLT, d_vals_ptr: int | None, d_scal_ptr: int | None, base: FactorOptions, reps: int = 2,
+             thresholds=DEFAULT_THRESHOLDS, tile_cols=DEFAULT_TILE_COLS, cache: str | None = None, timer=None,
+             device_name: str | None = None):
+    """(best options, [(candidate options as a dict, seconds)]) for factoring
+    the values at d_vals_ptr (device) with the solver's pattern.  `timer`
+    (options -> seconds) replaces the CUDA-event timing, `device_name` the
+    current device's name in the cache key."""
+    if device_name is None:
+        import torch
+        device_name = torch.cuda.get_device_name()
+    key = _key(solver, base, device_name)
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            got = json.load(f).get(key)
+        if got:
+            return dataclasses.replace(base, **got["best"]), [(c, t) for c, t in got["table"]]
+    run = timer or _event_timer(solver, d_vals_ptr, d_scal_ptr, reps)
+    table = []
+    for o in candidates(base, thresholds, tile_cols):
+        table.append(({"large_front_threshold": o.large_front_threshold, "mixed_tile_cols": o.mixed_tile_cols},
+                      float(run(o))))
     choice = min(table, key=lambda r: r[1])[0]
     if cache:
         data = {}

@@ -13,7 +13,7 @@ to plain FP64 by that prediction.  A mixed front whose largest |D| entry grows
 past growth_bound times its largest assembled entry makes the library factor
 again in FP64, and `timed_solve` (factor, then solve to the tolerance)
 refactors in FP64 when refinement stalls: the plain FP64 form is the
-selector's fallback and judge.
+selector's fallback and arbiter.
 
 Labels come from the solver itself (`label_fronts`): every matrix is factored
 twice, all large fronts in FP64 and all in the mixed form, and a front is

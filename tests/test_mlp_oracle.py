@@ -48,3 +48,28 @@ def test_adam_step(mlp_oracle):
     nz = np.abs(g) > 1e-3
     assert np.allclose(d[nz], 0.01 * np.sign(g[nz]), rtol=1e-4)
     assert np.array_equal(p1[mo.NTRAIN:], p[mo.NTRAIN:])  # normalisation untouched
+
+
+def test_gradient_matches_torch_autograd(mlp_oracle):
+    """The oracle's hand-written backward pass against torch autograd (float64, CPU)."""
+    import torch
+    mo = mlp_oracle
+    rng = np.random.default_rng(11)
+    p = random_params(mo, 12)
+    x = rng.normal(0, 1.5, (300, mo.IN))
+    y = (rng.uniform(size=300) < 0.4).astype(float)
+    w = rng.uniform(0.5, 2.0, 300)
+    loss, g = mo.loss_grad(p, x, y, w, norm=w.sum())
+    P = torch.tensor(p, dtype=torch.float64, requires_grad=True)
+    W1 = P[mo.W1:mo.B1].reshape(mo.H, mo.IN)
+    W2 = P[mo.W2:mo.B2].reshape(mo.H, mo.H)
+    xn = (torch.tensor(x) - P[mo.MU:mo.SD].detach()) / P[mo.SD:].detach()
+    h1 = torch.relu(xn @ W1.T + P[mo.B1:mo.W2])
+    h2 = torch.relu(h1 @ W2.T + P[mo.B2:mo.W3])
+    z = h2 @ P[mo.W3:mo.B3] + P[mo.B3]
+    lt = torch.sum(torch.tensor(w) * torch.nn.functional.binary_cross_entropy_with_logits(
+        z, torch.tensor(y), reduction="none")) / float(w.sum())
+    lt.backward()
+    assert np.isclose(lt.item(), loss, rtol=1e-12)
+    assert np.allclose(P.grad.numpy()[:mo.NTRAIN], g, rtol=1e-10, atol=1e-13)
+    assert np.all(P.grad.numpy()[mo.NTRAIN:] == 0)  # the normalisation is not trained
