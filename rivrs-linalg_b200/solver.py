@@ -86,6 +86,23 @@ class SolveBeforeFactor(SparseError):
     pass
 
 
+class IoError(SparseError):
+    """SparseError::IoError (error.rs:64-71): a file that cannot be read."""
+
+    def __init__(self, path, source):
+        super().__init__(f"IO error for '{path}': {source}")
+        self.path, self.source = path, source
+
+
+class ParseError(SparseError):
+    """SparseError::ParseError (error.rs:72-80): malformed input."""
+
+    def __init__(self, path, reason, line=None):
+        where = f"'{path}' at line {line}" if line is not None else f"'{path}'"
+        super().__init__(f"Parse error in {where}: {reason}")
+        self.path, self.reason, self.line = path, reason, line
+
+
 _ERRMAP = {1: DimensionMismatch, 2: InvalidInput, 3: SolveBeforeFactor}
 
 

@@ -1,9 +1,10 @@
 """Regenerates tests/golden/hand_constructed.json from the reference's own
 fixtures (rivrs-linalg: sparse/test-data/hand-constructed/*.mtx + *.json).
 
-Each entry keeps the matrix (lower-triangle coordinates, as in the .mtx) and
-the fields the reference's tests assert on: the exact inertia and, for the
-documentation of the case, the D-block sizes of the published factorization.
+Each entry keeps the matrix (lower-triangle coordinates, as in the .mtx), the
+fields the reference's tests assert on (the exact inertia, the D-block sizes)
+and the published factorization itself (permutation, strict lower L entries,
+D blocks) in the reference's JSON layout (sparse/src/io/reference.rs).
 
     python tests/golden/make_golden.py /path/to/rivrs-linalg
 """
@@ -37,6 +38,9 @@ def main(ref_root):
             "entries": entries,
             "inertia": [gold["inertia"]["positive"], gold["inertia"]["negative"], gold["inertia"]["zero"]],
             "d_block_sizes": [b["size"] for b in gold["d_blocks"]],
+            # the published factorization itself, in the reference's JSON layout
+            "reference": {k: gold[k] for k in ("matrix_name", "permutation", "l_entries", "d_blocks", "inertia")
+                          if k in gold},
         }
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hand_constructed.json")
     with open(dst, "w") as f:
