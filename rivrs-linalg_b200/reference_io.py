@@ -1,4 +1,11 @@
-"""Known-factorization fixtures in the reference's JSON layout.
+"""Input files in the reference's formats: Matrix Market matrices and the
+known-factorization JSON fixtures.
+
+`load_mtx` reads `coordinate real symmetric` Matrix Market files as the
+reference's `load_mtx` does (sparse/src/io/mtx.rs:27-172): any other header is
+rejected, indices are 1-based and bounds-checked, explicit zeros are dropped
+(they would add spurious edges to the ordering's graph), off-diagonal entries
+are mirrored, and every malformed line is a ParseError naming its line.
 
 The reference keeps, beside each hand-constructed test matrix, a companion
 JSON file with an analytically known LDL^T factorization and loads it with
@@ -21,6 +28,80 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .solver import IoError, ParseError
+
+_MTX_HEADER = "%%matrixmarket matrix coordinate real symmetric"
+
+
+def load_mtx(path, name: str | None = None):
+    """A problems.System (both triangles stored) from a `coordinate real
+    symmetric` Matrix Market file (mtx.rs:27-172)."""
+    import scipy.sparse as sp
+
+    from . import problems
+    path = os.fspath(path)
+    try:
+        with open(path) as f:
+            lines = f.read().splitlines()
+    except OSError as e:
+        raise IoError(path, str(e)) from None
+    if not lines:
+        raise ParseError(path, "empty file", 1)
+    if not lines[0].lower().startswith(_MTX_HEADER):
+        raise ParseError(path, "unsupported format: expected '%%MatrixMarket matrix coordinate real symmetric', "
+                         f"got '{lines[0]}'", 1)
+    i = 1
+    while i < len(lines) and lines[i].startswith("%"):
+        i += 1
+    if i >= len(lines):
+        raise ParseError(path, "missing size line")
+    parts = lines[i].split()
+    if len(parts) != 3:
+        raise ParseError(path, f"size line must have 3 values (nrows ncols nnz), got {len(parts)}", i + 1)
+    dims = []
+    for what, tok in zip(("nrows", "ncols", "nnz"), parts):
+        try:
+            v = int(tok)
+            if v < 0:
+                raise ValueError
+        except ValueError:
+            raise ParseError(path, f"invalid {what}: '{tok}'", i + 1) from None
+        dims.append(v)
+    nrows, ncols, _ = dims
+    rows, cols, vals = [], [], []
+    for j in range(i + 1, len(lines)):
+        line = lines[j].strip()
+        if not line or line.startswith("%"):
+            continue
+        p = line.split()
+        if len(p) != 3:
+            raise ParseError(path, f"data line must have 3 values (row col val), got {len(p)}", j + 1)
+        try:
+            r = int(p[0])
+        except ValueError:
+            raise ParseError(path, f"invalid row index: '{p[0]}'", j + 1) from None
+        try:
+            c = int(p[1])
+        except ValueError:
+            raise ParseError(path, f"invalid col index: '{p[1]}'", j + 1) from None
+        try:
+            v = float(p[2])
+        except ValueError:
+            raise ParseError(path, f"invalid value: '{p[2]}'", j + 1) from None
+        if r <= 0 or c <= 0:
+            raise ParseError(path, "Matrix Market indices are 1-based; got 0", j + 1)
+        r, c = r - 1, c - 1
+        if r >= nrows or c >= ncols:
+            raise ParseError(path, f"index ({r}, {c}) out of bounds for {nrows}x{ncols} matrix", j + 1)
+        if v == 0.0:
+            continue
+        rows.append(r); cols.append(c); vals.append(v)
+        if r != c:
+            rows.append(c); cols.append(r); vals.append(v)
+    a = sp.csc_matrix((np.array(vals, np.float64), (np.array(rows, np.int64), np.array(cols, np.int64))),
+                      shape=(nrows, ncols))
+    a.sum_duplicates()
+    a.sort_indices()
+    return problems.from_scipy(name or os.path.basename(path).rsplit(".", 1)[0], a)
 
 
 @dataclass

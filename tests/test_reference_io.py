@@ -76,3 +76,48 @@ def test_load_from_file_and_errors(rv, golden, tmp_path):
     for obj in cases:
         with pytest.raises(rv.solver.ParseError):
             io.parse_reference(obj)
+
+
+def write_mtx(path, e, header="%%MatrixMarket matrix coordinate real symmetric"):
+    with open(path, "w") as f:
+        f.write(header + "\n% a comment\n")
+        f.write(f"{e['n']} {e['n']} {len(e['entries'])}\n")
+        for r, c, v in e["entries"]:
+            f.write(f"{r + 1} {c + 1} {v!r}\n")
+
+
+def test_load_mtx_round_trip(rv, golden, tmp_path):
+    io = rv.reference_io
+    for name, e in golden.items():
+        p = tmp_path / f"{name}.mtx"
+        write_mtx(p, e)
+        s = io.load_mtx(p)
+        assert s.name == name and s.n == e["n"]
+        A = dense(e)
+        A[A == 0.0] = 0.0
+        assert np.array_equal(s.to_scipy().toarray(), A), name
+
+
+def test_load_mtx_errors(rv, tmp_path):
+    io = rv.reference_io
+    ok_head = "%%MatrixMarket matrix coordinate real symmetric\n"
+
+    def load(text):
+        p = tmp_path / "m.mtx"
+        p.write_text(text)
+        return io.load_mtx(p)
+    s = load(ok_head + "3 3 4\n1 1 2.0\n2 1 0.0\n3 2 -1.5\n3 3 4.0\n")  # the explicit zero is dropped
+    assert s.to_scipy().nnz == 4 and s.to_scipy()[1, 2] == -1.5 and s.to_scipy()[0, 1] == 0
+    with pytest.raises(rv.solver.IoError):
+        io.load_mtx(tmp_path / "none.mtx")
+    bad = [("", 1), ("%%MatrixMarket matrix coordinate real general\n2 2 1\n1 1 1.0\n", 1),
+           ("%%MatrixMarket matrix array real symmetric\n2 2\n1\n", 1),
+           (ok_head + "% only comments\n", None),
+           (ok_head + "2 2\n", 2), (ok_head + "2 x 1\n", 2),
+           (ok_head + "2 2 1\n1 1\n", 3), (ok_head + "2 2 1\n0 1 1.0\n", 3),
+           (ok_head + "2 2 1\n3 1 1.0\n", 3), (ok_head + "2 2 1\na 1 1.0\n", 3),
+           (ok_head + "2 2 1\n1 1 nan?\n", 3)]
+    for text, line in bad:
+        with pytest.raises(rv.solver.ParseError) as ei:
+            load(text)
+        assert ei.value.line == line, (text, ei.value)
