@@ -159,3 +159,80 @@ def test_nemin_and_small_leaf_equivalence(rv, orc):
         f, _ = oracle_factor(rv, orc, s, **opts)
         assert f.inertia() == s.inertia
         assert rv.problems.backward_error(s, f.solve(b), b) < 1e-14
+
+
+# ---- torture mix for the dense kernel (factor.rs:6862-6960; generators of testing/perturbations.rs) ----
+def _indefinite_dominant(m, rng):
+    """Random symmetric entries in [-1, 1) with a diagonal that dominates its
+    row, positive in the first half of the rows and negative in the rest."""
+    a = rng.uniform(-1.0, 1.0, (m, m))
+    a = np.tril(a) + np.tril(a, -1).T
+    off = np.abs(a).sum(1) - np.abs(np.diag(a))
+    margin = 1.0 + rng.uniform(0.0, 1.0, m)
+    sign = np.where(np.arange(m) < m // 2, 1.0, -1.0)
+    a[np.arange(m), np.arange(m)] = sign * (off + margin)
+    return a
+
+
+def _cause_delays(a, ib, rng):
+    """n/8 rows (with their columns) and n/8 single symmetric entries scaled by
+    1000; the first scaled row lies past the first inner block."""
+    m = a.shape[0]
+    if m < 8:
+        return
+    for t in range(m // 8):
+        r = ib + int(rng.integers(0, m - ib)) if (t == 0 and m > ib) else int(rng.integers(0, m))
+        a[r, :] *= 1000.0
+        a[:, r] *= 1000.0
+        a[r, r] /= 1000.0
+    for _ in range(m // 8):
+        i, j = int(rng.integers(0, m)), int(rng.integers(0, m))
+        a[i, j] *= 1000.0
+        if i != j:
+            a[j, i] *= 1000.0
+
+
+def _make_singular(a, c1, c2, scale=2.0):
+    """Column (and row) c2 becomes scale times column c1: rank drops by one."""
+    d1 = a[c1, c1]
+    col = a[:, c1].copy()
+    a[:, c2] = scale * col
+    a[c2, :] = scale * col
+    a[c2, c1] = a[c1, c2] = scale * d1
+    a[c2, c2] = scale * scale * d1
+
+
+@pytest.mark.parametrize("m,n", [(32, 32), (64, 64), (128, 128), (128, 48)])
+def test_dense_torture_mix(orc, m, n):
+    """70% delay-inducing, 20% singular, 10% singular-diagonal-block instances
+    (SPRAL's mix, as the reference's torture tests use it): every instance
+    accounts for all n fully-summed columns, and square non-singular ones that
+    are fully eliminated reconstruct to 5e-11."""
+    rng = np.random.default_rng(12345 + m + n)
+    ib = min(32, n)
+    opts = orc.options(inner_block_size=ib)
+    failures = []
+    for inst in range(150):
+        a = _indefinite_dominant(m, rng)
+        roll = rng.uniform()
+        singular = True
+        if roll < 0.70:
+            _cause_delays(a, ib, rng)
+            singular = False
+        elif roll < 0.90:
+            c1 = int(rng.integers(0, m))
+            c2 = int(rng.integers(0, m - 1))
+            c2 += c2 >= c1
+            _make_singular(a, c1, c2)
+        else:
+            b = int(rng.integers(0, m - ib + 1))
+            _make_singular(a, b, b + ib - 1)
+        af, perm, dt, dd, do, st, _ = orc.dense_aptp(a.copy(), p=n, opts=opts)
+        if st[1] + 2 * st[2] + st[3] != n:
+            failures.append((inst, "count", tuple(st)))
+            continue
+        if m == n and not singular and st[0] == n:
+            err = np.linalg.norm(reconstruct(af, perm, dt, dd, do, st[0]) - a) / np.linalg.norm(a)
+            if err > 5e-11:
+                failures.append((inst, "recon", err))
+    assert not failures, failures[:5]
