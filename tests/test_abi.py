@@ -56,3 +56,10 @@ def test_no_device_fails_loudly(rv):
     solver = rv.SparseLDLT.analyze(s)
     with pytest.raises(rv.SparseError, match="DeviceError"):
         solver.factor()
+
+
+def test_integration_guide_binds_every_symbol():
+    """Every entry point the header declares has its binding in INTEGRATION.md."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [n for n in declared_symbols() if f"fn {n}(" not in guide]
+    assert not missing, missing
