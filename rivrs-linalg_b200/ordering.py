@@ -21,29 +21,24 @@ import ctypes as C
 import numpy as np
 
 
-def nested_dissection_grid(dims, leaf: int = 8) -> np.ndarray:
-    """Geometric nested dissection of an nx*ny*nz grid (x fastest varying
-    within the linear index i*ny*nz + j*nz + k, i.e. C order of (i, j, k))."""
+def dissection_boxes(dims, leaf: int = 8) -> np.ndarray:
+    """The boxes of the geometric nested dissection of an nx*ny*nz grid in the
+    order their nodes are numbered (rows x0, x1, y0, y1, z0, z1): a box is
+    split along its longest side (x, then y, then z on ties) at the middle
+    plane; its first half, then its second half, then the plane; a box of at
+    most `leaf` nodes or with every side shorter than 3 is a leaf."""
     nx, ny, nz = dims
-    out = []
-
-    def emit(x0, x1, y0, y1, z0, z1):
-        i, j, k = np.meshgrid(np.arange(x0, x1), np.arange(y0, y1), np.arange(z0, z1), indexing="ij")
-        out.append((i * ny * nz + j * nz + k).ravel())
-
-    # explicit stack of (box, state): state 0 = visit, 1 = emit separator
-    stack = [((0, nx, 0, ny, 0, nz), None)]
+    boxes = []
+    # explicit stack of (box, is_separator)
+    stack = [((0, nx, 0, ny, 0, nz), False)]
     while stack:
-        box, sep = stack.pop()
-        if sep is not None:
-            emit(*sep)
-            continue
+        box, is_sep = stack.pop()
         x0, x1, y0, y1, z0, z1 = box
         sx, sy, sz = x1 - x0, y1 - y0, z1 - z0
         if sx <= 0 or sy <= 0 or sz <= 0:
             continue
-        if sx * sy * sz <= leaf or max(sx, sy, sz) < 3:
-            emit(*box)
+        if is_sep or sx * sy * sz <= leaf or max(sx, sy, sz) < 3:
+            boxes.append(box)
             continue
         if sx >= sy and sx >= sz:
             mid = x0 + sx // 2
@@ -54,13 +49,33 @@ def nested_dissection_grid(dims, leaf: int = 8) -> np.ndarray:
         else:
             mid = z0 + sz // 2
             a, b, s = (x0, x1, y0, y1, z0, mid), (x0, x1, y0, y1, mid + 1, z1), (x0, x1, y0, y1, mid, mid + 1)
-        # LIFO: push in reverse of the desired order (a, b, separator)
-        stack.append((None, s))
-        stack.append((b, None))
-        stack.append((a, None))
-    order = np.concatenate(out).astype(np.int64)
-    assert order.size == nx * ny * nz
-    return order
+        # LIFO: push in reverse of the order wanted (a, b, separator)
+        stack.append((s, True))
+        stack.append((b, False))
+        stack.append((a, False))
+    return np.array(boxes, dtype=np.int64).reshape(-1, 6)
+
+
+def nested_dissection_grid(dims, leaf: int = 8) -> np.ndarray:
+    """Geometric nested dissection of an nx*ny*nz grid (linear index
+    i*ny*nz + j*nz + k, i.e. C order of (i, j, k)); within a box its nodes
+    are numbered in C order too.  The boxes come from dissection_boxes; their
+    nodes are expanded for all boxes at once."""
+    nx, ny, nz = dims
+    b = dissection_boxes(dims, leaf)
+    sx, sy, sz = b[:, 1] - b[:, 0], b[:, 3] - b[:, 2], b[:, 5] - b[:, 4]
+    size = sx * sy * sz
+    n = int(size.sum())
+    assert n == nx * ny * nz
+    box = np.repeat(np.arange(b.shape[0]), size)
+    start = np.concatenate([[0], np.cumsum(size)[:-1]])
+    q = np.arange(n, dtype=np.int64) - start[box]
+    plane = (sy * sz)[box]
+    i = b[box, 0] + q // plane
+    r = q % plane
+    j = b[box, 2] + r // sz[box]
+    k = b[box, 4] + r % sz[box]
+    return (i * ny * nz + j * nz + k).astype(np.int64)
 
 
 def kkt_order(sysm, leaf: int = 8) -> np.ndarray:
