@@ -51,36 +51,52 @@ struct CostGraph {
 // Full symmetric pattern (an entry stored once or twice becomes both (i, j)
 // and (j, i)), explicit zeros dropped, rows sorted per column.
 CostGraph build_graph(int64_t n, const int64_t* colptr, const int64_t* rowidx, const double* val) {
-  std::vector<std::vector<std::pair<int64_t, double>>> cols(n);
+  using Entry = std::pair<int64_t, double>;  // (row, |a|)
+  // one array for every column's entries, both orientations: count, place, then sort each column
+  std::vector<int64_t> start(n + 1, 0);
   for (int64_t j = 0; j < n; ++j)
     for (int64_t k = colptr[j]; k < colptr[j + 1]; ++k) {
+      if (val[k] == 0.0) continue;
       const int64_t i = rowidx[k];
-      const double a = std::fabs(val[k]);
-      if (a == 0.0) continue;
-      cols[j].push_back({i, a});
-      if (i != j) cols[i].push_back({j, a});
+      ++start[j + 1];
+      if (i != j) ++start[i + 1];
     }
+  for (int64_t j = 0; j < n; ++j) start[j + 1] += start[j];
+  std::vector<Entry> ent(start[n]);
+  {
+    std::vector<int64_t> fill(start.begin(), start.end() - 1);
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t k = colptr[j]; k < colptr[j + 1]; ++k) {
+        const double a = std::fabs(val[k]);
+        if (a == 0.0) continue;
+        const int64_t i = rowidx[k];
+        ent[fill[j]++] = {i, a};
+        if (i != j) ent[fill[i]++] = {j, a};
+      }
+  }
   CostGraph g;
   g.n = n;
   g.ptr.assign(n + 1, 0);
   g.colmax_log.assign(n, -std::numeric_limits<double>::infinity());
+  g.row.resize(start[n]);
+  g.cost.resize(start[n]);
+  int64_t p = 0;
   for (int64_t j = 0; j < n; ++j) {
-    auto& c = cols[j];
-    std::sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first || (x.first == y.first && x.second < y.second); });
-    c.erase(std::unique(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first == y.first; }), c.end());
-    for (const auto& e : c) g.colmax_log[j] = std::max(g.colmax_log[j], std::log(e.second));
-    g.ptr[j + 1] = g.ptr[j] + (int64_t)c.size();
-  }
-  g.row.resize(g.ptr[n]);
-  g.cost.resize(g.ptr[n]);
-  for (int64_t j = 0; j < n; ++j) {
-    int64_t p = g.ptr[j];
-    for (const auto& e : cols[j]) {
-      g.row[p] = e.first;
-      g.cost[p] = g.colmax_log[j] - std::log(e.second);
-      ++p;
+    // rows in increasing order; an entry stored in both triangles appears twice: keep one (the smaller |a|)
+    auto b = ent.begin() + start[j], e = ent.begin() + start[j + 1];
+    std::sort(b, e, [](const Entry& x, const Entry& y) { return x.first < y.first || (x.first == y.first && x.second < y.second); });
+    e = std::unique(b, e, [](const Entry& x, const Entry& y) { return x.first == y.first; });
+    const int64_t p0 = p;
+    for (auto it = b; it != e; ++it, ++p) {
+      g.row[p] = it->first;
+      g.cost[p] = std::log(it->second);  // log |a| for now
+      g.colmax_log[j] = std::max(g.colmax_log[j], g.cost[p]);
     }
+    for (int64_t q = p0; q < p; ++q) g.cost[q] = g.colmax_log[j] - g.cost[q];
+    g.ptr[j + 1] = p;
   }
+  g.row.resize(p);
+  g.cost.resize(p);
   return g;
 }
 
