@@ -386,6 +386,19 @@ class SparseLDLT:
         _check(N.lib().rvg_front_info(self._handle, N.ptr(out, N.i64p), C.byref(ns)))
         return out[:9 * ns.value].reshape(ns.value, 9)
 
+    def per_supernode_stats(self):
+        """SparseLDLT::per_supernode_stats (solver.rs:533-543, PerSupernodeStats
+        numeric.rs:604-650): one dict per supernode of the last factorization,
+        or None before factor().  `max_l_entry` is not computed by this library
+        (None); the diagnostic timings of the reference's `diagnostic` feature
+        are not kept per supernode (see profile())."""
+        if not self._factored:
+            return None
+        fi = self.front_info()
+        return [dict(snode_id=s, front_size=int(r[0]), num_fully_summed=int(r[1]), num_eliminated=int(r[2]),
+                     num_delayed=int(r[1] - r[2]), num_1x1=int(r[3]), num_2x2=int(r[4]), max_l_entry=None)
+                for s, r in enumerate(fi)]
+
     # -- learned per-front precision ----------------------------------------
     def set_selector(self, selector, threshold: float | None = None, growth_bound: float | None = None):
         """Installs a trained selector (selector.PrecisionSelector) for
