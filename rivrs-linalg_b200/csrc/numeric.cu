@@ -902,6 +902,12 @@ __global__ void k_norms3(const double* r, const double* x, const double* b, int6
   }
   if ((threadIdx.x & 31) == 0) { atomicAdd(out, s0); atomicAdd(out + 1, s1); atomicAdd(out + 2, s2); }
 }
+// Raises *flag when any of the n values is NaN or infinite.
+__global__ void k_nonfinite(const double* v, int64_t n, int32_t* flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(v[i])) { atomicExch(flag, 1); return; }
+}
+
 __global__ void k_sumsq(const double* v, int64_t n, double* out) {
   double s = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) s += v[i] * v[i];
@@ -1215,6 +1221,7 @@ struct rvg_handle {
   std::vector<int32_t> sel_large;                    // the large fronts of the last factorization
   bool sel_force_fp64 = false;                       // the FP64 refactorization after a growth flag
   int aptp_ctas = 0;                                 // resident CTAs of the medium fronts' queue kernel
+  int32_t* d_nonfinite = nullptr;                    // set when the values or the scaling hold NaN or Inf
   int64_t sel_routed = 0, sel_flagged = 0, sel_fallback = 0;
   // measurement
   bool profiling = false;
@@ -2518,6 +2525,23 @@ static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
   }
   // the refinement needs the unfactored values and ||A||_F
   if (dv != h->d_vals && h->nnz) CK(cudaMemcpyAsync(h->d_vals, dv, h->nnz * 8, cudaMemcpyDeviceToDevice, h->st));
+  // NaN or Inf in the values or the scaling: a clean InvalidInput before any factor kernel runs (the
+  // reference rejects them in its MC64 scaling, ordering/matching.rs:143-157)
+  if (h->nnz || (ds && h->P.n)) {
+    if (!h->d_nonfinite) CK(cudaMalloc((void**)&h->d_nonfinite, sizeof(int32_t)));
+    CK(cudaMemsetAsync(h->d_nonfinite, 0, sizeof(int32_t), h->st));
+    if (h->nnz) k_nonfinite<<<296, 256, 0, h->st>>>(h->d_vals, h->nnz, h->d_nonfinite);
+    if (ds && h->P.n) k_nonfinite<<<296, 256, 0, h->st>>>(ds, h->P.n, h->d_nonfinite);
+    CK(cudaGetLastError());
+    int32_t bad = 0;
+    CK(cudaMemcpyAsync(&bad, h->d_nonfinite, 4, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (bad) {
+      h->factored = false;
+      set_error("the matrix values or the scaling contain NaN or Inf");
+      return RVG_ERR_INVALID_INPUT;
+    }
+  }
   bool done = false;
   if (h->opt.graph_refactor && h->rec_ok && h->opt.precision != 2) {
     if ((rc = replay_factor(h, ds, &done))) return rc;
@@ -3361,6 +3385,7 @@ void rvg_destroy(rvg_handle* h) {
   if (h->d_sel) cudaFree(h->d_sel);
   fr(h->d_feat);
   if (h->d_sel_flag) cudaFree(h->d_sel_flag);
+  if (h->d_nonfinite) cudaFree(h->d_nonfinite);
   if (h->d_mismatch) cudaFree(h->d_mismatch);
   if (h->h_stage_all) cudaFreeHost(h->h_stage_all);
   for (size_t t = 1; t < h->lfx.size(); ++t) {
