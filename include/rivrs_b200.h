@@ -353,9 +353,10 @@ void rvg_destroy(rvg_handle* h);
  * host application that owns the device's memory budget and forbids
  * allocation after start-up, code inside stream-ordered work that an
  * allocation would synchronise or fragment, real-time loops and callbacks.
- * It factors one dense symmetric front in place with the same kernels as
- * rvg_factor (aptp_factor_in_place semantics, factor.rs:301-404): d_a is
- * m x m column-major (lower triangle read, the first p columns factored),
+ * It factors one dense symmetric front in place with the same kernels and
+ * the same pivoting as rvg_factor uses for a front: d_a is m x m
+ * column-major (lower triangle read, the first p columns factored, the
+ * factored columns' rows below p updated as well),
  * d_perm receives the pivot order (p), d_dtype / d_ddiag / d_doff the D
  * entries (p; codes as in rvg_pivot_record), d_counts [ne, n1x1, n2x2].
  * All buffers are the caller's device memory; the call allocates nothing.

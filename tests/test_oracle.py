@@ -236,3 +236,29 @@ def test_dense_torture_mix(orc, m, n):
             if err > 5e-11:
                 failures.append((inst, "recon", err))
     assert not failures, failures[:5]
+
+
+@pytest.mark.parametrize("kind", ["lap", "kkt", "dense"])
+def test_thread_count_invariance(rv, orc, kind):
+    """The oracle's OpenMP blocking reorders only independent output entries:
+    its pivot record, D and statistics are the same for any thread count."""
+    if kind == "lap":
+        s = rv.problems.shifted_laplacian(20, 0.1)
+    elif kind == "kkt":
+        s = rv.problems.kkt(14, seed=2)
+    else:
+        rng = np.random.default_rng(9)
+        a = rng.standard_normal((700, 700))
+        a = a + a.T
+        a[np.arange(700), np.arange(700)] *= 1e-3
+        s = rv.problems.from_scipy("dense700", a)
+    sym = rv.symbolic_analyze(s.n, s.colptr, s.rowidx, rv.ordering.default_order(s))
+    recs = []
+    for nt in (1, 3, 8):
+        f = orc.OracleFactor(s, sym, None, orc.options(), nthreads=nt)
+        recs.append((f.pivot_record(), f.stats(), f.inertia()))
+        f.close()
+    for (p, st, ine) in recs[1:]:
+        for x, y in zip(p, recs[0][0]):
+            assert np.array_equal(x, y)
+        assert st == recs[0][1] and ine == recs[0][2]
