@@ -25,9 +25,14 @@ followed by GMRES-IR.  `value` is the fastest form that reaches 1e-14.
            the measured-peaks file for BF16).
 * `hbm_bound_parts` the solve and the assembly against the measured HBM
            copy bandwidth.
-* `cpu_baseline` the oracle (OpenMP restatement of the reference numeric
-           path) on a bounded KKT sample of the same family, its flop rate
-           extrapolated to the workload.
+* `cpu_baseline` the CPU restatement of the reference numeric phase
+           (oracle/, blocked, OpenMP on every host core) on a bounded part
+           of THIS workload's factorization (about 20 s), scaled to the
+           whole by flops.
+`--impl reference` runs that CPU restatement alone (oracle libraries only, no
+GPU library) through ONE complete factor + solve of the workload, timed in
+`--steps` consecutive slices of the factorization; its value is the sum of
+the slices.
 `--config batch64` times the many-systems workload instead (64 systems,
 grouped unions; see run_batch).  Multi-GPU runs are independent replicas
 (the single-system path does not shard): each rank factors its own copy, no
@@ -83,18 +88,6 @@ def build_system(rv, cfg):
     return s, b
 
 
-def sample_system(rv, cfg):
-    """Bounded CPU sample of the same family (about 10-30 s on 8 cores)."""
-    kind, g, _ = CONFIGS[cfg]
-    if kind == "kkt":
-        gs = min(g, 26)
-        s = rv.problems.kkt(gs, seed=0)
-        return s, rv.problems.rhs_normal(s.n, seed=0), f"kkt27_{gs}^3 (n={s.n})"
-    gs = min(g, 40)
-    s = rv.problems.shifted_laplacian(gs, 0.10 if g < 100 else 0.05)
-    return s, rv.problems.rhs_uniform(s.n, seed=0), f"laplace7_{gs}^3 (n={s.n})"
-
-
 def dense_flops(sym):
     """Delay-free factor + Schur flops of the supernode structure (2 per multiply-add)."""
     k = (sym.sup_end - sym.sup_begin).astype(np.float64)
@@ -113,26 +106,79 @@ def dense_flops(sym):
     return float(np.sum(s1 + s2))
 
 
-def cpu_baseline(rv, orc, cfg, full_flops, reps=1):
-    s, b, desc = sample_system(rv, cfg)
-    an, _ = analyze(rv, s)
-    sym = an.symbolic
-    threads = os.cpu_count() or 1
-    times = []
-    for _ in range(reps):
+def cpu_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+def cpu_analyze(rv, orc, s):
+    """The analysis for a CPU-only run: the project's ordering and the
+    library's host symbolic analysis + MC64 through the oracle's analysis
+    library (no GPU library loaded)."""
+    return orc.analyze(s, rv.ordering.default_order(s), mc64=True)
+
+
+def cpu_sample(rv, orc, s, b, budget_s=20.0):
+    """The CPU restatement of the reference's numeric phase on THIS workload
+    for a bounded time: the factorization runs in slices of 2% of its
+    delay-free flops until budget_s have passed; the time is scaled to the
+    whole factorization by flops (a bounded sample, not a full run)."""
+    sym, sc = cpu_analyze(rv, orc, s)
+    threads = cpu_threads()
+    f = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=threads, sliced=True)
+    tot = f.total_flops()
+    t, frac, ended = 0.0, 0.0, False
+    while t < budget_s and not ended:
+        frac = min(1.0, frac + 0.02)
         t0 = time.perf_counter()
-        f = orc.OracleFactor(s, sym, an._scaling, orc.options(), nthreads=threads)
-        x = f.solve(b)
-        times.append(time.perf_counter() - t0)
+        ended = f.advance(tot * frac if frac < 1.0 else 1e300)
+        t += time.perf_counter() - t0
+    done = orc.lib().orc_session_done(f.session) if not ended else tot
+    f.close()
+    orc.release_cache()
+    value = t * tot / max(done, 1.0)
+    return dict(value=value, unit="s", cores=threads, kind="port",
+                sample=f"CPU restatement of the reference numeric phase (blocked, OpenMP) on this workload: "
+                       f"the first {100 * done / tot:.1f}% of its delay-free flops ({done:.3e} of {tot:.3e}, "
+                       f"bottom-up) in {t:.1f} s on {threads} threads, scaled to the whole factorization by flops "
+                       f"(the full run is the reference arm, bench.py --impl reference)")
+
+
+def reference_full_run(rv, orc, s, b, steps, warmup):
+    """The reference arm: ONE complete factor + solve of the workload by the
+    CPU restatement of the reference numeric phase, on every host core,
+    timed in `steps` slices (each a bounded part of the factorization, cut by
+    delay-free flops; the last one also runs the solve).  The value is the
+    sum of the slices: the measured time of the whole factor + solve.  The
+    warm-up steps run the first slices of a separate factorization of the
+    same matrix, which is then discarded."""
+    sym, sc = cpu_analyze(rv, orc, s)
+    threads = cpu_threads()
+    for w in range(warmup):
+        f = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=threads, sliced=True)
+        f.advance(f.total_flops() * 0.005 * (w + 1))
         f.close()
-    t = statistics.median(times)
-    flops = dense_flops(sym)
-    rate = flops / t
+    orc.release_cache()
+    f = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=threads, sliced=True)  # pattern set-up, untimed
+    tot = f.total_flops()
+    times = []
+    x = None
+    for i in range(steps):
+        t0 = time.perf_counter()
+        if i < steps - 1:
+            f.advance(tot * (i + 1) / steps)
+        else:
+            f.finish()
+            x = f.solve(b)
+        times.append(time.perf_counter() - t0)
+    if x is None:  # steps == 0
+        f.finish()
+        x = f.solve(b)
     err = rv.problems.backward_error(s, x, b)
-    return dict(value=full_flops / rate, unit="s", cores=threads, kind="port",
-                sample=f"oracle factor+solve of {desc}: {t:.2f} s for {flops:.3e} flops "
-                       f"({rate / 1e9:.1f} GFLOP/s, bwd err {err:.1e}), extrapolated to the workload's "
-                       f"{full_flops:.3e} flops"), t
+    inertia = f.inertia()
+    st = f.stats()
+    f.close()
+    orc.release_cache()
+    return dict(value=sum(times), times=times, cores=threads, bwd_err=err, inertia=inertia, stats=st, flops=tot)
 
 
 class ClockSampler:
@@ -361,27 +407,28 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
     bl.close()
 
 
-def batch_cpu_baseline(rv, orc, systems, full_flops):
-    """The oracle on the first systems of the batch (a bounded sample, all host
-    cores), extrapolated to the whole batch by flops."""
-    threads = os.cpu_count() or 1
+def batch_cpu_baseline(rv, orc, systems, full_flops, budget_s=10.0):
+    """The CPU restatement on the first systems of the batch (a bounded
+    sample, all host cores), scaled to the whole batch by flops."""
+    threads = cpu_threads()
     t, fl, used = 0.0, 0.0, 0
     for sy in systems:
-        if t > 10.0:
+        if t > budget_s:
             break
-        an, _ = analyze(rv, sy)
+        sym, sc = cpu_analyze(rv, orc, sy)
         b = rv.problems.rhs_normal(sy.n, 0)
         t0 = time.perf_counter()
-        f = orc.OracleFactor(sy, an.symbolic, an._scaling, orc.options(), nthreads=threads)
+        f = orc.OracleFactor(sy, sym, sc, orc.options(), nthreads=threads)
         f.solve(b)
         t += time.perf_counter() - t0
         f.close()
-        fl += dense_flops(an.symbolic)
+        fl += dense_flops(sym)
         used += 1
+    orc.release_cache()
     rate = fl / t
     return dict(value=full_flops / rate, unit="s", cores=threads, kind="port",
-                sample=f"oracle factor+solve of the first {used} systems: {t:.2f} s for {fl:.3e} flops "
-                       f"({rate / 1e9:.1f} GFLOP/s), extrapolated to the batch's {full_flops:.3e} flops")
+                sample=f"CPU restatement, factor+solve of the first {used} systems: {t:.2f} s for {fl:.3e} flops "
+                       f"({rate / 1e9:.1f} GFLOP/s), scaled to the batch's {full_flops:.3e} flops")
 
 
 def time_form(rv, torch, solver, s, b, opts, warmup, steps):
@@ -473,6 +520,58 @@ def run_learned(args, rv, torch):
     print(json.dumps(line), flush=True)
 
 
+def run_reference(args, rv, entry, rank):
+    """The reference arm: the CPU restatement of the reference's numeric phase
+    (oracle/, OpenMP, all host cores) on this arm's workload, through the
+    oracle's own libraries only (its analysis library reuses the library's
+    host analysis sources without the GPU code).  Rank 0 alone runs it."""
+    if rank != 0:
+        return
+    orc = entry.load_oracle()
+    threads = cpu_threads()
+    base = {"metric": METRIC, "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "impl": "reference"}
+    if args.config in ("batch64", "learned"):
+        # bounded samples of these workloads, scaled by flops
+        if args.config == "batch64":
+            systems = [f[0] for f in rv.problems.batch_family(count=64, seed=1)]
+            full = sum(dense_flops(cpu_analyze(rv, orc, sy)[0]) for sy in systems)
+            cb = batch_cpu_baseline(rv, orc, systems, full)
+        else:
+            parts = []
+            for cfg in ("lap100", "kkt60"):
+                s, b = build_system(rv, cfg)
+                parts.append(cpu_sample(rv, orc, s, b))
+            cb = dict(parts[1])
+            cb["value"] = parts[0]["value"] + parts[1]["value"]
+            cb["sample"] = "; ".join(p["sample"] for p in parts) + " (sum of the two)"
+        v = cb["value"]
+        line = dict(base, value=v, ms_per_step=v * 1e3,
+                    config={"workload": CONFIGS[args.config][2], "form": "plain FP64 (CPU restatement)",
+                            "timing": "bounded sample scaled by flops"},
+                    cpu_baseline=cb, e2e={"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return
+    s, b = build_system(rv, args.config)
+    r = reference_full_run(rv, orc, s, b, max(args.steps, 1), args.warmup)
+    v = r["value"]
+    sample = (f"one complete factor+solve of this workload ({r['flops']:.3e} delay-free flops after amalgamation), "
+              f"timed in {len(r['times'])} slices cut by flops (the last with the solve); value = their sum")
+    line = dict(base, value=v, ms_per_step=1e3 * v / len(r["times"]),
+                config={"workload": CONFIGS[args.config][2],
+                        "form": "plain FP64, CPU restatement of the reference numeric phase (blocked rank-32 "
+                                "updates, OpenMP inside large fronts and across each wave's fronts)",
+                        "ordering": "geometric nested dissection, constraints last", "scaling": "MC64",
+                        "timing": "steps are consecutive slices of ONE factorization; value = sum of the slices",
+                        "l2": "working set far above the CPU caches"},
+                step_s=r["times"], bwd_err=r["bwd_err"], inertia=list(r["inertia"]), stats=r["stats"],
+                factor_gflops=r["flops"] / v / 1e9,
+                cpu_baseline={"value": v, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+                e2e={"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -498,48 +597,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
-        # the reference's numeric path restated on the CPU, all host cores, rank 0 only
-        if rank != 0:
-            return
-        orc = entry.load_oracle()
-        if args.config == "batch64":
-            systems = [f[0] for f in rv.problems.batch_family(count=64, seed=1)]
-            full = sum(dense_flops(rv.SparseLDLT.analyze(sy).symbolic) for sy in systems)
-            sample = lambda: (batch_cpu_baseline(rv, orc, systems, full), None)
-        elif args.config == "learned":
-            # the held-out pair in plain FP64 on the host: each extrapolated from a bounded sample of its family
-            fulls = {}
-            for cfg in ("lap100", "kkt60"):
-                sf, _ = build_system(rv, cfg)
-                fulls[cfg] = dense_flops(rv.symbolic_analyze(sf.n, sf.colptr, sf.rowidx,
-                                                             rv.ordering.default_order(sf)))
-
-            def sample():
-                parts = [cpu_baseline(rv, orc, cfg, fulls[cfg])[0] for cfg in ("lap100", "kkt60")]
-                cb = dict(parts[1])
-                cb["value"] = parts[0]["value"] + parts[1]["value"]
-                cb["sample"] = "; ".join(p["sample"] for p in parts) + " (sum of the two)"
-                return cb, None
-        else:
-            s_full, _ = build_system(rv, args.config)
-            sym_full = rv.symbolic_analyze(s_full.n, s_full.colptr, s_full.rowidx,
-                                           rv.ordering.default_order(s_full))
-            full = dense_flops(sym_full)
-            sample = lambda: cpu_baseline(rv, orc, args.config, full)
-        vals = []
-        for i in range(args.warmup + args.steps):
-            cb, _ = sample()
-            if i >= args.warmup:
-                vals.append(cb["value"])
-        v = statistics.median(vals)
-        cb["value"] = v
-        line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
-                "config": {"workload": CONFIGS[args.config][2], "form": "plain FP64",
-                           "l2": "working set far above L2 (126 MB)"},
-                "cpu_baseline": cb, "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
+        run_reference(args, rv, entry, rank)
         return
 
     import torch
@@ -779,7 +837,7 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         orc = entry.load_oracle()
-        cb, _ = cpu_baseline(rv, orc, args.config, full_flops)
+        cb = cpu_sample(rv, orc, s, b)
 
     if rank == 0:
         line = {

@@ -39,6 +39,16 @@
 #ifdef _OPENMP
 #include <omp.h>
 #endif
+#if defined(__x86_64__) && defined(__GNUC__)
+#include <immintrin.h>
+#endif
+#include <stdlib.h>
+#include <sys/mman.h>
+
+#include <condition_variable>
+#include <map>
+#include <mutex>
+#include <thread>
 
 namespace {
 
@@ -171,6 +181,104 @@ struct FactorResult {
   Stats st;
 };
 
+// A vector whose elements are not value-initialised on growth: large
+// front and factor buffers are filled in parallel instead (first touch by
+// the threads that use them).
+// Buffers of 32 MB and more (fronts, contribution blocks, factors) come
+// from a cache of released buffers when one of at most twice the size is
+// free (best fit), so the front-by-front allocation pattern of the
+// multifrontal method reuses memory that is already mapped instead of
+// faulting in fresh pages; new ones are 2 MB aligned and marked for
+// transparent huge pages.  The cache holds at most 48 GB and is emptied by
+// orc_release_cache().
+const size_t BIG = (size_t)32 << 20;
+struct BigCache {
+  std::mutex mu;
+  std::multimap<size_t, void*> free_;  // capacity -> block
+  std::map<void*, size_t> cap_;        // every live or cached block -> capacity
+  size_t cached = 0;
+  void* get(size_t bytes) {
+    const size_t HP = (size_t)2 << 20;
+    const size_t want = (bytes + HP - 1) / HP * HP;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      auto it = free_.lower_bound(want);
+      if (it != free_.end() && it->first <= 2 * want) {
+        void* p = it->second;
+        cached -= it->first;
+        free_.erase(it);
+        return p;
+      }
+    }
+    void* p = nullptr;
+    if (posix_memalign(&p, HP, want) != 0) throw std::bad_alloc();
+#ifdef MADV_HUGEPAGE
+    madvise(p, want, MADV_HUGEPAGE);
+#endif
+    std::lock_guard<std::mutex> lk(mu);
+    cap_[p] = want;
+    return p;
+  }
+  void put(void* p) {
+    std::lock_guard<std::mutex> lk(mu);
+    const size_t c = cap_.at(p);
+    const size_t LIMIT = (size_t)48 << 30;
+    while (cached + c > LIMIT && !free_.empty()) {  // drop the largest cached blocks first
+      auto it = std::prev(free_.end());
+      cached -= it->first;
+      cap_.erase(it->second);
+      free(it->second);
+      free_.erase(it);
+    }
+    if (cached + c > LIMIT) { cap_.erase(p); free(p); return; }
+    free_.emplace(c, p);
+    cached += c;
+  }
+  void release() {
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto& kv : free_) { cap_.erase(kv.second); free(kv.second); }
+    free_.clear();
+    cached = 0;
+  }
+};
+BigCache& big_cache() {
+  static BigCache* c = new BigCache();  // never destroyed: buffers may be released at exit
+  return *c;
+}
+
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U> struct rebind { using other = NoInitAlloc<U>; };
+  NoInitAlloc() = default;
+  template <class U> NoInitAlloc(const NoInitAlloc<U>&) {}
+  T* allocate(size_t n) {
+    if (n * sizeof(T) < BIG) return std::allocator<T>::allocate(n);
+    return static_cast<T*>(big_cache().get(n * sizeof(T)));
+  }
+  void deallocate(T* p, size_t n) {
+    if (n * sizeof(T) < BIG) std::allocator<T>::deallocate(p, n);
+    else big_cache().put(p);
+  }
+  template <class U> void construct(U* p) noexcept { ::new (static_cast<void*>(p)) U; }
+  template <class U, class... A> void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+typedef std::vector<double, NoInitAlloc<double>> dvec;
+
+void fill_zero(double* p, size_t n) {
+  const size_t CH = (size_t)1 << 20;
+  const i64 nch = (i64)((n + CH - 1) / CH);
+  bool par = n > (size_t)4 << 20;
+#ifdef _OPENMP
+  par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) if (par)
+#endif
+  for (i64 c = 0; c < nch; ++c) {
+    size_t b = (size_t)c * CH, e = std::min(n, b + CH);
+    std::memset(p + b, 0, (e - b) * sizeof(double));
+  }
+  (void)par;
+}
+
 // column-major dense view
 struct MV {
   double* a; i64 ld;
@@ -283,61 +391,74 @@ i64 adjust_2x2(i64 e, const MixedD& d) {
   return e;
 }
 
-// apply_and_check (factor.rs:1295-1408): TRSM, D^-1 scaling, first failing column
+// apply_and_check (factor.rs:1295-1408): TRSM, D^-1 scaling, first failing column.
+// Rows are independent in all three steps, so blocks of rows go to threads;
+// each block records, per column, its first row at or over the bound and the
+// near ties up to it, and the blocks are then read in row order, which gives
+// the serial scan's result and tie count exactly.
 i64 apply_and_check(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, const MixedD& d, double thr) {
   if (nelim == 0) return 0;
   i64 prows = m - col_start - bcols;
   if (prows == 0) return nelim;
   i64 ps = col_start + bcols;
-  // panel * L11^T = A21  (L11 unit lower, from a[col_start.., col_start..])
-  // faer TRSM (factor.rs:1338); per entry an fma chain over l ascending
-  {
-    const i64 RB = 256;
-    i64 nrb = (prows + RB - 1) / RB;
-    bool par = prows * nelim > 200000;
+  const double bound = 1.0 / thr;
+  const i64 RB = 256;
+  const i64 nrb = (prows + RB - 1) / RB;
+  std::vector<i64> first_fail((size_t)nrb * nelim), ties((size_t)nrb * nelim);
+  bool par = prows * nelim > 200000;
 #ifdef _OPENMP
-    par = par && !omp_in_parallel();
+  par = par && !omp_in_parallel();
 #pragma omp parallel for schedule(static) if (par)
 #endif
-    for (i64 rb = 0; rb < nrb; ++rb) {
-      i64 r0 = rb * RB, r1 = std::min(prows, r0 + RB);
-      for (i64 j = 0; j < nelim; ++j)
-        for (i64 l = 0; l < j; ++l) {
-          double lij = a(col_start + j, col_start + l);
-          for (i64 r = r0; r < r1; ++r)
-            a(ps + r, col_start + j) = std::fma(-a(ps + r, col_start + l), lij, a(ps + r, col_start + j));
-        }
-    }
-    (void)par;
-  }
-  i64 c = 0;
-  while (c < nelim) {
-    if (d.type[c] == PT_1X1) {
-      double inv = 1.0 / d.diag[c];
-      for (i64 r = 0; r < prows; ++r) a(ps + r, col_start + c) *= inv;
-      c += 1;
-    } else if (d.is2first(c)) {
-      double A = d.diag[c], B = d.off[c], C = d.diag[c + 1];
-      double inv_det = 1.0 / (A * C - B * B);
-      for (i64 r = 0; r < prows; ++r) {
-        double x1 = a(ps + r, col_start + c), x2 = a(ps + r, col_start + c + 1);
-        a(ps + r, col_start + c) = (x1 * C - x2 * B) * inv_det;
-        a(ps + r, col_start + c + 1) = (x2 * A - x1 * B) * inv_det;
+  for (i64 rb = 0; rb < nrb; ++rb) {
+    i64 r0 = rb * RB, r1 = std::min(prows, r0 + RB);
+    // panel * L11^T = A21  (L11 unit lower, from a[col_start.., col_start..])
+    // faer TRSM (factor.rs:1338); per entry an fma chain over l ascending
+    for (i64 j = 0; j < nelim; ++j)
+      for (i64 l = 0; l < j; ++l) {
+        double lij = a(col_start + j, col_start + l);
+        for (i64 r = r0; r < r1; ++r)
+          a(ps + r, col_start + j) = std::fma(-a(ps + r, col_start + l), lij, a(ps + r, col_start + j));
       }
-      c += 2;
-    } else c += 1;
+    i64 c = 0;
+    while (c < nelim) {
+      if (d.type[c] == PT_1X1) {
+        double inv = 1.0 / d.diag[c];
+        for (i64 r = r0; r < r1; ++r) a(ps + r, col_start + c) *= inv;
+        c += 1;
+      } else if (d.is2first(c)) {
+        double A = d.diag[c], B = d.off[c], C = d.diag[c + 1];
+        double inv_det = 1.0 / (A * C - B * B);
+        for (i64 r = r0; r < r1; ++r) {
+          double x1 = a(ps + r, col_start + c), x2 = a(ps + r, col_start + c + 1);
+          a(ps + r, col_start + c) = (x1 * C - x2 * B) * inv_det;
+          a(ps + r, col_start + c + 1) = (x2 * A - x1 * B) * inv_det;
+        }
+        c += 2;
+      } else c += 1;
+    }
+    for (i64 cc = 0; cc < nelim; ++cc) {
+      i64 ff = -1, t = 0;
+      for (i64 r = r0; r < r1; ++r) {
+        double v = std::fabs(a(ps + r, col_start + cc));
+        double sc = std::max(v, bound);
+        if (std::fabs(v - bound) <= TIE_REL * sc && sc > 0) t++;
+        if (v >= bound) { ff = r; break; }
+      }
+      first_fail[rb * nelim + cc] = ff;
+      ties[rb * nelim + cc] = t;
+    }
   }
-  double bound = 1.0 / thr;
+  (void)par;
   i64 eff = nelim, sc = 0;
   while (sc < nelim) {
     i64 w = d.is2first(sc) ? 2 : 1;
     bool ok = true;
     for (i64 cc = sc; cc < sc + w && ok; ++cc) {
       if (cc >= nelim) break;
-      for (i64 r = 0; r < prows; ++r) {
-        double v = std::fabs(a(ps + r, col_start + cc));
-        note_tie(v, bound);
-        if (v >= bound) { ok = false; break; }
+      for (i64 rb = 0; rb < nrb; ++rb) {
+        g_ties += ties[rb * nelim + cc];
+        if (first_fail[rb * nelim + cc] >= 0) { ok = false; break; }
       }
     }
     if (!ok) { eff = sc; break; }
@@ -346,54 +467,228 @@ i64 apply_and_check(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, const Mixe
   return eff;
 }
 
-// compute_ld_into (factor.rs:1536-1563): W = L * D
+// compute_ld_into (factor.rs:1536-1563): W = L * D.  Rows are independent;
+// large blocks are split over threads by rows (the arithmetic per entry is
+// unchanged).
 void compute_ld(const double* l, i64 ldl, i64 nrows, const MixedD& d, i64 nelim, double* w, i64 ldw) {
-  i64 c = 0;
-  while (c < nelim) {
-    if (d.type[c] == PT_1X1) {
-      double dv = d.diag[c];
-      for (i64 i = 0; i < nrows; ++i) w[i + c * ldw] = l[i + c * ldl] * dv;
-      c += 1;
-    } else if (d.is2first(c)) {
-      double A = d.diag[c], B = d.off[c], C = d.diag[c + 1];
-      for (i64 i = 0; i < nrows; ++i) {
-        double l1 = l[i + c * ldl], l2 = l[i + (c + 1) * ldl];
-        w[i + c * ldw] = l1 * A + l2 * B;
-        w[i + (c + 1) * ldw] = l1 * B + l2 * C;
-      }
-      c += 2;
-    } else c += 1;
+  const i64 RB = 2048;
+  const i64 nrb = (nrows + RB - 1) / RB;
+  bool par = nrows * nelim > 100000;
+#ifdef _OPENMP
+  par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) if (par)
+#endif
+  for (i64 rb = 0; rb < nrb; ++rb) {
+    const i64 r0 = rb * RB, r1 = std::min(nrows, r0 + RB);
+    i64 c = 0;
+    while (c < nelim) {
+      if (d.type[c] == PT_1X1) {
+        double dv = d.diag[c];
+        for (i64 i = r0; i < r1; ++i) w[i + c * ldw] = l[i + c * ldl] * dv;
+        c += 1;
+      } else if (d.is2first(c)) {
+        double A = d.diag[c], B = d.off[c], C = d.diag[c + 1];
+        for (i64 i = r0; i < r1; ++i) {
+          double l1 = l[i + c * ldl], l2 = l[i + (c + 1) * ldl];
+          w[i + c * ldw] = l1 * A + l2 * B;
+          w[i + (c + 1) * ldw] = l1 * B + l2 * C;
+        }
+        c += 2;
+      } else c += 1;
+    }
+  }
+  (void)par;
+}
+
+// Copy of the column block src[0..nrows, 0..ncols] (leading dimension lds)
+// into dst (leading dimension ldd), split over threads by rows when large.
+void copy_block(double* dst, i64 ldd, const double* src, i64 lds, i64 nrows, i64 ncols) {
+  const i64 RB = 4096;
+  const i64 nrb = (nrows + RB - 1) / RB;
+  bool par = nrows * ncols > 200000;
+#ifdef _OPENMP
+  par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) if (par)
+#endif
+  for (i64 rb = 0; rb < nrb; ++rb) {
+    const i64 r0 = rb * RB, r1 = std::min(nrows, r0 + RB);
+    for (i64 j = 0; j < ncols; ++j) std::memcpy(dst + r0 + j * ldd, src + r0 + j * lds, (size_t)(r1 - r0) * 8);
+  }
+  (void)par;
+}
+
+// Per-thread scratch that grows and is never zeroed (every entry used is written first).
+double* scratch(int slot, size_t n) {
+  static thread_local std::vector<double, NoInitAlloc<double>> buf[8];
+  if (buf[slot].size() < n) buf[slot].resize(n);
+  return buf[slot].data();
+}
+
+// ---------------------------------------------------------------------------
+// Rank-K update used by every faer GEMM call site:
+//   C[i, j] = fma(-W[i, c], L[j, c], C[i, j]) for c = 0..K-1 in order,
+// over i in [0, nr), j in [0, nc), where i + row_shift >= j (lower part of
+// the output relative to the diagonal).
+//
+// Each entry's fma chain keeps its order whatever the blocking: K is cut into
+// chunks taken one after another (an entry's running value is stored as a
+// double between chunks, exactly what the chain holds); per chunk W and L are
+// packed into tile-contiguous panels (24 rows x chunk for W, 8 columns x chunk
+// for L), and the output is cut into 64-column panels (OpenMP, dynamic),
+// 384-row blocks and 24 x 8 register tiles: 24 accumulator vectors of 8
+// doubles, each step c loading three vectors of W and broadcasting 8 entries
+// of L.  The tile arithmetic is vfnmadd (-(w * l) + acc, one rounding), equal
+// to fma(-w, l, acc).  Tiles that straddle the diagonal, columns past the last
+// full 8-column group and builds without AVX-512 take the scalar path, which
+// runs the same chain entry by entry on the unpacked operands.
+// ---------------------------------------------------------------------------
+void syrk_scalar(double* C, i64 ldc, const double* W, i64 ldw, const double* L, i64 ldl, i64 r0, i64 r1, i64 j0,
+                 i64 j1, i64 K, i64 row_shift) {
+  for (i64 j = j0; j < j1; ++j) {
+    double* col = C + j * ldc;
+    const i64 is = std::max(r0, j - row_shift);
+    for (i64 i = is; i < r1; ++i) {
+      double acc = col[i];
+      for (i64 c = 0; c < K; ++c) acc = std::fma(-W[i + c * ldw], L[j + c * ldl], acc);
+      col[i] = acc;
+    }
   }
 }
 
-// Cache-blocked rank-K update used by every faer GEMM call site:
-//   C[i, j] = fma(-W[i, c], L[j, c], C[i, j]) for c = 0..K-1 in order,
-// over i in [0, nr), j in [0, nc), where i + row_shift >= j (lower part of
-// the output relative to the diagonal).  Blocking reorders only independent
-// entries; each entry's fma chain keeps its order.  OpenMP over column blocks
-// when not already inside a parallel region.
+#if defined(__x86_64__) && defined(__GNUC__)
+#define ORC_HAVE_TILE 1
+// One tile: rows [0, mr) (mr <= 24) of C, columns [0, 8); Wp holds 24
+// doubles per step c, Lp 8.
+__attribute__((target("avx512f,fma"))) void syrk_tile24x8(double* C, i64 ldc, const double* Wp, const double* Lp,
+                                                           i64 K, int mr) {
+  const __mmask8 m0 = (__mmask8)(mr >= 8 ? 0xFF : ((1u << mr) - 1));
+  const __mmask8 m1 = (__mmask8)(mr >= 16 ? 0xFF : (mr <= 8 ? 0 : ((1u << (mr - 8)) - 1)));
+  const __mmask8 m2 = (__mmask8)(mr >= 24 ? 0xFF : (mr <= 16 ? 0 : ((1u << (mr - 16)) - 1)));
+  __m512d a0[8], a1[8], a2[8];
+  for (int j = 0; j < 8; ++j) {
+    a0[j] = _mm512_maskz_loadu_pd(m0, C + j * ldc);
+    a1[j] = _mm512_maskz_loadu_pd(m1, C + j * ldc + 8);
+    a2[j] = _mm512_maskz_loadu_pd(m2, C + j * ldc + 16);
+  }
+  for (i64 c = 0; c < K; ++c) {
+    const double* w = Wp + c * 24;
+    const __m512d w0 = _mm512_loadu_pd(w);
+    const __m512d w1 = _mm512_loadu_pd(w + 8);
+    const __m512d w2 = _mm512_loadu_pd(w + 16);
+    const double* l = Lp + c * 8;
+#pragma GCC unroll 8
+    for (int j = 0; j < 8; ++j) {
+      const __m512d lj = _mm512_set1_pd(l[j]);
+      a0[j] = _mm512_fnmadd_pd(w0, lj, a0[j]);
+      a1[j] = _mm512_fnmadd_pd(w1, lj, a1[j]);
+      a2[j] = _mm512_fnmadd_pd(w2, lj, a2[j]);
+    }
+  }
+  for (int j = 0; j < 8; ++j) {
+    _mm512_mask_storeu_pd(C + j * ldc, m0, a0[j]);
+    _mm512_mask_storeu_pd(C + j * ldc + 8, m1, a1[j]);
+    _mm512_mask_storeu_pd(C + j * ldc + 16, m2, a2[j]);
+  }
+}
+bool tile_ok() {
+  static const bool ok = __builtin_cpu_supports("avx512f") && __builtin_cpu_supports("fma");
+  return ok;
+}
+#else
+#define ORC_HAVE_TILE 0
+#endif
+
 void syrk_fma(double* C, i64 ldc, const double* W, i64 ldw, const double* L, i64 ldl, i64 nr, i64 nc, i64 K,
               i64 row_shift) {
-  const i64 JB = 32, IB = 512;
-  i64 njb = (nc + JB - 1) / JB;
+  if (nr <= 0 || nc <= 0 || K <= 0) return;
+  const i64 JB = 64, IB = 384, KB = 256;
+#if ORC_HAVE_TILE
+  const bool tiles = tile_ok() && nr >= 24 && nc >= 8;
+#else
+  const bool tiles = false;
+#endif
+  const i64 njb = (nc + JB - 1) / JB;
   bool par = (double)nr * (double)nc * (double)K > 4e6;
 #ifdef _OPENMP
   par = par && !omp_in_parallel();
+#endif
+  if (!tiles) {
+#ifdef _OPENMP
 #pragma omp parallel for schedule(dynamic, 1) if (par)
 #endif
-  for (i64 jb = 0; jb < njb; ++jb) {
-    i64 j0 = jb * JB, j1 = std::min(nc, j0 + JB);
-    i64 ilo = std::max<i64>(0, j0 - row_shift);
-    for (i64 i0 = ilo; i0 < nr; i0 += IB) {
-      i64 i1 = std::min(nr, i0 + IB);
-      for (i64 c = 0; c < K; ++c) {
-        const double* w = W + c * ldw;
-        for (i64 j = j0; j < j1; ++j) {
-          double lj = L[j + c * ldl];
-          double* col = C + j * ldc;
-          i64 is = std::max(i0, j - row_shift);
-          for (i64 i = is; i < i1; ++i) col[i] = std::fma(-w[i], lj, col[i]);
+    for (i64 jb = 0; jb < njb; ++jb)
+      syrk_scalar(C, ldc, W, ldw, L, ldl, 0, nr, jb * JB, std::min(nc, jb * JB + JB), K, row_shift);
+    return;
+  }
+  const i64 nt = (nr + 23) / 24, ng = nc / 8;  // 24-row tiles, full 8-column groups
+  for (i64 k0 = 0; k0 < K; k0 += KB) {
+    const i64 kn = std::min(KB, K - k0);
+    double* Wp = scratch(4, (size_t)nt * 24 * kn);
+    double* Lp = scratch(5, (size_t)std::max<i64>(ng, 1) * 8 * kn);
+#ifdef _OPENMP
+#pragma omp parallel if (par)
+#endif
+    {
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+      for (i64 t = 0; t < nt; ++t) {
+        double* dst = Wp + t * 24 * kn;
+        const i64 i0 = t * 24, mr = std::min<i64>(24, nr - i0);
+        for (i64 c = 0; c < kn; ++c) {
+          const double* src = W + i0 + (k0 + c) * ldw;
+          for (i64 r = 0; r < mr; ++r) dst[c * 24 + r] = src[r];
+          for (i64 r = mr; r < 24; ++r) dst[c * 24 + r] = 0.0;
         }
+      }
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+      for (i64 g = 0; g < ng; ++g) {
+        double* dst = Lp + g * 8 * kn;
+        for (i64 c = 0; c < kn; ++c)
+          for (i64 q = 0; q < 8; ++q) dst[c * 8 + q] = L[g * 8 + q + (k0 + c) * ldl];
+      }
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+      for (i64 jb = 0; jb < njb; ++jb) {
+        const i64 j0 = jb * JB, j1 = std::min(nc, j0 + JB);
+        const double* Wk = W + k0 * ldw;
+        const double* Lk = L + k0 * ldl;
+        i64 tstart[JB / 8];
+        i64 t_all = nt;
+        const i64 ngp = (j1 - j0 + 7) / 8;
+        for (i64 q = 0; q < ngp; ++q) {
+          const i64 jm = j0 + 8 * q, nj = std::min<i64>(8, j1 - jm);
+          if (nj < 8) {  // the last, partial group: scalar
+            syrk_scalar(C, ldc, Wk, ldw, Lk, ldl, 0, nr, jm, jm + nj, kn, row_shift);
+            tstart[q] = nt;
+            continue;
+          }
+          // first tile whose rows are all in the lower part for the group's 8 columns
+          const i64 need = jm + 7 - row_shift;  // row index from which every column qualifies
+          const i64 tf = need <= 0 ? 0 : std::min(nt, (need + 23) / 24);
+          const i64 first = std::max<i64>(0, jm - row_shift);
+          const i64 rfull = std::min(nr, tf * 24);
+          if (rfull > first) syrk_scalar(C, ldc, Wk, ldw, Lk, ldl, first, rfull, jm, jm + 8, kn, row_shift);
+          tstart[q] = tf;
+          t_all = std::min(t_all, tf);
+        }
+#if ORC_HAVE_TILE
+        const i64 TB = IB / 24;
+        for (i64 tb0 = t_all; tb0 < nt; tb0 += TB) {
+          const i64 tb1 = std::min(nt, tb0 + TB);
+          for (i64 q = 0; q < ngp; ++q) {
+            const i64 jm = j0 + 8 * q;
+            if (j1 - jm < 8) continue;
+            const double* lp = Lp + (jm / 8) * 8 * kn;
+            for (i64 t = std::max(tb0, tstart[q]); t < tb1; ++t)
+              syrk_tile24x8(C + t * 24 + jm * ldc, ldc, Wp + t * 24 * kn, lp, kn,
+                            (int)std::min<i64>(24, nr - t * 24));
+          }
+        }
+#endif
       }
     }
   }
@@ -405,16 +700,17 @@ void update_trailing(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, i64 p, co
   if (nelim == 0) return;
   i64 ts = col_start + bcols, tsz = m - ts;
   if (tsz <= 0) return;
-  std::vector<double> W((size_t)tsz * nelim, 0.0), L((size_t)tsz * nelim);
-  for (i64 c = 0; c < nelim; ++c)
-    for (i64 i = 0; i < tsz; ++i) L[i + c * tsz] = a(ts + i, col_start + c);
-  compute_ld(L.data(), tsz, tsz, d, nelim, W.data(), tsz);
   i64 fs = std::max<i64>(p - ts, 0);
+  if (fs <= 0) return;
+  double* L = scratch(0, (size_t)tsz * nelim);
+  double* W = scratch(1, (size_t)tsz * nelim);
+  copy_block(L, tsz, &a(ts, col_start), a.ld, tsz, nelim);
+  compute_ld(L, tsz, tsz, d, nelim, W, tsz);
   // faer triangular / rectangular GEMM (factor.rs:1491, 1513); per entry an
   // fma chain over c ascending.  Region 1 is the lower triangle of
   // A[ts..p, ts..p], region 2 the rectangle A[p..m, ts..p]: together the
   // rows i >= j of the trailing columns ts..p.
-  if (fs > 0) syrk_fma(&a(ts, ts), a.ld, W.data(), tsz, L.data(), tsz, tsz, fs, nelim, 0);
+  syrk_fma(&a(ts, ts), a.ld, W, tsz, L, tsz, tsz, fs, nelim, 0);
 }
 
 // update_cross_terms (factor.rs:1669-1766)
@@ -432,16 +728,26 @@ void update_cross_terms(MV a, i64 col_start, i64 nelim, i64 bcols, i64 m, const 
       a(col_start + nelim + i, col_start + nelim + j) -= s;
     }
   if (tsz > 0) {
-    std::vector<double> Lp((size_t)tsz * nelim), Wp((size_t)tsz * nelim, 0.0);
-    for (i64 c = 0; c < nelim; ++c)
-      for (i64 i = 0; i < tsz; ++i) Lp[i + c * tsz] = a(ts + i, col_start + c);
-    compute_ld(Lp.data(), tsz, tsz, d, nelim, Wp.data(), tsz);
-    for (i64 j = 0; j < nf; ++j)
-      for (i64 i = 0; i < tsz; ++i) {
-        double s = 0.0;
-        for (i64 c = 0; c < nelim; ++c) s += Wp[i + c * tsz] * Lb[j + c * nf];
-        a(ts + i, col_start + nelim + j) -= s;
-      }
+    double* Lp = scratch(0, (size_t)tsz * nelim);
+    double* Wp = scratch(1, (size_t)tsz * nelim);
+    copy_block(Lp, tsz, &a(ts, col_start), a.ld, tsz, nelim);
+    compute_ld(Lp, tsz, tsz, d, nelim, Wp, tsz);
+    const i64 RB = 1024, nrb = (tsz + RB - 1) / RB;
+    bool par = tsz * nf * nelim > 400000;
+#ifdef _OPENMP
+    par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) if (par)
+#endif
+    for (i64 rb = 0; rb < nrb; ++rb) {
+      const i64 r0 = rb * RB, r1 = std::min(tsz, r0 + RB);
+      for (i64 j = 0; j < nf; ++j)
+        for (i64 i = r0; i < r1; ++i) {
+          double s = 0.0;
+          for (i64 c = 0; c < nelim; ++c) s += Wp[i + c * tsz] * Lb[j + c * nf];
+          a(ts + i, col_start + nelim + j) -= s;
+        }
+    }
+    (void)par;
   }
 }
 
@@ -453,21 +759,19 @@ FactorResult factor_inner(MV a, i64 m, i64 p, i64 nfs_boundary, const Opts& o) {
   std::iota(R.perm.begin(), R.perm.end(), 0);
   R.d.init(p);
   i64 k = 0, end_pos = p;
-  std::vector<double> backup, buf(ib);
+  std::vector<double> buf(ib);
   std::vector<i64> obuf(ib);
   while (k < end_pos) {
     i64 bs = std::min(end_pos - k, ib), be = k + bs;
     // 1. backup a[k..m, k..k+bs]   (BlockBackup::create, factor.rs:1191-1206)
     i64 rows = m - k;
-    backup.assign((size_t)rows * bs, 0.0);
-    for (i64 j = 0; j < bs; ++j)
-      for (i64 i = 0; i < rows; ++i) backup[i + j * rows] = a(k + i, k + j);
+    double* backup = scratch(2, (size_t)rows * bs);
+    copy_block(backup, rows, &a(k, k), a.ld, rows, bs);
     // 2. factor diagonal block
     MixedD bd; std::vector<i64> bperm; i64 bnelim; Stats bst;
     factor_block_diagonal(a, k, bs, o.small, be, bd, bperm, bnelim, bst);
     if (bnelim == 0) {
-      for (i64 j = 0; j < bs; ++j)
-        for (i64 i = 0; i < rows; ++i) a(k + i, k + j) = backup[i + j * rows];
+      copy_block(&a(k, k), a.ld, backup, rows, rows, bs);
       for (i64 off = 0; off < bs; ++off) {
         end_pos -= 1;
         if (k + off < end_pos) { swap_sym(a, m, k + off, end_pos); std::swap(R.perm[k + off], R.perm[end_pos]); }
@@ -475,10 +779,22 @@ FactorResult factor_inner(MV a, i64 m, i64 p, i64 nfs_boundary, const Opts& o) {
       }
       continue;
     }
-    // 3. permute panel columns
-    for (i64 r = be; r < m; ++r) {
-      for (i64 i = 0; i < bs; ++i) buf[i] = a(r, k + bperm[i]);
-      for (i64 i = 0; i < bs; ++i) a(r, k + i) = buf[i];
+    // 3. permute panel columns (rows are independent: blocks of rows to threads)
+    {
+      const i64 nrow = m - be, RB = 4096, nrb = (nrow + RB - 1) / RB;
+      bool par = nrow * bs > 200000;
+#ifdef _OPENMP
+      par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) if (par)
+#endif
+      for (i64 rb = 0; rb < nrb; ++rb) {
+        double tb[64];
+        for (i64 r = be + rb * RB; r < std::min(m, be + (rb + 1) * RB); ++r) {
+          for (i64 i = 0; i < bs; ++i) tb[i] = a(r, k + bperm[i]);
+          for (i64 i = 0; i < bs; ++i) a(r, k + i) = tb[i];
+        }
+      }
+      (void)par;
     }
     // 4. zero D off-diagonals of 2x2 pivots
     {
@@ -510,7 +826,7 @@ FactorResult factor_inner(MV a, i64 m, i64 p, i64 nfs_boundary, const Opts& o) {
       }
       for (i64 j = eff; j < bs; ++j) {
         i64 c = bperm[j];
-        for (i64 i = bs; i < rows; ++i) a(k + i, k + j) = backup[i + c * rows];
+        std::memcpy(&a(k + bs, k + j), backup + bs + c * rows, (size_t)(rows - bs) * 8);
       }
     }
     i64 nelim = eff;
@@ -530,8 +846,19 @@ FactorResult factor_inner(MV a, i64 m, i64 p, i64 nfs_boundary, const Opts& o) {
       }
     }
     R.st.maxl = std::max(R.st.maxl, bst.maxl);
-    for (i64 c = 0; c < nelim; ++c)
-      for (i64 i = be; i < m; ++i) R.st.maxl = std::max(R.st.maxl, std::fabs(a(i, k + c)));
+    {
+      double ml = R.st.maxl;
+      const i64 nrow = m - be;
+      bool par = nrow * nelim > 200000;
+#ifdef _OPENMP
+      par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(static) reduction(max : ml) if (par)
+#endif
+      for (i64 c = 0; c < nelim; ++c)
+        for (i64 i = be; i < m; ++i) ml = std::max(ml, std::fabs(a(i, k + c)));
+      R.st.maxl = ml;
+      (void)par;
+    }
     // 12. delay failed columns to end_pos
     if (nelim < bs) {
       i64 nd = bs - nelim;
@@ -549,6 +876,23 @@ FactorResult factor_inner(MV a, i64 m, i64 p, i64 nfs_boundary, const Opts& o) {
   return R;
 }
 
+// Progress hook of a factorization run in slices (orc_session_*): the thread
+// that runs the factorization reports the delay-free flops done so far at
+// safe points, and waits there while its slice is used up.  Not called from
+// inside parallel regions.
+struct Run;
+thread_local Run* tl_run = nullptr;
+thread_local double tl_front_base = 0.0;  // flops of the fronts finished before the one in progress
+void checkpoint(double done_now);
+
+// Delay-free flops of the first `cols` eliminated columns of an m-row front:
+// sum_{j < cols} [(m - j - 1) + (m - j - 1)(m - j)].
+double front_flops(double m, double cols) {
+  double s = 0.0;
+  for (double j = 0; j < cols; j += 1.0) s += (m - j - 1.0) * (m - j + 1.0);
+  return s;
+}
+
 // two_level_factor (factor.rs:2108-2252)
 FactorResult two_level_factor(MV a, i64 m, i64 p, const Opts& o) {
   FactorResult R;
@@ -562,11 +906,22 @@ FactorResult two_level_factor(MV a, i64 m, i64 p, const Opts& o) {
     FactorResult B = factor_inner(a.sub(cs, cs), bm, bcols, p - cs, o);
     i64 bne = B.ne;
     if (cs > 0) {
-      std::vector<double> tmp(bcols);
-      for (i64 c = 0; c < cs; ++c) {
-        for (i64 i = 0; i < bcols; ++i) tmp[i] = a(cs + B.perm[i], c);
-        for (i64 i = 0; i < bcols; ++i) a(cs + i, c) = tmp[i];
+      bool par = cs * bcols > 200000;
+#ifdef _OPENMP
+      par = par && !omp_in_parallel();
+#pragma omp parallel if (par)
+#endif
+      {
+        std::vector<double> tmp(bcols);
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+        for (i64 c = 0; c < cs; ++c) {
+          for (i64 i = 0; i < bcols; ++i) tmp[i] = a(cs + B.perm[i], c);
+          for (i64 i = 0; i < bcols; ++i) a(cs + i, c) = tmp[i];
+        }
       }
+      (void)par;
     }
     {
       std::vector<i64> orig(R.perm.begin() + cs, R.perm.begin() + cs + bcols);
@@ -585,6 +940,7 @@ FactorResult two_level_factor(MV a, i64 m, i64 p, const Opts& o) {
     R.st.n1 += B.st.n1; R.st.n2 += B.st.n2; R.st.maxl = std::max(R.st.maxl, B.st.maxl);
     gne += bne;
     rem -= bcols;
+    if (tl_run) checkpoint(tl_front_base + front_flops((double)m, (double)(p - rem)));
   }
   R.ne = gne;
   R.d.truncate(gne);
@@ -774,10 +1130,10 @@ FactorResult aptp_factor_in_place(MV a, i64 m, i64 p, const Opts& o) {
 void contribution_gemm(const double* l, i64 ldl, i64 p, i64 ne, i64 m, const MixedD& d, double* cb, i64 ldc) {
   i64 nfs = m - p;
   if (nfs == 0 || ne == 0) return;
-  std::vector<double> W((size_t)nfs * ne, 0.0);
-  compute_ld(l + p, ldl, nfs, d, ne, W.data(), nfs);
+  double* W = scratch(3, (size_t)nfs * ne);
+  compute_ld(l + p, ldl, nfs, d, ne, W, nfs);
   // faer triangular GEMM (factor.rs:1639); per entry an fma chain over c ascending
-  syrk_fma(cb, ldc, W.data(), nfs, l + p, ldl, nfs, nfs, ne, 0);
+  syrk_fma(cb, ldc, W, nfs, l + p, ldl, nfs, nfs, ne, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -901,7 +1257,7 @@ std::vector<Subtree> classify_small_leaf(std::vector<SN>& sn, const std::vector<
 // ---------------------------------------------------------------------------
 struct Front {      // FrontFactors (numeric.rs:543-596) plus per-supernode stats
   i64 m = 0, k = 0, ne = 0;
-  std::vector<double> l11, l21;   // ne x ne, r x ne (column-major)
+  dvec l11, l21;                  // ne x ne, r x ne (column-major)
   MixedD d11;
   std::vector<i64> col_idx, row_idx, local_perm;
   i64 n1 = 0, n2 = 0;
@@ -909,7 +1265,7 @@ struct Front {      // FrontFactors (numeric.rs:543-596) plus per-supernode stat
   i64 ties = 0;
 };
 
-struct CB { std::vector<double> data; i64 size = 0; std::vector<i64> rows; i64 ndel = 0; };
+struct CB { dvec data; i64 size = 0; std::vector<i64> rows; i64 ndel = 0; };
 
 struct Problem {
   i64 n;
@@ -938,29 +1294,38 @@ struct Oracle {
 void extract_factors(Front& F, const double* a, i64 lda, i64 m, i64 k, const std::vector<i64>& rows, const FactorResult& R) {
   i64 ne = R.ne;
   F.m = m; F.k = k; F.ne = ne;
-  F.l11.assign((size_t)ne * ne, 0.0);
-  i64 c = 0;
-  while (c < ne) {
-    F.l11[c + c * ne] = 1.0;
-    if (R.d.type[c] == PT_1X1) {
-      for (i64 i = c + 1; i < ne; ++i) F.l11[i + c * ne] = a[i + c * lda];
-      c += 1;
-    } else if (R.d.is2first(c)) {
-      F.l11[(c + 1) + (c + 1) * ne] = 1.0;
-      for (i64 i = c + 2; i < ne; ++i) { F.l11[i + c * ne] = a[i + c * lda]; F.l11[i + (c + 1) * ne] = a[i + (c + 1) * lda]; }
-      c += 2;
-    } else c += 1;
+  F.l11.resize((size_t)ne * ne);
+  {
+    // column by column: zeros above the diagonal, 1 on it, L below (the
+    // second column of a 2x2 pivot keeps a zero at its first sub-diagonal)
+    bool par = ne * ne > (1 << 20);
+#ifdef _OPENMP
+    par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(dynamic, 16) if (par)
+#endif
+    for (i64 c = 0; c < ne; ++c) {
+      double* col = F.l11.data() + c * ne;
+      std::memset(col, 0, (size_t)c * sizeof(double));
+      col[c] = 1.0;
+      const bool second = R.d.type[c] == PT_2X2 && R.d.partner[c] < c;
+      const bool first = R.d.is2first(c);
+      const bool known = R.d.type[c] == PT_1X1 || first || second;
+      i64 i0 = c + 1;
+      if (first && c + 1 < ne) { col[c + 1] = 0.0; i0 = c + 2; }
+      if (known) std::memcpy(col + i0, a + i0 + c * lda, (size_t)std::max<i64>(0, ne - i0) * sizeof(double));
+      else std::memset(col + i0, 0, (size_t)std::max<i64>(0, ne - i0) * sizeof(double));
+    }
+    (void)par;
   }
   F.d11.init(ne);
-  c = 0;
+  i64 c = 0;
   while (c < ne) {
     if (R.d.type[c] == PT_1X1) { F.d11.set1(c, R.d.diag[c]); c += 1; }
     else { F.d11.set2(c, R.d.diag[c], R.d.off[c], R.d.diag[c + 1]); c += 2; }
   }
   i64 r = m - ne;
-  F.l21.assign((size_t)r * ne, 0.0);
-  for (i64 j = 0; j < ne; ++j)
-    for (i64 i = 0; i < r; ++i) F.l21[i + j * r] = a[ne + i + j * lda];
+  F.l21.resize((size_t)r * ne);
+  copy_block(F.l21.data(), r, a + ne, lda, r, ne);
   F.local_perm.assign(R.perm.begin(), R.perm.begin() + k);
   F.col_idx.resize(ne);
   for (i64 i = 0; i < ne; ++i) F.col_idx[i] = rows[R.perm[i]];
@@ -972,12 +1337,13 @@ void extract_factors(Front& F, const double* a, i64 lda, i64 m, i64 k, const std
 
 // extract_contribution (numeric.rs:2739-2809): delayed block from the front,
 // NFS x NFS from `nfsblk` (nfs x nfs).
-CB extract_contrib(const double* a, i64 lda, i64 m, i64 k, const std::vector<i64>& rows, const FactorResult& R, std::vector<double>&& nfsblk) {
+CB extract_contrib(const double* a, i64 lda, i64 m, i64 k, const std::vector<i64>& rows, const FactorResult& R, dvec&& nfsblk) {
   CB cb;
   i64 ne = R.ne, size = m - ne, nd = k - ne, nfs = m - k;
   cb.size = size; cb.ndel = nd;
   if (nd > 0) {
-    cb.data.assign((size_t)size * size, 0.0);
+    cb.data.resize((size_t)size * size);
+    fill_zero(cb.data.data(), cb.data.size());
     for (i64 j = 0; j < nd; ++j)
       for (i64 i = j; i < nd; ++i) cb.data[i + j * size] = a[ne + i + (ne + j) * lda];
     for (i64 j = 0; j < nd; ++j)
@@ -1029,17 +1395,36 @@ void assemble(const Oracle& O, const Problem& P, const SN& s, i64 m, i64 k, std:
         if (lr >= lc) put(lr, lc, v); else put(lc, lr, v);
       }
     }
+  std::vector<i64> loc;
   for (CB* cb : cbs) {
-    for (i64 j = 0; j < cb->size; ++j) {
-      i64 lj = g2l[cb->rows[j]];
-      for (i64 i = j; i < cb->size; ++i) {
-        double v = cb->data[i + j * cb->size];
+    // When the child's rows map to increasing front rows (no delayed rows
+    // out of order), column j of the child's block lands in front column lj
+    // only, so columns go to threads; each destination still receives its
+    // terms in the same order (children in turn, one term per child).
+    const i64 sz = cb->size;
+    loc.resize(sz);
+    bool mono = true;
+    for (i64 i = 0; i < sz; ++i) {
+      loc[i] = g2l[cb->rows[i]];
+      if (i > 0 && loc[i] <= loc[i - 1]) mono = false;
+    }
+    bool par = mono && sz > 512;
+#ifdef _OPENMP
+    par = par && !omp_in_parallel();
+#pragma omp parallel for schedule(dynamic, 8) if (par)
+#endif
+    for (i64 j = 0; j < sz; ++j) {
+      i64 lj = loc[j];
+      const double* col = cb->data.data() + j * sz;
+      for (i64 i = j; i < sz; ++i) {
+        double v = col[i];
         if (v != 0.0) {
-          i64 li = g2l[cb->rows[i]];
+          i64 li = loc[i];
           if (li >= lj) put(li, lj, v); else put(lj, li, v);
         }
       }
     }
+    (void)par;
   }
   (void)O;
 }
@@ -1072,8 +1457,10 @@ void factor_node(Oracle& O, const Problem& P, i64 s, std::vector<CB>& contrib, s
   for (i64 i = 0; i < m; ++i) g2l[rows[i]] = i;
   i64 nfs = m - k;
   bool has_nfs = nfs > 0 && S.parent >= 0;
-  std::vector<double> fs((size_t)m * k, 0.0);
-  std::vector<double> nfsb(has_nfs ? (size_t)nfs * nfs : 0, 0.0);
+  dvec fs((size_t)m * k);
+  fill_zero(fs.data(), fs.size());
+  dvec nfsb(has_nfs ? (size_t)nfs * nfs : 0);
+  fill_zero(nfsb.data(), nfsb.size());
   assemble(O, P, S, m, k, g2l, fs.data(), nfsb.data(), has_nfs, cbs);
   for (CB* cb : cbs) { cb->data.clear(); cb->data.shrink_to_fit(); cb->rows.clear(); cb->size = 0; }
   i64 t0 = g_ties;
@@ -1130,14 +1517,46 @@ struct orc_options {
   int32_t fallback_bk;
 };
 
-// Factor: the symbolic input is the pre-amalgamation supernode partition
-// (what AptpSymbolic exposes), the permutation perm_fwd[new] = old, the full
-// symmetric CSC and the MC64 scaling in elimination order (or NULL).
-void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end,
-                 const int64_t* pat_ptr, const int64_t* pat_idx, const int64_t* sup_parent,
-                 const int64_t* perm_fwd, const int64_t* colptr, const int64_t* rowidx,
-                 const double* values, const double* scaling, const orc_options* opt, int32_t nthreads) {
-  Oracle* O = new Oracle();
+}  // extern "C"
+
+namespace {
+
+// One factorization: the pattern-only set-up (amalgamation, children,
+// small-leaf classification), then the numeric phase, which runs either in
+// one go or in slices (a worker thread that stops at checkpoints).
+struct Run {
+  Oracle* O = nullptr;
+  Problem P;
+  std::vector<CB> contrib;
+  std::vector<Subtree> subs;
+  int nthreads = 0;
+  std::vector<double> fflops;  // delay-free flops per (amalgamated) front
+  double total = 0.0;
+  std::mutex mu;
+  std::condition_variable cv;
+  double target = 0.0, done = 0.0;
+  bool running = false, finished = false;
+  std::thread th;
+};
+
+void checkpoint(double done_now) {
+  Run* r = tl_run;
+  if (!r || omp_in_parallel()) return;
+  std::unique_lock<std::mutex> lk(r->mu);
+  r->done = done_now;
+  if (r->done >= r->target) {
+    r->running = false;
+    r->cv.notify_all();
+    r->cv.wait(lk, [&] { return r->running; });
+  }
+}
+
+Run* run_setup(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end, const int64_t* pat_ptr,
+               const int64_t* pat_idx, const int64_t* sup_parent, const int64_t* perm_fwd, const int64_t* colptr,
+               const int64_t* rowidx, const double* values, const double* scaling, const orc_options* opt,
+               int32_t nthreads) {
+  Run* r = new Run();
+  Oracle* O = r->O = new Oracle();
   O->n = n;
   if (opt) {
     O->o.threshold = opt->threshold; O->o.small = opt->small; O->o.nb = opt->outer_block_size;
@@ -1156,10 +1575,10 @@ void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_
   i64 ns = (i64)O->sn.size();
   O->ch.assign(ns, {});
   for (i64 s = 0; s < ns; ++s) if (O->sn[s].parent >= 0) O->ch[O->sn[s].parent].push_back(s);
-  auto subs = classify_small_leaf(O->sn, O->ch, O->o.small_leaf_threshold);
-  O->n_sl_sub = (i64)subs.size();
-  for (auto& st : subs) O->n_sl_nodes += (i64)st.nodes.size();
-  Problem P;
+  r->subs = classify_small_leaf(O->sn, O->ch, O->o.small_leaf_threshold);
+  O->n_sl_sub = (i64)r->subs.size();
+  for (auto& st : r->subs) O->n_sl_nodes += (i64)st.nodes.size();
+  Problem& P = r->P;
   P.n = n; P.colptr = colptr; P.rowidx = rowidx; P.val = values; P.scaling = scaling;
   P.pfwd.assign(perm_fwd, perm_fwd + n);
   P.pinv.assign(n, 0);
@@ -1167,38 +1586,99 @@ void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_
   O->pfwd = P.pfwd;
   if (scaling) { O->has_scaling = true; O->scaling.assign(scaling, scaling + n); }
   O->fr.assign(ns, Front());
-  std::vector<CB> contrib(ns);
+  r->contrib.resize(ns);
+  r->nthreads = nthreads;
+  r->fflops.resize(ns);
+  for (i64 s = 0; s < ns; ++s) {
+    const double k = (double)O->sn[s].n_owned();
+    r->fflops[s] = front_flops(k + (double)O->sn[s].pattern.size(), k);
+    r->total += r->fflops[s];
+  }
+  return r;
+}
+
+// The numeric phase: small-leaf pre-pass (numeric.rs:1984-2010), then
+// level-set waves (2038-2160), then the aggregate statistics (929-1009).
+void run_body(Run* r) {
+  Oracle* O = r->O;
+  Problem& P = r->P;
+  std::vector<CB>& contrib = r->contrib;
+  const i64 n = O->n, ns = (i64)O->sn.size();
+#ifdef _OPENMP
+  if (r->nthreads > 0) omp_set_num_threads(r->nthreads);
+#endif
   g_ties = 0;
-  // small-leaf pre-pass (numeric.rs:1984-2010) then level-set waves (2038-2160)
+  double done = 0.0;
   std::vector<i64> remaining(ns);
   for (i64 s = 0; s < ns; ++s) remaining[s] = (i64)O->ch[s].size();
   {
-    std::vector<i64> g2l(n, -1);
-    for (auto& st : subs) {
-      for (i64 x : st.nodes) factor_node(*O, P, x, contrib, g2l);
-      if (st.parent_of_root >= 0) remaining[st.parent_of_root] -= 1;
-    }
-  }
-  std::vector<i64> ready;
-  for (i64 s = 0; s < ns; ++s) if (remaining[s] == 0 && !O->sn[s].in_small_leaf) ready.push_back(s);
+    // the subtrees are independent (numeric.rs factors them in parallel);
+    // each one's fronts in order on one thread
+    const i64 nsub = (i64)r->subs.size();
 #ifdef _OPENMP
-  if (nthreads > 0) omp_set_num_threads(nthreads);
-#else
-  (void)nthreads;
+#pragma omp parallel if (nsub > 1)
 #endif
-  while (!ready.empty()) {
-    i64 nr = (i64)ready.size();
-#ifdef _OPENMP
-    // many fronts: one thread per front; few fronts: one at a time with the
-    // dense loops inside running in parallel
-    const bool wave_par = nr >= (i64)omp_get_max_threads() && nr > 1;
-#pragma omp parallel if (wave_par)
     {
       std::vector<i64> g2l(n, -1);
       i64 ties0 = g_ties; g_ties = 0;
+#ifdef _OPENMP
 #pragma omp for schedule(dynamic, 1)
-      for (i64 i = 0; i < nr; ++i) factor_node(*O, P, ready[i], contrib, g2l);
+#endif
+      for (i64 t = 0; t < nsub; ++t)
+        for (i64 x : r->subs[t].nodes) factor_node(*O, P, x, contrib, g2l);
       g_ties = ties0;
+    }
+    for (auto& st : r->subs) {
+      if (st.parent_of_root >= 0) remaining[st.parent_of_root] -= 1;
+      for (i64 x : st.nodes) done += r->fflops[x];
+    }
+    checkpoint(done);
+  }
+  std::vector<i64> ready;
+  for (i64 s = 0; s < ns; ++s) if (remaining[s] == 0 && !O->sn[s].in_small_leaf) ready.push_back(s);
+  while (!ready.empty()) {
+    i64 nr = (i64)ready.size();
+#ifdef _OPENMP
+    // The fronts of a wave are independent.  Fronts whose dense work would
+    // hold up the wave if one thread took them (more than the wave's average
+    // per thread, or large in absolute terms) run one at a time with the
+    // dense loops inside in parallel; the rest one front per thread.  Which
+    // thread takes a front changes nothing in its arithmetic.
+    {
+      const i64 nth = omp_get_max_threads();
+      std::vector<double> work(nr);
+      double tot = 0;
+      for (i64 i = 0; i < nr; ++i) {
+        const SN& S = O->sn[ready[i]];
+        double k = (double)S.n_owned(), m = k + (double)S.pattern.size();
+        work[i] = k * m * m;
+        tot += work[i];
+      }
+      std::vector<i64> big, small;
+      for (i64 i = 0; i < nr; ++i) {
+        const bool b = nth > 1 && (work[i] > 2e9 || (nr > 1 && work[i] > tot / (double)nth) || nr == 1);
+        (b ? big : small).push_back(ready[i]);
+      }
+      {
+        std::vector<i64> g2l(n, -1);
+        for (i64 s : big) {
+          tl_front_base = done;
+          factor_node(*O, P, s, contrib, g2l);
+          done += r->fflops[s];
+          checkpoint(done);
+        }
+      }
+      const i64 ns_ = (i64)small.size();
+#pragma omp parallel if (ns_ > 1)
+      {
+        std::vector<i64> g2l(n, -1);
+        i64 ties0 = g_ties; g_ties = 0;
+#pragma omp for schedule(dynamic, 1)
+        for (i64 i = 0; i < ns_; ++i) factor_node(*O, P, small[i], contrib, g2l);
+        g_ties = ties0;
+      }
+      for (i64 s : small) done += r->fflops[s];
+      checkpoint(done);
     }
 #else
     {
@@ -1222,10 +1702,89 @@ void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_
     for (i64 c = 0; c < F.ne; ++c) if (F.d11.type[c] == PT_1X1 && F.d11.diag[c] == 0.0) O->zero_piv++;
     if (O->sn[s].parent < 0 && F.ne < F.m) O->zero_piv += F.k - F.ne;
   }
+  contrib.clear();
+}
+
+}  // namespace
+
+extern "C" {
+
+// Factor: the symbolic input is the pre-amalgamation supernode partition
+// (what AptpSymbolic exposes), the permutation perm_fwd[new] = old, the full
+// symmetric CSC and the MC64 scaling in elimination order (or NULL).
+void* orc_factor(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end,
+                 const int64_t* pat_ptr, const int64_t* pat_idx, const int64_t* sup_parent,
+                 const int64_t* perm_fwd, const int64_t* colptr, const int64_t* rowidx,
+                 const double* values, const double* scaling, const orc_options* opt, int32_t nthreads) {
+  Run* r = run_setup(n, nsup, sup_begin, sup_end, pat_ptr, pat_idx, sup_parent, perm_fwd, colptr, rowidx, values,
+                     scaling, opt, nthreads);
+  run_body(r);
+  Oracle* O = r->O;
+  delete r;
+  return O;
+}
+
+// The same factorization in slices, for timing a long run step by step: the
+// set-up happens here; the numeric phase runs on a worker thread that stops
+// at checkpoints (after every front of a wave that is taken alone, after
+// every wave, after every 256-column outer block of such a front) once its
+// delay-free flops reach the target of the last orc_session_advance.
+// Every input array must stay alive until orc_session_finish.
+void* orc_session_begin(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end,
+                        const int64_t* pat_ptr, const int64_t* pat_idx, const int64_t* sup_parent,
+                        const int64_t* perm_fwd, const int64_t* colptr, const int64_t* rowidx,
+                        const double* values, const double* scaling, const orc_options* opt, int32_t nthreads) {
+  Run* r = run_setup(n, nsup, sup_begin, sup_end, pat_ptr, pat_idx, sup_parent, perm_fwd, colptr, rowidx, values,
+                     scaling, opt, nthreads);
+  r->th = std::thread([r] {
+    tl_run = r;
+    {
+      std::unique_lock<std::mutex> lk(r->mu);
+      r->cv.wait(lk, [&] { return r->running; });
+    }
+    run_body(r);
+    std::lock_guard<std::mutex> lk(r->mu);
+    r->finished = true;
+    r->running = false;
+    r->cv.notify_all();
+  });
+  return r;
+}
+
+// Delay-free flops of the whole factorization (the unit of the targets).
+double orc_session_total(void* h) { return ((Run*)h)->total; }
+
+// Flops done at the last checkpoint.
+double orc_session_done(void* h) { return ((Run*)h)->done; }
+
+// Runs the factorization until its flops reach `target` at a checkpoint or
+// it ends; returns 1 when it has ended.
+int32_t orc_session_advance(void* h, double target) {
+  Run* r = (Run*)h;
+  std::unique_lock<std::mutex> lk(r->mu);
+  if (r->finished) return 1;
+  r->target = target;
+  r->running = true;
+  r->cv.notify_all();
+  r->cv.wait(lk, [&] { return !r->running || r->finished; });
+  return r->finished ? 1 : 0;
+}
+
+// Runs the rest, ends the worker and returns the factorization handle (as
+// orc_factor does).
+void* orc_session_finish(void* h) {
+  Run* r = (Run*)h;
+  orc_session_advance(h, 1e300);
+  r->th.join();
+  Oracle* O = r->O;
+  delete r;
   return O;
 }
 
 void orc_free(void* h) { delete (Oracle*)h; }
+
+// Return the cached front buffers to the system.
+void orc_release_cache() { big_cache().release(); }
 
 // counts: [n1x1, n2x2, delayed, zero_pivots, max_front, sn_before, sn_after, merges, sl_subtrees, sl_nodes, ties]
 void orc_stats(void* h, int64_t* out) {
@@ -1274,6 +1833,108 @@ int64_t orc_elim(void* h, int64_t* col, int8_t* code, double* dd, double* doff) 
 }
 
 // SparseLDLT::solve_in_place (solver.rs:370-428) + aptp_solve (solve.rs:57-144)
+//
+// Large fronts split their triangular solves and products over threads
+// without changing what any thread computes for a given front size: the
+// forward L11 and L21 updates go by blocks of rows (each entry still takes
+// its terms in column order, as in the serial loop), the backward L21 and
+// L11 dot products by columns.  The backward L11 solve takes blocks of SB
+// columns from the bottom: the dot products against the rows below the block
+// run in parallel, then the block itself serially, so for fronts larger than
+// SB the order of the subtractions differs from the serial loop (rounding
+// only; the factor is not affected), and the result is the same for any
+// thread count.
+namespace {
+const i64 SOLVE_PAR = 2048;  // fronts at least this wide use the blocked, threaded loops
+const i64 SB = 256;
+
+void fwd_front(const Front& F, std::vector<double>& x, std::vector<double>& w, std::vector<double>& w2) {
+  i64 ne = F.ne;
+  i64 r = (i64)F.row_idx.size();
+  w.assign(ne, 0.0);
+  for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
+  const bool par = ne >= SOLVE_PAR && !omp_in_parallel();
+  if (!par) {
+    for (i64 j = 0; j < ne; ++j) { double xj = w[j]; for (i64 i = j + 1; i < ne; ++i) w[i] -= F.l11[i + j * ne] * xj; }
+  } else {
+    // column blocks: finish the block's own rows serially, then the rows below in parallel
+    for (i64 j0 = 0; j0 < ne; j0 += SB) {
+      const i64 j1 = std::min(ne, j0 + SB);
+      for (i64 j = j0; j < j1; ++j) { double xj = w[j]; for (i64 i = j + 1; i < j1; ++i) w[i] -= F.l11[i + j * ne] * xj; }
+      const i64 nrow = ne - j1, RB = 1024, nrb = (nrow + RB - 1) / RB;
+#pragma omp parallel for schedule(static)
+      for (i64 rb = 0; rb < nrb; ++rb) {
+        const i64 r0 = j1 + rb * RB, r1 = std::min(ne, r0 + RB);
+        for (i64 j = j0; j < j1; ++j) {
+          const double xj = w[j];
+          const double* l = F.l11.data() + j * ne;
+          for (i64 i = r0; i < r1; ++i) w[i] -= l[i] * xj;
+        }
+      }
+    }
+  }
+  for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
+  if (r > 0) {
+    w2.assign(r, 0.0);
+    if (!(par || (r * ne >= SOLVE_PAR * SOLVE_PAR && !omp_in_parallel()))) {
+      for (i64 j = 0; j < ne; ++j) { double xj = w[j]; const double* l = F.l21.data() + j * r; for (i64 i = 0; i < r; ++i) w2[i] += l[i] * xj; }
+    } else {
+      const i64 RB = 1024, nrb = (r + RB - 1) / RB;
+#pragma omp parallel for schedule(static)
+      for (i64 rb = 0; rb < nrb; ++rb) {
+        const i64 r0 = rb * RB, r1 = std::min(r, r0 + RB);
+        for (i64 j = 0; j < ne; ++j) {
+          const double xj = w[j];
+          const double* l = F.l21.data() + j * r;
+          for (i64 i = r0; i < r1; ++i) w2[i] += l[i] * xj;
+        }
+      }
+    }
+    for (i64 i = 0; i < r; ++i) x[F.row_idx[i]] -= w2[i];
+  }
+}
+
+void bwd_front(const Front& F, std::vector<double>& x, std::vector<double>& w, std::vector<double>& w2) {
+  i64 ne = F.ne;
+  i64 r = (i64)F.row_idx.size();
+  w.assign(ne, 0.0);
+  for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
+  const bool big = (ne >= SOLVE_PAR || r * ne >= SOLVE_PAR * SOLVE_PAR) && !omp_in_parallel();
+  if (r > 0) {
+    w2.assign(r, 0.0);
+    for (i64 i = 0; i < r; ++i) w2[i] = x[F.row_idx[i]];
+#pragma omp parallel for schedule(static) if (big)
+    for (i64 j = 0; j < ne; ++j) {
+      const double* l = F.l21.data() + j * r;
+      double s2 = 0.0;
+      for (i64 i = 0; i < r; ++i) s2 += l[i] * w2[i];
+      w[j] -= s2;
+    }
+  }
+  if (ne < SOLVE_PAR || omp_in_parallel()) {
+    for (i64 j = ne - 1; j >= 0; --j) { double s2 = w[j]; for (i64 i = j + 1; i < ne; ++i) s2 -= F.l11[i + j * ne] * w[i]; w[j] = s2; }
+  } else {
+    std::vector<double> t(SB);
+    for (i64 j1 = ne; j1 > 0; j1 -= SB) {
+      const i64 j0 = std::max<i64>(0, j1 - SB);
+#pragma omp parallel for schedule(static)
+      for (i64 j = j0; j < j1; ++j) {
+        const double* l = F.l11.data() + j * ne;
+        double s2 = 0.0;
+        for (i64 i = j1; i < ne; ++i) s2 += l[i] * w[i];
+        t[j - j0] = s2;
+      }
+      for (i64 j = j1 - 1; j >= j0; --j) {
+        double s2 = w[j] - t[j - j0];
+        for (i64 i = j + 1; i < j1; ++i) s2 -= F.l11[i + j * ne] * w[i];
+        w[j] = s2;
+      }
+    }
+  }
+  for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
+}
+}  // namespace
+
 void orc_solve(void* h, double* rhs) {
   Oracle* O = (Oracle*)h;
   i64 n = O->n;
@@ -1284,17 +1945,8 @@ void orc_solve(void* h, double* rhs) {
   std::vector<double> w, w2;
   // forward (solve.rs:161-225)
   for (auto& F : O->fr) {
-    i64 ne = F.ne; if (ne == 0) continue;
-    i64 r = (i64)F.row_idx.size();
-    w.assign(ne, 0.0);
-    for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
-    for (i64 j = 0; j < ne; ++j) { double xj = w[j]; for (i64 i = j + 1; i < ne; ++i) w[i] -= F.l11[i + j * ne] * xj; }
-    for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
-    if (r > 0) {
-      w2.assign(r, 0.0);
-      for (i64 j = 0; j < ne; ++j) { double xj = w[j]; const double* l = F.l21.data() + j * r; for (i64 i = 0; i < r; ++i) w2[i] += l[i] * xj; }
-      for (i64 i = 0; i < r; ++i) x[F.row_idx[i]] -= w2[i];
-    }
+    if (F.ne == 0) continue;
+    fwd_front(F, x, w, w2);
   }
   // diagonal (solve.rs:232-252)
   for (auto& F : O->fr) {
@@ -1307,17 +1959,8 @@ void orc_solve(void* h, double* rhs) {
   // backward (solve.rs:261-326)
   for (i64 s = (i64)O->fr.size() - 1; s >= 0; --s) {
     Front& F = O->fr[s];
-    i64 ne = F.ne; if (ne == 0) continue;
-    i64 r = (i64)F.row_idx.size();
-    w.assign(ne, 0.0);
-    for (i64 i = 0; i < ne; ++i) w[i] = x[F.col_idx[i]];
-    if (r > 0) {
-      w2.assign(r, 0.0);
-      for (i64 i = 0; i < r; ++i) w2[i] = x[F.row_idx[i]];
-      for (i64 j = 0; j < ne; ++j) { const double* l = F.l21.data() + j * r; double s2 = 0.0; for (i64 i = 0; i < r; ++i) s2 += l[i] * w2[i]; w[j] -= s2; }
-    }
-    for (i64 j = ne - 1; j >= 0; --j) { double s2 = w[j]; for (i64 i = j + 1; i < ne; ++i) s2 -= F.l11[i + j * ne] * w[i]; w[j] = s2; }
-    for (i64 i = 0; i < ne; ++i) x[F.col_idx[i]] = w[i];
+    if (F.ne == 0) continue;
+    bwd_front(F, x, w, w2);
   }
   if (O->has_scaling) for (i64 i = 0; i < n; ++i) x[i] *= O->scaling[i];
   for (i64 i = 0; i < n; ++i) rhs[O->pfwd[i]] = x[i];

@@ -58,6 +58,17 @@ def lib():
         L.orc_elim.argtypes = [C.c_void_p, i64p, i8p, dp, dp]
         L.orc_solve.argtypes = [C.c_void_p, dp]
         L.orc_dense_aptp.argtypes = [i64, i64, dp, C.POINTER(OrcOptions), i64p, i8p, dp, dp, i64p, dp]
+        L.orc_session_begin.restype = C.c_void_p
+        L.orc_session_begin.argtypes = L.orc_factor.argtypes
+        L.orc_session_total.restype = C.c_double
+        L.orc_session_total.argtypes = [C.c_void_p]
+        L.orc_session_done.restype = C.c_double
+        L.orc_session_done.argtypes = [C.c_void_p]
+        L.orc_session_advance.restype = C.c_int32
+        L.orc_session_advance.argtypes = [C.c_void_p, C.c_double]
+        L.orc_session_finish.restype = C.c_void_p
+        L.orc_session_finish.argtypes = [C.c_void_p]
+        L.orc_release_cache.argtypes = []
         _lib = L
     return _lib
 
@@ -73,7 +84,7 @@ class OracleFactor:
                  "supernodes_before_amalgamation", "supernodes_after_amalgamation", "merges_performed",
                  "small_leaf_subtrees", "small_leaf_nodes", "near_ties"]
 
-    def __init__(self, system, symbolic, scaling_elim=None, opts=None, nthreads=1):
+    def __init__(self, system, symbolic, scaling_elim=None, opts=None, nthreads=1, sliced=False):
         L = lib()
         self.n = system.n
         self._keep = [np.ascontiguousarray(x) for x in (symbolic.sup_begin, symbolic.sup_end, symbolic.pat_ptr,
@@ -83,9 +94,31 @@ class OracleFactor:
         sc = None if scaling_elim is None else np.ascontiguousarray(scaling_elim, dtype=np.float64)
         o = opts or options()
         k = self._keep
-        self.h = L.orc_factor(system.n, symbolic.sup_begin.size, _p(k[0], i64p), _p(k[1], i64p), _p(k[2], i64p),
-                              _p(k[3], i64p), _p(k[4], i64p), _p(k[5], i64p), _p(k[6], i64p), _p(k[7], i64p),
-                              _p(vals, dp), _p(sc, dp), C.byref(o), nthreads)
+        self._keep += [vals, sc, o]
+        args = (system.n, symbolic.sup_begin.size, _p(k[0], i64p), _p(k[1], i64p), _p(k[2], i64p),
+                _p(k[3], i64p), _p(k[4], i64p), _p(k[5], i64p), _p(k[6], i64p), _p(k[7], i64p),
+                _p(vals, dp), _p(sc, dp), C.byref(o), nthreads)
+        self.h = None
+        self.session = None
+        if sliced:
+            # the numeric phase runs in slices: advance() / finish()
+            self.session = L.orc_session_begin(*args)
+        else:
+            self.h = L.orc_factor(*args)
+
+    def total_flops(self):
+        """Delay-free flops of the factorization (sliced runs)."""
+        return lib().orc_session_total(self.session)
+
+    def advance(self, target_flops):
+        """Run the factorization until target_flops are done (at the next
+        checkpoint) or it ends; True when it has ended."""
+        return bool(lib().orc_session_advance(self.session, float(target_flops)))
+
+    def finish(self):
+        if self.session is not None:
+            self.h = lib().orc_session_finish(self.session)
+            self.session = None
 
     def stats(self):
         out = np.zeros(11, np.int64)
@@ -126,6 +159,8 @@ class OracleFactor:
         return x
 
     def close(self):
+        if self.session is not None:
+            self.finish()
         if self.h:
             lib().orc_free(self.h)
             self.h = None
@@ -135,6 +170,90 @@ class OracleFactor:
             self.close()
         except Exception:
             pass
+
+
+# ---- host analysis for CPU-only runs (libanalysis.so) ----------------------
+ALIB = os.path.join(HERE, "_build", "libanalysis.so")
+_alib = None
+
+
+def alib():
+    global _alib
+    if _alib is None:
+        if not os.path.exists(ALIB):
+            lib()  # builds both libraries
+            import importlib.util
+            spec = importlib.util.spec_from_file_location("_oracle_build", os.path.join(HERE, "build.py"))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            mod.build()
+        L = C.CDLL(ALIB)
+        L.rvg_last_error.restype = C.c_char_p
+        L.rvg_analyze.restype = C.c_int
+        L.rvg_analyze.argtypes = [i64, i64p, i64p, i64p, C.POINTER(C.c_void_p)]
+        L.rvg_symbolic_sizes.argtypes = [C.c_void_p, i64p]
+        L.rvg_symbolic_export.argtypes = [C.c_void_p, i64p, i64p, i64p, i64p, i64p, i64p]
+        L.rvg_symbolic_free.argtypes = [C.c_void_p]
+        L.rvg_mc64.restype = C.c_int
+        L.rvg_mc64.argtypes = [i64, i64p, i64p, dp, i64p, dp, i64p]
+        _alib = L
+    return _alib
+
+
+class Symbolic:
+    """The symbolic structure the numeric phase takes (what AptpSymbolic
+    exposes): perm_fwd[new] = old, supernode column ranges, parents and row
+    patterns."""
+
+    def __init__(self, n, perm_fwd, sup_begin, sup_end, sup_parent, pat_ptr, pat_idx):
+        self.n, self.perm_fwd, self.sup_begin, self.sup_end = n, perm_fwd, sup_begin, sup_end
+        self.sup_parent, self.pat_ptr, self.pat_idx = sup_parent, pat_ptr, pat_idx
+
+
+def _acheck(st):
+    if st != 0:
+        raise RuntimeError(f"analysis failed ({st}): {alib().rvg_last_error().decode()}")
+
+
+def analyze(system, order, mc64=True):
+    """Symbolic analysis for a fill-reducing `order` and, with mc64, the MC64
+    symmetric scaling in elimination order -- the library's host analysis
+    (the same code the GPU path uses), loaded without the GPU library.
+    Returns (Symbolic, scaling or None)."""
+    L = alib()
+    n = int(system.n)
+    colptr = np.ascontiguousarray(system.colptr, dtype=np.int64)
+    rowidx = np.ascontiguousarray(system.rowidx, dtype=np.int64)
+    order = np.ascontiguousarray(order, dtype=np.int64)
+    h = C.c_void_p()
+    _acheck(L.rvg_analyze(n, _p(colptr, i64p), _p(rowidx, i64p), _p(order, i64p), C.byref(h)))
+    try:
+        sz = np.zeros(4, np.int64)
+        _acheck(L.rvg_symbolic_sizes(h, _p(sz, i64p)))
+        nn, ns, npat, _ = (int(x) for x in sz)
+        perm = np.zeros(nn, np.int64)
+        b, e, par = np.zeros(ns, np.int64), np.zeros(ns, np.int64), np.zeros(ns, np.int64)
+        pp, pi = np.zeros(ns + 1, np.int64), np.zeros(max(npat, 1), np.int64)
+        _acheck(L.rvg_symbolic_export(h, _p(perm, i64p), _p(b, i64p), _p(e, i64p), _p(par, i64p), _p(pp, i64p),
+                                      _p(pi, i64p)))
+    finally:
+        L.rvg_symbolic_free(h)
+    sym = Symbolic(nn, perm, b, e, par, pp, pi[:npat])
+    scaling = None
+    if mc64 and n > 0:
+        vals = np.ascontiguousarray(system.values, dtype=np.float64)
+        matching = np.zeros(n, np.int64)
+        sc = np.zeros(n, np.float64)
+        matched = C.c_int64(0)
+        _acheck(L.rvg_mc64(n, _p(colptr, i64p), _p(rowidx, i64p), _p(vals, dp), _p(matching, i64p), _p(sc, dp),
+                           C.byref(matched)))
+        scaling = np.ascontiguousarray(sc[perm])
+    return sym, scaling
+
+
+def release_cache():
+    """Give the oracle's cached front buffers back to the system."""
+    lib().orc_release_cache()
 
 
 def dense_aptp(a, p=None, opts=None):

@@ -262,3 +262,36 @@ def test_thread_count_invariance(rv, orc, kind):
         for x, y in zip(p, recs[0][0]):
             assert np.array_equal(x, y)
         assert st == recs[0][1] and ine == recs[0][2]
+
+
+def test_cpu_only_analysis_matches_library(rv, orc):
+    """The oracle's analysis library (the library's host analysis sources
+    without the CUDA numeric phase) gives the same symbolic structure and
+    MC64 scaling as the library itself, so a CPU-only run factors the same
+    fronts as the GPU path."""
+    for s in (rv.problems.kkt(10, seed=3), rv.problems.shifted_laplacian(12, 0.1)):
+        solver = rv.SparseLDLT.analyze_with_matrix(s, rv.AnalyzeOptions(rv.OrderingStrategy.MATCH_ORDER_METIS))
+        sym, sc = orc.analyze(s, rv.ordering.default_order(s), mc64=True)
+        a = solver.symbolic
+        for f in ("perm_fwd", "sup_begin", "sup_end", "sup_parent", "pat_ptr", "pat_idx"):
+            assert np.array_equal(getattr(a, f), getattr(sym, f)), f
+        assert np.array_equal(solver._scaling, sc)
+
+
+def test_sliced_factorization_is_the_same(rv, orc):
+    """The factorization run in slices (the timed CPU reference: a worker that
+    stops at checkpoints between fronts and outer blocks) gives the same
+    pivot record and statistics as one uninterrupted run."""
+    s = rv.problems.kkt(16, seed=5)
+    sym, sc = orc.analyze(s, rv.ordering.default_order(s), mc64=True)
+    ref = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=4)
+    ses = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=4, sliced=True)
+    tot = ses.total_flops()
+    ends = [ses.advance(tot * (i + 1) / 5) for i in range(4)]
+    assert not any(ends)
+    ses.finish()
+    for x, y in zip(ref.pivot_record(), ses.pivot_record()):
+        assert np.array_equal(x, y)
+    assert ref.stats() == ses.stats()
+    b = rv.problems.rhs_normal(s.n, 0)
+    assert np.array_equal(ref.solve(b), ses.solve(b))
