@@ -1535,9 +1535,11 @@ struct Run {
   std::mutex mu;
   std::condition_variable cv;
   double target = 0.0, done = 0.0;
-  bool running = false, finished = false;
+  bool running = false, finished = false, abort = false;
   std::thread th;
 };
+
+struct Aborted {};
 
 void checkpoint(double done_now) {
   Run* r = tl_run;
@@ -1549,6 +1551,7 @@ void checkpoint(double done_now) {
     r->cv.notify_all();
     r->cv.wait(lk, [&] { return r->running; });
   }
+  if (r->abort) throw Aborted();  // unwinds the worker's stack (never inside a parallel region)
 }
 
 Run* run_setup(int64_t n, int64_t nsup, const int64_t* sup_begin, const int64_t* sup_end, const int64_t* pat_ptr,
@@ -1742,7 +1745,10 @@ void* orc_session_begin(int64_t n, int64_t nsup, const int64_t* sup_begin, const
       std::unique_lock<std::mutex> lk(r->mu);
       r->cv.wait(lk, [&] { return r->running; });
     }
-    run_body(r);
+    try {
+      if (!r->abort) run_body(r);
+    } catch (const Aborted&) {
+    }
     std::lock_guard<std::mutex> lk(r->mu);
     r->finished = true;
     r->running = false;
@@ -1768,6 +1774,20 @@ int32_t orc_session_advance(void* h, double target) {
   r->cv.notify_all();
   r->cv.wait(lk, [&] { return !r->running || r->finished; });
   return r->finished ? 1 : 0;
+}
+
+// Stops a sliced factorization at its current checkpoint and frees it.
+void orc_session_abort(void* h) {
+  Run* r = (Run*)h;
+  {
+    std::lock_guard<std::mutex> lk(r->mu);
+    r->abort = true;
+    r->running = true;
+    r->cv.notify_all();
+  }
+  r->th.join();
+  delete r->O;
+  delete r;
 }
 
 // Runs the rest, ends the worker and returns the factorization handle (as

@@ -69,6 +69,7 @@ def lib():
         L.orc_session_finish.restype = C.c_void_p
         L.orc_session_finish.argtypes = [C.c_void_p]
         L.orc_release_cache.argtypes = []
+        L.orc_session_abort.argtypes = [C.c_void_p]
         _lib = L
     return _lib
 
@@ -158,9 +159,14 @@ class OracleFactor:
             x[:, j] = col
         return x
 
-    def close(self):
+    def abort(self):
+        """Stop a sliced factorization where it is and free it."""
         if self.session is not None:
-            self.finish()
+            lib().orc_session_abort(self.session)
+            self.session = None
+
+    def close(self):
+        self.abort()
         if self.h:
             lib().orc_free(self.h)
             self.h = None

@@ -295,3 +295,19 @@ def test_sliced_factorization_is_the_same(rv, orc):
     assert ref.stats() == ses.stats()
     b = rv.problems.rhs_normal(s.n, 0)
     assert np.array_equal(ref.solve(b), ses.solve(b))
+
+
+def test_sliced_factorization_abort(rv, orc):
+    """A sliced run closed before its end stops at its checkpoint instead of
+    running the rest."""
+    import time
+    s = rv.problems.kkt(16, seed=5)
+    sym, sc = orc.analyze(s, rv.ordering.default_order(s), mc64=True)
+    ses = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=2, sliced=True)
+    ses.advance(ses.total_flops() * 0.01)
+    t0 = time.perf_counter()
+    ses.close()
+    assert ses.session is None and ses.h is None
+    full = orc.OracleFactor(s, sym, sc, orc.options(), nthreads=2)
+    assert full.inertia() == s.inertia
+    assert time.perf_counter() - t0 < 60
