@@ -56,6 +56,8 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # name: (builder, description)
     "kkt60": ("kkt", 60, "kkt27_60^3: H 27-pt 60^3 + diag U[0,1e-2], J 54000x216000 (4/row), n=270000"),
+    "kkt36": ("kkt", 36, "kkt27_36^3 (the KKT family at n=58320; profiling case)"),
+    "kkt48": ("kkt", 48, "kkt27_48^3 (the KKT family at n=138240; profiling case)"),
     "lap16": ("lap", 16, "laplace7_16^3 shifted to 10% negative, n=4096"),
     "lap100": ("lap", 100, "laplace7_100^3 shifted to 5% negative, n=1000000"),
     "batch64": ("batch", 64, "64 systems, n log-uniform in [5e3, 2e5] (seed 1), half shifted 7-pt Laplacians, "
@@ -520,6 +522,30 @@ def run_learned(args, rv, torch):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_step(args, rv, torch):
+    """One form on one system, W warm-up and K timed steps (factor + solve to
+    1e-14 with inputs in HBM), then one step with the library's per-launch
+    events: the command the ncu summaries under profiles/ were taken with."""
+    s, b = build_system(rv, args.config)
+    solver, _ = analyze(rv, s)
+    form = {"plain": dict(precision="fp64"),
+            "tf32": dict(precision="mixed", mixed_flush=4, mixed_operands="tf32"),
+            "bf16": dict(precision="mixed", mixed_flush=0, mixed_operands="bf16"),
+            "learned": dict(precision="learned", mixed_flush=0, mixed_operands="bf16")}[args.profile_step]
+    if args.profile_step == "learned":
+        solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
+    opts = rv.FactorOptions(**form)
+    r = time_form(rv, torch, solver, s, b, opts, args.warmup, args.steps)
+    solver.set_profiling(True)
+    time_form(rv, torch, solver, s, b, opts, 0, 1)
+    pr = solver.profile()
+    solver.close()
+    print(json.dumps({"config": args.config, "form": args.profile_step, "n": s.n, "s_per_step": r["s_per_step"],
+                      "bwd_err": r["bwd_err"], "inertia": r["inertia"], "solves_after_first": r["solves_after_first"],
+                      "phases_ms": {k: pr[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "host_sync_ms")},
+                      "parts_ms": pr["part_ms"]}), flush=True)
+
+
 def run_reference(args, rv, entry, rank):
     """The reference arm: the CPU restatement of the reference's numeric phase
     (oracle/, OpenMP, all host cores) on this arm's workload, through the
@@ -584,10 +610,14 @@ def main():
     ap.add_argument("--train-count", type=int, default=200, help="learned config: generated training matrices")
     ap.add_argument("--mixed-flush", default="4,0",
                     help="comma list of mixed-form flush depths to time (32-deep K chunks per FP32 partial sum; 0 = all K)")
+    ap.add_argument("--profile-step", default=None, choices=["plain", "tf32", "bf16", "learned"],
+                    help="profiling aid: time only this form (factor + solve to 1e-14) on --config and print "
+                         "its time and parts; no contract line")
     ap.add_argument("--bf16-flush", default="0",
                     help="the same for the mixed form with BF16 operand parts")
     args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
+    if not args.profile_step:
+        args.warmup = max(args.warmup, 3)
 
     import __graft_entry__ as entry
     rv = entry.load_package()
@@ -620,6 +650,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.profile_step:
+        run_profile_step(args, rv, torch)
+        return
     if args.config == "learned":
         if rank == 0:
             run_learned(args, rv, torch)

@@ -117,44 +117,94 @@ __global__ void k_scatter(const ScatterItem* items, const DFront* F, Statics S, 
   }
 }
 
-struct EaItem { int32_t parent; int32_t child; int32_t j0; int32_t pad; };
-
 // Extend-add of one child's contribution into its parent
-// (numeric.rs:2445-2559): columns [j0, j0+32) of the child block.  The child
-// block is [delayed; NFS] x [delayed; NFS]: its delayed columns live in the
-// child's panel (rows ne..k and k..m of columns ne..k), its NFS x NFS part in
-// the child's contribution buffer.
-__global__ void k_extend_add(const EaItem* items, const DFront* F, Statics S, Arenas A) {
-  EaItem it = items[blockIdx.x];
+// (numeric.rs:2445-2559).  The child block is [delayed; NFS] x [delayed;
+// NFS]: its delayed columns live in the child's panel (rows ne..k and k..m
+// of columns ne..k), its NFS x NFS part in the child's contribution buffer.
+// An item is a 32-column group [j0, j0+32) of one child's block and a
+// segment of its rows [i0, i0 + EA_ROWS), i >= j only.  Each CTA stages the group's 32 destination
+// columns in shared memory, then walks its rows in tiles of 256, one row per
+// thread: the thread maps its row once, then handles the 32 columns in
+// batches of 8 with all eight source loads, then all eight destination
+// loads, in flight together (the one-entry-at-a-time loop kept too few bytes
+// in flight per SM to reach HBM bandwidth).  Source reads are coalesced (a
+// column of the child block is contiguous); each destination entry still
+// receives exactly one term from this child, so the per-ordinal launches
+// keep the reference's order of terms.
+constexpr int EA_ROWS = 4096;  // rows per item
+struct EaTile { int32_t parent; int32_t child; int32_t j0; int32_t i0; };
+
+__global__ void __launch_bounds__(256, 3) k_extend_add_tiled(const EaTile* items, const DFront* F, Statics S, Arenas A) {
+  const EaTile it = items[blockIdx.x];
   const DFront P = F[it.parent];
   const DFront C = F[it.child];
   const int nd = C.k - C.ne;
   const int sz = C.m - C.ne;
-  const int32_t* ea = S.ea_map + S.ea_ptr[it.child];
-  const double* cp = A.panel + C.panel;
+  const int32_t* __restrict__ ea = S.ea_map + S.ea_ptr[it.child];
+  const double* __restrict__ cp = A.panel + C.panel;
+  const double* __restrict__ cb = A.cbase + (C.cb < 0 ? 0 : C.cb);
   double* pp = A.panel + P.panel;
+  double* pc = A.cbase + (P.cb < 0 ? 0 : P.cb);
+  const bool pcb = (P.flags & FF_HAS_CB) != 0;
   auto map = [&](int i) -> int {
     if (i < nd) return P.nown + C.dly_off + i;
-    int l = ea[i - nd];
+    int l = __ldg(ea + (i - nd));
     return l < P.nown ? l : l + P.ndin;
   };
-  int jend = min(it.j0 + 32, sz);
-  for (int j = it.j0; j < jend; ++j) {
-    int lj = map(j);
-    for (int i = j + threadIdx.x; i < sz; i += blockDim.x) {
-      double v;
-      if (j < nd) {
-        int64_t row = i < nd ? (C.ne + i) : (C.k + (i - nd));
-        v = cp[row + (int64_t)(C.ne + j) * C.m];
-      } else {
-        v = A.cbase[C.cb + (i - nd) + (int64_t)(j - nd) * C.nfs];
+  __shared__ int s_lj[32];
+  const int jn = min(32, sz - it.j0);
+  if (threadIdx.x < 32) s_lj[threadIdx.x] = threadIdx.x < jn ? map(it.j0 + threadIdx.x) : 0;
+  __syncthreads();
+  const int i1 = min(sz, it.i0 + EA_ROWS);
+  for (int ib = it.i0; ib < i1; ib += 256) {
+    const int i = ib + threadIdx.x;
+    if (i >= i1) break;
+    const int li = map(i);
+    // rows of the child block: delayed rows live in the child's panel rows ne.., NFS rows at k..
+    const int64_t prow = i < nd ? (int64_t)(C.ne + i) : (int64_t)(C.k + (i - nd));
+#pragma unroll 1
+    for (int jb = 0; jb < 32; jb += 8) {
+      double v[8];
+      double* dst[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int jj = jb + q, j = it.j0 + jj;
+        v[q] = 0.0;
+        if (jj < jn && i >= j) {
+          v[q] = j < nd ? cp[prow + (int64_t)(C.ne + j) * C.m] : cb[(i - nd) + (int64_t)(j - nd) * C.nfs];
+        }
       }
-      if (v == 0.0) continue;
-      int li = map(i);
-      int r = li >= lj ? li : lj, c = li >= lj ? lj : li;
-      if (c < P.k) pp[r + (int64_t)c * P.m] += v;
-      else if ((P.flags & FF_HAS_CB) && r >= P.k) A.cbase[P.cb + (r - P.k) + (int64_t)(c - P.k) * P.nfs] += v;
+      double old[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        dst[q] = nullptr;
+        if (v[q] != 0.0) {
+          const int lj = s_lj[jb + q];
+          const int r = li >= lj ? li : lj, c = li >= lj ? lj : li;
+          if (c < P.k) dst[q] = pp + r + (int64_t)c * P.m;
+          else if (pcb && r >= P.k) dst[q] = pc + (r - P.k) + (int64_t)(c - P.k) * P.nfs;
+        }
+        old[q] = dst[q] ? *dst[q] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if (dst[q]) *dst[q] = old[q] + v[q];
     }
+  }
+}
+
+// Zeros the lower triangle (rows j..nfs of column j) of the contribution
+// blocks of a wave: item = (front, first of 32 columns).  The upper
+// triangle is never read.
+struct CbZeroItem { int32_t front; int32_t j0; };
+__global__ void __launch_bounds__(256) k_zero_cb_lower(const CbZeroItem* items, const DFront* F, Arenas A) {
+  const CbZeroItem it = items[blockIdx.x];
+  const DFront f = F[it.front];
+  double* c = A.cbase + f.cb;
+  const int jend = min(f.nfs, it.j0 + 32);
+  for (int j = it.j0; j < jend; ++j) {
+    double* col = c + (int64_t)j * f.nfs;
+    for (int i = j + threadIdx.x; i < f.nfs; i += blockDim.x) col[i] = 0.0;
   }
 }
 
@@ -2011,7 +2061,6 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     if (cb_need) {
       if ((rc = cb_alloc(h, cb_need, &cb_block[w]))) return rc;
       cb_len[w] = cb_need;
-      CK(cudaMemsetAsync(h->cb_arena + cb_block[w], 0, (size_t)cb_need * 8, st));
     }
     h->host_alloc_ms += now_ms() - ta;
     {
@@ -2045,7 +2094,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       for (int64_t e = P.amap_ptr[s]; e < P.amap_ptr[s + 1]; e += 256) sitems.push_back(ScatterItem{(int32_t)s, 0, e});
     size_t maxch = 0;
     for (int64_t s : wave) maxch = std::max(maxch, P.children[s].size());
-    std::vector<std::vector<EaItem>> eitems(maxch);
+    std::vector<std::vector<EaTile>> eitems(maxch);
     for (size_t q = 0; q < maxch; ++q)
       for (int64_t s : wave) {
         if (q >= P.children[s].size()) continue;
@@ -2053,8 +2102,15 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
         const DFront& cf = h->h_fronts[c];
         if (!(cf.flags & FF_HAS_PARENT) || cf.ne >= cf.m) continue;
         int sz = cf.m - cf.ne;
-        for (int j0 = 0; j0 < sz; j0 += 32) eitems[q].push_back(EaItem{(int32_t)s, (int32_t)c, j0, 0});
+        for (int j0 = 0; j0 < sz; j0 += 32)
+          for (int i0 = j0; i0 < sz; i0 += EA_ROWS) eitems[q].push_back(EaTile{(int32_t)s, (int32_t)c, j0, i0});
       }
+    std::vector<CbZeroItem> zitems;
+    for (int64_t s : wave) {
+      const DFront& f = h->h_fronts[s];
+      if (f.flags & FF_HAS_CB)
+        for (int j0 = 0; j0 < f.nfs; j0 += 32) zitems.push_back(CbZeroItem{(int32_t)s, j0});
+    }
     std::vector<TileItem> witems, gitems;
     std::vector<int64_t> cb_syrk_fronts;
     for (int64_t s : wave) {
@@ -2071,7 +2127,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     size_t o_tpp = pk.add(tpp_ids), o_aptp = pk.add(aptp_ids), o_s = pk.add(sitems);
     std::vector<size_t> o_e(maxch);
     for (size_t q = 0; q < maxch; ++q) o_e[q] = pk.add(eitems[q]);
-    size_t o_w = pk.add(witems), o_g = pk.add(gitems);
+    size_t o_w = pk.add(witems), o_g = pk.add(gitems), o_z = pk.add(zitems);
     size_t o_cnt = pk.add(std::vector<int32_t>(3 * (size_t)nw + 4, 0));
     size_t o_q = pk.add(std::vector<int32_t>(4, 0));  // work-queue counter of the medium fronts' launch
     const bool learned = h->opt.precision == 2 && !large_ids.empty();
@@ -2100,6 +2156,9 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       k_put_dly<<<blocks_for(dly_ids.size(), 128), 128, 0, st>>>((const int32_t*)(D + o_dly_ids),
                                                                  (const int32_t*)(D + o_dly_vals), (int)dly_ids.size(),
                                                                  h->d_fronts);
+    // contribution blocks of this wave: zero lower triangles (the extend-add adds into them)
+    if (!zitems.empty())
+      k_zero_cb_lower<<<(unsigned)zitems.size(), 256, 0, st>>>((const CbZeroItem*)(D + o_z), h->d_fronts, A);
     CK(cudaEventRecord(h->ev[1], st));
     // ---- assembly
     k_front_rows<<<nw, 128, 0, st>>>(d_ids, nw, h->d_fronts, statics(h), A);
@@ -2108,8 +2167,8 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
                                                          d_vals, d_scal);
     for (size_t q = 0; q < maxch; ++q)
       if (!eitems[q].empty())
-        k_extend_add<<<(unsigned)eitems[q].size(), 256, 0, st>>>((const EaItem*)(D + o_e[q]), h->d_fronts,
-                                                                  statics(h), A);
+        k_extend_add_tiled<<<(unsigned)eitems[q].size(), 256, 0, st>>>((const EaTile*)(D + o_e[q]), h->d_fronts,
+                                                                        statics(h), A);
     CK(cudaEventRecord(h->ev[2], st));
     // contribution blocks whose parents are now all assembled
     for (size_t w2 = 0; w2 < w; ++w2)
@@ -2226,7 +2285,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     }
     h->launches += 1 + (int64_t)eitems.size() * 0 + (sitems.empty() ? 0 : 1) + (tpp_ids.empty() ? 0 : 1) +
                    (aptp_ids.empty() ? 0 : 1) + (witems.empty() ? 0 : 1) + (gitems.empty() ? 0 : 1) + 2 +
-                   (dly_ids.empty() ? 0 : 1);
+                   (dly_ids.empty() ? 0 : 1) + (zitems.empty() ? 0 : 1);
     for (size_t q = 0; q < maxch; ++q) h->launches += eitems[q].empty() ? 0 : 1;
     {
       size_t fb = 0, tb = 0;
