@@ -536,13 +536,17 @@ def run_profile_step(args, rv, torch):
         solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
     opts = rv.FactorOptions(**form)
     r = time_form(rv, torch, solver, s, b, opts, args.warmup, args.steps)
+    p0 = solver.profile()  # host counters of the last timed step (no per-launch events)
+    host = {k: p0[k] for k in ("host_total_ms", "host_sync_ms", "host_wait_ms", "lf_misses")}
     solver.set_profiling(True)
     time_form(rv, torch, solver, s, b, opts, 0, 1)
     pr = solver.profile()
     solver.close()
     print(json.dumps({"config": args.config, "form": args.profile_step, "n": s.n, "s_per_step": r["s_per_step"],
                       "bwd_err": r["bwd_err"], "inertia": r["inertia"], "solves_after_first": r["solves_after_first"],
-                      "phases_ms": {k: pr[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "host_sync_ms")},
+                      "phases_ms": {k: pr[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "host_sync_ms",
+                                                       "host_wait_ms")},
+                      "timed_step_host": host,
                       "parts_ms": pr["part_ms"]}), flush=True)
 
 
@@ -920,7 +924,8 @@ def main():
                          "launches_per_step": syrk_launch,
                          "share_of_step": (syrk_ms * 1e-3) / t_step if t_step else None},
             "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
-                                               "host_total_ms", "host_alloc_ms", "host_sync_ms")},
+                                               "host_total_ms", "host_alloc_ms", "host_sync_ms", "host_wait_ms")},
+            "lf_blocks_reissued": prof["lf_misses"],
             "parts_ms": prof["part_ms"],
             "work": work,
             "step_wall_s": walls, "step_event_s": times,

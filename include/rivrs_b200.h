@@ -235,11 +235,17 @@ typedef struct {
   int64_t factor_launches, solve_launches;
   int64_t peak_bytes;
   /* host wall time of the last factor: total, in allocation calls, waiting
-   * in stream synchronisations */
+   * in synchronisations after which the stream had nothing queued */
   double host_total_ms, host_alloc_ms, host_sync_ms;
   /* device time of the last factor by kind of work (CUDA events between
    * consecutive launches, profiling mode only), indexed by rvg_part */
   double part_ms[16];
+  /* large fronts issue their 256-column outer blocks ahead, on the guess
+   * that no column is delayed: host time spent waiting for the first of
+   * several queued blocks (the device stays busy with the rest), and the
+   * blocks issued past a delay (they return at once and are issued again) */
+  double host_wait_ms;
+  int64_t lf_misses;
 } rvg_profile;
 
 /* Indices of rvg_profile.part_ms.  Large fronts (whole GPU per front): */

@@ -46,6 +46,7 @@ struct SyrkArgs {
   // when set, the update runs only if *cond < cond_lt (decided on the device)
   const int32_t* cond;
   int32_t cond_lt;
+  const int32_t* skip;  // when set and nonzero, the launch does nothing
 };
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(NT, MINB) k_syrk_lower_t(SyrkArgs a) {
   const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
   if (i0 + BM - 1 < j0) return;  // tile entirely above the diagonal
-  if (a.cond && *a.cond >= a.cond_lt) return;
+  if ((a.cond && *a.cond >= a.cond_lt) || (a.skip && *a.skip)) return;
   const int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   extern __shared__ double gsm[];
   // stage s: W chunk [k][BM] then L chunk [k][BN]
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
   const int64_t j0 = a.c0 + (int64_t)blockIdx.x * BN;
   if (i0 >= a.r1 || j0 >= a.c1) return;
   if (i0 + BM - 1 < j0) return;
-  if (a.cond && *a.cond >= a.cond_lt) return;
+  if ((a.cond && *a.cond >= a.cond_lt) || (a.skip && *a.skip)) return;
   const int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K <= 0) return;  // nothing eliminated: C unchanged
   extern __shared__ double gsm[];

@@ -44,6 +44,10 @@ namespace rvg {
 struct LFState {
   int32_t k, end_pos, bs, bnelim, eff, nelim;
   int32_t gne, n1, n2, bne;
+  // set when an outer block was launched for another start column than the
+  // device reached (the host issues blocks ahead assuming no delays): every
+  // later launch of the front returns at once until the host clears it
+  int32_t spec_bad;
   int32_t bperm[32];
   int8_t bdt[32];
   double bdd[32], bdo[32];
@@ -67,19 +71,26 @@ struct LFArgs {
 };
 
 __global__ void k_lf_init(LFState* st, int32_t* perm, int64_t p) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) { st->gne = 0; st->n1 = 0; st->n2 = 0; }
+  if (blockIdx.x == 0 && threadIdx.x == 0) { st->gne = 0; st->n1 = 0; st->n2 = 0; st->spec_bad = 0; }
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < p; i += (int64_t)gridDim.x * blockDim.x)
     perm[i] = (int32_t)i;
 }
 
 __global__ void k_lf_begin_outer(LFArgs A) {
   LFState* st = A.st;
+  if (st->spec_bad) return;
+  if (st->gne != (int32_t)A.cs) {  // issued for a start column the factorization did not reach
+    __syncthreads();               // every thread has read gne before it is flagged
+    if (threadIdx.x == 0) st->spec_bad = 1;
+    return;
+  }
   if (threadIdx.x == 0) { st->k = 0; st->end_pos = (int32_t)A.bcols; st->bne = 0; }
   for (int i = threadIdx.x; i < A.bcols; i += blockDim.x) A.lp[i] = i;
 }
 
 // complete pivoting on the diagonal block (1 CTA)
 __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   __shared__ CtaShared sh;
   LFState* st = A.st;
   const int tid = threadIdx.x;
@@ -191,6 +202,7 @@ __device__ __forceinline__ void lf_w_row(const double* l, int64_t ld, int n, con
 // them is a compile-time constant)
 constexpr int LF_PANEL_T = 64;
 __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim;
   if (bnelim == 0) return;
@@ -286,6 +298,7 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
 // 2x2 boundary, restore of the failed diagonal part, failed x failed term,
 // D entries (1 CTA)
 __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim, bs = st->bs, k = st->k;
   const int tid = threadIdx.x;
@@ -359,6 +372,7 @@ __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
 // trailing columns that follows is the DMMA GEMM (k_syrk_dmma with the
 // region start read from the device), the same fma chain per entry.
 __global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim;
   if (bnelim == 0) return;
@@ -399,6 +413,7 @@ __global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
 
 // delayed columns of the inner block to the end of the outer block (1 CTA)
 __global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int tid = threadIdx.x;
   const int k = st->k, bs = st->bs, bnelim = st->bnelim, nelim = st->nelim;
@@ -434,6 +449,7 @@ __global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
 // 0..cs (two_level_factor, factor.rs:2165-2181): 16 columns per CTA
 constexpr int LF_PROP_COLS = 16;
 __global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   extern __shared__ double buf[];  // bcols x LF_PROP_COLS
   const int64_t c0 = (int64_t)blockIdx.x * LF_PROP_COLS;
   const int nc = (int)((A.cs - c0) < LF_PROP_COLS ? (A.cs - c0) : LF_PROP_COLS);
@@ -453,6 +469,7 @@ __global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
 // W = L D for the rows below the outer block, over its bne eliminated
 // columns, appended to the pending window
 __global__ void __launch_bounds__(128) k_lf_w(LFArgs A) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   const int bne = A.st->bne;
   const int64_t oe = A.cs + A.bcols;
   const int64_t i = oe + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -468,6 +485,7 @@ __global__ void __launch_bounds__(128) k_lf_w(LFArgs A) {
 // end of an outer block: column order, delays to the end of the remaining
 // fully-summed columns (two_level), eliminated total (1 CTA)
 __global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_level) {
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int tid = threadIdx.x;
   const int bne = st->bne;

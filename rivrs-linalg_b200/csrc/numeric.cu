@@ -33,6 +33,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <string>
@@ -1193,6 +1194,7 @@ using namespace rvg;
 // on the device and the packed window of its mixed-form updates.  Context 0
 // is the handle's own stream; the others let the large fronts of one wave run
 // side by side (one host thread each).
+constexpr int LF_AHEAD = 8;  // outer blocks of a large front issued ahead of the host's check of their start
 struct LfCtx {
   cudaStream_t st = nullptr;
   LFState* lf = nullptr;
@@ -1201,6 +1203,12 @@ struct LfCtx {
   bool marks = false;      // profiling marks (only one front in flight, on the handle's stream)
   int64_t launches = 0;
   double sync_ms = 0, syrk_flops = 0;
+  // issue-ahead of outer blocks: the device's eliminated total after each
+  // issued block lands in a pinned slot, with an event behind it
+  int32_t* h_gne = nullptr;
+  cudaEvent_t ring_ev[LF_AHEAD] = {};
+  double wait_ms = 0;     // host waits on blocks issued ahead (the stream still holds later blocks)
+  int64_t misses = 0;     // blocks issued for a start column the factorization did not reach
 };
 constexpr int LF_CONCURRENT = 8;  // large fronts of a wave in flight at once
 
@@ -1285,6 +1293,8 @@ struct rvg_handle {
   int64_t syrk_launches = 0, launches = 0, factor_launches = 0, solve_launches = 0;
   int64_t arena_bytes = 0, peak_bytes = 0;
   double host_alloc_ms = 0, host_sync_ms = 0, host_total_ms = 0;
+  double host_wait_ms = 0;  // waits on large-front blocks issued ahead (later blocks still queued)
+  int64_t lf_misses = 0;    // large-front blocks issued past a delay (returned at once, issued again)
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
   double t_assembly = 0, t_kernel = 0, t_gemm = 0, t_factor = 0, t_solve = 0, t_dom = 0, n_dom = 0;
@@ -1674,7 +1684,8 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax, bool mixed) {
 // cond set the launch only acts if *cond < cond_lt.
 int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int64_t c0, int64_t c1, int64_t wd,
                        int64_t wrow, int64_t F, const float* pk_w, const float* pk_l, int64_t kadd,
-                       const int32_t* kdev, const int32_t* cond, int32_t cond_lt, bool mixed) {
+                       const int32_t* kdev, const int32_t* cond, int32_t cond_lt, bool mixed,
+                       const int32_t* skip = nullptr) {
   cudaStream_t st = cx.st;
   if (c1 <= c0) return RVG_OK;
   int rc = syrk_ev(h, cx.marks);
@@ -1685,7 +1696,7 @@ int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int
     const int64_t ntiles = tc_count_tiles(nr, nc, c0, c0);
     const int64_t t0 = (c0 - wrow) / TC_BM;
     TcArgs ta{a.a, m, c0, m, c0, c1, pk_w + (size_t)t0 * Fq * TC_BLOCK, pk_l + (size_t)t0 * Fq * TC_BLOCK, Fq, kdev,
-              kadd, nr, nc, ntiles, h->d_err, cond, cond_lt};
+              kadd, nr, nc, ntiles, h->d_err, cond, cond_lt, 0, skip};
     launch_tc(h, st, ta);
   } else {
     SyrkArgs ga{};
@@ -1703,6 +1714,7 @@ int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int
     ga.Kdev = kdev;
     ga.cond = cond;
     ga.cond_lt = cond_lt;
+    ga.skip = skip;
     k_syrk_lower<<<syrk_grid(ga), G_T, G_SMEM, st>>>(ga);
   }
   if ((rc = syrk_ev(h, cx.marks))) return rc;
@@ -1750,11 +1762,23 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   mk(-1);
   k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
   cx.launches++;
-  int64_t rem = p, gne = 0;
-  size_t outer = 0;
   if (!h->replay) h->rec_g[s].clear();
-  while (rem > 0) {
-    const int64_t bcols = std::min(rem, nb), cs = gne, bm = m - cs, oe = cs + bcols;
+  const int32_t* skip = &a.st->spec_bad;
+  int irc = RVG_OK;  // first error of a launch helper inside issue()
+  // Host view of the loop before an outer block: start column (eliminated
+  // so far), remaining columns, the window of pending columns [wd, gne)
+  // whose W rows start at wrow, and the block's index.
+  struct HostLF { int64_t gne, rem, wd, wrow; size_t outer; };
+  // what the host decided when it issued a block
+  struct Issued { HostLF before; int64_t cs, bcols, oe, kadd, ncol; bool flush, window; int slot; };
+  // Launches one outer block for start column S.gne (2 + 6 per inner block + the outer-block steps).
+  auto issue = [&](const HostLF& S, int slot) -> Issued {
+    Issued I{};
+    I.before = S;
+    I.slot = slot;
+    const int64_t rem = S.rem, cs = S.gne, wd = S.wd, wrow = S.wrow;
+    const int64_t bcols = std::min(rem, nb), bm = m - cs, oe = cs + bcols;
+    I.cs = cs; I.bcols = bcols; I.oe = oe;
     a.cs = cs;
     a.bcols = bcols;
     k_lf_begin_outer<<<1, 256, 0, st>>>(a);
@@ -1774,6 +1798,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     gi.Kdev = &a.st->nelim;
     gi.dk = &a.st->k;
     gi.dbs = &a.st->bs;
+    gi.skip = skip;
     for (int64_t it = 0; it < ninner; ++it) {
       k_lf_block<<<1, NT, 0, st>>>(a);
       mk(RVG_PART_LF_BLOCK);
@@ -1788,8 +1813,6 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
       mk(RVG_PART_LF_DELAY);
     }
     cx.launches += 1 + 6 * ninner;
-    bool flush = false;
-    int64_t kadd = 0, ncol = 0;
     if (two_level) {
       if (cs > 0) {
         k_lf_prop<<<(unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256, (size_t)bcols * LF_PROP_COLS * 8, st>>>(a);
@@ -1797,8 +1820,10 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         mk(RVG_PART_LF_PROP);
       }
       if (oe < p) {
+        I.window = true;
         // this block's W joins the window [wd, gne + bne)
-        kadd = cs - wd;
+        const int64_t kadd = cs - wd;
+        I.kadd = kadd;
         a.wld = m - wrow;
         a.wrow0 = wrow;
         a.wcol0 = kadd;
@@ -1809,33 +1834,30 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         // rem (delayed ones parked at the end) belong to no later block.  The
         // window is applied everywhere when it is full, or when the next block
         // is the last one (so no column is left pending for the end of the front).
-        flush = kadd + bcols >= F || rem - bcols < nb;
-        ncol = nb;
+        I.flush = kadd + bcols >= F || rem - bcols < nb;
+        I.ncol = nb;
         const int32_t* bne_dev = &a.st->bne;
         if (mixed) {
           // append this block's chunks of W (rows [oe, m)) and L (rows [oe, p))
           const int64_t q0 = kadd / TC_BK, nqb = (bcols + TC_BK - 1) / TC_BK, t0 = (oe - wrow) / TC_BM;
-          PackArgs pw{a.wo + (oe - wrow), a.wld, m - oe, Fq, bne_dev, kadd, pk_w, q0, t0, nullptr, 0};
-          PackArgs pl{a.a + wd * m + oe, m, p - oe, Fq, bne_dev, kadd, pk_l, q0, t0, nullptr, 0};
+          PackArgs pw{a.wo + (oe - wrow), a.wld, m - oe, Fq, bne_dev, kadd, pk_w, q0, t0, nullptr, 0, skip};
+          PackArgs pl{a.a + wd * m + oe, m, p - oe, Fq, bne_dev, kadd, pk_l, q0, t0, nullptr, 0, skip};
           launch_pack(h, st, dim3((unsigned)nqb, blocks_for(m - oe, TC_BM)), pw);
           launch_pack(h, st, dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), pl);
           cx.launches += 2;
         }
-        int rc;
-        if (flush) {
+        if (I.flush) {
           // the window is full: every trailing column takes it (one GEMM)
-          rc = launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0, mixed);
-          if (rc) return rc;
+          irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0,
+                                               mixed, skip);
         } else {
           // near field: the next outer block's columns (oe + nb <= p here) take the whole window
-          rc = launch_window_gemm(h, cx, a, m, oe, oe + ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0, mixed);
-          if (rc) return rc;
+          irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, oe + I.ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
+                                               nullptr, 0, mixed, skip);
           // far field: only if this block delayed columns (decided on the device)
-          if (oe + nb < p) {
-            rc = launch_window_gemm(h, cx, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, bne_dev,
-                                    (int32_t)bcols, mixed);
-            if (rc) return rc;
-          }
+          if (oe + nb < p)
+            irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
+                                                 bne_dev, (int32_t)bcols, mixed, skip);
         }
         mk(RVG_PART_LF_SYRK);
       }
@@ -1843,40 +1865,110 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level);
     cx.launches++;
     mk(RVG_PART_LF_OUTER);
-    CK(cudaGetLastError());
-    int32_t g = 0;
-    if (h->replay) {  // the progress of the recorded factorization, checked on the device
-      const std::vector<int32_t>& rg = h->rec_g[s];
-      if (outer >= rg.size()) { set_error("refactorization replay: record too short"); return RVG_ERR_DEVICE; }
-      g = rg[outer];
-      k_check_gne<<<1, 32, 0, st>>>(a.st, g, h->d_mismatch);
-    } else {
-      CK(cudaMemcpyAsync(&g, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
-      double ts0 = now_ms();
-      CK(cudaStreamSynchronize(st));
-      cx.sync_ms += now_ms() - ts0;
-      h->rec_g[s].push_back(g);
-    }
-    ++outer;
-    if (cx.marks) mark_flush(h);
-    mk(-1);
-    const int64_t bne = g - gne;
-    if (two_level && oe < p) {
-      const bool delayed = bne < bcols;
-      const double K = (double)(kadd + bne);
-      if (flush) {
-        cx.syrk_flops += 2.0 * K * lower_entries(oe, m, oe, p);
+    return I;
+  };
+  // The state after block I once the device's eliminated total g is known.
+  auto after = [&](const Issued& I, int32_t g) -> HostLF {
+    HostLF S = I.before;
+    const int64_t bne = g - I.cs;
+    if (two_level && I.window) {
+      const bool delayed = bne < I.bcols;
+      const double K = (double)(I.kadd + bne);
+      if (I.flush) {
+        cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, p);
       } else {
-        cx.syrk_flops += 2.0 * K * lower_entries(oe, m, oe, oe + ncol);
-        if (oe + nb < p && delayed) cx.syrk_flops += 2.0 * K * lower_entries(oe + nb, m, oe + nb, p);
+        cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, I.oe + I.ncol);
+        if (I.oe + nb < p && delayed) cx.syrk_flops += 2.0 * K * lower_entries(I.oe + nb, m, I.oe + nb, p);
       }
-      if (flush || delayed) {  // every column is up to date: a new, empty window
-        wd = g;
-        wrow = g + std::min(rem - bcols, nb);
+      if (I.flush || delayed) {  // every column is up to date: a new, empty window
+        S.wd = g;
+        S.wrow = g + std::min(S.rem - I.bcols, nb);
       }
     }
-    gne = g;
-    rem -= bcols;
+    S.gne = g;
+    S.rem -= I.bcols;
+    S.outer += 1;
+    return S;
+  };
+  HostLF S{0, p, 0, std::min(p, nb), 0};
+  if (h->replay) {
+    // the progress of the recorded factorization, checked on the device
+    const std::vector<int32_t>& rg = h->rec_g[s];
+    while (S.rem > 0) {
+      Issued I = issue(S, 0);
+      if (irc) return irc;
+      if (S.outer >= rg.size()) { set_error("refactorization replay: record too short"); return RVG_ERR_DEVICE; }
+      const int32_t g = rg[S.outer];
+      k_check_gne<<<1, 32, 0, st>>>(a.st, g, h->d_mismatch);
+      CK(cudaGetLastError());
+      S = after(I, g);
+    }
+  } else {
+    // Blocks go out ahead on the guess that none delays a column (the next
+    // start column is then this one plus its width); the device checks each
+    // guess when the block begins (k_lf_begin_outer), and a wrong one turns
+    // every later launch of the front into a no-op.  The host reads the
+    // device's eliminated total after each block in issue order, at most
+    // LF_AHEAD blocks behind; at the first one that differs it waits for the
+    // stream, clears the flag and issues again from the true start column.
+    if (!cx.h_gne) {
+      if (tl_no_alloc) return no_alloc_fail();
+      CK(cudaHostAlloc((void**)&cx.h_gne, LF_AHEAD * sizeof(int32_t), cudaHostAllocDefault));
+      for (int i = 0; i < LF_AHEAD; ++i) CK(cudaEventCreateWithFlags(&cx.ring_ev[i], cudaEventDisableTiming));
+    }
+    std::deque<Issued> q;
+    int next_slot = 0;
+    // with the profiling marks on, one block at a time: the marks are read back after each block
+    const int ahead = cx.marks ? 1 : LF_AHEAD;
+    while (S.rem > 0 || !q.empty()) {
+      if (S.rem > 0 && (int)q.size() < ahead) {
+        const int slot = next_slot;
+        next_slot = (next_slot + 1) % LF_AHEAD;
+        Issued I = issue(S, slot);
+        if (irc) return irc;
+        CK(cudaMemcpyAsync(cx.h_gne + slot, &a.st->gne, 4, cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(cx.ring_ev[slot], st));
+        CK(cudaGetLastError());
+        q.push_back(I);
+        // the guess: no delayed column in this block
+        HostLF G = I.before;
+        if (two_level && I.window && I.flush) {
+          G.wd = I.cs + I.bcols;
+          G.wrow = G.wd + std::min(G.rem - I.bcols, nb);
+        }
+        G.gne = I.cs + I.bcols;
+        G.rem -= I.bcols;
+        G.outer += 1;
+        S = G;
+        continue;
+      }
+      const Issued I = q.front();
+      q.pop_front();
+      const double t0 = now_ms();
+      CK(cudaEventSynchronize(cx.ring_ev[I.slot]));
+      const double waited = now_ms() - t0;
+      const int32_t g = cx.h_gne[I.slot];
+      h->rec_g[s].push_back(g);
+      if (cx.marks) {
+        mark_flush(h);
+        mk(-1);
+      }
+      const HostLF T = after(I, g);
+      if (g == I.cs + I.bcols) {
+        // as guessed; while later blocks are queued the wait overlaps their work
+        if (q.empty()) cx.sync_ms += waited; else cx.wait_ms += waited;
+        continue;
+      }
+      // a block delayed columns: the blocks issued after it did nothing
+      cx.sync_ms += waited;
+      const double t1 = now_ms();
+      CK(cudaStreamSynchronize(st));
+      cx.sync_ms += now_ms() - t1;
+      cx.misses += (int64_t)q.size();
+      q.clear();
+      CK(cudaMemsetAsync(&a.st->spec_bad, 0, sizeof(int32_t), st));
+      S = T;
+    }
   }
   k_lf_finish<<<1, 32, 0, st>>>(a, h->d_fronts, s);
   cx.launches++;
@@ -1899,8 +1991,10 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
   auto fold = [&](LfCtx& c) {
     h->launches += c.launches;
     h->host_sync_ms += c.sync_ms;
+    h->host_wait_ms += c.wait_ms;
+    h->lf_misses += c.misses;
     h->syrk_flops += c.syrk_flops;
-    c.launches = 0; c.sync_ms = 0; c.syrk_flops = 0;
+    c.launches = 0; c.sync_ms = 0; c.syrk_flops = 0; c.wait_ms = 0; c.misses = 0;
   };
   // (a capture forks into the same contexts with the fronts dealt the same way:
   // the replayed graph runs them concurrently on the buffers the dynamic run sized)
@@ -1983,6 +2077,8 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   const double t_start = now_ms();
   h->host_alloc_ms = 0;
   h->host_sync_ms = 0;
+  h->host_wait_ms = 0;
+  h->lf_misses = 0;
   h->ev_used = 0;
   h->mk_used = 0;
   for (double& v : h->part_ms) v = 0;
@@ -2572,6 +2668,8 @@ static int replay_factor(rvg_handle* h, const double* ds, bool* done) {
   }
   h->factor_launches = 1;
   h->host_sync_ms = 0;
+  h->host_wait_ms = 0;
+  h->lf_misses = 0;
   *done = true;
   return RVG_OK;
 }
@@ -3309,6 +3407,8 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
   o->host_alloc_ms = h->host_alloc_ms;
   o->host_sync_ms = h->host_sync_ms;
   for (int i = 0; i < RVG_PARTS; ++i) o->part_ms[i] = h->part_ms[i];
+  o->host_wait_ms = h->host_wait_ms;
+  o->lf_misses = h->lf_misses;
   return RVG_OK;
 }
 
@@ -3447,8 +3547,11 @@ void rvg_destroy(rvg_handle* h) {
   if (h->d_nonfinite) cudaFree(h->d_nonfinite);
   if (h->d_mismatch) cudaFree(h->d_mismatch);
   if (h->h_stage_all) cudaFreeHost(h->h_stage_all);
-  for (size_t t = 1; t < h->lfx.size(); ++t) {
+  for (size_t t = 0; t < h->lfx.size(); ++t) {
     LfCtx& c = h->lfx[t];
+    if (c.h_gne) cudaFreeHost(c.h_gne);
+    for (auto& e : c.ring_ev) if (e) cudaEventDestroy(e);
+    if (t == 0) continue;  // the handle's own stream, state and window buffer
     fr(c.wpack);
     if (c.lf) cudaFree(c.lf);
     if (c.own && c.st) { cudaStreamSynchronize(c.st); cudaStreamDestroy(c.st); }

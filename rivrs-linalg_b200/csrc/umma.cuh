@@ -103,6 +103,7 @@ struct TcArgs {
   const int32_t* cond;  // when set, the update runs only if *cond < cond_lt
   int32_t cond_lt;
   int32_t stall;        // self-test of the bounded waits: the producer issues no copies
+  const int32_t* skip;  // when set and nonzero, the launch does nothing
 };
 
 struct PackArgs {
@@ -114,6 +115,7 @@ struct PackArgs {
   int64_t q0, t0;   // first chunk packed (blockIdx.x = q - q0), first tile
   const int32_t* cond;  // when set, packs only if *cond < cond_lt
   int32_t cond_lt;
+  const int32_t* skip;  // when set and nonzero, the launch does nothing
 };
 
 // ---------------------------------------------------------------- PTX helpers
@@ -231,7 +233,7 @@ __device__ __forceinline__ void split_tf32_exact(double x, float& hi, float& lo)
 
 // grid (Q chunks, tiles), 256 threads; thread item = one row x 4 consecutive k
 __global__ void __launch_bounds__(256) k_pack_tf32x3(PackArgs a) {
-  if (a.cond && *a.cond >= a.cond_lt) return;
+  if ((a.cond && *a.cond >= a.cond_lt) || (a.skip && *a.skip)) return;
   int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the chunks the buffer holds
   const int64_t q = a.q0 + blockIdx.x, t = blockIdx.y;
@@ -266,7 +268,7 @@ __device__ __forceinline__ float bf16_to_f32(uint16_t h) { return __uint_as_floa
 // BF16 parts: hi = bf16(x), lo = bf16(x - hi); grid (Q chunks, tiles), 256
 // threads; thread item = one row x 8 consecutive k (one 16-byte core-matrix row)
 __global__ void __launch_bounds__(256) k_pack_bf16x3(PackArgs a) {
-  if (a.cond && *a.cond >= a.cond_lt) return;
+  if ((a.cond && *a.cond >= a.cond_lt) || (a.skip && *a.skip)) return;
   int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;
   const int64_t q = a.q0 + blockIdx.x, t = blockIdx.y;
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc(TcArgs a) {
   __shared__ uint32_t tslot;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (a.cond && *a.cond >= a.cond_lt) return;  // uniform over the CTA
+  if ((a.cond && *a.cond >= a.cond_lt) || (a.skip && *a.skip)) return;  // uniform over the CTA
   int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the packed chunks
   if (K <= 0) return;  // nothing eliminated: C unchanged (uniform over the CTA)
@@ -569,7 +571,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_syrk_tc_pair(TcArgs a) {
   __shared__ uint32_t tslot;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (a.cond && *a.cond >= a.cond_lt) return;  // uniform over the CTA
+  if ((a.cond && *a.cond >= a.cond_lt) || (a.skip && *a.skip)) return;  // uniform over the CTA
   int64_t K = (a.Kdev ? (int64_t)*a.Kdev : 0) + a.K;
   if (K > a.Q * TC_BK) K = a.Q * TC_BK;  // never beyond the packed chunks
   if (K <= 0) return;
