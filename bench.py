@@ -522,6 +522,95 @@ def run_learned(args, rv, torch):
     print(json.dumps(line), flush=True)
 
 
+def form_dtype(opts):
+    """The arithmetic a form computes in (not a precision claim: every form
+    reaches the same 1e-14 backward error)."""
+    if opts.precision == "fp64":
+        return "f64"
+    parts = "bf16x3" if opts.mixed_operands == "bf16" else "tf32x3"
+    lead = "learned per front: f64 or " if opts.precision == "learned" else ""
+    return f"{lead}{parts} Schur products, fp32 accumulation (fp64 sums), fp64 pivoting/storage/solve, fp64 refinement"
+
+
+def side_config(rv, torch, name, s, b, warmup, steps, selector=None, bf16_opts=None):
+    """A further configuration on the same line: plain FP64, the BF16 mixed
+    form and the learned form, each factor + solve to 1e-14 with inputs in
+    HBM (W warm-up, K timed steps); the fastest accurate one is its value.
+    One extra profiled step of that form gives its Schur-GEMM rate."""
+    t0 = time.perf_counter()
+    solver, an_ms = analyze(rv, s)
+    if selector is not None:
+        solver.set_selector(selector)
+    forms = {"plain_fp64": rv.FactorOptions(precision="fp64"),
+             "mixed_bf16_flush0": bf16_opts or rv.FactorOptions(precision="mixed", mixed_flush=0,
+                                                                  mixed_operands="bf16")}
+    if selector is not None:
+        forms["learned_bf16_flush0"] = rv.FactorOptions(precision="learned", mixed_flush=0, mixed_operands="bf16")
+    res = {}
+    for k, o in forms.items():
+        r = time_form(rv, torch, solver, s, b, o, warmup, steps)
+        res[k] = {"s_per_step": r["s_per_step"], "bwd_err": r["bwd_err"], "inertia": r["inertia"],
+                  "solves_after_first": r["solves_after_first"], "methods": r["methods"]}
+        if "selector" in r:
+            res[k]["selector"] = r["selector"]
+    ok = [k for k in res if res[k]["bwd_err"] <= 1e-14] or ["plain_fp64"]
+    chosen = min(ok, key=lambda k: res[k]["s_per_step"])
+    solver._ensure_handle(forms[chosen])
+    solver.set_profiling(True)
+    time_form(rv, torch, solver, s, b, forms[chosen], 0, 1)
+    pr = solver.profile()
+    solver.set_profiling(False)
+    work = solver.work()
+    solver.close()
+    torch.cuda.empty_cache()
+    c = res[chosen]
+    gemm = None
+    if pr["syrk_ms"] > 0:
+        gemm = {"tflops_fp64_equiv": pr["syrk_flops"] / (pr["syrk_ms"] * 1e-3) / 1e12,
+                "share_of_step": pr["syrk_ms"] * 1e-3 / c["s_per_step"], "launches": pr["syrk_launches"]}
+    return {"workload": name, "n": s.n, "value": c["s_per_step"], "unit": "s", "chosen_form": chosen,
+            "dtype": form_dtype(forms[chosen]), "bwd_err": c["bwd_err"], "inertia": c["inertia"],
+            "inertia_expected": list(s.inertia), "inertia_exact": list(c["inertia"]) == list(s.inertia),
+            "speedup_vs_plain_fp64": res["plain_fp64"]["s_per_step"] / c["s_per_step"],
+            "forms": res, "schur_gemm": gemm, "factor_gflops": work["flops_factor"] / c["s_per_step"] / 1e9,
+            "solve_gbs_per_rhs": None, "analyze_ms": an_ms, "wall_s": time.perf_counter() - t0,
+            "steps": steps, "warmup": warmup}
+
+
+def batch_subset(rv, torch, count, warmup, steps):
+    """The first `count` systems of the many-systems workload (64 systems, n
+    log-uniform in [5e3, 2e5] from seed 1, 1-32 RHS each), plain FP64, end
+    to end through BatchLDLT.factor_solve (values and right-hand sides from
+    host memory, solutions back): a bounded part of that workload."""
+    fam = rv.problems.batch_family(count=64, seed=1)[:count]
+    systems, nrhs = [f[0] for f in fam], [f[1] for f in fam]
+    rhs = [rv.problems.rhs_normal(sy.n, 100 + i, r) for i, (sy, r) in enumerate(zip(systems, nrhs))]
+    bl = rv.BatchLDLT(systems)
+    opts = rv.FactorOptions(precision="fp64")
+    for _ in range(warmup):
+        bl.factor_solve(None, rhs, opts)
+    times = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xs = bl.factor_solve(None, rhs, opts)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+    errs = []
+    for sy, bb, xx in zip(systems, rhs, xs):
+        bb2 = bb if bb.ndim == 2 else bb[:, None]
+        xx2 = xx if xx.ndim == 2 else xx[:, None]
+        errs.append(max(rv.problems.backward_error(sy, xx2[:, j], bb2[:, j]) for j in range(bb2.shape[1])))
+    inert_ok = bl.inertias() == [sy.inertia for sy in systems]
+    flops = sum(dense_flops(g.solver.symbolic) for g in bl.groups)
+    bl.close()
+    torch.cuda.empty_cache()
+    return {"workload": f"first {count} of the 64-system batch (n {min(sy.n for sy in systems)}-"
+                        f"{max(sy.n for sy in systems)}, {sum(nrhs)} right-hand sides), plain FP64, end to end",
+            "value": statistics.mean(times), "unit": "s", "bwd_err_max": max(errs), "inertia_exact": inert_ok,
+            "factor_gflops": flops / statistics.mean(times) / 1e9, "steps": steps, "warmup": warmup}
+
+
 def run_profile_step(args, rv, torch):
     """One form on one system, W warm-up and K timed steps (factor + solve to
     1e-14 with inputs in HBM), then one step with the library's per-launch
@@ -537,7 +626,7 @@ def run_profile_step(args, rv, torch):
     opts = rv.FactorOptions(**form)
     r = time_form(rv, torch, solver, s, b, opts, args.warmup, args.steps)
     p0 = solver.profile()  # host counters of the last timed step (no per-launch events)
-    host = {k: p0[k] for k in ("host_total_ms", "host_sync_ms", "host_wait_ms", "lf_misses")}
+    host = {k: p0[k] for k in ("host_total_ms", "host_sync_ms", "host_wait_ms", "host_gap_ms", "lf_misses")}
     solver.set_profiling(True)
     time_form(rv, torch, solver, s, b, opts, 0, 1)
     pr = solver.profile()
@@ -611,6 +700,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-precision form")
+    ap.add_argument("--no-side", action="store_true",
+                    help="default workload only: skip the C1, C4 Laplacian and C3-subset measurements")
     ap.add_argument("--train-count", type=int, default=200, help="learned config: generated training matrices")
     ap.add_argument("--mixed-flush", default="4,0",
                     help="comma list of mixed-form flush depths to time (32-deep K chunks per FP32 partial sum; 0 = all K)")
@@ -880,7 +971,8 @@ def main():
         line = {
             "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no public suite)",
+            "vs_baseline": None, "dtype": form_dtype(chosen["opts"]),
+            "data": "synthetic (seeded generator, no public suite)",
             "config": {"workload": CONFIGS[args.config][2],
                        "form": (f"{chosen_key}: " + (("Schur updates on tcgen05 tensor cores (FP64 operands split "
                                 "into %s hi+lo, FP32 accumulation added in FP64), FP64 pivoting/storage; FP64 "
@@ -924,7 +1016,8 @@ def main():
                          "launches_per_step": syrk_launch,
                          "share_of_step": (syrk_ms * 1e-3) / t_step if t_step else None},
             "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
-                                               "host_total_ms", "host_alloc_ms", "host_sync_ms", "host_wait_ms")},
+                                               "host_total_ms", "host_alloc_ms", "host_sync_ms", "host_wait_ms",
+                                               "host_gap_ms")},
             "lf_blocks_reissued": prof["lf_misses"],
             "parts_ms": prof["part_ms"],
             "work": work,
@@ -933,8 +1026,29 @@ def main():
             "clocks": clk,
             "cpu_baseline": cb,
         }
-        print(json.dumps(line), flush=True)
     solver.close()
+    del d_vals, d_b, d_x, d_scal
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and args.config == "kkt60" and not args.no_side:
+        # the other configurations, each with its own measured value, accuracy and inertia
+        sel = rv.PrecisionSelector.load(SELECTOR) if os.path.exists(SELECTOR) else None
+        k = max(1, min(args.steps, 3))
+        side = {}
+        s1, b1 = build_system(rv, "lap16")
+        side["C1_laplace16"] = side_config(rv, torch, CONFIGS["lap16"][2], s1, b1, 3, k, sel)
+        s4, b4 = build_system(rv, "lap100")
+        side["C4_laplace100"] = side_config(rv, torch, CONFIGS["lap100"][2], s4, b4, 3, k, sel)
+        del s4, b4
+        side["C3_first8"] = batch_subset(rv, torch, 8, 1, k)
+        side["C4_kkt80"] = {"unavailable": "KKT on an 80^3 27-point H (n = 640,000): its symbolic factor holds "
+                                           "98 GB of L (lower triangles), 76 GB of it in one dense root front of "
+                                           "order 137,520, and the root's three children hand it contribution "
+                                           "blocks of order 126,472, 92,341 and 91,034 (64 + 34 + 33 GB, lower "
+                                           "triangles): 229 GB together, and 151 GB for the root alone in this "
+                                           "build's full m x k front panels: beyond one B200's 180 GB"}
+        line["configs"] = side
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 

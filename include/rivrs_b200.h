@@ -235,7 +235,7 @@ typedef struct {
   int64_t factor_launches, solve_launches;
   int64_t peak_bytes;
   /* host wall time of the last factor: total, in allocation calls, waiting
-   * in synchronisations after which the stream had nothing queued */
+   * at wave boundaries and after a large-front block issued past a delay */
   double host_total_ms, host_alloc_ms, host_sync_ms;
   /* device time of the last factor by kind of work (CUDA events between
    * consecutive launches, profiling mode only), indexed by rvg_part */
@@ -246,6 +246,10 @@ typedef struct {
    * blocks issued past a delay (they return at once and are issued again) */
   double host_wait_ms;
   int64_t lf_misses;
+  /* host time from a wave's synchronisation (the eliminated counts size the
+   * next wave's fronts) to the next wave's first launch: the device has
+   * nothing of this factorization queued meanwhile */
+  double host_gap_ms;
 } rvg_profile;
 
 /* Indices of rvg_profile.part_ms.  Large fronts (whole GPU per front): */

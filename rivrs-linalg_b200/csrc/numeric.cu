@@ -1294,6 +1294,7 @@ struct rvg_handle {
   int64_t arena_bytes = 0, peak_bytes = 0;
   double host_alloc_ms = 0, host_sync_ms = 0, host_total_ms = 0;
   double host_wait_ms = 0;  // waits on large-front blocks issued ahead (later blocks still queued)
+  double host_gap_ms = 0;   // host time between a wave's synchronisation and the next wave's first launch
   int64_t lf_misses = 0;    // large-front blocks issued past a delay (returned at once, issued again)
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
@@ -1954,13 +1955,11 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         mk(-1);
       }
       const HostLF T = after(I, g);
-      if (g == I.cs + I.bcols) {
-        // as guessed; while later blocks are queued the wait overlaps their work
-        if (q.empty()) cx.sync_ms += waited; else cx.wait_ms += waited;
-        continue;
-      }
-      // a block delayed columns: the blocks issued after it did nothing
-      cx.sync_ms += waited;
+      // the device worked on this and the queued blocks meanwhile
+      cx.wait_ms += waited;
+      if (g == I.cs + I.bcols) continue;  // as guessed
+      // a block delayed columns: the blocks issued after it did nothing; the
+      // stream runs dry while the host issues them again
       const double t1 = now_ms();
       CK(cudaStreamSynchronize(st));
       cx.sync_ms += now_ms() - t1;
@@ -2078,6 +2077,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   h->host_alloc_ms = 0;
   h->host_sync_ms = 0;
   h->host_wait_ms = 0;
+  h->host_gap_ms = 0;
   h->lf_misses = 0;
   h->ev_used = 0;
   h->mk_used = 0;
@@ -2102,6 +2102,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     h->rec_stage.assign(P.waves.size(), 0);
   }
   CK(cudaEventRecord(h->ev[0], st));
+  double t_ret = -1;  // host time the last wave synchronisation returned, until the next wave's first launch
   for (size_t w = 0; w < P.waves.size(); ++w) {
     const std::vector<int64_t>& wave = P.waves[w];
     const int nw = (int)wave.size();
@@ -2149,6 +2150,10 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       }
     }
     double ta = now_ms();
+    if (t_ret >= 0) {  // the stream has been empty since the last wave's synchronisation returned
+      h->host_gap_ms += ta - t_ret;
+      t_ret = -1;
+    }
     if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st))) return rc;
     if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx_used + idx_need), st))) return rc;
     if ((rc = ensure_d_arrays(h, (size_t)(d_used + d_need)))) return rc;
@@ -2363,7 +2368,8 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     {
       double ts0 = now_ms();
       CK(cudaStreamSynchronize(st));
-      h->host_sync_ms += now_ms() - ts0;
+      t_ret = now_ms();
+      h->host_sync_ms += t_ret - ts0;
     }
     mark_flush(h);
     if (h->h_counts[3 * nw]) {
@@ -2669,6 +2675,7 @@ static int replay_factor(rvg_handle* h, const double* ds, bool* done) {
   h->factor_launches = 1;
   h->host_sync_ms = 0;
   h->host_wait_ms = 0;
+  h->host_gap_ms = 0;
   h->lf_misses = 0;
   *done = true;
   return RVG_OK;
@@ -3409,6 +3416,7 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
   for (int i = 0; i < RVG_PARTS; ++i) o->part_ms[i] = h->part_ms[i];
   o->host_wait_ms = h->host_wait_ms;
   o->lf_misses = h->lf_misses;
+  o->host_gap_ms = h->host_gap_ms;
   return RVG_OK;
 }
 

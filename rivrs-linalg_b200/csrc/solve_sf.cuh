@@ -162,20 +162,24 @@ __global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Aren
 #pragma unroll
       for (int r = 0; r < R; ++r) acc[r] = 0.0;
     }
+    // The factor is final: the L strips are read before the waits on the
+    // blocks they multiply, so only the y values are on the chain.
+    const int nr = (int)(r1 - r0);
+    if (diag && row) sf_load_strip(L + i + r0 * m, m, nr, &Ls[t][0]);  // the diagonal block, staged early
     const int ncb = diag ? b : sf.nbd;
     for (int cb = 0; cb < ncb; ++cb) {
-      if (t == 0) sf_wait(&flags[cb], w.err);
-      __syncthreads();
       const int64_t c0 = (int64_t)cb * SF_B;
       const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
+      double lr[SF_B];
+      if (row) sf_load_strip(L + i + c0 * m, m, nc, lr);
+      if (t == 0) sf_wait(&flags[cb], w.err);
+      __syncthreads();
       if (t < nc) {
 #pragma unroll
         for (int r = 0; r < R; ++r) yb[r][t] = __ldcg(&v[r * m + c0 + t]);
       }
       __syncthreads();
       if (row) {
-        double lr[SF_B];
-        sf_load_strip(L + i + c0 * m, m, nc, lr);
 #pragma unroll
         for (int c = 0; c < SF_B; ++c)
           if (c < nc) {
@@ -187,9 +191,7 @@ __global__ void __launch_bounds__(SF_B) k_sf_fwd(SfWave w, const DFront* F, Aren
     }
     if (diag) {
       // unit lower solve of rows [r0, r1) by warp 0 (lane: rows r0 + lane, r0 + 32 + lane),
-      // the diagonal block staged in shared memory first
-      const int nr = (int)(r1 - r0);
-      if (row) sf_load_strip(L + i + r0 * m, m, nr, &Ls[t][0]);
+      // on the diagonal block staged in shared memory above
 #pragma unroll
       for (int r = 0; r < R; ++r) yb[r][t] = acc[r];
       __syncthreads();
@@ -240,6 +242,7 @@ template <int R>
 __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Arenas A) {
   __shared__ int s_blk;
   __shared__ double Ls[SF_B][SF_B + 1];
+  __shared__ double Ld[SF_B][SF_B + 1];  // a column block's diagonal block, staged before its waits
   __shared__ double xs[R][SF_B];
   const int t = threadIdx.x;
   for (;;) {
@@ -314,6 +317,7 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
     const int64_t c0 = (int64_t)b * SF_B;
     const int nc = (int)((c0 + SF_B < ne ? c0 + SF_B : ne) - c0);
     const bool col = t < nc;
+    if (col) sf_load_strip(L + (c0 + t) + c0 * m, m, nc, &Ld[t][0]);  // Ld[row][col]; the factor is final
     double acc[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r] = col ? sf_dinv(fr, A, y + r * m, c0 + t) : 0.0;
@@ -329,14 +333,17 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
     // rows of later diagonal blocks, from the last one down, as they finish
     const int cb0 = nbr + npart;  // flag of column block q' at flags[cb0 + q']
     for (int rblk = sf.nbd - 1; rblk > b; --rblk) {
-      if (t == 0) sf_wait(&flags[cb0 + (sf.nbd - 1 - rblk)], w.err);
       const int64_t i0 = (int64_t)rblk * SF_B;
       const int nr = (int)((i0 + SF_B < ne ? i0 + SF_B : ne) - i0);
+      double lr[SF_B];  // the strip, read before the wait on its block
+      if (t < nr) sf_load_strip(L + i0 + t + c0 * m, m, nc, lr);
+      if (t == 0) sf_wait(&flags[cb0 + (sf.nbd - 1 - rblk)], w.err);
       __syncthreads();
       if (t < nr) {
 #pragma unroll
         for (int r = 0; r < R; ++r) xs[r][t] = __ldcg(&xf[r * m + i0 + t]);
-        sf_load_strip(L + i0 + t + c0 * m, m, nc, &Ls[t][0]);
+#pragma unroll
+        for (int c = 0; c < SF_B; ++c) Ls[t][c] = lr[c];
       }
       __syncthreads();
       if (col)
@@ -348,7 +355,6 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
     }
     // the diagonal block: x_c = acc_c - sum_{c < i < c0 + nc} L(i, c) x_i, from the bottom
     __syncthreads();
-    if (t < nc) sf_load_strip(L + (c0 + t) + c0 * m, m, nc, &Ls[t][0]);  // Ls[row][col]
 #pragma unroll
     for (int r = 0; r < R; ++r) xs[r][t] = acc[r];
     __syncthreads();
@@ -358,8 +364,8 @@ __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Aren
         double a0 = xs[r][t], a1 = xs[r][t + 32];
         for (int j = nc - 1; j >= 0; --j) {
           const double xj = __shfl_sync(0xffffffffu, j < 32 ? a0 : a1, j & 31);
-          if (t < j) a0 = __fma_rn(-Ls[j][t], xj, a0);
-          if (t + 32 < j) a1 = __fma_rn(-Ls[j][t + 32], xj, a1);
+          if (t < j) a0 = __fma_rn(-Ld[j][t], xj, a0);
+          if (t + 32 < j) a1 = __fma_rn(-Ld[j][t + 32], xj, a1);
         }
         if (t < nc) {
           xf[r * m + c0 + t] = a0;
