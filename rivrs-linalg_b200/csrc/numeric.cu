@@ -1295,6 +1295,7 @@ struct rvg_handle {
   double host_alloc_ms = 0, host_sync_ms = 0, host_total_ms = 0;
   double host_wait_ms = 0;  // waits on large-front blocks issued ahead (later blocks still queued)
   double host_gap_ms = 0;   // host time between a wave's synchronisation and the next wave's first launch
+  bool sf_attr = false;     // the backward solve kernels' shared-memory limit raised
   int64_t lf_misses = 0;    // large-front blocks issued past a delay (returned at once, issued again)
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
@@ -2858,13 +2859,20 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
       default: k_sf_fwd<1><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
     }
   };
+  if (!h->sf_attr) {  // the backward kernels' static + dynamic shared memory exceeds the default 48 KB
+    CK(cudaFuncSetAttribute(k_sf_bwd<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, SF_BWD_DYN));
+    CK(cudaFuncSetAttribute(k_sf_bwd<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, SF_BWD_DYN));
+    CK(cudaFuncSetAttribute(k_sf_bwd<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, SF_BWD_DYN));
+    CK(cudaFuncSetAttribute(k_sf_bwd<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, SF_BWD_DYN));
+    h->sf_attr = true;
+  }
   auto bwd = [&](int r, size_t w, const SfWave& sw) {
     const unsigned g = (unsigned)std::min<int64_t>(nbb[w], 6LL * h->nsm);
     switch (r) {
-      case 8: k_sf_bwd<8><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
-      case 4: k_sf_bwd<4><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
-      case 2: k_sf_bwd<2><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
-      default: k_sf_bwd<1><<<g, SF_B, 0, st>>>(sw, h->d_fronts, A); break;
+      case 8: k_sf_bwd<8><<<g, SF_B, SF_BWD_DYN, st>>>(sw, h->d_fronts, A); break;
+      case 4: k_sf_bwd<4><<<g, SF_B, SF_BWD_DYN, st>>>(sw, h->d_fronts, A); break;
+      case 2: k_sf_bwd<2><<<g, SF_B, SF_BWD_DYN, st>>>(sw, h->d_fronts, A); break;
+      default: k_sf_bwd<1><<<g, SF_B, SF_BWD_DYN, st>>>(sw, h->d_fronts, A); break;
     }
   };
   for (int64_t rh = 0; rh < nrhs;) {

@@ -47,6 +47,7 @@ constexpr uint64_t SF_TIMEOUT_NS = 1000000000ull;   // 1 s per wait
 
 // one front of a wave: its first ticket and its block counts
 constexpr int SF_PG = 8;  // backward: L21 row blocks per partial-sum ticket (512 rows)
+constexpr int SF_BWD_DYN = SF_B * (SF_B + 1) * 8;  // k_sf_bwd's dynamic shared memory
 
 struct SfFront {
   int32_t s;      // supernode
@@ -242,7 +243,9 @@ template <int R>
 __global__ void __launch_bounds__(SF_B) k_sf_bwd(SfWave w, const DFront* F, Arenas A) {
   __shared__ int s_blk;
   __shared__ double Ls[SF_B][SF_B + 1];
-  __shared__ double Ld[SF_B][SF_B + 1];  // a column block's diagonal block, staged before its waits
+  // a column block's diagonal block, staged before its waits (dynamic shared memory: SF_BWD_DYN bytes)
+  extern __shared__ double sf_dyn[];
+  double(*Ld)[SF_B + 1] = reinterpret_cast<double(*)[SF_B + 1]>(sf_dyn);
   __shared__ double xs[R][SF_B];
   const int t = threadIdx.x;
   for (;;) {
