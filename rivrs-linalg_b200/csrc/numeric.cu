@@ -2291,12 +2291,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       CK(cudaGetLastError());
       if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(std::max(3 * nw + 4, nl)) * 4))) return rc;
       CK(cudaMemcpyAsync(h->h_counts, d_rt, (size_t)nl * 4, cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      for (int i = 0; i < nl; ++i) {
-        h->route[large_ids[i]] = (int8_t)(h->h_counts[i] != 0);
-        h->sel_routed += h->h_counts[i] != 0;
-      }
-      h->sel_large.insert(h->sel_large.end(), large_ids.begin(), large_ids.end());
+      CK(cudaEventRecord(h->ev[6], st));  // read below, once the wave's small and medium fronts are queued
       h->launches += 3;
     }
     // ---- dense factorization
@@ -2317,6 +2312,17 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
                                                                         (int32_t*)(D + o_q), h->d_fronts, A, dop);
     }
     mark(h, RVG_PART_APTP);
+    if (learned) {  // the routes of the large fronts (the device is busy with the fronts queued above)
+      const int nl = (int)large_ids.size();
+      const double ts0 = now_ms();
+      CK(cudaEventSynchronize(h->ev[6]));
+      h->host_wait_ms += now_ms() - ts0;
+      for (int i = 0; i < nl; ++i) {
+        h->route[large_ids[i]] = (int8_t)(h->h_counts[i] != 0);
+        h->sel_routed += h->h_counts[i] != 0;
+      }
+      h->sel_large.insert(h->sel_large.end(), large_ids.begin(), large_ids.end());
+    }
     if ((rc = factor_large_fronts(h, large_ids, A, dop))) return rc;
     CK(cudaEventRecord(h->ev[3], st));
     // ---- contribution GEMM (fronts with nothing eliminated skip inside)
