@@ -274,12 +274,15 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
     vals = bl.values()
     d_vals = torch.from_numpy(vals).to("cuda")
     G = []  # per group: scaling, right-hand sides (R columns of length n_g), solution buffer, stream
-    for g in bl.groups:
+    scals = [torch.from_numpy(g.solver._scaling).to("cuda") for g in bl.groups]
+    # each union's scheduling options tuned on its own pattern and values (plain FP64: results unchanged)
+    tables = bl.autotune_groups(d_vals.data_ptr(), [t.data_ptr() for t in scals], opts, reps=1)
+    for g, sc in zip(bl.groups, scals):
         big = bl.rhs_matrix(rhs, g.first, g.count)
-        g.solver._ensure_handle(opts)
+        g.solver._ensure_handle(g.options)
         g.solver.trim(workspace=True, factor=True)  # creation sized the arenas: give them back until its turn
         g.solver.set_profiling(True)
-        G.append(dict(g=g, scal=torch.from_numpy(g.solver._scaling).to("cuda"), R=big.shape[1],
+        G.append(dict(g=g, scal=sc, R=big.shape[1],
                       rhs=torch.from_numpy(np.ascontiguousarray(big.T)).to("cuda"),
                       x=torch.empty(big.shape[1], big.shape[0], dtype=torch.float64, device="cuda"),
                       stream=torch.cuda.ExternalStream(g.solver.stream()), voff=int(bl.voffsets[g.first])))
@@ -302,7 +305,7 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
     def step(dv):
         for e in G:
             g = e["g"]
-            g.solver.factor_device(dv.data_ptr() + 8 * e["voff"], e["scal"].data_ptr(), opts)
+            g.solver.factor_device(dv.data_ptr() + 8 * e["voff"], e["scal"].data_ptr(), g.options)
             with torch.cuda.stream(e["stream"]):  # the handle's stream orders the copy before the solve
                 e["x"].copy_(e["rhs"])
             g.solver.solve_device(e["x"].data_ptr(), e["R"], g.union.n)
@@ -362,7 +365,7 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
     for _ in range(max(1, min(args.steps, 2))):
         barrier()
         t1 = time.perf_counter()
-        bl.factor_solve(None, rhs, opts)
+        bl.factor_solve(None, rhs)  # each union with its tuned options
         torch.cuda.synchronize()
         e2e_t.append(time.perf_counter() - t1)
     inert_ok = bl.inertias() == [sy.inertia for sy in systems]
@@ -402,6 +405,10 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
             "e2e": {"value": e2e_v, "unit": "s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(sum(e["rhs"].numel() * 8 for e in G))},
             "gpu_launches": int(launches),
+            "autotune": [{"group": gi, "chosen": {"large_front_threshold": g.options.large_front_threshold,
+                                                  "mixed_tile_cols": g.options.mixed_tile_cols},
+                          "candidates": [dict(c, factor_s=t) for c, t in tab]}
+                         for gi, (g, tab) in enumerate(zip(bl.groups, tables))],
             "parts_ms": parts, "step_event_s": times, "peak_device_bytes": peak, "clocks": clk,
             "cpu_baseline": cb,
         }

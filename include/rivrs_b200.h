@@ -351,7 +351,8 @@ rvg_status rvg_set_selector(rvg_handle* h, const float* params, int64_t nparams,
  * out == NULL: *nrows only. */
 rvg_status rvg_front_features(rvg_handle* h, double* out, int64_t cap_rows, int64_t* nrows);
 /* [large fronts, fronts the selector sent to the mixed form, mixed fronts
- * over the growth bound, 1 if the factor in place is the FP64 rerun]. */
+ * over the growth bound, fronts factored again in FP64 at the end of their
+ * wave because they were over it]. */
 rvg_status rvg_selector_stats(rvg_handle* h, int64_t out4[4]);
 /* The CUDA stream the handle launches on (cudaStream_t as void*). */
 rvg_status rvg_stream(rvg_handle* h, void** stream);

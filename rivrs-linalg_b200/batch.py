@@ -81,6 +81,7 @@ class _Group:
     union: problems.System
     solver: SparseLDLT
     sys_of_pos: np.ndarray  # elimination position -> system index within the group
+    options: FactorOptions | None = None  # scheduling options tuned on this union (autotune_groups)
 
 
 class BatchLDLT:
@@ -176,7 +177,7 @@ class BatchLDLT:
         vals = self.values(per_system)
         inert = []
         for g in self.groups:
-            g.solver.factor(self.group_values(g, vals), options)
+            g.solver.factor(self.group_values(g, vals), g.options if (options is None and g.options) else options)
             inert += self._group_inertias(g)
             if len(self.groups) > 1:
                 g.solver.trim(workspace=True)
@@ -197,6 +198,28 @@ class BatchLDLT:
                 g.solver.trim(workspace=True)
         return out
 
+    def autotune_groups(self, d_values_ptr: int, d_scaling_ptrs=None, base: FactorOptions | None = None,
+                        reps: int = 1, cache: str | None = None) -> list:
+        """Tune the scheduling options of every group on its own union (the
+        autotuner's candidates: large-front cutoff, and the tile width in the
+        mixed form without flushing), the batch's values at d_values_ptr on
+        the device (d_scaling_ptrs: one device scaling per group, or None).
+        Each group keeps its choice in `options` (results are unchanged in
+        the plain form) and releases its device memory afterwards.  Returns
+        each group's table of (candidate, seconds)."""
+        from . import autotune as at
+        base = base or FactorOptions()
+        tables = []
+        for i, g in enumerate(self.groups):
+            sp = None if d_scaling_ptrs is None else d_scaling_ptrs[i]
+            tuned, table = at.autotune(g.solver, d_values_ptr + 8 * int(self.voffsets[g.first]), sp, base,
+                                       reps=reps, cache=cache)
+            g.options = tuned
+            g.solver._ensure_handle(tuned)
+            g.solver.trim(workspace=True, factor=True)
+            tables.append(table)
+        return tables
+
     def factor_solve(self, per_system, rhs_list, options: FactorOptions | None = None) -> list:
         """Factor and solve group by group, releasing each group's device
         memory (factor included) before the next: the batch only needs the
@@ -206,7 +229,7 @@ class BatchLDLT:
         vals = self.values(per_system)
         out, inert = [], []
         for g in self.groups:
-            g.solver.factor(self.group_values(g, vals), options)
+            g.solver.factor(self.group_values(g, vals), g.options if (options is None and g.options) else options)
             inert += self._group_inertias(g)
             big = self.rhs_matrix(rhs_list, g.first, g.count)
             x = g.solver.solve(big if big.shape[1] > 1 else big[:, 0])

@@ -1165,7 +1165,7 @@ __global__ void k_mlp_route(const int32_t* ids, int n, const DFront* F, const fl
 // After the wave's factorization: max |D| of each large front; a front that
 // took the mixed form and whose max |D| exceeds bound * max |a| raises flag.
 __global__ void k_front_growth(const int32_t* ids, const DFront* F, Arenas A, double bound, unsigned* feat,
-                               int32_t* flag) {
+                               int32_t* flag, int32_t* route) {
   const int s = ids[blockIdx.x];
   const DFront f = F[s];
   __shared__ double sm[8];
@@ -1182,7 +1182,10 @@ __global__ void k_front_growth(const int32_t* ids, const DFront* F, Arenas A, do
     unsigned* row = feat + (size_t)s * FEAT_STRIDE;
     row[7] = fbits(mx);
     const double amax = (double)__uint_as_float(row[0]);
-    if (__uint_as_float(row[21]) == 1.f && mx > bound * amax) atomicAdd(flag, 1);
+    if (__uint_as_float(row[21]) == 1.f && mx > bound * amax) {
+      atomicAdd(flag, 1);
+      route[blockIdx.x] = 2;  // refactored in FP64 once the wave is done
+    }
   }
 }
 
@@ -1296,6 +1299,9 @@ struct rvg_handle {
   double host_wait_ms = 0;  // waits on large-front blocks issued ahead (later blocks still queued)
   double host_gap_ms = 0;   // host time between a wave's synchronisation and the next wave's first launch
   bool sf_attr = false;     // the backward solve kernels' shared-memory limit raised
+  char* d_stage2 = nullptr; size_t stage2_cap = 0;  // launch data of FP64 refactorizations of single fronts
+  char* h_stage2 = nullptr; size_t h_stage2_cap = 0;
+  int64_t sel_refactored = 0;                       // fronts refactored in FP64 after their growth check
   int64_t lf_misses = 0;    // large-front blocks issued past a delay (returned at once, issued again)
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
@@ -2056,6 +2062,99 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
 
 int finish_factor(rvg_handle* h, int64_t d_used);
 
+// Learned precision: large fronts of the wave just factored whose mixed-form
+// D grew past the bound (k_front_growth) are factored again in FP64, alone.
+// Each is assembled again from scratch -- original entries and its children's
+// contribution blocks, which the wave released to the allocator but which no
+// allocation overwrites before the next wave -- then factored on the
+// large-front path with FP64 updates, and its contribution block is formed
+// again with the FP64 GEMM.  The results are those a plain FP64 factorization
+// gives the front from the same children.
+int refactor_fp64(rvg_handle* h, const std::vector<int32_t>& redo, const Arenas& A, const DevOpts& dop,
+                  const double* d_vals, const double* d_scal) {
+  cudaStream_t st = h->st;
+  const Plan& P = h->P;
+  int rc;
+  for (int32_t s : redo) h->route[s] = 0;
+  h->sel_refactored += (int64_t)redo.size();
+  for (int32_t s : redo) {
+    const DFront& f = h->h_fronts[s];
+    CK(cudaMemsetAsync(A.panel + f.panel, 0, (size_t)f.m * f.k * 8, st));
+    if (f.flags & FF_HAS_CB) CK(cudaMemsetAsync(A.cbase + f.cb, 0, (size_t)f.nfs * f.nfs * 8, st));
+  }
+  const int n = (int)redo.size();
+  std::vector<ScatterItem> sitems;
+  for (int32_t s : redo)
+    for (int64_t e = P.amap_ptr[s]; e < P.amap_ptr[s + 1]; e += 256) sitems.push_back(ScatterItem{s, 0, e});
+  size_t maxch = 0;
+  for (int32_t s : redo) maxch = std::max(maxch, P.children[s].size());
+  std::vector<std::vector<EaTile>> eitems(maxch);
+  for (size_t q = 0; q < maxch; ++q)
+    for (int32_t s : redo) {
+      if (q >= P.children[s].size()) continue;
+      const int64_t c = P.children[s][q];
+      const DFront& cf = h->h_fronts[c];
+      if (!(cf.flags & FF_HAS_PARENT) || cf.ne >= cf.m) continue;
+      const int sz = cf.m - cf.ne;
+      for (int j0 = 0; j0 < sz; j0 += 32)
+        for (int i0 = j0; i0 < sz; i0 += EA_ROWS) eitems[q].push_back(EaTile{s, (int32_t)c, j0, i0});
+    }
+  std::vector<TileItem> witems, gitems;
+  std::vector<int32_t> big_cb;
+  for (int32_t s : redo) {
+    const DFront& f = h->h_fronts[s];
+    if (!(f.flags & FF_HAS_CB) || f.k == 0) continue;
+    for (int ti = 0; ti * 256 < f.nfs; ++ti) witems.push_back(TileItem{s, ti, 0, 0});
+    if (f.nfs >= 256) { big_cb.push_back(s); continue; }  // GEMM by launch_syrk
+    const int nt = (f.nfs + GT - 1) / GT;
+    for (int tj = 0; tj < nt; ++tj)
+      for (int ti = tj; ti < nt; ++ti) gitems.push_back(TileItem{s, ti, tj, 0});
+  }
+  Packer pk;
+  const size_t o_ids = pk.add(redo), o_s = pk.add(sitems), o_w = pk.add(witems), o_g = pk.add(gitems);
+  std::vector<size_t> o_e(maxch);
+  for (size_t q = 0; q < maxch; ++q) o_e[q] = pk.add(eitems[q]);
+  const size_t o_cnt = pk.add(std::vector<int32_t>(3 * (size_t)n, 0));
+  if ((rc = ensure(h->d_stage2, h->stage2_cap, pk.buf.size(), st))) return rc;
+  if ((rc = ensure_host(h->h_stage2, h->h_stage2_cap, std::max(pk.buf.size(), (size_t)3 * n * 4)))) return rc;
+  std::memcpy(h->h_stage2, pk.buf.data(), pk.buf.size());
+  CK(cudaMemcpyAsync(h->d_stage2, h->h_stage2, pk.buf.size(), cudaMemcpyHostToDevice, st));
+  char* D = h->d_stage2;
+  const int32_t* d_ids = (const int32_t*)(D + o_ids);
+  k_front_rows<<<n, 128, 0, st>>>(d_ids, n, h->d_fronts, statics(h), A);
+  if (!sitems.empty())
+    k_scatter<<<(unsigned)sitems.size(), 256, 0, st>>>((const ScatterItem*)(D + o_s), h->d_fronts, statics(h), A,
+                                                       d_vals, d_scal);
+  for (size_t q = 0; q < maxch; ++q)
+    if (!eitems[q].empty())
+      k_extend_add_tiled<<<(unsigned)eitems[q].size(), 256, 0, st>>>((const EaTile*)(D + o_e[q]), h->d_fronts,
+                                                                      statics(h), A);
+  CK(cudaGetLastError());
+  if ((rc = factor_large_fronts(h, redo, A, dop))) return rc;
+  if (!witems.empty())
+    k_cb_w<<<(unsigned)witems.size(), 256, 0, st>>>((const TileItem*)(D + o_w), h->d_fronts, A);
+  if (!gitems.empty())
+    k_cb_gemm<<<(unsigned)gitems.size(), 256, 0, st>>>((const TileItem*)(D + o_g), h->d_fronts, A);
+  for (int32_t s : big_cb) {
+    const DFront& f = h->h_fronts[s];
+    SyrkArgs ga{A.cbase + f.cb, f.nfs, A.scratch + f.scratch, f.nfs, A.panel + f.panel + f.k, f.m,
+                0, f.nfs, 0, f.nfs, 0, &h->d_fronts[s].ne};
+    if ((rc = launch_syrk(h, ga, f.k, false))) return rc;
+  }
+  k_get_counts<<<blocks_for(n, 128), 128, 0, st>>>(d_ids, n, h->d_fronts, (int32_t*)(D + o_cnt));
+  int32_t* hc = (int32_t*)h->h_stage2;
+  CK(cudaMemcpyAsync(hc, D + o_cnt, (size_t)3 * n * 4, cudaMemcpyDeviceToHost, st));
+  const double ts0 = now_ms();
+  CK(cudaStreamSynchronize(st));
+  h->host_sync_ms += now_ms() - ts0;
+  for (int i = 0; i < n; ++i) {
+    DFront& f = h->h_fronts[redo[i]];
+    f.ne = hc[3 * i]; f.n1 = hc[3 * i + 1]; f.n2 = hc[3 * i + 2];
+  }
+  h->launches += 4 + (int64_t)maxch + (sitems.empty() ? 0 : 1);
+  return RVG_OK;
+}
+
 // The numeric factorization proper: the level-set schedule of
 // factor_tree_levelset (numeric.rs:1957-2163) with every front of a wave
 // processed by the same launches.
@@ -2096,6 +2195,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     h->route.assign(ns, 0);
     h->sel_large.clear();
     h->sel_routed = 0;
+    h->sel_refactored = 0;
   }
   if (!h->replay) {
     h->rec_ok = false;
@@ -2344,7 +2444,8 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     }
     if (learned) {
       k_front_growth<<<(unsigned)large_ids.size(), 256, 0, st>>>((const int32_t*)(D + o_lg), h->d_fronts, A,
-                                                                 h->sel_bound, h->d_feat, h->d_sel_flag);
+                                                                 h->sel_bound, h->d_feat, h->d_sel_flag,
+                                                                 (int32_t*)(D + o_rt));
       h->launches++;
     }
     CK(cudaEventRecord(h->ev[4], st));
@@ -2369,9 +2470,11 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       continue;
     }
     k_get_counts<<<blocks_for(nw, 128), 128, 0, st>>>(d_ids, nw, h->d_fronts, (int32_t*)(D + o_cnt));
-    if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4) * 4))) return rc;
+    const size_t nlr = learned ? large_ids.size() : 0;  // the large fronts' routes after the growth check
+    if ((rc = ensure_host((char*&)h->h_counts, h->h_counts_cap, (size_t)(3 * nw + 4 + nlr) * 4))) return rc;
     CK(cudaMemcpyAsync(h->h_counts, D + o_cnt, (size_t)3 * nw * 4, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(h->h_counts + 3 * nw, h->d_err, 4, cudaMemcpyDeviceToHost, st));
+    if (nlr) CK(cudaMemcpyAsync(h->h_counts + 3 * nw + 4, D + o_rt, nlr * 4, cudaMemcpyDeviceToHost, st));
     {
       double ts0 = now_ms();
       CK(cudaStreamSynchronize(st));
@@ -2387,6 +2490,12 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     for (int i = 0; i < nw; ++i) {
       DFront& f = h->h_fronts[wave[i]];
       f.ne = h->h_counts[3 * i]; f.n1 = h->h_counts[3 * i + 1]; f.n2 = h->h_counts[3 * i + 2];
+    }
+    if (nlr) {
+      std::vector<int32_t> redo;
+      for (size_t i = 0; i < nlr; ++i)
+        if (h->h_counts[3 * nw + 4 + i] == 2) redo.push_back(large_ids[i]);
+      if (!redo.empty() && (rc = refactor_fp64(h, redo, A, dop, d_vals, d_scal))) return rc;
     }
     for (int64_t s : cb_syrk_fronts) {
       const DFront& f = h->h_fronts[s];
@@ -2723,22 +2832,13 @@ static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
     if (rc) return rc;
   }
   if (h->opt.precision == 2) {
-    // a front that took the mixed form and grew past the bound: the whole
-    // factorization again in FP64 (the plain form is the selector's fallback)
+    // fronts that took the mixed form and grew past the bound were factored
+    // again in FP64 at the end of their wave (refactor_fp64)
     int32_t flagged = 0;
     CK(cudaMemcpyAsync(&flagged, h->d_sel_flag, 4, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->sel_flagged = flagged;
-    h->sel_fallback = 0;
-    if (flagged) {
-      const int64_t routed = h->sel_routed;
-      h->sel_force_fp64 = true;
-      rc = run_factor(h, h->d_vals, ds);
-      h->sel_force_fp64 = false;
-      if (rc) return rc;
-      h->sel_routed = routed;  // what the selector chose (the factor in place is FP64)
-      h->sel_fallback = 1;
-    }
+    h->sel_fallback = h->sel_refactored;
   }
   double* d_acc = nullptr;
   CK(cudaMallocAsync((void**)&d_acc, 8, h->st));
@@ -3518,6 +3618,7 @@ rvg_status rvg_trim(rvg_handle* h, int32_t what) {
     for (size_t t = 1; t < h->lfx.size(); ++t) RVG_TRIM(h->lfx[t].wpack, h->lfx[t].wpack_cap);
     if (!h->lfx.empty()) { h->lfx[0].wpack = nullptr; h->lfx[0].wpack_cap = 0; }
     RVG_TRIM(h->d_stage, h->stage_cap);
+    RVG_TRIM(h->d_stage2, h->stage2_cap);
     h->cb_free.clear();
   }
   if (what & 2) {
@@ -3560,7 +3661,7 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
   fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_stage2); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
   drop_graph(h);
   fr(h->d_rec);
   if (h->d_sel) cudaFree(h->d_sel);
@@ -3582,6 +3683,7 @@ void rvg_destroy(rvg_handle* h) {
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
   if (h->h_stage) cudaFreeHost(h->h_stage);
+  if (h->h_stage2) cudaFreeHost(h->h_stage2);
   if (h->h_counts) cudaFreeHost(h->h_counts);
   if (h->h_norms) cudaFreeHost(h->h_norms);
   if (h->h_norms_m) cudaFreeHost(h->h_norms_m);

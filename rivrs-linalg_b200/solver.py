@@ -428,7 +428,7 @@ class SparseLDLT:
         out = np.zeros(4, np.int64)
         _check(N.lib().rvg_selector_stats(self._handle, N.ptr(out, N.i64p)))
         return dict(large_fronts=int(out[0]), routed_mixed=int(out[1]), over_bound=int(out[2]),
-                    fp64_rerun=bool(out[3]))
+                    fp64_refactored=int(out[3]), fp64_rerun=bool(out[3]))
 
     def work(self):
         out = np.zeros(6)

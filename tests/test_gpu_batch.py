@@ -108,3 +108,29 @@ def test_groups_and_trim_match_one_union(rv):
         g.solver.solve(np.zeros(g.union.n))
     one.close()
     many.close()
+
+
+def test_autotuned_groups_give_the_same_factors(rv):
+    # each union's scheduling options tuned on its own pattern; in the plain form the choice changes no
+    # result, so every system's pivots and D equal those of the untuned factorization
+    import torch
+    systems, nrhs = family(rv, count=5, seed=7)
+    bl = rv.BatchLDLT(systems, device_budget=0)
+    bl.factor(None, rv.FactorOptions())
+    ref = [bl.system_record(i) for i in range(len(systems))]
+    d_vals = torch.from_numpy(bl.values()).to("cuda")
+    scals = [torch.from_numpy(g.solver._scaling).to("cuda") for g in bl.groups]
+    tables = bl.autotune_groups(d_vals.data_ptr(), [t.data_ptr() for t in scals],
+                                rv.FactorOptions(large_front_threshold=2048), reps=1)
+    assert len(tables) == len(bl.groups) and all(len(t) >= 2 for t in tables)
+    assert all(g.options is not None for g in bl.groups)
+    rhs = [rv.problems.rhs_normal(s.n, i, r) for i, (s, r) in enumerate(zip(systems, nrhs))]
+    bl.factor(None)  # each union with its tuned options
+    xs = bl.solve(rhs)
+    for i, s in enumerate(systems):
+        got = bl.system_record(i)
+        assert all(np.array_equal(a, b) for a, b in zip(got, ref[i])), i
+        bb = rhs[i] if rhs[i].ndim == 2 else rhs[i][:, None]
+        xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
+        assert max(rv.problems.backward_error(s, xx[:, j], bb[:, j]) for j in range(bb.shape[1])) <= 1e-14
+    bl.close()

@@ -149,16 +149,21 @@ def test_forced_routes_reproduce_the_uniform_forms(rv, mixed):
     solver.close()
 
 
-def test_growth_flag_reruns_in_fp64(rv):
+def test_growth_flag_refactors_the_front_in_fp64(rv):
+    # every mixed front is over the bound: each is assembled again and factored in FP64 at the end of its
+    # wave, so the whole factor is the plain FP64 one, bit for bit
     s = rv.problems.kkt(10, seed=2)
     solver = rv.SparseLDLT.analyze(s)
     solver.factor(None, rv.FactorOptions(precision="fp64", **BASE))
     ref = record(solver)
-    solver.set_selector(forced(rv, True, bound=1e-300))  # every mixed front is over the bound
+    solver.set_selector(forced(rv, True, bound=1e-300))
     solver.factor(None, rv.FactorOptions(precision="learned", **BASE))
     st = solver.selector_stats()
-    assert st["over_bound"] > 0 and st["fp64_rerun"]
+    assert st["over_bound"] > 0 and st["fp64_refactored"] == st["over_bound"] == st["large_fronts"]
     assert same(record(solver), ref)
+    b = rv.problems.rhs_normal(s.n, 4)
+    x = solver.solve(b)
+    assert rv.problems.backward_error(s, x, b) <= 1e-14
     solver.close()
 
 
