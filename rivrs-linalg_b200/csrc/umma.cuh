@@ -547,17 +547,53 @@ __host__ __device__ inline int64_t tp_count_tiles(int64_t nr, int64_t nc, int64_
   }
   return n;
 }
-__device__ inline void tp_tile(const TcArgs& a, int64_t t, int64_t& px, int64_t& by) {
-  for (px = 0; 2 * px < a.nc; ++px) {
-    const int64_t f = tc_first_row_tile(2 * px, a.r0, a.c0);
-    const int64_t cnt = f < a.nr ? a.nr - f : 0;
-    if (t < cnt) {
-      by = f + t;
-      return;
+// Tile t of the pair kernel.  The column pairs go TP_GROUP at a time; inside a
+// group the row tiles go in order and, for each row tile, the group's pairs
+// whose lower part reaches it.  The CTAs working at the same time then share
+// a few row tiles of W and the group's L tiles (a few MB, resident in L2),
+// where walking one column pair at a time streamed every row tile of W once
+// per pair (~240 MB per pair on a 59k-row front, more than the L2 holds).
+// Every tile is computed the same way in any order.
+constexpr int TP_GROUP = 8;
+__host__ __device__ inline void tp_tile_at(int64_t nr, int64_t nc, int64_t r0, int64_t c0, int64_t t, int64_t& px,
+                                           int64_t& by) {
+  const int64_t np = (nc + 1) / 2;
+  for (int64_t p0 = 0; p0 < np; p0 += TP_GROUP) {
+    const int g = (int)(np - p0 < TP_GROUP ? np - p0 : TP_GROUP);
+    int64_t f[TP_GROUP];
+    int64_t cnt = 0;
+    for (int j = 0; j < g; ++j) {
+      const int64_t fj = tc_first_row_tile(2 * (p0 + j), r0, c0);
+      f[j] = fj < nr ? fj : nr;
+      cnt += nr - f[j];
     }
-    t -= cnt;
+    if (t >= cnt) {
+      t -= cnt;
+      continue;
+    }
+    // rows [f[0], f[g-1]): the pairs j with f[j] <= row, in order of j
+    for (int64_t b = f[0]; b < f[g - 1]; ++b) {
+      int v = 0;
+      for (int j = 0; j < g; ++j) v += f[j] <= b;
+      if (t < v) {
+        for (int j = 0; j < g; ++j)
+          if (f[j] <= b) {
+            if (t == 0) { px = p0 + j; by = b; return; }
+            --t;
+          }
+      }
+      t -= v;
+    }
+    // rows from f[g-1]: all g pairs
+    by = f[g - 1] + t / g;
+    px = p0 + t % g;
+    return;
   }
-  by = 0;  // not reached for t < ntiles
+  px = 0;  // not reached for t < ntiles
+  by = 0;
+}
+__device__ inline void tp_tile(const TcArgs& a, int64_t t, int64_t& px, int64_t& by) {
+  tp_tile_at(a.nr, a.nc, a.r0, a.c0, t, px, by);
 }
 
 template <int FMT>
