@@ -643,6 +643,8 @@ def run_profile_step(args, rv, torch):
                       "phases_ms": {k: pr[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "host_sync_ms",
                                                        "host_wait_ms")},
                       "timed_step_host": host,
+                      "schur_gemm": {"ms": pr["syrk_ms"], "flops_fp64_equiv": pr["syrk_flops"],
+                                     "launches": pr["syrk_launches"]},
                       "parts_ms": pr["part_ms"]}), flush=True)
 
 
