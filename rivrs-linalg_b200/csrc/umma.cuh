@@ -554,7 +554,7 @@ __host__ __device__ inline int64_t tp_count_tiles(int64_t nr, int64_t nc, int64_
 // where walking one column pair at a time streamed every row tile of W once
 // per pair (~240 MB per pair on a 59k-row front, more than the L2 holds).
 // Every tile is computed the same way in any order.
-constexpr int TP_GROUP = 32;
+constexpr int TP_GROUP = 8;
 __host__ __device__ inline void tp_tile_at(int64_t nr, int64_t nc, int64_t r0, int64_t c0, int64_t t, int64_t& px,
                                            int64_t& by) {
   // first row tile of pair q, at most nr (non-decreasing in q)
