@@ -938,9 +938,12 @@ def main():
                               "frac": asm_gbs / hbm if (hbm and asm_gbs) else None}}
     dpeak = gemm_peak_tflops(torch, torch.float64)
     tpeak = gemm_peak_tflops(torch, torch.float32)
+    # The dominant kernel's rate on ALGORITHMIC flops: the Schur-GEMM launches' FP64-equivalent work (2 K per
+    # lower output entry; the mixed form executes 3 products per term, reported beside as "executed")
+    syrk_ms, syrk_flops, syrk_launch = chosen["syrk_ms"], chosen["syrk_flops"], chosen["syrk_launch"]
+    products = 1.0
     if chosen_name == "mixed":
-        # TF32 tensor flops the kernel executes: three products per FP64-equivalent term
-        syrk_ms, syrk_flops, syrk_launch = chosen["syrk_ms"], 3.0 * chosen["syrk_flops"], chosen["syrk_launch"]
+        products = 3.0
         peak = tpeak
         if chosen["opts"].mixed_operands == "bf16":
             mp = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
@@ -961,16 +964,16 @@ def main():
         rl_kernel = "k_syrk_dmma (FP64 Schur-complement GEMM, plain form)"
         rl_source = "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in the measured-peaks file)"
     achieved = (syrk_flops / (syrk_ms * 1e-3) / 1e12) if syrk_ms > 0 else None
-    # DRAM traffic of the chosen kernel per launch: the ncu capture of its longest launch on the KKT 36^3
-    # (profiles/k_syrk_tc_pair_bf16_kkt36.md: 1,569.6 MB for 148.1 GFLOP FP64-equivalent at K = 1024) scaled
-    # to this run's average launch by its flops (C traffic grows with the entries, operands with K x rows)
+    # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum summed over EVERY k_syrk_tc_pair
+    # launch of one factorization of this workload (the BF16 form, one pass, full size): 970.0 GB for 8.62e13
+    # FP64-equivalent flops, i.e. 0.01125 bytes per flop, applied to this run's average launch
     traffic = traffic_src = None
     if chosen_name == "mixed" and chosen["opts"].mixed_operands == "bf16" and chosen["opts"].mixed_flush == 0 \
-            and chosen["syrk_launch"]:
-        fp64_flops_per_launch = chosen["syrk_flops"] / chosen["syrk_launch"]
-        traffic = 1569.6e6 / 148.1e9 * fp64_flops_per_launch
-        traffic_src = ("ncu dram__bytes_read+write of one k_syrk_tc_pair<BF16> launch (KKT 36^3, K = 1024), "
-                       "scaled by FP64-equivalent flops to this run's average launch")
+            and chosen["syrk_launch"] and args.config == "kkt60":
+        traffic = 970.0e9 / 8.62055e13 * (chosen["syrk_flops"] / chosen["syrk_launch"])
+        traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum over every k_syrk_tc_pair<BF16> launch of "
+                       "one factorization of this workload (970.0 GB for 8.62e13 FP64-equivalent flops), at this "
+                       "run's average launch")
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         orc = entry.load_oracle()
@@ -1020,6 +1023,10 @@ def main():
             "roofline": {"kernel": rl_kernel, "bound": "tensor",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "achieved_unit_note": "FP64-equivalent algorithmic flops (2 K per lower output entry)",
+                         "executed": {"tflops": achieved * products if achieved else None,
+                                      "frac": (achieved * products / peak) if achieved else None,
+                                      "products_per_term": products},
                          "traffic_unit": "bytes per launch", "traffic_source": traffic_src,
                          "peak_source": rl_source, "dgemm_peak": dpeak, "tf32_gemm_peak": tpeak,
                          "launches_per_step": syrk_launch,

@@ -1881,7 +1881,8 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     const int64_t bne = g - I.cs;
     if (two_level && I.window) {
       const bool delayed = bne < I.bcols;
-      const double K = (double)(I.kadd + bne);
+      // the Schur-GEMM flops count where the GEMM's events are recorded (the front carrying the marks)
+      const double K = cx.marks ? (double)(I.kadd + bne) : 0.0;
       if (I.flush) {
         cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, p);
       } else {
