@@ -250,6 +250,9 @@ typedef struct {
    * next wave's fronts) to the next wave's first launch: the device has
    * nothing of this factorization queued meanwhile */
   double host_gap_ms;
+  /* full-window updates of a large front whose far field (the columns after
+   * the next three outer blocks) ran on a second stream beside those blocks */
+  int64_t lf_far_updates;
 } rvg_profile;
 
 /* Indices of rvg_profile.part_ms.  Large fronts (whole GPU per front): */

@@ -50,7 +50,8 @@ class Profile(C.Structure):
                 ("syrk_flops", C.c_double), ("syrk_launches", i64), ("factor_launches", i64),
                 ("solve_launches", i64), ("peak_bytes", i64), ("host_total_ms", C.c_double),
                 ("host_alloc_ms", C.c_double), ("host_sync_ms", C.c_double), ("part_ms", C.c_double * 16),
-                ("host_wait_ms", C.c_double), ("lf_misses", i64), ("host_gap_ms", C.c_double)]
+                ("host_wait_ms", C.c_double), ("lf_misses", i64), ("host_gap_ms", C.c_double),
+                ("lf_far_updates", i64)]
 
     PARTS = ("lf_setup", "lf_block", "lf_panel", "lf_post", "lf_update", "lf_delay", "lf_prop", "lf_w", "lf_syrk",
              "lf_outer", "tpp", "aptp", "cb_w", "cb_gemm", "cb_syrk", "other")

@@ -484,7 +484,28 @@ __global__ void __launch_bounds__(128) k_lf_w(LFArgs A) {
 
 // end of an outer block: column order, delays to the end of the remaining
 // fully-summed columns (two_level), eliminated total (1 CTA)
-__global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_level) {
+// The delayed columns of the outer block [cs, cs + bcols) (its last
+// bcols - bne) swap places with the last columns of the remaining range
+// [cs, cs + rem), so the next block starts on columns that were not tried
+// (two_level_factor's swap, factor.rs:2108-2252).  One CTA.
+__device__ __forceinline__ void lf_swap_delayed(const LFArgs& A, int64_t cs, int64_t bcols, int64_t rem, int bne) {
+  const int tid = threadIdx.x;
+  PanelView F{A.a, A.m};
+  const int nf = (int)(bcols - bne);
+  for (int i = 0; i < nf; ++i) {
+    int64_t fp = cs + bne + i, e = cs + rem - 1 - i;
+    if (fp < e) {
+      cta_swap(F, A.m, fp, e);
+      if (tid == 0) { int32_t t = A.perm[fp]; A.perm[fp] = A.perm[e]; A.perm[e] = t; }
+    }
+  }
+}
+
+// End of an outer block: its column order into the front's pivot order, the
+// delay swap (unless `swap` is 0: a far-field update may still be running on
+// another stream, and the host issues the swap itself, k_lf_swap, once it has
+// seen the delay), the eliminated total.
+__global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_level, int swap) {
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int tid = threadIdx.x;
@@ -496,19 +517,16 @@ __global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_
   __syncthreads();
   for (int i = tid; i < bcols; i += NT) A.perm[cs + i] = orig[A.lp[i]];
   __syncthreads();
-  if (two_level && bne < bcols) {
-    PanelView F{A.a, A.m};
-    const int nf = (int)(bcols - bne);
-    for (int i = 0; i < nf; ++i) {
-      int64_t fp = cs + bne + i, e = cs + rem - 1 - i;
-      if (fp < e) {
-        cta_swap(F, A.m, fp, e);
-        if (tid == 0) { int32_t t = A.perm[fp]; A.perm[fp] = A.perm[e]; A.perm[e] = t; }
-      }
-    }
-  }
+  if (swap && two_level && bne < bcols) lf_swap_delayed(A, cs, bcols, rem, bne);
   __syncthreads();
   if (tid == 0) st->gne += bne;
+}
+
+// The delay swap of an outer block issued without it (k_lf_outer with swap =
+// 0), with the block's start column, width, remaining range and eliminated
+// count as the host read them.  One CTA.
+__global__ void __launch_bounds__(NT) k_lf_swap(LFArgs A, int64_t cs, int64_t bcols, int64_t rem, int bne) {
+  lf_swap_delayed(A, cs, bcols, rem, bne);
 }
 
 // TPP fallback on the leftover columns, then the front's results

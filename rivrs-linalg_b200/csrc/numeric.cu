@@ -1212,7 +1212,16 @@ struct LfCtx {
   cudaEvent_t ring_ev[LF_AHEAD] = {};
   double wait_ms = 0;     // host waits on blocks issued ahead (the stream still holds later blocks)
   int64_t misses = 0;     // blocks issued for a start column the factorization did not reach
+  // far-field part of a full window's update, beside the next outer blocks (mixed form)
+  cudaStream_t far_st = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
+  int64_t far_launches = 0;
 };
+// A full window's far field (the columns after the next LF_FAR_AHEAD outer
+// blocks) is updated on a second stream while those blocks are factored; the
+// GEMM leaves LF_FAR_SMS multiprocessors to their latency-bound kernels.
+constexpr int LF_FAR_AHEAD = 3;
+constexpr int LF_FAR_SMS = 24;
 constexpr int LF_CONCURRENT = 8;  // large fronts of a wave in flight at once
 
 struct rvg_handle {
@@ -1303,6 +1312,7 @@ struct rvg_handle {
   char* h_stage2 = nullptr; size_t h_stage2_cap = 0;
   int64_t sel_refactored = 0;                       // fronts refactored in FP64 after their growth check
   int64_t lf_misses = 0;    // large-front blocks issued past a delay (returned at once, issued again)
+  int64_t lf_far = 0;       // far-field window updates run on a large front's second stream
   // results
   int64_t tot1 = 0, tot2 = 0, totdel = 0, zero_piv = 0, max_front = 0;
   double t_assembly = 0, t_kernel = 0, t_gemm = 0, t_factor = 0, t_solve = 0, t_dom = 0, n_dom = 0;
@@ -1617,14 +1627,15 @@ int syrk_ev(rvg_handle* h, bool on = true) {
 // depth picks the k_syrk_tc instance; without flushing, 256-column CTA tiles
 // (k_syrk_tc_pair, over column-tile pairs) unless 128 is asked for.
 template <int FMT>
-static void launch_tc_fmt(rvg_handle* h, cudaStream_t st, TcArgs ta) {
+static void launch_tc_fmt(rvg_handle* h, cudaStream_t st, TcArgs ta, int max_ctas) {
+  const int64_t cap = max_ctas > 0 ? std::min<int64_t>(max_ctas, h->nsm) : h->nsm;
   if (h->opt.mixed_flush == 0 && h->opt.mixed_tile_cols == 256) {
     ta.ntiles = tp_count_tiles(ta.nr, ta.nc, ta.r0, ta.c0);
-    const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
+    const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, cap);
     k_syrk_tc_pair<FMT><<<grid, TC_THREADS, TP_SMEM, st>>>(ta);
     return;
   }
-  const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, h->nsm);
+  const unsigned grid = (unsigned)std::min<int64_t>(ta.ntiles, cap);
   switch (h->opt.mixed_flush) {
     case 1: k_syrk_tc<1, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
     case 2: k_syrk_tc<2, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
@@ -1633,9 +1644,9 @@ static void launch_tc_fmt(rvg_handle* h, cudaStream_t st, TcArgs ta) {
     default: k_syrk_tc<TC_NO_FLUSH, FMT><<<grid, TC_THREADS, TC_SMEM, st>>>(ta); break;
   }
 }
-static void launch_tc(rvg_handle* h, cudaStream_t st, TcArgs ta) {
-  if (h->opt.mixed_operands == 1) launch_tc_fmt<TC_BF16>(h, st, ta);
-  else launch_tc_fmt<TC_TF32>(h, st, ta);
+static void launch_tc(rvg_handle* h, cudaStream_t st, TcArgs ta, int max_ctas = 0) {
+  if (h->opt.mixed_operands == 1) launch_tc_fmt<TC_BF16>(h, st, ta, max_ctas);
+  else launch_tc_fmt<TC_TF32>(h, st, ta, max_ctas);
 }
 // the operand split of the mixed form (TF32 or BF16 parts)
 static void launch_pack(rvg_handle* h, cudaStream_t st, dim3 grid, const PackArgs& pa) {
@@ -1693,8 +1704,8 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax, bool mixed) {
 int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int64_t c0, int64_t c1, int64_t wd,
                        int64_t wrow, int64_t F, const float* pk_w, const float* pk_l, int64_t kadd,
                        const int32_t* kdev, const int32_t* cond, int32_t cond_lt, bool mixed,
-                       const int32_t* skip = nullptr) {
-  cudaStream_t st = cx.st;
+                       const int32_t* skip = nullptr, cudaStream_t on = nullptr, int max_ctas = 0) {
+  cudaStream_t st = on ? on : cx.st;
   if (c1 <= c0) return RVG_OK;
   int rc = syrk_ev(h, cx.marks);
   if (rc) return rc;
@@ -1705,7 +1716,7 @@ int launch_window_gemm(rvg_handle* h, LfCtx& cx, const LFArgs& a, int64_t m, int
     const int64_t t0 = (c0 - wrow) / TC_BM;
     TcArgs ta{a.a, m, c0, m, c0, c1, pk_w + (size_t)t0 * Fq * TC_BLOCK, pk_l + (size_t)t0 * Fq * TC_BLOCK, Fq, kdev,
               kadd, nr, nc, ntiles, h->d_err, cond, cond_lt, 0, skip};
-    launch_tc(h, st, ta);
+    launch_tc(h, st, ta, max_ctas);
   } else {
     SyrkArgs ga{};
     ga.C = a.a;
@@ -1756,16 +1767,27 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   a.nfsb = p;
   a.o = dop;
   const int two_level = p > nb;
-  // window of pending columns [wd, gne) of the deferred updates; its W rows start at wrow
-  int64_t wd = 0, wrow = std::min(p, nb);
   const int64_t Fq = F / TC_BK;
-  float *pk_w = nullptr, *pk_l = nullptr;
+  // the packed window (W and L parts), twice: a full window's far-field update may still read one
+  // buffer on the far stream while the next blocks pack into the other
+  float* pk_wb[2] = {nullptr, nullptr};
+  float* pk_lb[2] = {nullptr, nullptr};
   if (mixed && two_level) {
     const int64_t tiles = (m + TC_BM - 1) / TC_BM;
-    int rc = ensure_nocopy(cx.wpack, cx.wpack_cap, (size_t)2 * tiles * Fq * TC_BLOCK, st);
+    const size_t one = (size_t)tiles * Fq * TC_BLOCK;
+    int rc = ensure_nocopy(cx.wpack, cx.wpack_cap, 4 * one, st);
     if (rc) return rc;
-    pk_w = cx.wpack;
-    pk_l = cx.wpack + (size_t)tiles * Fq * TC_BLOCK;
+    pk_wb[0] = cx.wpack; pk_lb[0] = cx.wpack + one;
+    pk_wb[1] = cx.wpack + 2 * one; pk_lb[1] = cx.wpack + 3 * one;
+  }
+  // far-field updates beside the next blocks: the mixed form in the dynamic schedule (not while
+  // recording profiling marks, not inside a captured graph)
+  const bool async_far = mixed && two_level && !cx.marks && !h->replay;
+  if (async_far && !cx.far_st) {
+    if (tl_no_alloc) return no_alloc_fail();
+    CK(cudaStreamCreateWithFlags(&cx.far_st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&cx.ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&cx.ev_far, cudaEventDisableTiming));
   }
   mk(-1);
   k_lf_init<<<blocks_for(p, 256), 256, 0, st>>>(a.st, a.perm, p);
@@ -1773,12 +1795,24 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   if (!h->replay) h->rec_g[s].clear();
   const int32_t* skip = &a.st->spec_bad;
   int irc = RVG_OK;  // first error of a launch helper inside issue()
-  // Host view of the loop before an outer block: start column (eliminated
-  // so far), remaining columns, the window of pending columns [wd, gne)
-  // whose W rows start at wrow, and the block's index.
-  struct HostLF { int64_t gne, rem, wd, wrow; size_t outer; };
+  // Host view of the loop before an outer block: start column (eliminated so far), remaining
+  // columns, the window of pending columns [wd, gne) whose W rows start at wrow, the block's index,
+  // the packed-window buffer in use, and the block at which a far-field update running on the far
+  // stream must be waited for (-1: none running).
+  struct HostLF { int64_t gne, rem, wd, wrow; size_t outer; int par; int64_t far_due; };
   // what the host decided when it issued a block
-  struct Issued { HostLF before; int64_t cs, bcols, oe, kadd, ncol; bool flush, window; int slot; };
+  struct Issued { HostLF before; int64_t cs, bcols, oe, kadd, ncol; bool flush, window, far, waited; int slot; };
+  // a CUDA call inside issue(): its failure becomes issue()'s error
+  auto ck = [&](cudaError_t e, const char* what) {
+    if (e != cudaSuccess && !irc) {
+      set_error(std::string("CUDA error: ") + cudaGetErrorString(e) + " at " + what);
+      irc = RVG_ERR_DEVICE;
+    }
+  };
+  auto far_wait = [&]() {  // the stream takes up after the running far-field update
+    ck(cudaStreamWaitEvent(st, cx.ev_far, 0), "cudaStreamWaitEvent (far-field update)");
+    return irc;
+  };
   // Launches one outer block for start column S.gne (2 + 6 per inner block + the outer-block steps).
   auto issue = [&](const HostLF& S, int slot) -> Issued {
     Issued I{};
@@ -1786,6 +1820,8 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     I.slot = slot;
     const int64_t rem = S.rem, cs = S.gne, wd = S.wd, wrow = S.wrow;
     const int64_t bcols = std::min(rem, nb), bm = m - cs, oe = cs + bcols;
+    float* pk_w = pk_wb[S.par];
+    float* pk_l = pk_lb[S.par];
     I.cs = cs; I.bcols = bcols; I.oe = oe;
     a.cs = cs;
     a.bcols = bcols;
@@ -1854,52 +1890,77 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
           launch_pack(h, st, dim3((unsigned)nqb, blocks_for(p - oe, TC_BM)), pl);
           cx.launches += 2;
         }
+        // columns of a far-field update still running: the next block's (the near field) from the
+        // block it was launched for on, every trailing column at a flush
+        if (S.far_due >= 0 && ((int64_t)S.outer >= S.far_due || I.flush)) {
+          irc = irc ? irc : far_wait();
+          I.waited = true;
+        }
         if (I.flush) {
-          // the window is full: every trailing column takes it (one GEMM)
-          irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev, nullptr, 0,
-                                               mixed, skip);
+          const int64_t split = oe + LF_FAR_AHEAD * nb;
+          if (async_far && p - split >= 2 * nb) {
+            // the next LF_FAR_AHEAD blocks' columns now, the rest on the far stream beside them (both
+            // after the packs; they touch different columns)
+            ck(cudaEventRecord(cx.ev_fork, st), "cudaEventRecord (far-field fork)");
+            ck(cudaStreamWaitEvent(cx.far_st, cx.ev_fork, 0), "cudaStreamWaitEvent (far-field fork)");
+            irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, split, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
+                                                 nullptr, 0, mixed, skip);
+            irc = irc ? irc : launch_window_gemm(h, cx, a, m, split, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
+                                                 nullptr, 0, mixed, skip, cx.far_st, h->nsm - LF_FAR_SMS);
+            ck(cudaEventRecord(cx.ev_far, cx.far_st), "cudaEventRecord (far-field join)");
+            cx.far_launches++;
+            I.far = true;
+          } else {
+            // the window is full: every trailing column takes it (one GEMM)
+            irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
+                                                 nullptr, 0, mixed, skip);
+          }
         } else {
           // near field: the next outer block's columns (oe + nb <= p here) take the whole window
           irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, oe + I.ncol, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
                                                nullptr, 0, mixed, skip);
-          // far field: only if this block delayed columns (decided on the device)
-          if (oe + nb < p)
+          // far field: only if this block delayed columns (decided on the device); with far-field
+          // updates on the far stream the host issues it once it has seen the delay
+          if (oe + nb < p && !async_far)
             irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe + nb, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
                                                  bne_dev, (int32_t)bcols, mixed, skip);
         }
         mk(RVG_PART_LF_SYRK);
       }
     }
-    k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level);
+    k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level, async_far ? 0 : 1);
     cx.launches++;
     mk(RVG_PART_LF_OUTER);
     return I;
   };
-  // The state after block I once the device's eliminated total g is known.
-  auto after = [&](const Issued& I, int32_t g) -> HostLF {
+  // The state after block I if it eliminated up to column g (no side effects).
+  auto next_state = [&](const Issued& I, int32_t g) -> HostLF {
     HostLF S = I.before;
     const int64_t bne = g - I.cs;
-    if (two_level && I.window) {
-      const bool delayed = bne < I.bcols;
-      // the Schur-GEMM flops count where the GEMM's events are recorded (the front carrying the marks)
-      const double K = cx.marks ? (double)(I.kadd + bne) : 0.0;
-      if (I.flush) {
-        cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, p);
-      } else {
-        cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, I.oe + I.ncol);
-        if (I.oe + nb < p && delayed) cx.syrk_flops += 2.0 * K * lower_entries(I.oe + nb, m, I.oe + nb, p);
-      }
-      if (I.flush || delayed) {  // every column is up to date: a new, empty window
-        S.wd = g;
-        S.wrow = g + std::min(S.rem - I.bcols, nb);
-      }
+    if (two_level && I.window && (I.flush || bne < I.bcols)) {  // every column is up to date: a new, empty window
+      S.wd = g;
+      S.wrow = g + std::min(S.rem - I.bcols, nb);
     }
+    if (I.flush) S.par ^= 1;
+    S.far_due = I.far ? (int64_t)I.before.outer + LF_FAR_AHEAD : (I.waited ? -1 : I.before.far_due);
     S.gne = g;
     S.rem -= I.bcols;
     S.outer += 1;
     return S;
   };
-  HostLF S{0, p, 0, std::min(p, nb), 0};
+  // The Schur-GEMM flops of block I (where the GEMM's events are recorded: the front carrying the marks).
+  auto account = [&](const Issued& I, int32_t g) {
+    if (!(two_level && I.window) || !cx.marks) return;
+    const int64_t bne = g - I.cs;
+    const double K = (double)(I.kadd + bne);
+    if (I.flush) {
+      cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, p);
+    } else {
+      cx.syrk_flops += 2.0 * K * lower_entries(I.oe, m, I.oe, I.oe + I.ncol);
+      if (I.oe + nb < p && bne < I.bcols) cx.syrk_flops += 2.0 * K * lower_entries(I.oe + nb, m, I.oe + nb, p);
+    }
+  };
+  HostLF S{0, p, 0, std::min(p, nb), 0, 0, -1};
   if (h->replay) {
     // the progress of the recorded factorization, checked on the device
     const std::vector<int32_t>& rg = h->rec_g[s];
@@ -1910,7 +1971,8 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
       const int32_t g = rg[S.outer];
       k_check_gne<<<1, 32, 0, st>>>(a.st, g, h->d_mismatch);
       CK(cudaGetLastError());
-      S = after(I, g);
+      account(I, g);
+      S = next_state(I, g);
     }
   } else {
     // Blocks go out ahead on the guess that none delays a column (the next
@@ -1919,7 +1981,9 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     // every later launch of the front into a no-op.  The host reads the
     // device's eliminated total after each block in issue order, at most
     // LF_AHEAD blocks behind; at the first one that differs it waits for the
-    // stream, clears the flag and issues again from the true start column.
+    // streams, issues what that block's delay asks for (with far-field
+    // updates on the far stream: the far field's update by the window and the
+    // delay swap), clears the flag and issues again from the true start column.
     if (!cx.h_gne) {
       if (tl_no_alloc) return no_alloc_fail();
       CK(cudaHostAlloc((void**)&cx.h_gne, LF_AHEAD * sizeof(int32_t), cudaHostAllocDefault));
@@ -1939,16 +2003,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         CK(cudaEventRecord(cx.ring_ev[slot], st));
         CK(cudaGetLastError());
         q.push_back(I);
-        // the guess: no delayed column in this block
-        HostLF G = I.before;
-        if (two_level && I.window && I.flush) {
-          G.wd = I.cs + I.bcols;
-          G.wrow = G.wd + std::min(G.rem - I.bcols, nb);
-        }
-        G.gne = I.cs + I.bcols;
-        G.rem -= I.bcols;
-        G.outer += 1;
-        S = G;
+        S = next_state(I, (int32_t)(I.cs + I.bcols));  // the guess: no delayed column in this block
         continue;
       }
       const Issued I = q.front();
@@ -1962,21 +2017,40 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         mark_flush(h);
         mk(-1);
       }
-      const HostLF T = after(I, g);
+      account(I, g);
       // the device worked on this and the queued blocks meanwhile
       cx.wait_ms += waited;
       if (g == I.cs + I.bcols) continue;  // as guessed
       // a block delayed columns: the blocks issued after it did nothing; the
-      // stream runs dry while the host issues them again
+      // streams run dry while the host issues them again
       const double t1 = now_ms();
       CK(cudaStreamSynchronize(st));
+      if (cx.far_st) CK(cudaStreamSynchronize(cx.far_st));
       cx.sync_ms += now_ms() - t1;
       cx.misses += (int64_t)q.size();
       q.clear();
+      HostLF T = next_state(I, g);
+      T.far_due = -1;  // nothing runs on the far stream any more
+      if (async_far) {
+        const int64_t bne = g - I.cs;
+        a.cs = I.cs;
+        a.bcols = I.bcols;
+        if (two_level && I.window && !I.flush && I.oe + nb < p) {
+          // the far field takes the window, this block's eliminated columns included
+          irc = launch_window_gemm(h, cx, a, m, I.oe + nb, p, I.before.wd, I.before.wrow, F, pk_wb[I.before.par],
+                                   pk_lb[I.before.par], I.kadd + bne, nullptr, nullptr, 0, mixed);
+          if (irc) return irc;
+        }
+        if (two_level && bne < I.bcols)
+          k_lf_swap<<<1, NT, 0, st>>>(a, I.cs, I.bcols, I.before.rem, (int)bne);
+        cx.launches += 2;
+      }
       CK(cudaMemsetAsync(&a.st->spec_bad, 0, sizeof(int32_t), st));
+      CK(cudaGetLastError());
       S = T;
     }
   }
+  if (S.far_due >= 0) CK(cudaStreamWaitEvent(st, cx.ev_far, 0));  // a far-field update still running
   k_lf_finish<<<1, 32, 0, st>>>(a, h->d_fronts, s);
   cx.launches++;
   mk(RVG_PART_LF_SETUP);
@@ -2000,8 +2074,9 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
     h->host_sync_ms += c.sync_ms;
     h->host_wait_ms += c.wait_ms;
     h->lf_misses += c.misses;
+    h->lf_far += c.far_launches;
     h->syrk_flops += c.syrk_flops;
-    c.launches = 0; c.sync_ms = 0; c.syrk_flops = 0; c.wait_ms = 0; c.misses = 0;
+    c.launches = 0; c.sync_ms = 0; c.syrk_flops = 0; c.wait_ms = 0; c.misses = 0; c.far_launches = 0;
   };
   // (a capture forks into the same contexts with the fronts dealt the same way:
   // the replayed graph runs them concurrently on the buffers the dynamic run sized)
@@ -2180,6 +2255,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
   h->host_wait_ms = 0;
   h->host_gap_ms = 0;
   h->lf_misses = 0;
+  h->lf_far = 0;
   h->ev_used = 0;
   h->mk_used = 0;
   for (double& v : h->part_ms) v = 0;
@@ -2794,6 +2870,7 @@ static int replay_factor(rvg_handle* h, const double* ds, bool* done) {
   h->host_wait_ms = 0;
   h->host_gap_ms = 0;
   h->lf_misses = 0;
+  h->lf_far = 0;
   *done = true;
   return RVG_OK;
 }
@@ -3532,6 +3609,7 @@ rvg_status rvg_get_profile(rvg_handle* h, rvg_profile* o) {
   o->host_wait_ms = h->host_wait_ms;
   o->lf_misses = h->lf_misses;
   o->host_gap_ms = h->host_gap_ms;
+  o->lf_far_updates = h->lf_far;
   return RVG_OK;
 }
 
@@ -3675,6 +3753,9 @@ void rvg_destroy(rvg_handle* h) {
     LfCtx& c = h->lfx[t];
     if (c.h_gne) cudaFreeHost(c.h_gne);
     for (auto& e : c.ring_ev) if (e) cudaEventDestroy(e);
+    if (c.far_st) { cudaStreamSynchronize(c.far_st); cudaStreamDestroy(c.far_st); }
+    if (c.ev_fork) cudaEventDestroy(c.ev_fork);
+    if (c.ev_far) cudaEventDestroy(c.ev_far);
     if (t == 0) continue;  // the handle's own stream, state and window buffer
     fr(c.wpack);
     if (c.lf) cudaFree(c.lf);

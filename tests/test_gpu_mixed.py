@@ -234,3 +234,42 @@ def test_auto_refinement_escalates_only_when_needed(rv):
     assert err <= 1e-14 and how == "gmres", (err, its, how)
     assert rv.problems.backward_error(s, x, b) <= 1e-14
     solver.close()
+
+
+@pytest.mark.parametrize("case", ["dense_delay", "kkt26"])
+def test_far_field_overlap_is_bit_identical(rv, case):
+    """A full window's far-field update runs on a second stream beside the next three outer blocks, and a
+    delayed block's far-field update and swap wait until the host has seen the delay; the factor equals
+    the one-block-at-a-time schedule of the profiling mode (no second stream) bit for bit."""
+    import numpy as np
+    if case == "dense_delay":
+        rng = np.random.default_rng(4000)
+        a = rng.standard_normal((4000, 4000))
+        a = a + a.T
+        a[np.arange(4000), np.arange(4000)] *= 1e-6
+        s = rv.problems.from_scipy("dense4000_delay", a)
+        opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16", large_front_threshold=33)
+        solver = rv.SparseLDLT.analyze(s)
+    else:
+        s = rv.problems.kkt(26, seed=26)
+        opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16")
+        solver = rv.SparseLDLT.analyze_with_matrix(s, rv.AnalyzeOptions(rv.OrderingStrategy.MATCH_ORDER_METIS))
+    solver.factor(None, opts)
+    far = solver.profile()["lf_far_updates"]
+    got = [x.copy() for x in solver.pivot_record()]
+    st = solver.stats()
+    assert far > 0
+    if case == "dense_delay":
+        assert st["total_delayed"] > 0
+    solver.set_profiling(True)
+    solver.factor(None, opts)
+    assert solver.profile()["lf_far_updates"] == 0
+    ref = solver.pivot_record()
+    assert all(np.array_equal(x, y) for x, y in zip(got, ref))
+    assert solver.stats() == st
+    solver.set_profiling(False)
+    if case == "kkt26":
+        b = rv.problems.rhs_normal(s.n, 3)
+        x, its, err, how = solver.solve_auto(b)
+        assert err <= 1e-14 and solver.inertia() == s.inertia
+    solver.close()
