@@ -1782,7 +1782,8 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   }
   // far-field updates beside the next blocks: the mixed form in the dynamic schedule (not while
   // recording profiling marks, not inside a captured graph)
-  const bool async_far = mixed && two_level && !cx.marks && !h->replay;
+  const bool profiling_marks = cx.marks && h->profiling;  // this front's launches carry the profiling events
+  const bool async_far = mixed && two_level && !profiling_marks && !h->replay;
   if (async_far && !cx.far_st) {
     if (tl_no_alloc) return no_alloc_fail();
     CK(cudaStreamCreateWithFlags(&cx.far_st, cudaStreamNonBlocking));
@@ -1992,7 +1993,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     std::deque<Issued> q;
     int next_slot = 0;
     // with the profiling marks on, one block at a time: the marks are read back after each block
-    const int ahead = cx.marks ? 1 : LF_AHEAD;
+    const int ahead = profiling_marks ? 1 : LF_AHEAD;
     while (S.rem > 0 || !q.empty()) {
       if (S.rem > 0 && (int)q.size() < ahead) {
         const int slot = next_slot;
@@ -2013,7 +2014,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
       const double waited = now_ms() - t0;
       const int32_t g = cx.h_gne[I.slot];
       h->rec_g[s].push_back(g);
-      if (cx.marks) {
+      if (profiling_marks) {
         mark_flush(h);
         mk(-1);
       }

@@ -246,7 +246,9 @@ def test_far_field_overlap_is_bit_identical(rv, case):
         rng = np.random.default_rng(4000)
         a = rng.standard_normal((4000, 4000))
         a = a + a.T
-        a[np.arange(4000), np.arange(4000)] *= 1e-6
+        weak = np.arange(2050, 2114)  # rows and columns scaled down: their block's pivots fail the threshold test
+        a[weak, :] *= 1e-3
+        a[:, weak] *= 1e-3
         s = rv.problems.from_scipy("dense4000_delay", a)
         opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16", large_front_threshold=33)
         solver = rv.SparseLDLT.analyze(s)
@@ -259,8 +261,8 @@ def test_far_field_overlap_is_bit_identical(rv, case):
     got = [x.copy() for x in solver.pivot_record()]
     st = solver.stats()
     assert far > 0
-    if case == "dense_delay":
-        assert st["total_delayed"] > 0
+    if case == "dense_delay":  # outer blocks delayed columns after full windows had gone to the far stream
+        assert solver.profile()["lf_misses"] > 0
     solver.set_profiling(True)
     solver.factor(None, opts)
     assert solver.profile()["lf_far_updates"] == 0
