@@ -1783,7 +1783,9 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   // far-field updates beside the next blocks: the mixed form in the dynamic schedule (not while
   // recording profiling marks, not inside a captured graph)
   const bool profiling_marks = cx.marks && h->profiling;  // this front's launches carry the profiling events
-  const bool async_far = mixed && two_level && !profiling_marks && !h->replay;
+  // (the far part starts LF_FAR_AHEAD blocks after the window's first W row: a whole number of the packed
+  // window's 128-row tiles only when the block width is a multiple of 128)
+  const bool async_far = mixed && two_level && !profiling_marks && !h->replay && nb % TC_BM == 0;
   if (async_far && !cx.far_st) {
     if (tl_no_alloc) return no_alloc_fail();
     CK(cudaStreamCreateWithFlags(&cx.far_st, cudaStreamNonBlocking));
