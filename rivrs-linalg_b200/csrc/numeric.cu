@@ -2585,7 +2585,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
                    (aptp_ids.empty() ? 0 : 1) + (witems.empty() ? 0 : 1) + (gitems.empty() ? 0 : 1) + 2 +
                    (dly_ids.empty() ? 0 : 1) + (zitems.empty() ? 0 : 1);
     for (size_t q = 0; q < maxch; ++q) h->launches += eitems[q].empty() ? 0 : 1;
-    {
+    if (h->profiling) {  // the device memory in use (profiling runs only: the query costs host time)
       size_t fb = 0, tb = 0;
       cudaMemGetInfo(&fb, &tb);
       h->peak_bytes = std::max<int64_t>(h->peak_bytes, (int64_t)(tb - fb));

@@ -557,25 +557,24 @@ __host__ __device__ inline int64_t tp_count_tiles(int64_t nr, int64_t nc, int64_
 constexpr int TP_GROUP = 8;
 __host__ __device__ inline void tp_tile_at(int64_t nr, int64_t nc, int64_t r0, int64_t c0, int64_t t, int64_t& px,
                                            int64_t& by) {
-  // first row tile of pair q, at most nr (non-decreasing in q)
-  auto first = [&](int64_t q) {
-    const int64_t f = tc_first_row_tile(2 * q, r0, c0);
-    return f < nr ? f : nr;
-  };
   const int64_t np = (nc + 1) / 2;
   for (int64_t p0 = 0; p0 < np; p0 += TP_GROUP) {
-    const int64_t g = np - p0 < TP_GROUP ? np - p0 : TP_GROUP;
+    const int g = (int)(np - p0 < TP_GROUP ? np - p0 : TP_GROUP);
+    int64_t f[TP_GROUP];  // first row tile of each pair of the group, at most nr (non-decreasing)
     int64_t cnt = 0;
-    for (int64_t j = 0; j < g; ++j) cnt += nr - first(p0 + j);
+    for (int j = 0; j < g; ++j) {
+      const int64_t fj = tc_first_row_tile(2 * (p0 + j), r0, c0);
+      f[j] = fj < nr ? fj : nr;
+      cnt += nr - f[j];
+    }
     if (t >= cnt) {
       t -= cnt;
       continue;
     }
-    // rows [first(p0), first(p0 + g - 1)): the pairs whose lower part reaches the row, in order
-    const int64_t flast = first(p0 + g - 1);
-    for (int64_t b = first(p0); b < flast; ++b) {
-      int64_t v = 0;
-      while (v < g && first(p0 + v) <= b) ++v;  // pairs p0 .. p0 + v - 1
+    // rows [f[0], f[g-1]): the pairs j with f[j] <= row, in order of j
+    int v = 0;
+    for (int64_t b = f[0]; b < f[g - 1]; ++b) {
+      while (v < g && f[v] <= b) ++v;  // pairs 0 .. v - 1 reach row b
       if (t < v) {
         px = p0 + t;
         by = b;
@@ -583,8 +582,8 @@ __host__ __device__ inline void tp_tile_at(int64_t nr, int64_t nc, int64_t r0, i
       }
       t -= v;
     }
-    // rows from flast: all g pairs
-    by = flast + t / g;
+    // rows from f[g-1]: all g pairs
+    by = f[g - 1] + t / g;
     px = p0 + t % g;
     return;
   }
