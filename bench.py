@@ -630,7 +630,7 @@ def run_profile_step(args, rv, torch):
             "learned": dict(precision="learned", mixed_flush=0, mixed_operands="bf16")}[args.profile_step]
     if args.profile_step == "learned":
         solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
-    opts = rv.FactorOptions(**form)
+    opts = rv.FactorOptions(far_field_sms=args.far_sms, **form)
     r = time_form(rv, torch, solver, s, b, opts, args.warmup, args.steps)
     p0 = solver.profile()  # host counters of the last timed step (no per-launch events)
     host = {k: p0[k] for k in ("host_total_ms", "host_sync_ms", "host_wait_ms", "host_gap_ms", "lf_misses")}
@@ -717,6 +717,8 @@ def main():
     ap.add_argument("--profile-step", default=None, choices=["plain", "tf32", "bf16", "learned"],
                     help="profiling aid: time only this form (factor + solve to 1e-14) on --config and print "
                          "its time and parts; no contract line")
+    ap.add_argument("--far-sms", type=int, default=-1,
+                    help="profiling step: SMs a window's far-field update leaves to the next blocks (0 = no split)")
     ap.add_argument("--bf16-flush", default="0",
                     help="the same for the mixed form with BF16 operand parts")
     args = ap.parse_args()

@@ -94,6 +94,12 @@ typedef struct {
    * redone dynamically, which records anew.  Results are the dynamic path's,
    * bit for bit.  Default 0. */
   int32_t graph_refactor;
+  /* Mixed form, large fronts: multiprocessors a full window's far-field
+   * update leaves to the next outer blocks while it runs on a second stream
+   * (no reference counterpart; scheduling only, results do not depend on
+   * it).  0 = no split (the whole window update before the next block),
+   * -1 = the default (24). */
+  int32_t far_field_sms;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */

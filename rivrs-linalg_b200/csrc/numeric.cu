@@ -1221,7 +1221,7 @@ struct LfCtx {
 // blocks) is updated on a second stream while those blocks are factored; the
 // GEMM leaves LF_FAR_SMS multiprocessors to their latency-bound kernels.
 constexpr int LF_FAR_AHEAD = 3;
-constexpr int LF_FAR_SMS = 24;
+constexpr int LF_FAR_SMS = 24;  // the default of rvg_options::far_field_sms
 constexpr int LF_CONCURRENT = 8;  // large fronts of a wave in flight at once
 
 struct rvg_handle {
@@ -1785,7 +1785,9 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   const bool profiling_marks = cx.marks && h->profiling;  // this front's launches carry the profiling events
   // (the far part starts LF_FAR_AHEAD blocks after the window's first W row: a whole number of the packed
   // window's 128-row tiles only when the block width is a multiple of 128)
-  const bool async_far = mixed && two_level && !profiling_marks && !h->replay && nb % TC_BM == 0;
+  const int far_sms = h->opt.far_field_sms < 0 ? LF_FAR_SMS : h->opt.far_field_sms;
+  const bool async_far = mixed && two_level && !profiling_marks && !h->replay && nb % TC_BM == 0 && far_sms > 0 &&
+                         far_sms < h->nsm;
   if (async_far && !cx.far_st) {
     if (tl_no_alloc) return no_alloc_fail();
     CK(cudaStreamCreateWithFlags(&cx.far_st, cudaStreamNonBlocking));
@@ -1909,7 +1911,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
             irc = irc ? irc : launch_window_gemm(h, cx, a, m, oe, split, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
                                                  nullptr, 0, mixed, skip);
             irc = irc ? irc : launch_window_gemm(h, cx, a, m, split, p, wd, wrow, F, pk_w, pk_l, kadd, bne_dev,
-                                                 nullptr, 0, mixed, skip, cx.far_st, h->nsm - LF_FAR_SMS);
+                                                 nullptr, 0, mixed, skip, cx.far_st, h->nsm - far_sms);
             ck(cudaEventRecord(cx.ev_far, cx.far_st), "cudaEventRecord (far-field join)");
             cx.far_launches++;
             I.far = true;
@@ -2681,6 +2683,7 @@ void rvg_default_options(rvg_options* o) {
   o->mixed_tile_cols = 256;
   o->mixed_operands = 0;
   o->graph_refactor = 0;
+  o->far_field_sms = -1;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347 (precision and below: no counterpart)
@@ -2708,6 +2711,7 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347 (precision a
     set_error("mixed_tile_cols must be 128 or 256");
     return RVG_ERR_INVALID_INPUT;
   }
+  if (o.far_field_sms < -1) { set_error("far_field_sms must be -1 (default), 0 (no split) or a count"); return RVG_ERR_INVALID_INPUT; }
   return RVG_OK;
 }
 
