@@ -277,11 +277,15 @@ def misprediction_of(p: np.ndarray, threshold: float, y: np.ndarray) -> dict:
                 rate=float(((route & ~safe) | (~route & safe)).sum() / n))
 
 
-def timed_solve(solver, system, opts: FactorOptions, b, tol=1e-14):
+def timed_solve(solver, system, opts: FactorOptions, b, tol=1e-14, warmup: int = 0):
     """Factor + solve to `tol` (refinement escalating to GMRES-IR; FP64
     refactorization when that stalls), timed on the host with the device
-    synchronised; returns a dict."""
+    synchronised, after `warmup` untimed runs (the first run with new
+    options also creates the handle and sizes its arenas); returns a dict."""
     import torch
+    for _ in range(warmup):
+        solver.factor(None, opts)
+        solver.solve_auto(b, tol=tol)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     solver.factor(None, opts)
