@@ -215,22 +215,25 @@ __global__ void __launch_bounds__(256) k_zero_cb_lower(const CbZeroItem* items, 
 
 // One warp per front: TPP on all k columns (small-leaf fronts, numeric.rs:
 // 1805; fronts with k < ib, factor.rs:360-362).
-__global__ void k_tpp(const int32_t* ids, int n, DFront* F, Arenas A, DevOpts o) {
-  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (w >= n) return;
-  __shared__ int cnt[8][2];
-  int wl = threadIdx.x >> 5;
-  int s = ids[w];
-  DFront fr = F[s];
-  if (lane == 0) { cnt[wl][0] = 0; cnt[wl][1] = 0; }
+// TPP on all k columns of front s by one warp; cnt: the warp's two shared counters.
+__device__ void warp_tpp_front(int s, DFront* F, const Arenas& A, const DevOpts& o, int* cnt) {
+  const int lane = threadIdx.x & 31;
+  const DFront fr = F[s];
+  if (lane == 0) { cnt[0] = 0; cnt[1] = 0; }
   __syncwarp();
   WarpTpp T{PanelView{A.panel + fr.panel, fr.m}, fr.m, fr.k, lane};
   int32_t* perm = A.idx + fr.idx + fr.m;
   DRec d{A.dtype + fr.dpos, A.ddiag + fr.dpos, A.doff + fr.dpos};
-  int64_t ne = T.run(0, fr.k, perm, d, &cnt[wl][0], &cnt[wl][1], o);
+  int64_t ne = T.run(0, fr.k, perm, d, &cnt[0], &cnt[1], o);
   __syncwarp();
-  if (lane == 0) { F[s].ne = (int32_t)ne; F[s].n1 = cnt[wl][0]; F[s].n2 = cnt[wl][1]; }
+  if (lane == 0) { F[s].ne = (int32_t)ne; F[s].n1 = cnt[0]; F[s].n2 = cnt[1]; }
+}
+
+__global__ void k_tpp(const int32_t* ids, int n, DFront* F, Arenas A, DevOpts o) {
+  int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= n) return;
+  __shared__ int cnt[8][2];
+  warp_tpp_front(ids[w], F, A, o, cnt[threadIdx.x >> 5]);
 }
 
 constexpr int NT = APTP_THREADS;  // threads of the CTA APTP kernel
@@ -787,18 +790,32 @@ __global__ void __launch_bounds__(NT) k_aptp(const int32_t* ids, int n, DFront* 
 // done.  The host lists the fronts largest first, so the long ones start
 // early and the short ones fill in behind them.  Which CTA factors a front
 // changes nothing in its result.
-__global__ void __launch_bounds__(NT) k_aptp_queue(const int32_t* ids, int n, int32_t* next, DFront* F, Arenas A,
-                                                   DevOpts o) {
+// One persistent launch for a wave's small and medium fronts: items
+// [0, na) are medium fronts (one CTA each, listed largest first), items
+// [na, na + ceil(nt / 8)) groups of 8 small fronts (TPP, one warp each),
+// taken in order from one atomic counter, so the small fronts fill the
+// multiprocessors the long medium fronts leave.  Which CTA or warp takes a
+// front changes nothing in its arithmetic.
+__global__ void __launch_bounds__(NT) k_front_queue(const int32_t* ids, int na, const int32_t* tids, int nt,
+                                                    int32_t* next, DFront* F, Arenas A, DevOpts o) {
+  static_assert(NT == 256, "a group of small fronts is one per warp of the CTA");
   __shared__ CtaShared sh;
   __shared__ int tpp_cnt[2];
+  __shared__ int wcnt[NT / 32][2];
   __shared__ int s_i;
+  const int ng = (nt + 7) / 8;
   for (;;) {
     if (threadIdx.x == 0) s_i = atomicAdd(next, 1);
     __syncthreads();
     const int i = s_i;
     __syncthreads();  // every thread has read s_i before thread 0 takes the next item
-    if (i >= n) break;
-    cta_aptp_front(sh, tpp_cnt, ids[i], F, A, o);
+    if (i >= na + ng) break;
+    if (i < na) {
+      cta_aptp_front(sh, tpp_cnt, ids[i], F, A, o);
+    } else {
+      const int wl = threadIdx.x >> 5, f = (i - na) * 8 + wl;
+      if (f < nt) warp_tpp_front(tids[f], F, A, o, wcnt[wl]);
+    }
   }
 }
 
@@ -2478,20 +2495,18 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
     }
     // ---- dense factorization
     mark(h, -1);
-    if (!tpp_ids.empty())
-      k_tpp<<<blocks_for(tpp_ids.size(), 8), 256, 0, st>>>((const int32_t*)(D + o_tpp), (int)tpp_ids.size(),
-                                                            h->d_fronts, A, dop);
-    mark(h, RVG_PART_TPP);
-    if (!aptp_ids.empty()) {
+    if (!tpp_ids.empty() || !aptp_ids.empty()) {
+      // the wave's small and medium fronts in one persistent launch (profiling: part "aptp")
       if (!h->aptp_ctas) {  // resident CTAs of the queue kernel on this device
         int occ = 0, sms = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_aptp_queue, NT, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_front_queue, NT, 0));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
         h->aptp_ctas = std::max(1, occ) * std::max(1, sms);
       }
-      const int na = (int)aptp_ids.size();
-      k_aptp_queue<<<(unsigned)std::min(na, h->aptp_ctas), NT, 0, st>>>((const int32_t*)(D + o_aptp), na,
-                                                                        (int32_t*)(D + o_q), h->d_fronts, A, dop);
+      const int na = (int)aptp_ids.size(), nt = (int)tpp_ids.size(), items = na + (nt + 7) / 8;
+      k_front_queue<<<(unsigned)std::min(items, h->aptp_ctas), NT, 0, st>>>(
+          (const int32_t*)(D + o_aptp), na, (const int32_t*)(D + o_tpp), nt, (int32_t*)(D + o_q), h->d_fronts, A,
+          dop);
     }
     mark(h, RVG_PART_APTP);
     if (learned) {  // the routes of the large fronts (the device is busy with the fronts queued above)
@@ -2583,8 +2598,8 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       const DFront& f = h->h_fronts[s];
       h->syrk_flops += 2.0 * (double)f.ne * (double)f.nfs * (double)(f.nfs + 1) / 2.0;
     }
-    h->launches += 1 + (int64_t)eitems.size() * 0 + (sitems.empty() ? 0 : 1) + (tpp_ids.empty() ? 0 : 1) +
-                   (aptp_ids.empty() ? 0 : 1) + (witems.empty() ? 0 : 1) + (gitems.empty() ? 0 : 1) + 2 +
+    h->launches += 1 + (int64_t)eitems.size() * 0 + (sitems.empty() ? 0 : 1) +
+                   ((tpp_ids.empty() && aptp_ids.empty()) ? 0 : 1) + (witems.empty() ? 0 : 1) + (gitems.empty() ? 0 : 1) + 2 +
                    (dly_ids.empty() ? 0 : 1) + (zitems.empty() ? 0 : 1);
     for (size_t q = 0; q < maxch; ++q) h->launches += eitems[q].empty() ? 0 : 1;
     if (h->profiling) {  // the device memory in use (profiling runs only: the query costs host time)
