@@ -65,8 +65,8 @@ typedef struct {
    * with rvg_solve_refine.  2 = learned: each large front takes the mixed
    * form or plain FP64 as the per-front selector (rvg_set_selector) predicts
    * from the features of the assembled front; a mixed front whose pivots grow
-   * past the selector's bound makes the whole factorization run again in
-   * FP64 (rvg_selector_stats). */
+   * past the selector's bound is assembled again and factored in FP64 at the
+   * end of its wave, before any parent reads it (rvg_selector_stats). */
   int32_t precision;
   /* Mixed form only: 32-deep K chunks per FP32 partial sum before it is
    * added in FP64 (1, 2, 4 or 8; 0 = one partial sum over the whole K range).
@@ -346,7 +346,7 @@ rvg_status rvg_mlp_adam(float* d_params, const float* d_grad, float* d_m, float*
 /* Installs a selector on a handle (host parameters, copied): fronts whose
  * probability is >= threshold take the mixed form; a mixed front whose
  * largest |D| entry exceeds growth_bound times its largest assembled |a|
- * triggers the FP64 refactorization. */
+ * is refactored in FP64 (that front alone). */
 rvg_status rvg_set_selector(rvg_handle* h, const float* params, int64_t nparams, float threshold,
                             double growth_bound);
 /* The large fronts of the last learned-precision factorization, one row of
