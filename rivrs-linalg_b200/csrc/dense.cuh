@@ -28,6 +28,18 @@ namespace rvg {
 // pivot codes: 1x1, first and second column of a 2x2 pair
 enum : int8_t { PT_DELAYED = 0, PT_1X1 = 1, PT_2X2 = 2, PT_2X2B = 3 };
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization may start while the kernel before it on the stream still
+// runs; chain_enter() is its first statement: it waits until that kernel has
+// completed and its stores are visible (a no-op for a plain launch), then lets
+// the next kernel of the stream be launched early in turn.  Every kernel that
+// may be launched this way calls it unconditionally, so completion is
+// transitive along the chain.
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct DevOpts {
   double threshold;
   double small;

@@ -179,6 +179,7 @@ template <int WR, int WC, int MINB, bool DEV = false>
 __global__ void __launch_bounds__(32 * WR * WC, MINB) k_syrk_dmma(SyrkArgs a) {
   using Cfg = DmmaCfg<WR, WC>;
   constexpr int NT = Cfg::NT, BM = Cfg::BM, BN = Cfg::BN, LDW = Cfg::LDW, LDL = Cfg::LDL;
+  if (DEV) chain_enter();  // the inner update runs in the large-front chain
   if (DEV) {
     const int64_t k = *a.dk, ts = k + *a.dbs;
     a.L += k * a.ldl;

@@ -77,6 +77,7 @@ __global__ void k_lf_init(LFState* st, int32_t* perm, int64_t p) {
 }
 
 __global__ void k_lf_begin_outer(LFArgs A) {
+  chain_enter();
   LFState* st = A.st;
   if (st->spec_bad) return;
   if (st->gne != (int32_t)A.cs) {  // issued for a start column the factorization did not reach
@@ -90,6 +91,7 @@ __global__ void k_lf_begin_outer(LFArgs A) {
 
 // complete pivoting on the diagonal block (1 CTA)
 __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   __shared__ CtaShared sh;
   LFState* st = A.st;
@@ -202,6 +204,7 @@ __device__ __forceinline__ void lf_w_row(const double* l, int64_t ld, int n, con
 // them is a compile-time constant)
 constexpr int LF_PANEL_T = 64;
 __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim;
@@ -298,6 +301,7 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
 // 2x2 boundary, restore of the failed diagonal part, failed x failed term,
 // D entries (1 CTA)
 __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim, bs = st->bs, k = st->k;
@@ -372,6 +376,7 @@ __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
 // trailing columns that follows is the DMMA GEMM (k_syrk_dmma with the
 // region start read from the device), the same fma chain per entry.
 __global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim;
@@ -413,6 +418,7 @@ __global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
 
 // delayed columns of the inner block to the end of the outer block (1 CTA)
 __global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int tid = threadIdx.x;
@@ -449,6 +455,7 @@ __global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
 // 0..cs (two_level_factor, factor.rs:2165-2181): 16 columns per CTA
 constexpr int LF_PROP_COLS = 16;
 __global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   extern __shared__ double buf[];  // bcols x LF_PROP_COLS
   const int64_t c0 = (int64_t)blockIdx.x * LF_PROP_COLS;
@@ -469,6 +476,7 @@ __global__ void __launch_bounds__(256) k_lf_prop(LFArgs A) {
 // W = L D for the rows below the outer block, over its bne eliminated
 // columns, appended to the pending window
 __global__ void __launch_bounds__(128) k_lf_w(LFArgs A) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   const int bne = A.st->bne;
   const int64_t oe = A.cs + A.bcols;
@@ -506,6 +514,7 @@ __device__ __forceinline__ void lf_swap_delayed(const LFArgs& A, int64_t cs, int
 // another stream, and the host issues the swap itself, k_lf_swap, once it has
 // seen the delay), the eliminated total.
 __global__ void __launch_bounds__(NT) k_lf_outer(LFArgs A, int64_t rem, int two_level, int swap) {
+  chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int tid = threadIdx.x;

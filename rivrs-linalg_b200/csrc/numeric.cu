@@ -32,6 +32,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -1281,6 +1282,7 @@ struct rvg_handle {
   int32_t* sf_sync = nullptr; size_t sf_sync_cap = 0; // solve: ticket counter and block flags of one wave
   double* sf_part = nullptr; size_t sf_part_cap = 0;   // backward solve: partial sums of one wave
   int nsm = 0;                                       // SMs of the device (persistent grids)
+  bool chain_pdl = true;                             // large-front chain kernels by programmatic dependent launch
   std::map<int64_t, int64_t> cb_free;                // offset -> length of the free ranges
   bool factored = false;
   bool need_presize = false;                         // arenas released by rvg_trim
@@ -1681,6 +1683,30 @@ bool front_mixed(const rvg_handle* h, int64_t s) {
   return s >= 0 && s < (int64_t)h->route.size() && h->route[s] != 0;
 }
 
+// A kernel of the large-front chain: with programmatic stream serialization
+// it may start while the previous kernel of the stream still runs (each chain
+// kernel waits for its predecessor in chain_enter() before any memory access),
+// which hides the launch gap between the chain's short dependent kernels.
+template <typename... KP, typename... AP>
+static void launch_chain(const rvg_handle* h, void (*kern)(KP...), dim3 grid, dim3 block, size_t smem,
+                         cudaStream_t st, AP... args) {
+  if (!h->chain_pdl) {
+    kern<<<grid, block, smem, st>>>(args...);
+    return;
+  }
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, kern, args...);  // a failure stays the thread's last error, checked as for <<<>>>
+}
+
 int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax, bool mixed) {
   cudaStream_t st = h->st;
   if (mixed) {
@@ -1847,7 +1873,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     I.cs = cs; I.bcols = bcols; I.oe = oe;
     a.cs = cs;
     a.bcols = bcols;
-    k_lf_begin_outer<<<1, 256, 0, st>>>(a);
+    launch_chain(h, k_lf_begin_outer, 1, 256, 0, st, a);
     mk(RVG_PART_LF_SETUP);
     const int64_t ninner = (bcols + ib - 1) / ib;
     // the inner block's trailing update: rows and columns from ts = k + bs
@@ -1866,22 +1892,23 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     gi.dbs = &a.st->bs;
     gi.skip = skip;
     for (int64_t it = 0; it < ninner; ++it) {
-      k_lf_block<<<1, NT, 0, st>>>(a);
+      launch_chain(h, k_lf_block, 1, NT, 0, st, a);
       mk(RVG_PART_LF_BLOCK);
-      k_lf_panel<<<blocks_for(bm, LF_PANEL_T), LF_PANEL_T, 0, st>>>(a);
+      launch_chain(h, k_lf_panel, blocks_for(bm, LF_PANEL_T), LF_PANEL_T, 0, st, a);
       mk(RVG_PART_LF_PANEL);
-      k_lf_post<<<1, 256, 0, st>>>(a);
+      launch_chain(h, k_lf_post, 1, 256, 0, st, a);
       mk(RVG_PART_LF_POST);
-      k_lf_wi<<<blocks_for(bm, 256), 256, 0, st>>>(a);
-      k_syrk_inner<<<syrk_grid(gi), G_T, G_SMEM, st>>>(gi);
+      launch_chain(h, k_lf_wi, blocks_for(bm, 256), 256, 0, st, a);
+      launch_chain(h, k_syrk_inner, syrk_grid(gi), G_T, G_SMEM, st, gi);
       mk(RVG_PART_LF_UPDATE);
-      k_lf_delay<<<1, NT, 0, st>>>(a);
+      launch_chain(h, k_lf_delay, 1, NT, 0, st, a);
       mk(RVG_PART_LF_DELAY);
     }
     cx.launches += 1 + 6 * ninner;
     if (two_level) {
       if (cs > 0) {
-        k_lf_prop<<<(unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256, (size_t)bcols * LF_PROP_COLS * 8, st>>>(a);
+        launch_chain(h, k_lf_prop, (unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256,
+                     (size_t)bcols * LF_PROP_COLS * 8, st, a);
         cx.launches++;
         mk(RVG_PART_LF_PROP);
       }
@@ -1893,7 +1920,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         a.wld = m - wrow;
         a.wrow0 = wrow;
         a.wcol0 = kadd;
-        k_lf_w<<<blocks_for(m - oe, 128), 128, 0, st>>>(a);
+        launch_chain(h, k_lf_w, blocks_for(m - oe, 128), 128, 0, st, a);
         cx.launches++;
         mk(RVG_PART_LF_W);
         // The next outer block is [g, g + min(rem - bcols, nb)); columns past
@@ -1950,7 +1977,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
         mk(RVG_PART_LF_SYRK);
       }
     }
-    k_lf_outer<<<1, NT, 0, st>>>(a, rem, two_level, async_far ? 0 : 1);
+    launch_chain(h, k_lf_outer, 1, NT, 0, st, a, rem, (int)two_level, async_far ? 0 : 1);
     cx.launches++;
     mk(RVG_PART_LF_OUTER);
     return I;
@@ -2801,6 +2828,10 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   CK(cudaFuncSetAttribute(k_syrk_tc<TC_NO_FLUSH, TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_tc_pair<TC_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP_SMEM));
   CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
+  {  // RVG_CHAIN_PDL=0 launches the large-front chain kernels plainly (same results; for timing comparisons)
+    const char* e = std::getenv("RVG_CHAIN_PDL");
+    h->chain_pdl = !(e && e[0] == '0');
+  }
   CK(cudaMallocAsync((void**)&h->d_err, sizeof(int32_t), st));
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
   CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
