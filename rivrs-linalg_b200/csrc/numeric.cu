@@ -1513,11 +1513,21 @@ DevOpts devopts(const rvg_options& o) {
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 // Columns of the pending window of a large front's deferred updates: LF_WINDOW
-// outer blocks, except in the mixed form when the outer block is not a whole
-// number of 128-row tiles (its packed TF32 operands are appended tile- and
-// chunk-aligned): then one block (every block's update applied at once).
+// outer blocks in plain FP64, LF_WINDOW_MIXED in the mixed form (a full
+// window's update reads and writes every trailing entry once in FP64 for K =
+// window columns of BF16 or TF32 products: at K = 1024 that C stream already
+// asks for most of the HBM bandwidth at the tensor cores' rate, so the mixed
+// form defers twice as deep), except in the mixed form when the outer block is
+// not a whole number of 128-row tiles (its packed operands are appended tile-
+// and chunk-aligned): then one block (every block's update applied at once).
 constexpr int64_t LF_WINDOW = 4;
-int64_t lf_window_cols(int64_t nb, bool mixed) { return (!mixed || nb % 128 == 0) ? LF_WINDOW * nb : nb; }
+constexpr int64_t LF_WINDOW_MIXED = 8;
+int64_t lf_window_cols(int64_t nb, bool mixed) {
+  return !mixed ? LF_WINDOW * nb : (nb % 128 == 0 ? LF_WINDOW_MIXED * nb : nb);
+}
+// outer blocks of window storage a large front's scratch holds (any front of the handle may take the mixed
+// form unless the precision is plain FP64)
+int64_t lf_window_blocks(const rvg_handle* h) { return h->opt.precision == 0 ? LF_WINDOW : LF_WINDOW_MIXED; }
 
 // Which fronts of a wave take the multi-kernel path (the whole GPU, one front
 // after another) instead of one CTA each: every front of order >= T, and
@@ -1556,7 +1566,7 @@ int presize_arenas(rvg_handle* h) {
       bool tpp = x.in_small_leaf || k < ib;
       bool large = front_is_large(m, tpp, T, mid);
       int64_t sc = tpp ? 0 : (2 * IBMAX * m + nb);
-      if (large) sc = m * (2 * IBMAX + LF_WINDOW * nb) + nb;
+      if (large) sc = m * (2 * IBMAX + lf_window_blocks(h) * nb) + nb;
       if (has_cb) sc = std::max<int64_t>(sc, nfs * k);
       sc_w += sc;
       if (x.parent >= 0) rel[w] = std::max<int64_t>(rel[w], P.height[x.parent]);
@@ -1806,7 +1816,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   a.wo = sc + 2 * m * IBMAX;
   const bool mixed = front_mixed(h, s);
   const int64_t F = lf_window_cols(nb, mixed);
-  a.lp = (int32_t*)(sc + m * (2 * IBMAX + LF_WINDOW * nb));
+  a.lp = (int32_t*)(sc + m * (2 * IBMAX + lf_window_blocks(h) * nb));
   a.nfsb = p;
   a.o = dop;
   const int two_level = p > nb;
@@ -2371,7 +2381,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
         const bool large = front_is_large(m, tpp, T, mid);
         if (large) f.flags |= FF_LARGE;
         int64_t sc = tpp ? 0 : (2 * IBMAX * m + h->opt.outer_block_size);
-        if (large) sc = m * (2 * IBMAX + LF_WINDOW * h->opt.outer_block_size) + h->opt.outer_block_size;
+        if (large) sc = m * (2 * IBMAX + lf_window_blocks(h) * h->opt.outer_block_size) + h->opt.outer_block_size;
         if (f.flags & FF_HAS_CB) sc = std::max<int64_t>(sc, nfs * k);
         f.scratch = scratch_need; scratch_need += sc;
       }
