@@ -573,7 +573,9 @@ def side_config(rv, torch, name, s, b, warmup, steps, selector=None, bf16_opts=N
                   "solves_after_first": r["solves_after_first"], "methods": r["methods"]}
         if "selector" in r:
             res[k]["selector"] = r["selector"]
-    ok = [k for k in res if res[k]["bwd_err"] <= 1e-14] or ["plain_fp64"]
+    # accurate forms with the plain form's (exact) inertia
+    ok = [k for k in res if res[k]["bwd_err"] <= 1e-14 and res[k]["inertia"] == res["plain_fp64"]["inertia"]]
+    ok = ok or ["plain_fp64"]
     chosen = min(ok, key=lambda k: res[k]["s_per_step"])
     solver._ensure_handle(forms[chosen])
     solver.set_profiling(True)
@@ -643,7 +645,7 @@ def run_profile_step(args, rv, torch):
             "learned": dict(precision="learned", mixed_flush=0, mixed_operands="bf16")}[args.profile_step]
     if args.profile_step == "learned":
         solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
-    opts = rv.FactorOptions(far_field_sms=args.far_sms, **form)
+    opts = rv.FactorOptions(far_field_sms=args.far_sms, mixed_window=args.mixed_window, **form)
     r = time_form(rv, torch, solver, s, b, opts, args.warmup, args.steps)
     p0 = solver.profile()  # host counters of the last timed step (no per-launch events)
     host = {k: p0[k] for k in ("host_total_ms", "host_sync_ms", "host_wait_ms", "host_gap_ms", "lf_misses")}
@@ -730,6 +732,8 @@ def main():
     ap.add_argument("--profile-step", default=None, choices=["plain", "tf32", "bf16", "learned"],
                     help="profiling aid: time only this form (factor + solve to 1e-14) on --config and print "
                          "its time and parts; no contract line")
+    ap.add_argument("--mixed-window", type=int, default=0,
+                    help="--profile-step: outer blocks per window of deferred mixed-form updates (0 = default)")
     ap.add_argument("--far-sms", type=int, default=-1,
                     help="profiling step: SMs a window's far-field update leaves to the next blocks (0 = no split)")
     ap.add_argument("--bf16-flush", default="0",
@@ -849,23 +853,31 @@ def main():
     for fl in [int(v) for v in args.mixed_flush.split(",") if v.strip()]:
         forms[f"mixed_flush{fl}"] = run_form("mixed", fl, "tf32", "auto")
     # the scheduling options of the BF16 form tuned on this pattern (results do not depend on them)
+    # and its window depth, which changes the arithmetic: a deeper window only with a faster factor + solve
+    # and the plain form's inertia
+    def window_step(o):
+        r = time_form(rv, torch, solver, s, b, o, 1, 1)
+        return r["s_per_step"], r["inertia"]
     tuned, tune_table = rv.autotune.autotune(solver, d_vals.data_ptr(), d_scal.data_ptr() if d_scal is not None else None,
                                              rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16"),
-                                             reps=1)
-    autotune_rep = {"candidates": [dict(c, factor_s=s_) for c, s_ in tune_table],
+                                             reps=1, step=window_step, expect_inertia=plain["inertia"])
+    autotune_rep = {"candidates": [dict(c, **({"step_s": s_} if c.get("step") else {"factor_s": s_}))
+                                   for c, s_ in tune_table],
                     "chosen": {"large_front_threshold": tuned.large_front_threshold,
-                               "mixed_tile_cols": tuned.mixed_tile_cols}}
+                               "mixed_tile_cols": tuned.mixed_tile_cols, "mixed_window": tuned.mixed_window}}
     for fl in [int(v) for v in args.bf16_flush.split(",") if v.strip()]:
-        extra = ({"large_front_threshold": tuned.large_front_threshold, "mixed_tile_cols": tuned.mixed_tile_cols}
-                 if fl == 0 else {})
+        extra = ({"large_front_threshold": tuned.large_front_threshold, "mixed_tile_cols": tuned.mixed_tile_cols,
+                  "mixed_window": tuned.mixed_window} if fl == 0 else {})
         forms[f"mixed_bf16_flush{fl}"] = run_form("mixed", fl, "bf16", "auto", **extra)
     if os.path.exists(SELECTOR) and not args.no_learned:
         # the shipped selector picks the form per large front (BF16 parts where it predicts safe, FP64 elsewhere)
         solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
         forms["learned_bf16_flush0"] = run_form("learned", 0, "bf16", "auto")
         forms["learned_bf16_flush0"]["selector"] = solver.selector_stats()
-    # the chosen form: the fastest that reaches the accuracy target (plain always does)
-    chosen_key = min((k for k, f in forms.items() if f["bwd"] <= 1e-14 or k == "plain_fp64"),
+    # the chosen form: the fastest that reaches the accuracy target with the plain form's inertia (plain always
+    # does)
+    chosen_key = min((k for k, f in forms.items()
+                      if (f["bwd"] <= 1e-14 and list(f["inertia"]) == list(plain["inertia"])) or k == "plain_fp64"),
                      key=lambda k: forms[k]["t"])
     chosen = forms[chosen_key]
     chosen_name = "plain" if chosen_key == "plain_fp64" else "mixed"
@@ -980,15 +992,18 @@ def main():
         rl_source = "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in the measured-peaks file)"
     achieved = (syrk_flops / (syrk_ms * 1e-3) / 1e12) if syrk_ms > 0 else None
     # DRAM traffic per launch: ncu dram__bytes_read.sum + dram__bytes_write.sum summed over EVERY k_syrk_tc_pair
-    # launch of one factorization of this workload (the BF16 form, one pass, full size): 970.0 GB for 8.62e13
-    # FP64-equivalent flops, i.e. 0.01125 bytes per flop, applied to this run's average launch
+    # launch of one factorization of this workload (the BF16 form, one pass, full size), per window depth:
+    # (bytes, FP64-equivalent flops) of that factorization, applied to this run's average launch
+    captured = {4: (970.0e9, 8.62055e13, 712), 8: (818.1e9, 8.59948e13, 591)}
     traffic = traffic_src = None
+    win = (chosen["opts"].mixed_window or 4) if chosen_name == "mixed" else None
     if chosen_name == "mixed" and chosen["opts"].mixed_operands == "bf16" and chosen["opts"].mixed_flush == 0 \
-            and chosen["syrk_launch"] and args.config == "kkt60":
-        traffic = 970.0e9 / 8.62055e13 * (chosen["syrk_flops"] / chosen["syrk_launch"])
+            and chosen["syrk_launch"] and args.config == "kkt60" and win in captured:
+        gb, fl, nl = captured[win]
+        traffic = gb / fl * (chosen["syrk_flops"] / chosen["syrk_launch"])
         traffic_src = ("ncu dram__bytes_read.sum + dram__bytes_write.sum over every k_syrk_tc_pair<BF16> launch of "
-                       "one factorization of this workload (970.0 GB for 8.62e13 FP64-equivalent flops), at this "
-                       "run's average launch")
+                       "one factorization of this workload at window depth %d (%.1f GB over %d launches for %.4g "
+                       "FP64-equivalent flops), at this run's average launch" % (win, gb / 1e9, nl, fl))
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         orc = entry.load_oracle()

@@ -100,6 +100,14 @@ typedef struct {
    * it).  0 = no split (the whole window update before the next block),
    * -1 = the default (24). */
   int32_t far_field_sms;
+  /* Mixed form, large fronts: outer blocks per window of deferred Schur
+   * updates (no reference counterpart), 1 to 8; 0 = the default, 4.  A deeper
+   * window reads and writes each trailing entry fewer times (faster where the
+   * update is bound by that traffic) but sums longer runs of products in
+   * FP32 before they reach FP64, so the mixed factor is less accurate; the
+   * autotuner (autotune.py) takes 8 only where a full factor + solve is faster
+   * and the inertia is unchanged. */
+  int32_t mixed_window;
 } rvg_options;
 
 /* FactorizationStats (sparse/src/symmetric/numeric.rs:661-719). */

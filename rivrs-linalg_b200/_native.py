@@ -31,7 +31,8 @@ class Options(C.Structure):
                 ("failed_pivot_tpp", C.c_int32), ("fallback_bk", C.c_int32), ("large_front_threshold", i64),
                 ("precision", C.c_int32), ("mixed_flush", C.c_int32),
                 ("mixed_tile_cols", C.c_int32), ("mixed_operands", C.c_int32),
-                ("graph_refactor", C.c_int32), ("far_field_sms", C.c_int32)]
+                ("graph_refactor", C.c_int32), ("far_field_sms", C.c_int32),
+                ("mixed_window", C.c_int32)]
 
 
 class Stats(C.Structure):

@@ -14,6 +14,14 @@ the candidates on the caller's own matrix with device-resident values (CUDA
 events on the handle's stream, best of `reps` after one warm-up) and returns
 the fastest; with `cache` set, results are kept in a JSON file keyed by the
 pattern's fingerprint, the precision and the device, so a pattern is tuned once.
+
+A third option changes the mixed factor's arithmetic: the window depth
+(`mixed_window`, outer blocks of deferred updates).  Deeper windows move less
+data and sum longer runs of products in FP32, so they are tried second, at the
+best cutoff and tile width, only when the caller gives `step` (options ->
+(seconds of one factor + solve to the caller's accuracy target, inertia)): a
+deeper window is taken only if its whole step is faster and its inertia equals
+`expect_inertia` (or, without it, the default window's).
 There is no counterpart in the reference (its CPU path has no such options).
 """
 from __future__ import annotations
@@ -29,6 +37,7 @@ from .solver import FactorOptions, SparseLDLT
 
 DEFAULT_THRESHOLDS = (1024, 2048, 4096)
 DEFAULT_TILE_COLS = (128, 256)
+DEFAULT_WINDOWS = (4, 8)
 
 
 def fingerprint(solver: SparseLDLT) -> str:
@@ -77,13 +86,34 @@ def _event_timer(solver: SparseLDLT, d_vals_ptr: int, d_scal_ptr: int | None, re
     return run
 
 
+def tune_window(best: FactorOptions, step, expect_inertia=None, windows=DEFAULT_WINDOWS):
+    """(options, [(candidate as a dict, step seconds, inertia, accepted)]):
+    the window depths tried at `best`'s other options; the default depth (the
+    first of `windows`) is always acceptable, a deeper one only with the same
+    inertia (expect_inertia, else the default depth's) and a faster step."""
+    rows = []
+    base_inertia = None
+    for i, w in enumerate(windows):
+        o = dataclasses.replace(best, mixed_window=int(w))
+        sec, inertia = step(o)
+        inertia = [int(v) for v in inertia]
+        if i == 0:
+            base_inertia = inertia
+        ref = list(expect_inertia) if expect_inertia is not None else base_inertia
+        rows.append(({"mixed_window": int(w)}, float(sec), inertia, i == 0 or inertia == [int(v) for v in ref]))
+    pick = min((r for r in rows if r[3]), key=lambda r: r[1])
+    return dataclasses.replace(best, **pick[0]), rows
+
+
 def autotune(solver: SparseLDLT, d_vals_ptr: int | None, d_scal_ptr: int | None, base: FactorOptions, reps: int = 2,
              thresholds=DEFAULT_THRESHOLDS, tile_cols=DEFAULT_TILE_COLS, cache: str | None = None, timer=None,
-             device_name: str | None = None):
+             device_name: str | None = None, step=None, expect_inertia=None, windows=DEFAULT_WINDOWS):
     """(best options, [(candidate options as a dict, seconds)]) for factoring
     the values at d_vals_ptr (device) with the solver's pattern.  `timer`
     (options -> seconds) replaces the CUDA-event timing, `device_name` the
-    current device's name in the cache key."""
+    current device's name in the cache key.  With `step` (mixed form without
+    flushing), the window depth is tuned afterwards (tune_window); its rows
+    follow the others in the table, with the step's seconds."""
     if device_name is None:
         import torch
         device_name = torch.cuda.get_device_name()
@@ -99,6 +129,10 @@ def autotune(solver: SparseLDLT, d_vals_ptr: int | None, d_scal_ptr: int | None,
         table.append(({"large_front_threshold": o.large_front_threshold, "mixed_tile_cols": o.mixed_tile_cols},
                       float(run(o))))
     choice = min(table, key=lambda r: r[1])[0]
+    if step is not None and base.precision != "fp64" and base.mixed_flush == 0 and len(windows) > 1:
+        best, rows = tune_window(dataclasses.replace(base, **choice), step, expect_inertia, windows)
+        choice = dict(choice, mixed_window=best.mixed_window)
+        table += [(dict(c, step=True, inertia=inr, accepted=ok), sec) for c, sec, inr, ok in rows]
     if cache:
         data = {}
         if os.path.exists(cache):

@@ -1513,21 +1513,25 @@ DevOpts devopts(const rvg_options& o) {
 unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
 // Columns of the pending window of a large front's deferred updates: LF_WINDOW
-// outer blocks in plain FP64, LF_WINDOW_MIXED in the mixed form (a full
+// outer blocks, or rvg_options::mixed_window of them in the mixed form (a full
 // window's update reads and writes every trailing entry once in FP64 for K =
 // window columns of BF16 or TF32 products: at K = 1024 that C stream already
-// asks for most of the HBM bandwidth at the tensor cores' rate, so the mixed
-// form defers twice as deep), except in the mixed form when the outer block is
-// not a whole number of 128-row tiles (its packed operands are appended tile-
-// and chunk-aligned): then one block (every block's update applied at once).
+// asks for most of the HBM bandwidth at the tensor cores' rate, so a deeper
+// window is faster, and less accurate), except in the mixed form when the
+// outer block is not a whole number of 128-row tiles (its packed operands are
+// appended tile- and chunk-aligned): then one block (every block's update
+// applied at once).
 constexpr int64_t LF_WINDOW = 4;
-constexpr int64_t LF_WINDOW_MIXED = 8;
-int64_t lf_window_cols(int64_t nb, bool mixed) {
-  return !mixed ? LF_WINDOW * nb : (nb % 128 == 0 ? LF_WINDOW_MIXED * nb : nb);
+constexpr int64_t LF_WINDOW_MAX = 8;
+int64_t lf_mixed_window(const rvg_handle* h) { return h->opt.mixed_window > 0 ? h->opt.mixed_window : LF_WINDOW; }
+int64_t lf_window_cols(const rvg_handle* h, int64_t nb, bool mixed) {
+  return !mixed ? LF_WINDOW * nb : (nb % 128 == 0 ? lf_mixed_window(h) * nb : nb);
 }
 // outer blocks of window storage a large front's scratch holds (any front of the handle may take the mixed
 // form unless the precision is plain FP64)
-int64_t lf_window_blocks(const rvg_handle* h) { return h->opt.precision == 0 ? LF_WINDOW : LF_WINDOW_MIXED; }
+int64_t lf_window_blocks(const rvg_handle* h) {
+  return h->opt.precision == 0 ? LF_WINDOW : std::max(LF_WINDOW, lf_mixed_window(h));
+}
 
 // Which fronts of a wave take the multi-kernel path (the whole GPU, one front
 // after another) instead of one CTA each: every front of order >= T, and
@@ -1815,7 +1819,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   a.w = sc + m * IBMAX;
   a.wo = sc + 2 * m * IBMAX;
   const bool mixed = front_mixed(h, s);
-  const int64_t F = lf_window_cols(nb, mixed);
+  const int64_t F = lf_window_cols(h, nb, mixed);
   a.lp = (int32_t*)(sc + m * (2 * IBMAX + lf_window_blocks(h) * nb));
   a.nfsb = p;
   a.o = dop;
@@ -2736,6 +2740,7 @@ void rvg_default_options(rvg_options* o) {
   o->mixed_operands = 0;
   o->graph_refactor = 0;
   o->far_field_sms = -1;
+  o->mixed_window = 0;
 }
 
 static int check_opts(const rvg_options& o) {  // factor.rs:307-347 (precision and below: no counterpart)
@@ -2764,6 +2769,10 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347 (precision a
     return RVG_ERR_INVALID_INPUT;
   }
   if (o.far_field_sms < -1) { set_error("far_field_sms must be -1 (default), 0 (no split) or a count"); return RVG_ERR_INVALID_INPUT; }
+  if (o.mixed_window < 0 || o.mixed_window > LF_WINDOW_MAX) {
+    set_error("mixed_window must be 0 (default) or 1 to 8 outer blocks");
+    return RVG_ERR_INVALID_INPUT;
+  }
   return RVG_OK;
 }
 

@@ -57,6 +57,7 @@ class FactorOptions:
     mixed_operands: str = "tf32"  # mixed form: FP64 operands split into two "tf32" or two "bf16" parts
     graph_refactor: bool = False  # refactorizations of one handle replayed as one CUDA graph (same pivoting)
     far_field_sms: int = -1  # mixed form: SMs a window's far-field update leaves to the next blocks (0 = no split)
+    mixed_window: int = 0  # mixed form: outer blocks per window of deferred updates, 1-8 (0 = default 4)
 
     def native(self) -> N.Options:
         return N.default_options(threshold=self.threshold, small=self.small,
@@ -68,7 +69,8 @@ class FactorOptions:
                                  precision={"fp64": 0, "mixed": 1, "learned": 2}[self.precision],
                                  mixed_flush=self.mixed_flush, mixed_tile_cols=self.mixed_tile_cols,
                                  mixed_operands={"tf32": 0, "bf16": 1}[self.mixed_operands],
-                                 graph_refactor=int(self.graph_refactor), far_field_sms=int(self.far_field_sms))
+                                 graph_refactor=int(self.graph_refactor), far_field_sms=int(self.far_field_sms),
+                                 mixed_window=int(self.mixed_window))
 
 
 class SparseError(RuntimeError):

@@ -28,11 +28,13 @@ def test_default_options_match_reference(rv):
     o = rv._native.default_options()
     assert (o.threshold, o.small, o.outer_block_size, o.inner_block_size, o.nemin, o.small_leaf_threshold,
             o.failed_pivot_tpp, o.fallback_bk) == (0.01, 1e-20, 256, 32, 32, 256, 1, 1)
+    assert (o.far_field_sms, o.mixed_window) == (-1, 0)  # scheduling options: their defaults
 
 
 @pytest.mark.parametrize("bad", [dict(threshold=0.0), dict(threshold=1.5), dict(small=-1.0),
                                  dict(outer_block_size=0), dict(inner_block_size=0),
-                                 dict(inner_block_size=64, outer_block_size=32)])
+                                 dict(inner_block_size=64, outer_block_size=32), dict(far_field_sms=-2),
+                                 dict(mixed_window=-1), dict(mixed_window=9)])
 def test_invalid_options_rejected(rv, bad):
     s = rv.problems.shifted_laplacian(3, 0.1)
     solver = rv.SparseLDLT.analyze(s)

@@ -275,3 +275,21 @@ def test_far_field_overlap_is_bit_identical(rv, case):
         x, its, err, how = solver.solve_auto(b)
         assert err <= 1e-14 and solver.inertia() == s.inertia
     solver.close()
+
+
+@pytest.mark.parametrize("window", [1, 2, 8])
+def test_window_depth_option(rv, window):
+    """mixed_window changes how many outer blocks of updates are deferred (and
+    so the FP32 partial sums' length): every depth reaches 1e-14 after
+    refinement with the exact inertia, with and without the far-field split,
+    on a KKT whose large fronts span several full windows."""
+    s = rv.problems.kkt(26, seed=4)
+    b = rv.problems.rhs_normal(s.n, 6)
+    solver = rv.SparseLDLT.analyze_with_matrix(s, rv.AnalyzeOptions(rv.OrderingStrategy.MATCH_ORDER_METIS))
+    for far in (-1, 0):
+        solver.factor(None, rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16",
+                                             large_front_threshold=512, mixed_window=window, far_field_sms=far))
+        assert tuple(solver.inertia()) == tuple(s.inertia)
+        x, its, err, how = solver.solve_auto(b)
+        assert err <= 1e-14 and rv.problems.backward_error(s, x, b) <= 1e-14, (window, far, its, how)
+    solver.close()
