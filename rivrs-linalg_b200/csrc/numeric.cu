@@ -1235,10 +1235,9 @@ struct LfCtx {
   cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
   int64_t far_launches = 0;
 };
-// A full window's far field (the columns after the next LF_FAR_AHEAD outer
-// blocks) is updated on a second stream while those blocks are factored; the
-// GEMM leaves LF_FAR_SMS multiprocessors to their latency-bound kernels.
-constexpr int LF_FAR_AHEAD = 3;
+// A full window's far field (the columns after the next window's blocks but
+// its last) is updated on a second stream while those blocks are factored;
+// the GEMM leaves LF_FAR_SMS multiprocessors to their latency-bound kernels.
 constexpr int LF_FAR_SMS = 24;  // the default of rvg_options::far_field_sms
 constexpr int LF_CONCURRENT = 8;  // large fronts of a wave in flight at once
 
@@ -1840,8 +1839,11 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   // far-field updates beside the next blocks: the mixed form in the dynamic schedule (not while
   // recording profiling marks, not inside a captured graph)
   const bool profiling_marks = cx.marks && h->profiling;  // this front's launches carry the profiling events
-  // (the far part starts LF_FAR_AHEAD blocks after the window's first W row: a whole number of the packed
-  // window's 128-row tiles only when the block width is a multiple of 128)
+  // (the far part starts far_ahead blocks after the window's first W row: a whole number of the packed
+  // window's 128-row tiles only when the block width is a multiple of 128).  The far part of a flush
+  // runs beside every block of the next window but its last, whose near-field update writes the first
+  // far-field columns and so waits for it.
+  const int64_t far_ahead = std::max<int64_t>(1, F / nb - 1);
   const int far_sms = h->opt.far_field_sms < 0 ? LF_FAR_SMS : h->opt.far_field_sms;
   const bool async_far = mixed && two_level && !profiling_marks && !h->replay && nb % TC_BM == 0 && far_sms > 0 &&
                          far_sms < h->nsm;
@@ -1960,9 +1962,9 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
           I.waited = true;
         }
         if (I.flush) {
-          const int64_t split = oe + LF_FAR_AHEAD * nb;
+          const int64_t split = oe + far_ahead * nb;
           if (async_far && p - split >= 2 * nb) {
-            // the next LF_FAR_AHEAD blocks' columns now, the rest on the far stream beside them (both
+            // the next far_ahead blocks' columns now, the rest on the far stream beside them (both
             // after the packs; they touch different columns)
             ck(cudaEventRecord(cx.ev_fork, st), "cudaEventRecord (far-field fork)");
             ck(cudaStreamWaitEvent(cx.far_st, cx.ev_fork, 0), "cudaStreamWaitEvent (far-field fork)");
@@ -2005,7 +2007,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
       S.wrow = g + std::min(S.rem - I.bcols, nb);
     }
     if (I.flush) S.par ^= 1;
-    S.far_due = I.far ? (int64_t)I.before.outer + LF_FAR_AHEAD : (I.waited ? -1 : I.before.far_due);
+    S.far_due = I.far ? (int64_t)I.before.outer + far_ahead : (I.waited ? -1 : I.before.far_due);
     S.gne = g;
     S.rem -= I.bcols;
     S.outer += 1;

@@ -236,25 +236,30 @@ def test_auto_refinement_escalates_only_when_needed(rv):
     solver.close()
 
 
-@pytest.mark.parametrize("case", ["dense_delay", "kkt26"])
-def test_far_field_overlap_is_bit_identical(rv, case):
-    """A full window's far-field update runs on a second stream beside the next three outer blocks, and a
-    delayed block's far-field update and swap wait until the host has seen the delay; the factor equals
-    the one-block-at-a-time schedule of the profiling mode (no second stream) bit for bit."""
+@pytest.mark.parametrize("case,window", [("dense_delay", 0), ("kkt26", 0), ("dense_delay", 8), ("kkt26", 8)])
+def test_far_field_overlap_is_bit_identical(rv, case, window):
+    """A full window's far-field update runs on a second stream beside the next window's outer blocks but
+    its last (three at the default depth, seven at eight), and a delayed block's far-field update and swap
+    wait until the host has seen the delay; the factor equals the one-block-at-a-time schedule of the
+    profiling mode (no second stream) bit for bit."""
     import numpy as np
     if case == "dense_delay":
+        # order 4000 at the default depth; at eight blocks the far part of the first full window (from column
+        # 2048 + 7 * 256) needs more trailing columns
+        n = 4000 if window == 0 else 6000
         rng = np.random.default_rng(4000)
-        a = rng.standard_normal((4000, 4000))
+        a = rng.standard_normal((n, n))
         a = a + a.T
         weak = np.arange(2050, 2114)  # rows and columns scaled down: their block's pivots fail the threshold test
         a[weak, :] *= 1e-3
         a[:, weak] *= 1e-3
-        s = rv.problems.from_scipy("dense4000_delay", a)
-        opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16", large_front_threshold=33)
+        s = rv.problems.from_scipy(f"dense{n}_delay", a)
+        opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16", large_front_threshold=33,
+                                mixed_window=window)
         solver = rv.SparseLDLT.analyze(s)
     else:
         s = rv.problems.kkt(26, seed=26)
-        opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16")
+        opts = rv.FactorOptions(precision="mixed", mixed_flush=0, mixed_operands="bf16", mixed_window=window)
         solver = rv.SparseLDLT.analyze_with_matrix(s, rv.AnalyzeOptions(rv.OrderingStrategy.MATCH_ORDER_METIS))
     solver.factor(None, opts)
     far = solver.profile()["lf_far_updates"]
