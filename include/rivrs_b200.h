@@ -274,7 +274,7 @@ enum {
   RVG_PART_LF_SETUP = 0,   /* per-front and per-outer-block bookkeeping */
   RVG_PART_LF_BLOCK = 1,   /* 32x32 diagonal block, complete pivoting */
   RVG_PART_LF_PANEL = 2,   /* TRSM + D^-1 of the rows below, threshold test */
-  RVG_PART_LF_POST = 3,    /* first failing column */
+  RVG_PART_LF_POST = 3,    /* (unused: the first failing column is handled inside LF_UPDATE) */
   RVG_PART_LF_UPDATE = 4,  /* rank-32 update inside the outer block */
   RVG_PART_LF_DELAY = 5,   /* delayed columns to the end */
   RVG_PART_LF_PROP = 6,    /* row order propagated to earlier columns */

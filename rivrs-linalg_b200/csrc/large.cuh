@@ -5,18 +5,21 @@
 // device, so the host issues a fixed launch sequence:
 //
 //   per 32-column inner block (view-local position k):
-//     lf_block   1 CTA    complete pivoting on the diagonal block, row
-//                         permutation of the outer block's earlier columns
+//     lf_block   1 CTA    the previous inner block's delayed columns to the
+//                         end of the outer block (lf_delay_cta), complete
+//                         pivoting on the diagonal block, row permutation of
+//                         the outer block's earlier columns
 //     lf_panel   grid     backup, column permutation, TRSM, D^-1 scaling and
 //                         the a-posteriori threshold scan of every panel row
-//     lf_post    1 CTA    2x2 boundary adjustment, restore of the failed part
-//                         of the diagonal block, failed x failed cross term,
-//                         D entries
-//     lf_wi      grid     restore of the failed panel columns, W = L D, the
-//                         trailing x failed cross term
+//     lf_wi      grid     CTA 0 first (lf_post_cta): 2x2 boundary adjustment,
+//                         restore of the failed part of the diagonal block,
+//                         failed x failed cross term, D entries; then every
+//                         CTA: restore of the failed panel columns, W = L D,
+//                         the trailing x failed cross term
 //     k_syrk_dmma         rank-nelim update of the outer block's trailing
 //                         columns (region start read from the device)
-//     lf_delay   1 CTA    delayed columns to the end of the outer block
+//   after the last inner block:
+//     lf_delay   1 CTA    its delayed columns to the end of the outer block
 //   per 256-column outer block:
 //     lf_prop    grid     row permutation of the front's earlier columns
 //     lf_w       grid     W = L D for the rows below the outer block, into
@@ -89,10 +92,18 @@ __global__ void k_lf_begin_outer(LFArgs A) {
   for (int i = threadIdx.x; i < A.bcols; i += blockDim.x) A.lp[i] = i;
 }
 
-// complete pivoting on the diagonal block (1 CTA)
-__global__ void __launch_bounds__(NT) k_lf_block(LFArgs A) {
+__device__ void lf_delay_cta(const LFArgs& A);
+
+// complete pivoting on the diagonal block (1 CTA); with after_delay set it
+// first moves the previous inner block's delayed columns to the end of the
+// outer block (lf_delay_cta, that block's last step)
+__global__ void __launch_bounds__(NT) k_lf_block(LFArgs A, int after_delay) {
   chain_enter();
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
+  if (after_delay) {
+    lf_delay_cta(A);
+    __syncthreads();
+  }
   __shared__ CtaShared sh;
   LFState* st = A.st;
   const int tid = threadIdx.x;
@@ -299,10 +310,11 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
 }
 
 // 2x2 boundary, restore of the failed diagonal part, failed x failed term,
-// D entries (1 CTA)
-__global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
-  chain_enter();
-  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
+// D entries: one CTA of 256 threads (CTA 0 of k_lf_wi, before its rows).  It
+// writes only the block's own rows, the D entries and the counters; the
+// adjusted eliminated count it stores in st->eff / st->nelim is the one every
+// CTA of k_lf_wi derives from st->eff itself (the adjustment is idempotent).
+__device__ __forceinline__ void lf_post_cta(const LFArgs& A) {
   LFState* st = A.st;
   const int bnelim = st->bnelim, bs = st->bs, k = st->k;
   const int tid = threadIdx.x;
@@ -328,21 +340,26 @@ __global__ void __launch_bounds__(256) k_lf_post(LFArgs A) {
     for (int t = tid; t < nf * nf; t += blockDim.x) {
       int i = t % nf, j = t / nf;
       if (i < j) continue;
-      double wb[IBMAX];
+      // sum over the eliminated columns c of (L D)(row i, c) * L(row j, c), each W entry formed as it is
+      // added (no local array), in column order
       const double* l = &V(k + nelim + i, k);
+      const double* lj = &V(k + nelim + j, k);
+      double s = 0.0;
       int c = 0;
       while (c < nelim) {
-        if (st->bdt[c] == PT_1X1) { wb[c] = __dmul_rn(l[c * A.m], st->bdd[c]); c += 1; }
-        else {
-          double A_ = st->bdd[c], B_ = st->bdo[c], C_ = st->bdd[c + 1];
-          double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
-          wb[c] = __dadd_rn(__dmul_rn(l1, A_), __dmul_rn(l2, B_));
-          wb[c + 1] = __dadd_rn(__dmul_rn(l1, B_), __dmul_rn(l2, C_));
+        if (st->bdt[c] == PT_1X1) {
+          s = __dadd_rn(s, __dmul_rn(__dmul_rn(l[c * A.m], st->bdd[c]), lj[c * A.m]));
+          c += 1;
+        } else {
+          const double A_ = st->bdd[c], B_ = st->bdo[c], C_ = st->bdd[c + 1];
+          const double l1 = l[c * A.m], l2 = l[(c + 1) * A.m];
+          const double w0 = __dadd_rn(__dmul_rn(l1, A_), __dmul_rn(l2, B_));
+          const double w1 = __dadd_rn(__dmul_rn(l1, B_), __dmul_rn(l2, C_));
+          s = __dadd_rn(s, __dmul_rn(w0, lj[c * A.m]));
+          s = __dadd_rn(s, __dmul_rn(w1, lj[(c + 1) * A.m]));
           c += 2;
         }
       }
-      double s = 0.0;
-      for (int c2 = 0; c2 < nelim; ++c2) s = __dadd_rn(s, __dmul_rn(wb[c2], V(k + nelim + j, k + c2)));
       V(k + nelim + i, k + nelim + j) = __dsub_rn(V(k + nelim + i, k + nelim + j), s);
     }
   }
@@ -380,46 +397,54 @@ __global__ void __launch_bounds__(256) k_lf_wi(LFArgs A) {
   if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
   LFState* st = A.st;
   const int bnelim = st->bnelim;
-  if (bnelim == 0) return;
-  const int bs = st->bs, k = st->k, nelim = st->nelim, eff = st->eff;
-  const int64_t bm = A.m - A.cs;
-  const int64_t ts = k + bs;
-  const int nf = bs - nelim;
-  __shared__ double Ls[IBMAX][IBMAX + 1];
-  __shared__ int bperm[IBMAX];
-  __shared__ int8_t bdt[IBMAX];
-  __shared__ double bdd[IBMAX], bdo[IBMAX];
-  PanelView V{A.a + A.cs + A.cs * A.m, A.m};
-  if (threadIdx.x < IBMAX) {
-    bperm[threadIdx.x] = st->bperm[threadIdx.x];
-    bdt[threadIdx.x] = st->bdt[threadIdx.x];
-    bdd[threadIdx.x] = st->bdd[threadIdx.x];
-    bdo[threadIdx.x] = st->bdo[threadIdx.x];
-  }
-  if (nelim > 0 && nf > 0)
-    for (int t = threadIdx.x; t < nf * nelim; t += blockDim.x) {
-      int jj = t % nf, c = t / nf;
-      Ls[jj][c] = V(k + nelim + jj, k + c);
+  if (bnelim > 0) {
+    const int bs = st->bs, k = st->k;
+    // the eliminated count: the panel's first failing column, one less where it would split a 2x2 (the
+    // value CTA 0 stores below)
+    int eff = st->eff;
+    if (eff > 0 && st->bdt[eff - 1] == PT_2X2) eff -= 1;
+    const int nelim = eff;
+    const int64_t bm = A.m - A.cs;
+    const int64_t ts = k + bs;
+    const int nf = bs - nelim;
+    __shared__ double Ls[IBMAX][IBMAX + 1];
+    __shared__ int bperm[IBMAX];
+    __shared__ int8_t bdt[IBMAX];
+    __shared__ double bdd[IBMAX], bdo[IBMAX];
+    PanelView V{A.a + A.cs + A.cs * A.m, A.m};
+    if (threadIdx.x < IBMAX) {
+      bperm[threadIdx.x] = st->bperm[threadIdx.x];
+      bdt[threadIdx.x] = st->bdt[threadIdx.x];
+      bdd[threadIdx.x] = st->bdd[threadIdx.x];
+      bdo[threadIdx.x] = st->bdo[threadIdx.x];
     }
-  __syncthreads();
-  const int64_t i = ts + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= bm) return;
-  if (eff < bnelim)
-    for (int j = eff; j < bs; ++j) V(i, k + j) = A.pb[i + (int64_t)bperm[j] * bm];
-  if (nelim == 0) return;
-  double* W = A.w + i;
-  lf_w_row(&V(i, k), A.m, nelim, bdt, bdd, bdo, W, bm);
-  for (int jj = 0; jj < nf; ++jj) {
-    double s = 0.0;
-    for (int c2 = 0; c2 < nelim; ++c2) s = __dadd_rn(s, __dmul_rn(W[(int64_t)c2 * bm], Ls[jj][c2]));
-    V(i, k + nelim + jj) = __dsub_rn(V(i, k + nelim + jj), s);
+    if (nelim > 0 && nf > 0)
+      for (int t = threadIdx.x; t < nf * nelim; t += blockDim.x) {
+        int jj = t % nf, c = t / nf;
+        Ls[jj][c] = V(k + nelim + jj, k + c);
+      }
+    __syncthreads();
+    const int64_t i = ts + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < bm) {
+      if (eff < bnelim)
+        for (int j = eff; j < bs; ++j) V(i, k + j) = A.pb[i + (int64_t)bperm[j] * bm];
+      if (nelim > 0) {
+        double* W = A.w + i;
+        lf_w_row(&V(i, k), A.m, nelim, bdt, bdd, bdo, W, bm);
+        for (int jj = 0; jj < nf; ++jj) {
+          double s = 0.0;
+          for (int c2 = 0; c2 < nelim; ++c2) s = __dadd_rn(s, __dmul_rn(W[(int64_t)c2 * bm], Ls[jj][c2]));
+          V(i, k + nelim + jj) = __dsub_rn(V(i, k + nelim + jj), s);
+        }
+      }
+    }
   }
+  // the block's own rows, its D entries and counts (CTA 0, after its rows: the two touch different rows)
+  if (blockIdx.x == 0) lf_post_cta(A);  // uniform over the CTA
 }
 
 // delayed columns of the inner block to the end of the outer block (1 CTA)
-__global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
-  chain_enter();
-  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
+__device__ void lf_delay_cta(const LFArgs& A) {
   LFState* st = A.st;
   const int tid = threadIdx.x;
   const int k = st->k, bs = st->bs, bnelim = st->bnelim, nelim = st->nelim;
@@ -449,6 +474,12 @@ __global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
   }
   __syncthreads();
   if (tid == 0) { st->k = k + nelim; st->end_pos = end_pos; st->bne = k + nelim; }
+}
+// the last inner block's delays (the others run at the start of the next k_lf_block)
+__global__ void __launch_bounds__(NT) k_lf_delay(LFArgs A) {
+  chain_enter();
+  if (A.st->spec_bad) return;  // a block issued past a mispredicted start column
+  lf_delay_cta(A);
 }
 
 // row permutation of the outer block applied to the front's earlier columns

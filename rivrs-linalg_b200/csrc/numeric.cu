@@ -1907,20 +1907,21 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
     gi.dk = &a.st->k;
     gi.dbs = &a.st->bs;
     gi.skip = skip;
+    // per inner block: the diagonal block (after the previous inner block's delays), the panel rows, the
+    // post-processing with W = L D (k_lf_wi, its CTA 0 doing the block's own rows and D entries), the
+    // rank-nelim update; the last inner block's delays on their own
     for (int64_t it = 0; it < ninner; ++it) {
-      launch_chain(h, k_lf_block, 1, NT, 0, st, a);
+      launch_chain(h, k_lf_block, 1, NT, 0, st, a, it > 0 ? 1 : 0);
       mk(RVG_PART_LF_BLOCK);
       launch_chain(h, k_lf_panel, blocks_for(bm, LF_PANEL_T), LF_PANEL_T, 0, st, a);
       mk(RVG_PART_LF_PANEL);
-      launch_chain(h, k_lf_post, 1, 256, 0, st, a);
-      mk(RVG_PART_LF_POST);
       launch_chain(h, k_lf_wi, blocks_for(bm, 256), 256, 0, st, a);
       launch_chain(h, k_syrk_inner, syrk_grid(gi), G_T, G_SMEM, st, gi);
       mk(RVG_PART_LF_UPDATE);
-      launch_chain(h, k_lf_delay, 1, NT, 0, st, a);
-      mk(RVG_PART_LF_DELAY);
     }
-    cx.launches += 1 + 6 * ninner;
+    launch_chain(h, k_lf_delay, 1, NT, 0, st, a);
+    mk(RVG_PART_LF_DELAY);
+    cx.launches += 2 + 4 * ninner;
     if (two_level) {
       if (cs > 0) {
         launch_chain(h, k_lf_prop, (unsigned)((cs + LF_PROP_COLS - 1) / LF_PROP_COLS), 256,
