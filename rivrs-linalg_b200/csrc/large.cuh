@@ -146,16 +146,7 @@ __global__ void __launch_bounds__(NT) k_lf_block(LFArgs A, int after_delay) {
         else bc += 1;
       }
     }
-    // row permutation of the view columns 0..k (step 5): all loads of a column
-    // before its stores
-    for (int64_t c = tid; c < k; c += NT) {
-      double buf[IBMAX];
-#pragma unroll
-      for (int i = 0; i < IBMAX; ++i) buf[i] = i < bs ? V(k + sh.bperm[i], c) : 0.0;
-#pragma unroll
-      for (int i = 0; i < IBMAX; ++i)
-        if (i < bs) V(k + i, c) = buf[i];
-    }
+    // (the row permutation of the view columns 0..k, step 5, is done by k_lf_panel's threads c < k)
     if (tid < 32) {  // column order (step 6): lane i takes the entry of lane bperm[i]
       const int32_t ob = tid < bs ? A.lp[k + tid] : 0;
       const int32_t nbv = __shfl_sync(0xffffffffu, ob, sh.bperm[tid] & 31);
@@ -259,6 +250,17 @@ __global__ void __launch_bounds__(LF_PANEL_T) k_lf_panel(LFArgs A) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t be = k + bs;
   const double bound = 1.0 / A.o.threshold;
+  if (r < k) {
+    // the block's row permutation applied to the view's earlier column r (step 5 of the block, left to
+    // the threads that have no panel row: they touch rows k .. be of columns before k, which no other
+    // thread of this launch reads); all loads of the column before its stores
+    double buf[IBMAX];
+#pragma unroll
+    for (int i = 0; i < IBMAX; ++i) buf[i] = i < bs ? V(k + bperm[i], r) : 0.0;
+#pragma unroll
+    for (int i = 0; i < IBMAX; ++i)
+      if (i < bs) V(k + i, r) = buf[i];
+  }
   if (r >= be && r < bm) {
     // every load of the row before the first store: the backup may alias the
     // panel as far as the compiler knows, so a load placed after a store
