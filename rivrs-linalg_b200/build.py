@@ -6,7 +6,11 @@ CUDA sources are compiled with `-gencode arch=compute_100a,code=sm_100a` and
 `--fmad=false`: the kernels place every fused multiply-add explicitly
 (`__fma_rn`) where the arithmetic contract calls for one, and nothing else
 may be contracted.  Host C++ is compiled with `-ffp-contract=off` for the
-same reason.
+same reason.  The selector network's training kernels (`mlp.cu`: forward for
+prediction, gradient, Adam) have no bit-for-bit contract (they are checked
+against a float64 oracle within tolerances), so they are compiled with
+`--fmad=true`; the network's inference during a factorization is part of
+`numeric.cu` and keeps the contract.
 """
 import os
 import subprocess
@@ -20,8 +24,9 @@ BUILD = os.path.join(HERE, "_build")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+CU_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
             "-I", os.path.join(ROOT, "include")] + ARCH
+CU_FMAD = {"mlp.cu": True}  # sources without the exact-arithmetic contract (default: --fmad=false)
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", os.path.join(ROOT, "include")]
 
 CU_SOURCES = ["numeric.cu", "noalloc.cu", "mlp.cu"]
@@ -51,8 +56,9 @@ def build(verbose=False):
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
-        if _stale(o, [s] + headers):
-            _run([NVCC] + CU_FLAGS + ["-c", s, "-o", o])
+        if _stale(o, [s] + headers + [os.path.abspath(__file__)]):
+            fmad = "--fmad=true" if CU_FMAD.get(src) else "--fmad=false"
+            _run([NVCC] + CU_FLAGS + [fmad, "-c", s, "-o", o])
         objs.append(o)
     for src in CXX_SOURCES:
         s = os.path.join(CSRC, src)
