@@ -1064,7 +1064,7 @@ def main():
             "phases_ms": {k: prof[k] for k in ("factor_ms", "solve_ms", "assembly_ms", "dense_ms", "cbgemm_ms",
                                                "host_total_ms", "host_alloc_ms", "host_sync_ms", "host_wait_ms",
                                                "host_gap_ms")},
-            "phases_note": ("host_sync_ms: the host blocked at the 14 wave boundaries while the device runs the wave "
+            "phases_note": ("host_sync_ms: the host blocked at each wave boundary while the device runs the wave "
                             "(it needs the wave's eliminated counts to lay out the next one); host_wait_ms: the "
                             "large-front threads blocked behind outer blocks issued ahead (summed over threads); "
                             "host_gap_ms: the only time the device has nothing of the factorization queued"),
