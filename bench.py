@@ -888,23 +888,28 @@ def main():
     bwd, inertia, stats, prof = chosen["bwd"], chosen["inertia"], chosen["stats"], chosen["prof"]
     times, walls = chosen["times"], chosen["walls"]
 
-    # end to end through the public API with host buffers (the chosen form)
+    # end to end through the public API with host buffers (the chosen form): values and right-hand side in
+    # pinned host memory, copied to the device inside the timed region by rvg_factor / the solve, the solution
+    # copied back; one untimed call first (the handle for these options and its arenas are set up there)
     e2e_times = []
     xh = None
     opts = chosen["opts"]
     solver._ensure_handle(opts)
-    for _ in range(max(1, min(args.steps, 3))):
+    vals_pinned = torch.from_numpy(s.values).pin_memory().numpy()
+    b_pinned = torch.from_numpy(b).pin_memory().numpy()
+    for it in range(1 + max(1, min(args.steps, 3))):
         barrier()
         t0 = time.perf_counter()
-        solver.factor(s.values, opts)
+        solver.factor(vals_pinned, opts)
         if chosen["method"] == "gmres":
-            xh, _, _ = solver.solve_gmres(b, tol=1e-14, max_iter=100, restart=30)
+            xh, _, _ = solver.solve_gmres(b_pinned, tol=1e-14, max_iter=100, restart=30)
         elif chosen["method"] == "auto":
-            xh, _, _, _ = solver.solve_auto(b, tol=1e-14, max_iter=100)
+            xh, _, _, _ = solver.solve_auto(b_pinned, tol=1e-14, max_iter=100)
         else:
-            xh, _, _ = solver.solve_refine(b, tol=1e-14, max_iter=10)
+            xh, _, _ = solver.solve_refine(b_pinned, tol=1e-14, max_iter=10)
         torch.cuda.synchronize()
-        e2e_times.append(time.perf_counter() - t0)
+        if it > 0:
+            e2e_times.append(time.perf_counter() - t0)
     e2e = max_over_ranks(statistics.mean(e2e_times))
     bwd_e2e = rv.problems.backward_error(s, xh, b)
 
