@@ -26,6 +26,7 @@
 // -> dense factorization (warp TPP or CTA APTP) -> contribution GEMM.  One
 // small device->host copy per wave returns the eliminated counts that size
 // the next wave (delays change front sizes at run time).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,6 +40,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include <thread>
@@ -1234,6 +1236,7 @@ struct LfCtx {
   cudaStream_t far_st = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
   int64_t far_launches = 0;
+  int id = 0;  // position in the handle's contexts (its window buffer's address-stable arena)
 };
 // A full window's far field (the columns after the next window's blocks but
 // its last) is updated on a second stream while those blocks are factored;
@@ -1241,9 +1244,12 @@ struct LfCtx {
 constexpr int LF_FAR_SMS = 24;  // the default of rvg_options::far_field_sms
 constexpr int LF_CONCURRENT = 8;  // large fronts of a wave in flight at once
 
+struct VmArenas;
+
 struct rvg_handle {
   Plan P;
   rvg_options opt;
+  VmArenas* vm = nullptr;  // address-stable arenas (graph_refactor = 2), else nullptr
   int device = 0;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[8] = {};
@@ -1402,7 +1408,9 @@ int ensure_host(char*& p, size_t& cap, size_t need) {
   return RVG_OK;
 }
 
+int vm_d_arrays(rvg_handle* h, size_t need);
 int ensure_d_arrays(rvg_handle* h, size_t need) {  // type / diag / off share one capacity
+  if (h->vm) return vm_d_arrays(h, need);
   if (need <= h->d_cap && h->dtype) return RVG_OK;
   if (tl_no_alloc) return no_alloc_fail();
   size_t nc = std::max(need, h->d_cap + h->d_cap / 2);
@@ -1433,6 +1441,263 @@ int ensure_nocopy(T*& p, size_t& cap, size_t need, cudaStream_t st) {
   return RVG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Address-stable arenas (graph_refactor = 2).  A captured refactorization
+// graph holds the addresses of the factorization's arenas, and rvg_trim
+// releases their memory so that many handles can take turns on one device.
+// In this mode each arena is a range of virtual addresses reserved once for
+// the handle's life (as large as the device's memory); physical memory is
+// mapped into it in chunks as the arena grows (contents and address kept),
+// unmapped by rvg_trim, and mapped again by the next factorization up to the
+// largest size the arena reached, so the graph's addresses stay valid.
+enum VmSlotId {
+  VM_PANEL = 0, VM_IDX, VM_DTYPE, VM_DDIAG, VM_DOFF, VM_SCRATCH, VM_CB, VM_PACK, VM_STAGE,
+  VM_WPACK0,  // + context id
+  VM_NSLOTS = VM_WPACK0 + LF_CONCURRENT
+};
+}  // namespace (the arenas' types complete the handle's forward declaration, at file scope)
+struct VmSlot {
+  CUdeviceptr va = 0;
+  size_t reserved = 0, mapped = 0, high = 0;
+  std::vector<std::pair<size_t, CUmemGenericAllocationHandle>> chunks;  // (bytes, physical memory) from va on
+};
+struct VmArenas {
+  size_t gran = 0, reserve = 0;  // reserve: the device's memory, the most any range grows to
+  CUmemAllocationProp prop = {};
+  CUmemAccessDesc access = {};
+  VmSlot slot[VM_NSLOTS];
+};
+namespace {
+
+// The driver's virtual-memory calls, looked up through the runtime
+// (cudaGetDriverEntryPoint) so that the library does not link the driver
+// library itself and still loads on a machine without one.
+struct VmApi {
+  decltype(&cuGetErrorString) err = nullptr;
+  decltype(&cuMemGetAllocationGranularity) gran = nullptr;
+  decltype(&cuMemAddressReserve) reserve = nullptr;
+  decltype(&cuMemAddressFree) free = nullptr;
+  decltype(&cuMemCreate) create = nullptr;
+  decltype(&cuMemRelease) release = nullptr;
+  decltype(&cuMemMap) map = nullptr;
+  decltype(&cuMemUnmap) unmap = nullptr;
+  decltype(&cuMemSetAccess) access = nullptr;
+};
+VmApi g_vm;
+
+int vm_api() {
+  if (g_vm.access) return RVG_OK;
+  VmApi a;
+  bool ok = true;
+  auto get = [&](const char* name, auto& fp) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint(name, &f, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess ||
+        !f)
+      ok = false;
+    fp = reinterpret_cast<std::remove_reference_t<decltype(fp)>>(f);
+  };
+  get("cuGetErrorString", a.err);
+  get("cuMemGetAllocationGranularity", a.gran);
+  get("cuMemAddressReserve", a.reserve);
+  get("cuMemAddressFree", a.free);
+  get("cuMemCreate", a.create);
+  get("cuMemRelease", a.release);
+  get("cuMemMap", a.map);
+  get("cuMemUnmap", a.unmap);
+  get("cuMemSetAccess", a.access);
+  if (!ok) {
+    cudaGetLastError();
+    set_error("the driver's virtual-memory calls are not available (graph_refactor = 2)");
+    return RVG_ERR_DEVICE;
+  }
+  g_vm = a;
+  return RVG_OK;
+}
+
+int cu_fail(CUresult r, const char* what) {
+  const char* msg = nullptr;
+  if (g_vm.err) g_vm.err(r, &msg);
+  set_error(std::string("CUDA driver error: ") + (msg ? msg : "unknown") + " at " + what);
+  return r == CUDA_ERROR_OUT_OF_MEMORY ? RVG_ERR_OUT_OF_MEMORY : RVG_ERR_DEVICE;
+}
+#define CU(x)                                  \
+  do {                                         \
+    const CUresult cu_r_ = (x);                \
+    if (cu_r_ != CUDA_SUCCESS) return cu_fail(cu_r_, #x); \
+  } while (0)
+
+int vm_create(rvg_handle* h) {
+  if (int rc = vm_api()) return rc;
+  std::unique_ptr<VmArenas> v(new VmArenas);
+  v->prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+  v->prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  v->prop.location.id = h->device;
+  CU(g_vm.gran(&v->gran, &v->prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED));
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  v->reserve = (tot + v->gran - 1) / v->gran * v->gran;
+  v->access.location = v->prop.location;
+  v->access.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+  h->vm = v.release();
+  return RVG_OK;
+}
+
+void vm_unmap(VmSlot& s);
+
+// backs at least `bytes` of slot `id` (at least its largest earlier size).
+// A range is reserved at four times its first size (256 MB at least); one that
+// must grow past its reservation moves to a larger one (contents copied, the
+// replay graph dropped: it held the old addresses).
+int vm_map(rvg_handle* h, int id, size_t bytes) {
+  VmArenas* v = h->vm;
+  VmSlot& s = v->slot[id];
+  const size_t want = std::max((bytes + v->gran - 1) / v->gran * v->gran, s.high);
+  if (want <= s.mapped) return RVG_OK;
+  if (want > v->reserve) {
+    set_error("an arena would exceed the device's memory");
+    return RVG_ERR_OUT_OF_MEMORY;
+  }
+  if (!s.va || want > s.reserved) {
+    const size_t r = std::min(v->reserve, std::max<size_t>(4 * want, (size_t)256 << 20) / v->gran * v->gran);
+    CUdeviceptr nva = 0;
+    CU(g_vm.reserve(&nva, r, v->gran, 0, 0));
+    if (s.va) {  // move: map the new range, copy what the old one held, release the old one
+      VmSlot old = s;
+      s = VmSlot();
+      s.va = nva;
+      s.reserved = r;
+      int rc = vm_map(h, id, old.mapped);
+      if (rc) return rc;
+      CK(cudaDeviceSynchronize());
+      CK(cudaMemcpy((void*)s.va, (const void*)old.va, old.mapped, cudaMemcpyDeviceToDevice));
+      vm_unmap(old);
+      g_vm.free(old.va, old.reserved);
+      s.high = std::max(s.high, old.high);
+      if (h->gexec) cudaGraphExecDestroy(h->gexec);  // the replay graph held the old addresses
+      if (h->graph) cudaGraphDestroy(h->graph);
+      h->gexec = nullptr;
+      h->graph = nullptr;
+    } else {
+      s.va = nva;
+      s.reserved = r;
+    }
+  }
+  size_t add = std::max(want - s.mapped, (s.mapped / 4 + v->gran - 1) / v->gran * v->gran);  // fewer, larger chunks
+  add = std::min(add, s.reserved - s.mapped);
+  CUmemGenericAllocationHandle m = 0;
+  CUresult r = g_vm.create(&m, add, &v->prop, 0);
+  if (r == CUDA_ERROR_OUT_OF_MEMORY) {  // memory kept by the stream-ordered pool: hand it back, try again
+    cudaDeviceSynchronize();
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    r = g_vm.create(&m, add, &v->prop, 0);
+  }
+  if (r != CUDA_SUCCESS) return cu_fail(r, "cuMemCreate");
+  r = g_vm.map(s.va + s.mapped, add, 0, m, 0);
+  if (r != CUDA_SUCCESS) {
+    g_vm.release(m);
+    return cu_fail(r, "cuMemMap");
+  }
+  r = g_vm.access(s.va + s.mapped, add, &v->access, 1);
+  if (r != CUDA_SUCCESS) {
+    g_vm.unmap(s.va + s.mapped, add);
+    g_vm.release(m);
+    return cu_fail(r, "cuMemSetAccess");
+  }
+  s.chunks.emplace_back(add, m);
+  s.mapped += add;
+  s.high = std::max(s.high, s.mapped);
+  return RVG_OK;
+}
+
+// releases a slot's physical memory, keeping its addresses (the device must
+// be done with it: the callers synchronise the device first)
+void vm_unmap(VmSlot& s) {
+  size_t off = 0;
+  for (auto& c : s.chunks) {
+    g_vm.unmap(s.va + off, c.first);
+    g_vm.release(c.second);
+    off += c.first;
+  }
+  s.chunks.clear();
+  s.mapped = 0;
+}
+
+void vm_destroy(rvg_handle* h) {
+  if (!h->vm) return;
+  cudaDeviceSynchronize();
+  for (VmSlot& s : h->vm->slot) {
+    vm_unmap(s);
+    if (s.va) g_vm.free(s.va, s.reserved);
+  }
+  delete h->vm;
+  h->vm = nullptr;
+}
+
+// The arena of slot `id` with room for `need` elements: address-stable in the
+// graph_refactor = 2 mode (growth maps more memory behind the contents), else
+// ensure()'s stream-ordered reallocation (`copy`: the contents move along).
+template <class T>
+int arena_ensure(rvg_handle* h, int id, T*& p, size_t& cap, size_t need, cudaStream_t st, bool copy) {
+  if (!h->vm) return copy ? ensure(p, cap, need, st) : ensure_nocopy(p, cap, need, st);
+  if (need <= cap && p) return RVG_OK;
+  if (tl_no_alloc) return no_alloc_fail();
+  int rc = vm_map(h, id, std::max<size_t>(need, 1) * sizeof(T));
+  if (rc) return rc;
+  p = reinterpret_cast<T*>(h->vm->slot[id].va);
+  cap = h->vm->slot[id].mapped / sizeof(T);
+  return RVG_OK;
+}
+
+// Every arena mapped again up to its largest size and bound to its pointer:
+// a replayed graph touches them all without the host's ensure calls.
+int vm_restore(rvg_handle* h) {
+  for (int id = 0; id < VM_NSLOTS; ++id) {
+    VmSlot& sl = h->vm->slot[id];
+    if (sl.high > sl.mapped) {
+      int rc = vm_map(h, id, sl.high);
+      if (rc) return rc;
+    }
+  }
+  auto bind = [&](int id, auto*& p, size_t& cap) {
+    const VmSlot& sl = h->vm->slot[id];
+    if (sl.mapped && !p) {
+      p = reinterpret_cast<std::remove_reference_t<decltype(p)>>(sl.va);
+      cap = sl.mapped / sizeof(*p);
+    }
+  };
+  bind(VM_PANEL, h->panel, h->panel_cap);
+  bind(VM_IDX, h->idx, h->idx_cap);
+  bind(VM_SCRATCH, h->scratch, h->scratch_cap);
+  bind(VM_CB, h->cb_arena, h->cb_cap);
+  bind(VM_PACK, h->pack, h->pack_cap);
+  bind(VM_STAGE, h->d_stage, h->stage_cap);
+  bind(VM_WPACK0, h->wpack, h->wpack_cap);
+  for (size_t t = 1; t < h->lfx.size(); ++t) bind(VM_WPACK0 + (int)t, h->lfx[t].wpack, h->lfx[t].wpack_cap);
+  if (!h->dtype && h->vm->slot[VM_DTYPE].mapped) {
+    size_t ct = 0, ca = 0, cb = 0;
+    bind(VM_DTYPE, h->dtype, ct);
+    bind(VM_DDIAG, h->ddiag, ca);
+    bind(VM_DOFF, h->doff, cb);
+    h->d_cap = std::min(ct, std::min(ca, cb));
+  }
+  return RVG_OK;
+}
+
+int vm_d_arrays(rvg_handle* h, size_t need) {
+  if (need <= h->d_cap && h->dtype) return RVG_OK;
+  if (tl_no_alloc) return no_alloc_fail();
+  size_t ct = 0, ca = 0, cb = 0;
+  int rc;
+  if ((rc = arena_ensure(h, VM_DTYPE, h->dtype, ct, need, h->st, true)) ||
+      (rc = arena_ensure(h, VM_DDIAG, h->ddiag, ca, need, h->st, true)) ||
+      (rc = arena_ensure(h, VM_DOFF, h->doff, cb, need, h->st, true)))
+    return rc;
+  h->d_cap = std::min(ct, std::min(ca, cb));
+  return RVG_OK;
+}
+
 // first-fit allocation of `len` doubles in the CB arena; grows (with a copy of
 // the live contents) when no free range fits
 int cb_alloc(rvg_handle* h, int64_t len, int64_t* off) {
@@ -1449,13 +1714,20 @@ int cb_alloc(rvg_handle* h, int64_t len, int64_t* off) {
   // grow: new capacity covers the old one plus the request
   size_t old = h->cb_cap;
   size_t nc = std::max(old + (size_t)len, old + old / 4);
-  double* np = nullptr;
-  CK(cudaMallocAsync((void**)&np, nc * sizeof(double), h->st));
-  if (h->cb_arena) {
-    if (old) CK(cudaMemcpyAsync(np, h->cb_arena, old * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
-    CK(cudaFreeAsync(h->cb_arena, h->st));
+  if (h->vm) {  // more memory behind the same addresses
+    size_t cap = old;
+    int rc = arena_ensure(h, VM_CB, h->cb_arena, cap, nc, h->st, true);
+    if (rc) return rc;
+    nc = cap;
+  } else {
+    double* np = nullptr;
+    CK(cudaMallocAsync((void**)&np, nc * sizeof(double), h->st));
+    if (h->cb_arena) {
+      if (old) CK(cudaMemcpyAsync(np, h->cb_arena, old * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+      CK(cudaFreeAsync(h->cb_arena, h->st));
+    }
+    h->cb_arena = np;
   }
-  h->cb_arena = np;
   h->cb_cap = nc;
   // the tail [old, nc) is free; merge with a free range ending at `old`
   int64_t start = (int64_t)old, length = (int64_t)(nc - old);
@@ -1620,13 +1892,22 @@ int presize_arenas(rvg_handle* h) {
   }
   int rc;
   cudaStream_t st = h->st;
-  if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel + panel / 16 + 1024), st))) return rc;
-  if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx + idx / 16 + 1024), st))) return rc;
+  if ((rc = arena_ensure(h, VM_PANEL, h->panel, h->panel_cap, (size_t)(panel + panel / 16 + 1024), st, true)))
+    return rc;
+  if ((rc = arena_ensure(h, VM_IDX, h->idx, h->idx_cap, (size_t)(idx + idx / 16 + 1024), st, true))) return rc;
   if ((rc = ensure_d_arrays(h, (size_t)(dsz + dsz / 8 + 1024)))) return rc;
-  if ((rc = ensure_nocopy(h->scratch, h->scratch_cap, (size_t)(scratch + 1024), st))) return rc;
+  if ((rc = arena_ensure(h, VM_SCRATCH, h->scratch, h->scratch_cap, (size_t)(scratch + 1024), st, false)))
+    return rc;
   if (hw > 0 && !h->cb_arena) {
-    h->cb_cap = (size_t)(hw + hw / 16 + 1024);
-    CK(cudaMallocAsync((void**)&h->cb_arena, h->cb_cap * sizeof(double), st));
+    const size_t want = (size_t)(hw + hw / 16 + 1024);
+    if (h->vm) {
+      size_t cap = 0;
+      if ((rc = arena_ensure(h, VM_CB, h->cb_arena, cap, want, st, false))) return rc;
+      h->cb_cap = cap;
+    } else {
+      h->cb_cap = want;
+      CK(cudaMallocAsync((void**)&h->cb_arena, h->cb_cap * sizeof(double), st));
+    }
   }
   return RVG_OK;
 }
@@ -1727,7 +2008,7 @@ int launch_syrk(rvg_handle* h, const SyrkArgs& ga, int64_t kmax, bool mixed) {
     const int64_t Q = (kmax + TC_BK - 1) / TC_BK;
     const int64_t ntiles = (nr > 0 && nc > 0) ? tc_count_tiles(nr, nc, ga.r0, ga.c0) : 0;
     if (ntiles > 0 && Q > 0) {
-      int rc = ensure_nocopy(h->pack, h->pack_cap, (size_t)(nr + nc) * Q * TC_BLOCK, st);
+      int rc = arena_ensure(h, VM_PACK, h->pack, h->pack_cap, (size_t)(nr + nc) * Q * TC_BLOCK, st, false);
       if (rc) return rc;
       float* pl = h->pack + (size_t)nr * Q * TC_BLOCK;
       PackArgs aw{ga.W, ga.ldw, ga.r1 - ga.r0, Q, ga.Kdev, ga.K, h->pack};
@@ -1831,7 +2112,7 @@ int factor_large_front(rvg_handle* h, LfCtx& cx, int32_t s, const Arenas& Ar, co
   if (mixed && two_level) {
     const int64_t tiles = (m + TC_BM - 1) / TC_BM;
     const size_t one = (size_t)tiles * Fq * TC_BLOCK;
-    int rc = ensure_nocopy(cx.wpack, cx.wpack_cap, 4 * one, st);
+    int rc = arena_ensure(h, VM_WPACK0 + cx.id, cx.wpack, cx.wpack_cap, 4 * one, st, false);
     if (rc) return rc;
     pk_wb[0] = cx.wpack; pk_lb[0] = cx.wpack + one;
     pk_wb[1] = cx.wpack + 2 * one; pk_lb[1] = cx.wpack + 3 * one;
@@ -2151,6 +2432,7 @@ int factor_large_fronts(rvg_handle* h, const std::vector<int32_t>& ids, const Ar
     if (tl_no_alloc) return no_alloc_fail();
     LfCtx c;
     c.own = true;
+    c.id = (int)h->lfx.size();
     CK(cudaStreamCreateWithFlags(&c.st, cudaStreamNonBlocking));
     CK(cudaMalloc((void**)&c.lf, sizeof(LFState)));
     h->lfx.push_back(c);
@@ -2398,10 +2680,13 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       h->host_gap_ms += ta - t_ret;
       t_ret = -1;
     }
-    if ((rc = ensure(h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st))) return rc;
-    if ((rc = ensure(h->idx, h->idx_cap, (size_t)(idx_used + idx_need), st))) return rc;
+    if ((rc = arena_ensure(h, VM_PANEL, h->panel, h->panel_cap, (size_t)(panel_used + panel_need), st, true)))
+      return rc;
+    if ((rc = arena_ensure(h, VM_IDX, h->idx, h->idx_cap, (size_t)(idx_used + idx_need), st, true))) return rc;
     if ((rc = ensure_d_arrays(h, (size_t)(d_used + d_need)))) return rc;
-    if ((rc = ensure_nocopy(h->scratch, h->scratch_cap, (size_t)std::max<int64_t>(scratch_need, 1), st))) return rc;
+    if ((rc = arena_ensure(h, VM_SCRATCH, h->scratch, h->scratch_cap, (size_t)std::max<int64_t>(scratch_need, 1), st,
+                           false)))
+      return rc;
     double* scratch = h->scratch;
     if (cb_need) {
       if ((rc = cb_alloc(h, cb_need, &cb_block[w]))) return rc;
@@ -2481,7 +2766,7 @@ int run_factor(rvg_handle* h, const double* d_vals, const double* d_scal) {
       o_lg = pk.add(large_ids);
       o_rt = pk.add(std::vector<int32_t>(large_ids.size(), 0));
     }
-    if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size(), st))) return rc;
+    if ((rc = arena_ensure(h, VM_STAGE, h->d_stage, h->stage_cap, pk.buf.size(), st, true))) return rc;
     char* hs;
     if (h->replay) {  // a slice of its own: the graph copies from it at every replay
       if (pk.buf.size() != h->rec_stage[w]) { set_error("refactorization replay: launch data differ"); return RVG_ERR_DEVICE; }
@@ -2776,6 +3061,10 @@ static int check_opts(const rvg_options& o) {  // factor.rs:307-347 (precision a
     set_error("mixed_window must be 0 (default) or 1 to 8 outer blocks");
     return RVG_ERR_INVALID_INPUT;
   }
+  if (o.graph_refactor < 0 || o.graph_refactor > 2) {
+    set_error("graph_refactor must be 0 (off), 1 (replay) or 2 (replay, arenas kept at their addresses across rvg_trim)");
+    return RVG_ERR_INVALID_INPUT;
+  }
   return RVG_OK;
 }
 
@@ -2853,6 +3142,10 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
   {  // RVG_CHAIN_PDL=0 launches the large-front chain kernels plainly (same results; for timing comparisons)
     const char* e = std::getenv("RVG_CHAIN_PDL");
     h->chain_pdl = !(e && e[0] == '0');
+  }
+  if (o.graph_refactor == 2) {  // address-stable arenas: a replay graph survives rvg_trim
+    int rc2 = vm_create(h.get());
+    if (rc2) return (rvg_status)rc2;
   }
   CK(cudaMallocAsync((void**)&h->d_err, sizeof(int32_t), st));
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
@@ -2954,6 +3247,7 @@ static int factor_common(rvg_handle* h, const double* dv, const double* ds) {
   int rc;
   if (h->need_presize) {  // after rvg_trim: the arenas at their delay-free size again
     if ((rc = presize_arenas(h))) return rc;
+    if (h->vm && (rc = vm_restore(h))) return rc;  // (address-stable: up to their largest size, all of them)
     h->need_presize = false;
   }
   // the refinement needs the unfactored values and ||A||_F
@@ -3089,7 +3383,7 @@ static int solve_common(rvg_handle* h, double* d_rhs, int64_t nrhs, int64_t ldb)
     offb[w] = pk.add(vb);
     maxblk = std::max(maxblk, std::max(nbf[w], nbb[w]));
   }
-  if ((rc = ensure(h->d_stage, h->stage_cap, pk.buf.size() + 16, st))) return rc;
+  if ((rc = arena_ensure(h, VM_STAGE, h->d_stage, h->stage_cap, pk.buf.size() + 16, st, true))) return rc;
   if ((rc = ensure_host(h->h_stage, h->h_stage_cap, pk.buf.size() + 16))) return rc;
   std::memcpy(h->h_stage, pk.buf.data(), pk.buf.size());
   CK(cudaMemcpyAsync(h->d_stage, h->h_stage, pk.buf.size(), cudaMemcpyHostToDevice, st));
@@ -3759,23 +4053,47 @@ rvg_status rvg_trim(rvg_handle* h, int32_t what) {
     p = nullptr;                                      \
     cap = 0;                                          \
   } while (0)
-  if (what & 1) {
+  if (h->vm && what) CK(cudaDeviceSynchronize());  // nothing may use an arena whose memory goes
+  auto vm_trim = [&](int id, auto*& p, size_t& cap) {  // address-stable arenas: the memory goes, the addresses stay
+    vm_unmap(h->vm->slot[id]);
+    p = nullptr;
+    cap = 0;
+  };
+  if ((what & 1) && h->vm) {
+    vm_trim(VM_SCRATCH, h->scratch, h->scratch_cap);
+    vm_trim(VM_CB, h->cb_arena, h->cb_cap);
+    vm_trim(VM_PACK, h->pack, h->pack_cap);
+    vm_trim(VM_WPACK0, h->wpack, h->wpack_cap);
+    for (size_t t = 1; t < h->lfx.size(); ++t) vm_trim(VM_WPACK0 + (int)t, h->lfx[t].wpack, h->lfx[t].wpack_cap);
+    if (!h->lfx.empty()) { h->lfx[0].wpack = nullptr; h->lfx[0].wpack_cap = 0; }
+    vm_trim(VM_STAGE, h->d_stage, h->stage_cap);
+  } else if (what & 1) {
     RVG_TRIM(h->scratch, h->scratch_cap);
     RVG_TRIM(h->cb_arena, h->cb_cap);
     RVG_TRIM(h->pack, h->pack_cap);
     RVG_TRIM(h->wpack, h->wpack_cap);
+    for (size_t t = 1; t < h->lfx.size(); ++t) RVG_TRIM(h->lfx[t].wpack, h->lfx[t].wpack_cap);
+    if (!h->lfx.empty()) { h->lfx[0].wpack = nullptr; h->lfx[0].wpack_cap = 0; }
+    RVG_TRIM(h->d_stage, h->stage_cap);
+  }
+  if (what & 1) {
     RVG_TRIM(h->solve_work, h->solve_work_cap);
     RVG_TRIM(h->sf_part, h->sf_part_cap);
     RVG_TRIM(h->d_x, h->x_cap);
     RVG_TRIM(h->d_ref, h->ref_cap);
     RVG_TRIM(h->d_gm, h->gm_cap);
-    for (size_t t = 1; t < h->lfx.size(); ++t) RVG_TRIM(h->lfx[t].wpack, h->lfx[t].wpack_cap);
-    if (!h->lfx.empty()) { h->lfx[0].wpack = nullptr; h->lfx[0].wpack_cap = 0; }
-    RVG_TRIM(h->d_stage, h->stage_cap);
     RVG_TRIM(h->d_stage2, h->stage2_cap);
     h->cb_free.clear();
   }
-  if (what & 2) {
+  if ((what & 2) && h->vm) {
+    vm_trim(VM_PANEL, h->panel, h->panel_cap);
+    vm_trim(VM_IDX, h->idx, h->idx_cap);
+    size_t c1 = 0, c2 = 0;
+    vm_trim(VM_DTYPE, h->dtype, h->d_cap);
+    vm_trim(VM_DDIAG, h->ddiag, c1);
+    vm_trim(VM_DOFF, h->doff, c2);
+    h->factored = false;
+  } else if (what & 2) {
     RVG_TRIM(h->panel, h->panel_cap);
     RVG_TRIM(h->idx, h->idx_cap);
     if ((rc = trim_buf(h->dtype, st)) || (rc = trim_buf(h->ddiag, st)) || (rc = trim_buf(h->doff, st)))
@@ -3786,7 +4104,7 @@ rvg_status rvg_trim(rvg_handle* h, int32_t what) {
 #undef RVG_TRIM
   if (what) {
     h->need_presize = true;
-    drop_graph(h);  // it holds the addresses of the released buffers
+    if (!h->vm) drop_graph(h);  // it holds the addresses of the released buffers (kept in the vm mode)
   }
   CK(cudaStreamSynchronize(st));  // the memory is back in the pool when this returns
   return RVG_OK;
@@ -3814,8 +4132,12 @@ void rvg_destroy(rvg_handle* h) {
   auto fr = [&](void* p) { if (p) cudaFreeAsync(p, st); };
   fr(h->d_own_ptr); fr(h->d_own_idx); fr(h->d_pat_ptr); fr(h->d_pat_idx); fr(h->d_amap_ptr); fr(h->d_amap);
   fr(h->d_ea_ptr); fr(h->d_ea_map); fr(h->d_ch_ptr); fr(h->d_ch_idx); fr(h->d_pfwd); fr(h->d_fronts);
-  fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff); fr(h->d_vals); fr(h->d_scal);
-  fr(h->d_x); fr(h->solve_work); fr(h->d_stage); fr(h->d_stage2); fr(h->d_lf); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
+  if (!h->vm) {  // (address-stable arenas are released by vm_destroy below)
+    fr(h->panel); fr(h->idx); fr(h->dtype); fr(h->ddiag); fr(h->doff);
+    fr(h->d_stage); fr(h->scratch); fr(h->cb_arena); fr(h->pack); fr(h->wpack);
+  }
+  fr(h->d_vals); fr(h->d_scal);
+  fr(h->d_x); fr(h->solve_work); fr(h->d_stage2); fr(h->d_lf); fr(h->sf_sync); fr(h->sf_part); fr(h->d_gm);
   drop_graph(h);
   fr(h->d_rec);
   if (h->d_sel) cudaFree(h->d_sel);
@@ -3832,13 +4154,14 @@ void rvg_destroy(rvg_handle* h) {
     if (c.ev_fork) cudaEventDestroy(c.ev_fork);
     if (c.ev_far) cudaEventDestroy(c.ev_far);
     if (t == 0) continue;  // the handle's own stream, state and window buffer
-    fr(c.wpack);
+    if (!h->vm) fr(c.wpack);
     if (c.lf) cudaFree(c.lf);
     if (c.own && c.st) { cudaStreamSynchronize(c.st); cudaStreamDestroy(c.st); }
   }
   fr(h->d_err);
   fr(h->d_colptr); fr(h->d_rowidx); fr(h->d_ref);
   if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); }
+  vm_destroy(h);
   if (h->h_stage) cudaFreeHost(h->h_stage);
   if (h->h_stage2) cudaFreeHost(h->h_stage2);
   if (h->h_counts) cudaFreeHost(h->h_counts);

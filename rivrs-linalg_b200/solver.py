@@ -55,7 +55,8 @@ class FactorOptions:
     mixed_flush: int = 4  # mixed form: 32-deep K chunks per FP32 partial sum (1, 2, 4, 8; 0 = all of K)
     mixed_tile_cols: int = 256  # mixed form, mixed_flush 0: Schur GEMM output columns per CTA tile (128, 256)
     mixed_operands: str = "tf32"  # mixed form: FP64 operands split into two "tf32" or two "bf16" parts
-    graph_refactor: bool = False  # refactorizations of one handle replayed as one CUDA graph (same pivoting)
+    graph_refactor: int = 0  # 1: refactorizations replayed as one CUDA graph (same pivoting); 2: the same, with
+    #                          the arenas kept at their addresses while SparseLDLT.trim gives their memory back
     far_field_sms: int = -1  # mixed form: SMs a window's far-field update leaves to the next blocks (0 = no split)
     mixed_window: int = 0  # mixed form: outer blocks per window of deferred updates, 1-8 (0 = default 4)
 

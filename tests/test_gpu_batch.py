@@ -134,3 +134,49 @@ def test_autotuned_groups_give_the_same_factors(rv):
         xx = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
         assert max(rv.problems.backward_error(s, xx[:, j], bb[:, j]) for j in range(bb.shape[1])) <= 1e-14
     bl.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_refactorizations_replay_as_graphs_across_turns(rv, precision):
+    """graph_refactor = 2: each union's arenas keep their addresses while rvg_trim gives their memory back,
+    so the unions take turns on the device and each still replays its captured refactorization graph (one
+    launch per factorization from the third on). Every system's pivot order, codes and D equal those of a
+    batch that factors dynamically, round after round of new values; the solutions meet the gate."""
+    import dataclasses
+    fam = rv.problems.batch_family(count=6, seed=5, n_lo=300, n_hi=6000, max_rhs=9)
+    systems, nrhs = [s for s, _ in fam], [r for _, r in fam]
+    base = rv.FactorOptions(precision=precision, mixed_flush=0, large_front_threshold=256)
+    budget = 14 * 2 ** 20  # several unions of these systems' estimated memory
+    dyn = rv.BatchLDLT(systems, device_budget=budget)
+    rep = rv.BatchLDLT(systems, device_budget=budget)
+    assert len(rep.groups) >= 2
+    opts = dataclasses.replace(base, graph_refactor=2)
+    rhs = [rv.problems.rhs_normal(s.n, i, r) for i, (s, r) in enumerate(zip(systems, nrhs))]
+    for rnd in range(4):
+        # factorization 0: dynamic (records); 1: captured and replayed; 2-3: replayed.  The values change by
+        # a factor per round, which keeps every pivot decision (a replay whose checks see another decision
+        # falls back to a dynamic factorization, tested for one handle in test_gpu_graph.py)
+        vals = None if rnd == 0 else [s.values * (1.0 + 0.25 * rnd) for s in systems]
+        dyn.factor(vals, base)
+        rep.factor(vals, opts)
+        launches = [g.solver.profile()["factor_launches"] for g in rep.groups]
+        if rnd >= 2:
+            assert all(n == 1 for n in launches), launches  # replayed
+        for i in range(len(systems)):
+            a, b = dyn.system_record(i), rep.system_record(i)
+            assert all(np.array_equal(x, y) for x, y in zip(a, b)), ("record differs", rnd, i)
+        assert rep.inertias() == dyn.inertias()
+        xs = rep.solve(rhs)
+        if precision == "fp64":
+            for i, s in enumerate(systems):
+                a = s.to_scipy()
+                if vals is not None:
+                    a = a.copy()
+                    a.data = vals[i]
+                sv = rv.problems.from_scipy("v", a)
+                bb = rhs[i] if rhs[i].ndim == 2 else rhs[i][:, None]
+                x = xs[i] if xs[i].ndim == 2 else xs[i][:, None]
+                for j in range(bb.shape[1]):
+                    assert rv.problems.backward_error(sv, x[:, j], bb[:, j]) <= 1e-14
+    dyn.close()
+    rep.close()
