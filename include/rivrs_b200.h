@@ -92,7 +92,10 @@ typedef struct {
    * on the device compare the pivoting the new values give with the recorded
    * one; when they differ (other delays or 2x2 pivots) the factorization is
    * redone dynamically, which records anew.  Results are the dynamic path's,
-   * bit for bit.  Default 0. */
+   * bit for bit.  2 = the same, and the factorization's arenas are kept at
+   * fixed virtual addresses (the driver's virtual-memory calls): rvg_trim
+   * gives their memory back without dropping the graph, so handles that take
+   * turns on one device each keep replaying theirs.  Default 0. */
   int32_t graph_refactor;
   /* Mixed form, large fronts: multiprocessors a full window's far-field
    * update leaves to the next outer blocks while it runs on a second stream
