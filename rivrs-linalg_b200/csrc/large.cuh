@@ -28,7 +28,8 @@
 //                         two: the next outer block's columns take every
 //                         pending column at once (near field); the columns
 //                         after it (far field) only when the window is full
-//                         (LF_WINDOW outer blocks) or when this block delayed
+//                         (LF_WINDOW outer blocks, mixed_window in the mixed
+//                         form) or when this block delayed
 //                         a column (decided on the device), so each far-field
 //                         entry is read and written once per window instead
 //                         of once per block.  Each entry still takes one fma
