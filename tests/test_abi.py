@@ -34,7 +34,8 @@ def test_default_options_match_reference(rv):
 @pytest.mark.parametrize("bad", [dict(threshold=0.0), dict(threshold=1.5), dict(small=-1.0),
                                  dict(outer_block_size=0), dict(inner_block_size=0),
                                  dict(inner_block_size=64, outer_block_size=32), dict(far_field_sms=-2),
-                                 dict(mixed_window=-1), dict(mixed_window=9)])
+                                 dict(mixed_window=-1), dict(mixed_window=9), dict(graph_refactor=-1),
+                                 dict(graph_refactor=3)])
 def test_invalid_options_rejected(rv, bad):
     s = rv.problems.shifted_laplacian(3, 0.1)
     solver = rv.SparseLDLT.analyze(s)
