@@ -432,7 +432,8 @@ def run_batch(args, rv, entry, torch, barrier, max_over_ranks, rank, world, loca
                                "union_factorizations": ngr * len(G), "bwd_err_max_last": bwd_gr,
                                "how": "graph_refactor = 2 (arenas at fixed addresses across rvg_trim); the first "
                                       "refactorization records, the second captures, later ones replay while the "
-                                      "pivoting stays the same"},
+                                      "pivoting stays the same (with 1% random perturbations it changes in some "
+                                      "system of every union, and the device checks fall back to the dynamic path)"},
             "factor_flops": flops_all, "factor_gflops": flops_all / t_step / 1e9,
             "e2e": {"value": e2e_v, "unit": "s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(sum(e["rhs"].numel() * 8 for e in G))},
