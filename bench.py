@@ -669,7 +669,7 @@ def batch_subset(rv, torch, count, warmup, steps):
 def run_profile_step(args, rv, torch):
     """One form on one system, W warm-up and K timed steps (factor + solve to
     1e-14 with inputs in HBM), then one step with the library's per-launch
-    events: the command the ncu summaries under profiles/ were taken with."""
+    events: the command the committed ncu summaries were taken with."""
     s, b = build_system(rv, args.config)
     solver, _ = analyze(rv, s)
     form = {"plain": dict(precision="fp64"),
