@@ -1568,7 +1568,12 @@ int vm_map(rvg_handle* h, int id, size_t bytes) {
       s.va = nva;
       s.reserved = r;
       int rc = vm_map(h, id, old.mapped);
-      if (rc) return rc;
+      if (rc) {  // the old range stays the arena; the new one goes
+        vm_unmap(s);
+        g_vm.free(nva, r);
+        s = old;
+        return rc;
+      }
       CK(cudaDeviceSynchronize());
       CK(cudaMemcpy((void*)s.va, (const void*)old.va, old.mapped, cudaMemcpyDeviceToDevice));
       vm_unmap(old);
@@ -3123,6 +3128,7 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
     if ((rc = upload(h->d_colptr, cp, st)) || (rc = upload(h->d_rowidx, ri, st))) return (rvg_status)rc;
   }
   CK(cudaMallocHost((void**)&h->h_norms, 4 * sizeof(double)));
+  if (o.graph_refactor == 2 && (rc = vm_create(h.get()))) return (rvg_status)rc;  // address-stable arenas
   if ((rc = presize_arenas(h.get()))) return (rvg_status)rc;
   CK(cudaFuncSetAttribute(k_syrk_lower, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
   CK(cudaFuncSetAttribute(k_syrk_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G_SMEM));
@@ -3143,10 +3149,7 @@ rvg_status rvg_create(int64_t n, int64_t nsup, const int64_t* sup_begin, const i
     const char* e = std::getenv("RVG_CHAIN_PDL");
     h->chain_pdl = !(e && e[0] == '0');
   }
-  if (o.graph_refactor == 2) {  // address-stable arenas: a replay graph survives rvg_trim
-    int rc2 = vm_create(h.get());
-    if (rc2) return (rvg_status)rc2;
-  }
+
   CK(cudaMallocAsync((void**)&h->d_err, sizeof(int32_t), st));
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(int32_t), st));
   CK(cudaMallocAsync((void**)&h->d_vals, std::max<int64_t>(h->nnz, 1) * 8, st));
