@@ -575,6 +575,15 @@ def run_learned(args, rv, torch):
     print(json.dumps(line), flush=True)
 
 
+def choose_form(forms: dict, plain: str = "plain_fp64", tol: float = 1e-14):
+    """The fastest form whose backward error reaches tol and whose inertia
+    equals the plain FP64 form's (exact); the plain form always qualifies.
+    forms: name -> {"t": seconds, "bwd": backward error, "inertia": (p, n, z)}."""
+    ref = list(forms[plain]["inertia"])
+    ok = [k for k, f in forms.items() if k == plain or (f["bwd"] <= tol and list(f["inertia"]) == ref)]
+    return min(ok, key=lambda k: forms[k]["t"])
+
+
 def form_dtype(opts):
     """The arithmetic a form computes in (not a precision claim: every form
     reaches the same 1e-14 backward error)."""
@@ -606,10 +615,9 @@ def side_config(rv, torch, name, s, b, warmup, steps, selector=None, bf16_opts=N
                   "solves_after_first": r["solves_after_first"], "methods": r["methods"]}
         if "selector" in r:
             res[k]["selector"] = r["selector"]
-    # accurate forms with the plain form's (exact) inertia
-    ok = [k for k in res if res[k]["bwd_err"] <= 1e-14 and res[k]["inertia"] == res["plain_fp64"]["inertia"]]
-    ok = ok or ["plain_fp64"]
-    chosen = min(ok, key=lambda k: res[k]["s_per_step"])
+    # the fastest accurate form with the plain form's (exact) inertia
+    chosen = choose_form({k: {"t": r["s_per_step"], "bwd": r["bwd_err"], "inertia": r["inertia"]}
+                          for k, r in res.items()})
     solver._ensure_handle(forms[chosen])
     solver.set_profiling(True)
     time_form(rv, torch, solver, s, b, forms[chosen], 0, 1)
@@ -907,11 +915,8 @@ def main():
         solver.set_selector(rv.PrecisionSelector.load(SELECTOR))
         forms["learned_bf16_flush0"] = run_form("learned", 0, "bf16", "auto")
         forms["learned_bf16_flush0"]["selector"] = solver.selector_stats()
-    # the chosen form: the fastest that reaches the accuracy target with the plain form's inertia (plain always
-    # does)
-    chosen_key = min((k for k, f in forms.items()
-                      if (f["bwd"] <= 1e-14 and list(f["inertia"]) == list(plain["inertia"])) or k == "plain_fp64"),
-                     key=lambda k: forms[k]["t"])
+    # the chosen form: the fastest that reaches the accuracy target with the plain form's inertia
+    chosen_key = choose_form(forms)
     chosen = forms[chosen_key]
     chosen_name = "plain" if chosen_key == "plain_fp64" else "mixed"
     t_step = chosen["t"]
